@@ -1,0 +1,436 @@
+"""BM3D throughput benchmark (megapixels per second).
+
+Workload (one "step"): plain BM3D, basic + final, fast profile, on four
+1920x1080 float32 luma planes -- the sigma sweep {5, 10, 25, 50}/255 --
+generated by isp_mw_b200.synth (seeded piecewise-smooth planes + Gaussian
+noise; synthetic, no dataset). Inputs rotate over a ring of sets whose total
+size exceeds the 126 MB L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Our arm times K steps with CUDA events (barrier + synchronize on both sides,
+max over ranks) on device-resident planes -> ``value``; then the same steps
+through the C ABI with pinned host planes (host->device copy, filter,
+device->host copy inside the timed region) -> ``e2e``. The reference arm
+(--impl reference) runs the reference's own CPU BM3D (oracle/_ref, compiled
+from the reference sources; the C restatement when that build is absent) on
+the host cores, one bounded sample of the workload per step.
+Multi-GPU: every rank filters its own planes (independent images, no
+collective on the data path): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H = 1920, 1080
+SIGMAS = (5.0, 10.0, 25.0, 50.0)
+RING = 4
+METRIC = "BM3D MP/s (basic+final, 1920x1080 luma, sigma sweep 5/10/25/50)"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_inputs(rank: int):
+    from isp_mw_b200 import synth
+    sets = []
+    for r in range(RING):
+        planes = []
+        for k, s in enumerate(SIGMAS):
+            seed = 1000 * rank + 100 * r + k
+            _, noisy = synth.pair(H, W, s, seed)
+            planes.append(noisy)
+        sets.append(planes)
+    return sets
+
+
+def params_for(sigma_255: float):
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    sp = [synth.sigma_param(sigma_255)] * 3
+    return (isp_mw_b200.stage_params_default("fast", False, sp),
+            isp_mw_b200.stage_params_default("fast", True, sp))
+
+
+def algorithmic_flops(stats, wiener: bool, bs: int = 8) -> float:
+    """Direct-formulation FLOPs of one stage launch from its counters:
+    block matching 3 BS^2 per candidate; per group of n blocks a 3-D DCT of
+    4 n BS^3 + 2 BS^2 n^2 (x2 basic: forward + inverse, x3 final: two forward
+    + inverse); shrinkage 1 (hard threshold) or 5 (Wiener) per coefficient;
+    aggregation 3 per pixel of every block."""
+    sum_n, sum_n2, cand = stats[0], stats[1], stats[2]
+    t = 3 if wiener else 2
+    per_coef = 5 if wiener else 1
+    dct = t * (4 * bs ** 3 * sum_n + 2 * bs ** 2 * sum_n2)
+    return 3 * bs * bs * cand + dct + per_coef * bs * bs * sum_n + 3 * bs * bs * sum_n
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import isp_mw_b200
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    ctx = isp_mw_b200.Context(local)
+    params = [params_for(s) for s in SIGMAS]
+    host_sets = make_inputs(rank)
+    dev_sets = [[torch.from_numpy(p).to(dev) for p in planes] for planes in host_sets]
+    outs = [torch.empty((H, W), dtype=torch.float32, device=dev) for _ in SIGMAS]
+    stream = torch.cuda.current_stream(dev)
+
+    def step(i):
+        planes = dev_sets[i % RING]
+        for k in range(len(SIGMAS)):
+            ctx.full(params[k][0], params[k][1], outs[k], planes[k])
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for i in range(args.warmup):
+        step(i)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for i in range(args.steps):
+            step(args.warmup + i)
+        ev1.record(stream)
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    mp_step = len(SIGMAS) * W * H / 1e6
+    value = world * mp_step * args.steps / (ms_max / 1e3)
+
+    # Kernel roofline: per-launch times of the final-stage kernel (the larger
+    # of the two) from events on its launch stream, over a separate pass.
+    ctx.set_kernel_timing(True)
+    flops = {False: 0.0, True: 0.0}
+    for i in range(args.steps):
+        planes = dev_sets[i % RING]
+        for k in range(len(SIGMAS)):
+            b = torch.empty_like(outs[k])
+            ctx.stage(params[k][0], False, b, planes[k])
+            flops[False] += algorithmic_flops(ctx.last_stats(), False)
+            ctx.stage(params[k][1], True, outs[k], planes[k], b)
+            flops[True] += algorithmic_flops(ctx.last_stats(), True)
+    t_basic, n_basic = ctx.kernel_time(False)
+    t_final, n_final = ctx.kernel_time(True)
+    ctx.set_kernel_timing(False)
+    dom = True if t_final >= t_basic else False
+    t_dom, n_dom = (t_final, n_final) if dom else (t_basic, n_basic)
+    per_launch_ms = t_dom / max(1, n_dom)
+    achieved = flops[dom] / max(1, n_dom) / (per_launch_ms / 1e3) / 1e12
+    clocks = clk.summary()
+    sm_max = clocks.get("sm_max_mhz") or 1965.0
+    peak_fp32 = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+
+    # End to end through the C ABI: pinned host planes in, results out.
+    pinned_in = [[torch.from_numpy(p).pin_memory() for p in planes] for planes in host_sets]
+    pinned_out = [torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in SIGMAS]
+
+    def step_e2e(i):
+        planes = pinned_in[i % RING]
+        for k in range(len(SIGMAS)):
+            ctx.full(params[k][0], params[k][1], pinned_out[k], planes[k])
+
+    for i in range(min(args.warmup, 3)):
+        step_e2e(i)
+    barrier()
+    e0 = time.perf_counter()
+    ev0.record(stream)
+    for i in range(args.steps):
+        step_e2e(i)
+    ev1.record(stream)
+    barrier()
+    e_wall = (time.perf_counter() - e0) * 1e3
+    e_ms = max(ev0.elapsed_time(ev1), e_wall)
+    te = torch.tensor([e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * mp_step * args.steps / (float(te.item()) / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(host_sets[0], budget_s=args.cpu_seconds)
+
+    if rank == 0:
+        peaks = load_peaks()
+        line = {
+            "metric": METRIC,
+            "value": round(value, 3),
+            "unit": "MP/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded piecewise-smooth planes + Gaussian noise)",
+            "config": {"workload": "BM3D basic+final, fast profile, 4 x 1920x1080 f32 luma "
+                                   "planes (sigma 5/10/25/50 per 255) per step",
+                       "width": W, "height": H, "planes_per_step": len(SIGMAS),
+                       "profile": "fast", "sigma_255": list(SIGMAS),
+                       "l2": f"inputs rotate over {RING} sets ({RING * len(SIGMAS) * W * H * 4 / 1e6:.0f} MB) "
+                             "> 126 MB L2",
+                       "parallelism": f"replicas x{world} (independent planes per GPU)"},
+            "e2e": {"value": round(e2e_value, 3), "unit": "MP/s",
+                    "h2d_bytes_per_step": len(SIGMAS) * W * H * 4,
+                    "d2h_bytes_per_step": len(SIGMAS) * W * H * 4},
+            "gpu_launches": args.steps * len(SIGMAS) * 4,
+            "roofline": {
+                "bound": "fp32",
+                "kernel": "stage_kernel (final)" if dom else "stage_kernel (basic)",
+                "achieved": round(achieved, 3),
+                "peak": round(peak_fp32, 2),
+                "unit": "TFLOP/s",
+                "frac": round(achieved / peak_fp32, 4),
+                "traffic": None,
+                "peak_source": "nominal FP32 FMA rate 148 SM x 128 lanes x 2 flop x max SM clock "
+                               "(MEASURED_PEAKS.json has no FP32 SIMT figure)",
+                "per_launch_ms": round(per_launch_ms, 4),
+                "algorithmic_gflop_per_launch": round(flops[dom] / max(1, n_dom) / 1e9, 3),
+                "hbm_peak_gbs": peaks.get("hbm_gbs"),
+            },
+            "stage_ms_per_plane": {"basic": round(t_basic / max(1, n_basic), 4),
+                                   "final": round(t_final / max(1, n_final), 4)},
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _ref_backend():
+    import oracle
+    kind = "reference" if oracle.reference_available() else "port"
+    if kind == "port":
+        oracle.build(reference=False)
+    return kind, oracle.backend(kind, np.float32)
+
+
+def _cpu_tasks(planes, rows: int):
+    """(plane index, strip) tasks of `rows` rows each over the step's planes."""
+    tasks = []
+    for k, p in enumerate(planes):
+        for y0 in range(0, H, rows):
+            y1 = min(H, y0 + rows)
+            if y1 - y0 >= 16:
+                tasks.append((k, np.ascontiguousarray(p[y0:y1])))
+    return tasks
+
+
+def _run_cpu(backend, tasks, cores):
+    px = sum(t[1].size for t in tasks)
+
+    def one(t):
+        k, strip = t
+        backend.full(_PARAMS[k][0], _PARAMS[k][1], strip)
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(one, tasks))
+    return px, time.perf_counter() - t0
+
+
+_PARAMS = []
+
+
+def _init_params():
+    import oracle
+    from isp_mw_b200 import synth
+    _PARAMS.clear()
+    for s in SIGMAS:
+        sp = [synth.sigma_param(s)] * 3
+        if oracle.reference_available():
+            _PARAMS.append((oracle.reference_stage_default("fast", False, sp),
+                            oracle.reference_stage_default("fast", True, sp)))
+        else:
+            import isp_mw_b200
+            _PARAMS.append((isp_mw_b200.stage_params_default("fast", False, sp).as_dict(),
+                            isp_mw_b200.stage_params_default("fast", True, sp).as_dict()))
+
+
+def cpu_baseline(planes, budget_s: float = 20.0):
+    """The reference's CPU BM3D on this host's cores, on a bounded sample:
+    horizontal strips of the step's planes, one strip per task."""
+    kind, backend = _ref_backend()
+    _init_params()
+    cores = len(os.sched_getaffinity(0))
+    # size the sample: strips of 120 rows; take as many as fit the budget
+    tasks = _cpu_tasks(planes, 120)
+    px1, t1 = _run_cpu(backend, tasks[:cores], cores)  # calibration
+    rate = px1 / t1
+    n = max(cores, min(len(tasks), int(budget_s * rate / (tasks[0][1].size))))
+    px, t = _run_cpu(backend, tasks[:n], cores)
+    return {"value": round(px / t / 1e6, 4), "unit": "MP/s", "cores": cores, "kind": kind,
+            "sample": f"{n} strips of 1920x120 from the step's 4 planes (sigma sweep), "
+                      f"basic+final fast profile, {px / 1e6:.2f} MP in {t:.1f} s, "
+                      f"one strip per thread"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    kind, backend = _ref_backend()
+    _init_params()
+    cores = len(os.sched_getaffinity(0))
+    planes = make_inputs(0)[0]
+    tasks = _cpu_tasks(planes, 120)
+    # calibrate: one wave of `cores` strips in parallel; a step is as many
+    # waves as fit so that warm-up + timed steps take about 150 s
+    _, t1 = _run_cpu(backend, tasks[:cores], cores)
+    budget = 150.0 / max(1, args.steps + args.warmup)
+    per_step = min(len(tasks), cores * max(1, int(budget / max(1e-6, t1))))
+    for i in range(args.warmup):
+        _run_cpu(backend, tasks[:per_step], cores)
+    tot_px, tot_t = 0, 0.0
+    for i in range(args.steps):
+        px, t = _run_cpu(backend, tasks[:per_step], cores)
+        tot_px += px
+        tot_t += t
+    value = tot_px / tot_t / 1e6
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(value, 4),
+        "unit": "MP/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(tot_t / args.steps * 1e3, 2),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded piecewise-smooth planes + Gaussian noise)",
+        "config": {"workload": "BM3D basic+final, fast profile, 1920x1080 f32 luma planes "
+                               "(sigma 5/10/25/50 per 255)", "width": W, "height": H,
+                   "profile": "fast", "sigma_255": list(SIGMAS)},
+        "cpu_baseline": {"value": round(value, 4), "unit": "MP/s", "cores": cores, "kind": kind,
+                         "sample": f"{per_step} strips of 1920x120 per step, one per thread, "
+                                   f"from the 4 planes of the sigma sweep"},
+        "e2e": {"value": round(value, 4), "unit": "MP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

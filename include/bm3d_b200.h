@@ -1,0 +1,165 @@
+/* bm3d_b200: B200-native BM3D (basic hard-threshold estimate and final Wiener
+ * estimate) behind a plain C ABI.
+ *
+ * This is the drop-in boundary for the BM3D path of mawen1250/ISP_MW. Each
+ * entry point below names the reference interface it replaces. The C++
+ * classes in bm3d_b200/BM3D.hpp (BM3D_Para, BM3D_Basic, BM3D_Final, BM3D)
+ * mirror the reference's filter classes on top of these functions.
+ *
+ * Conventions
+ *   - Planes are row-major float32 (or float64 for the *_f64 entry points)
+ *     with a row pitch `stride` in elements (stride >= width).
+ *   - `mem` says whether the plane pointers are host or device memory. With
+ *     BM3D_MEM_HOST the call copies in, filters and copies out before it
+ *     returns. With BM3D_MEM_DEVICE it only enqueues work on `stream`
+ *     (a cudaStream_t, NULL = the legacy default stream) and returns.
+ *   - The caller owns every plane. The context owns its device scratch
+ *     (accumulators, staging, tables) and grows it on demand.
+ *   - A context belongs to one host thread at a time.
+ *   - No CPU fallback: without a usable sm_100 device every call fails with
+ *     BM3D_ERR_CUDA.
+ */
+#ifndef BM3D_B200_H_
+#define BM3D_B200_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+enum {
+    BM3D_OK = 0,
+    /* The reference's parameter guard fired (sigma <= 0, GroupSize == 0,
+     * BlockSize <= 0, BMrange <= 0, BMrange < BMstep or thMSE <= 0), so src was
+     * copied to dst unchanged, as source/BM3D.cpp:82-87 and 143-151 do. */
+    BM3D_COPIED = 1,
+    BM3D_ERR_INVALID = -1,     /* null pointer, width/height < BlockSize, stride < width, ... */
+    BM3D_ERR_UNSUPPORTED = -2, /* parameters valid in the reference but not built here */
+    BM3D_ERR_CUDA = -3,        /* CUDA runtime error (message via bm3d_last_error) */
+    BM3D_ERR_NOMEM = -4        /* device allocation failed */
+};
+
+enum { BM3D_MEM_HOST = 0, BM3D_MEM_DEVICE = 1 };
+
+/* Numeric fields of one stage's parameters.
+ * Replaces BM3D_Para_Base / BM3D_Basic_Para / BM3D_Final_Para
+ * (reference include/BM3D.h:15-151). `sigma` is on the 0-255 scale, one
+ * value per plane; thMSE and sigma are the unscaled user values: the OPP
+ * normalisation of include/BM3D.h:241-258 is applied inside. */
+typedef struct bm3d_stage_params {
+    int block_size;  /* BlockSize */
+    int block_step;  /* BlockStep */
+    int group_size;  /* GroupSize */
+    int bm_range;    /* BMrange */
+    int bm_step;     /* BMstep */
+    double thMSE;    /* thMSE */
+    double lambda;   /* lambda (hard-threshold multiplier; unused by the final stage) */
+    double sigma[3]; /* sigma per plane, 0-255 scale */
+} bm3d_stage_params;
+
+/* Profile defaults of one stage ("fast", "lc", "np", "high", "vn"), with
+ * `sigma` applied and thMSE recomputed from sigma[0] as thMSE_Default() does.
+ * Replaces the BM3D_Basic_Para(profile) / BM3D_Final_Para(profile) constructors
+ * and thMSE_Default() (reference include/BM3D.h:54-97, 107-150). The reference
+ * never initialises the final stage's lambda; here it is 0.
+ * Returns BM3D_OK or BM3D_ERR_INVALID for an unknown profile (the reference
+ * exits the process, include/BM3D.h:79-84). */
+int bm3d_stage_params_default(const char *profile, int wiener, const double sigma[3],
+                              bm3d_stage_params *out);
+
+/* Recompute thMSE from sigma[0] for the given profile (reference
+ * BM3D_{Basic,Final}_Para::thMSE_Default, include/BM3D.h:89-97, 142-150). */
+int bm3d_stage_params_thmse_default(const char *profile, int wiener, bm3d_stage_params *p);
+
+typedef struct bm3d_ctx bm3d_ctx;
+
+/* Create a context on CUDA device `device`. Replaces the per-filter FFTW
+ * planning and table setup of the BM3D_Base constructor
+ * (reference include/BM3D.h:237-259, source/BM3D.cpp:9-73), which here happens
+ * per call from the parameters (a few hundred bytes of constants). */
+int bm3d_ctx_create(bm3d_ctx **out, int device);
+void bm3d_ctx_destroy(bm3d_ctx *ctx);
+
+/* Last error message of this context (or of the last failed create), never NULL. */
+const char *bm3d_last_error(const bm3d_ctx *ctx);
+
+/* One BM3D stage on one plane: dst = stage(src, ref).
+ *   wiener = 0: basic estimate, matching and hard thresholding on `ref`
+ *               (usually ref == src).
+ *   wiener = 1: final estimate; `ref` is the basic estimate.
+ * `value_range` is the plane's ValueRange() (Ceil - Floor, 1 for the
+ * reference's default Plane_FL); it scales the matching threshold.
+ * Replaces BM3D_Basic::process(dst, src, ref) / BM3D_Final::process(dst, src, ref)
+ * through FilterIF2::process (reference include/Filter.h:174) and
+ * BM3D_Base::Kernel(dst, src, ref) (source/BM3D.cpp:80-136). */
+int bm3d_stage(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, float *dst,
+               const float *src, const float *ref, int width, int height, size_t stride,
+               float value_range, int mem, void *stream);
+
+/* Three planes (Y, U, V) sharing the groups matched on ref[0]; planes with
+ * sigma[p] <= 0 are left untouched in dst. Replaces the 9-plane
+ * BM3D_Base::Kernel (reference source/BM3D.cpp:139-218). */
+int bm3d_stage3(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, float *const dst[3],
+                const float *const src[3], const float *const ref[3], int width, int height,
+                size_t stride, float value_range, int mem, void *stream);
+
+/* Basic then final on one plane, the basic estimate held in context scratch.
+ * Replaces BM3D::process_Plane_FL (reference source/BM3D.cpp:464-472) with
+ * the intermediate sized from src (the reference passes an empty plane there). */
+int bm3d_full(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *final_,
+              float *dst, const float *src, int width, int height, size_t stride,
+              float value_range, int mem, void *stream);
+
+/* Three-plane basic then final (reference BM3D::process_Frame's YUV core,
+ * source/BM3D.cpp:512-521). */
+int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *final_,
+               float *const dst[3], const float *const src[3], int width, int height,
+               size_t stride, float value_range, int mem, void *stream);
+
+/* FP64 forms of bm3d_stage / bm3d_full: the same kernels instantiated for
+ * double (the reference's FLType without _CUDA_, include/Type.h:26-30). */
+int bm3d_stage_f64(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, double *dst,
+                   const double *src, const double *ref, int width, int height, size_t stride,
+                   double value_range, int mem, void *stream);
+
+/* Number of reference blocks a stage visits on a width x height plane
+ * (the scan of reference source/BM3D.cpp:98-121), or -1 for bad arguments. */
+long long bm3d_ref_block_count(const bm3d_stage_params *params, int width, int height);
+
+/* Group of every reference block, in scan order (ref-block index = row-major
+ * over the scan): counts[r], pos_yx[(r * 16 + k) * 2 + {0, 1}] = (y, x) and
+ * keys[r * 16 + k] of member k. Arrays are host memory sized from
+ * bm3d_ref_block_count. Replaces BM3D_Base::BlockMatching
+ * (reference source/BM3D.cpp:221-236) for parity checks. */
+int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, const float *ref,
+                      int width, int height, size_t stride, float value_range, int *counts,
+                      int *pos_yx, float *keys);
+
+/* Counters of the last stage run on this context: out[0] = sum of group
+ * sizes, out[1] = sum of squared group sizes, out[2] = candidate blocks
+ * evaluated, out[3] = groups re-ordered to follow std::partial_sort's tie
+ * placement. Synchronises the context's last stream. */
+int bm3d_last_stats(bm3d_ctx *ctx, unsigned long long out[4]);
+
+/* Per-launch timing of the stage kernels with CUDA events recorded on the
+ * launch stream (off by default). Turning it on or off resets the totals.
+ * No counterpart in the reference, which has no timing hooks beyond an
+ * untimed loop (source/ISP_MW.cpp:38-107). */
+int bm3d_set_kernel_timing(bm3d_ctx *ctx, int on);
+
+/* Total device time (ms) and launch count of the basic (wiener = 0) or final
+ * (wiener = 1) stage kernel since timing was turned on. Waits for the
+ * recorded launches to finish. */
+int bm3d_kernel_time(bm3d_ctx *ctx, int wiener, double *ms, long long *launches);
+
+/* Tile shape used by the stage kernels: reference blocks per CTA tile
+ * (tile_x x tile_y) and warps per CTA. 0 keeps the current value. */
+int bm3d_set_tiling(bm3d_ctx *ctx, int tile_x, int tile_y, int warps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,401 @@
+"""isp_mw_b200: B200-native BM3D behind the C ABI of ``include/bm3d_b200.h``.
+
+Python binding over ``lib/libisp_mw_b200.so`` (ctypes). It mirrors the
+reference's BM3D filter API (mawen1250/ISP_MW ``include/BM3D.h``):
+``BM3D_Basic_Para`` / ``BM3D_Final_Para`` / ``BM3D_Para`` with their profiles
+and ``thMSE_Default``, and filters ``BM3D_Basic``, ``BM3D_Final`` and ``BM3D``
+whose ``process(dst, src[, ref])`` / ``__call__(src[, ref])`` follow
+``FilterIF2`` (``include/Filter.h:138-217``). Planes are numpy arrays (host
+memory: copied in and out) or CUDA torch tensors (device memory: work is
+enqueued on the current torch stream).
+
+There is no CPU path: without the compiled library or a B200 every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libisp_mw_b200.so")
+
+BM3D_OK = 0
+BM3D_COPIED = 1
+BM3D_ERR_INVALID = -1
+BM3D_ERR_UNSUPPORTED = -2
+BM3D_ERR_CUDA = -3
+BM3D_ERR_NOMEM = -4
+MEM_HOST = 0
+MEM_DEVICE = 1
+
+EXPORTS = [
+    "bm3d_stage_params_default", "bm3d_stage_params_thmse_default", "bm3d_ctx_create",
+    "bm3d_ctx_destroy", "bm3d_last_error", "bm3d_stage", "bm3d_stage3", "bm3d_full",
+    "bm3d_full3", "bm3d_stage_f64", "bm3d_ref_block_count", "bm3d_debug_groups",
+    "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
+]
+
+
+class BM3DError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"bm3d status {code}: {msg}")
+        self.code = code
+
+
+class StageParams(ctypes.Structure):
+    """``bm3d_stage_params``: numeric fields of BM3D_Para_Base (include/BM3D.h:15-45)."""
+
+    _fields_ = [
+        ("block_size", ctypes.c_int),
+        ("block_step", ctypes.c_int),
+        ("group_size", ctypes.c_int),
+        ("bm_range", ctypes.c_int),
+        ("bm_step", ctypes.c_int),
+        ("thMSE", ctypes.c_double),
+        ("lambda_", ctypes.c_double),
+        ("sigma", ctypes.c_double * 3),
+    ]
+
+    def as_dict(self) -> dict:
+        return {
+            "block_size": self.block_size, "block_step": self.block_step,
+            "group_size": self.group_size, "bm_range": self.bm_range,
+            "bm_step": self.bm_step, "thMSE": self.thMSE, "lambda": self.lambda_,
+            "sigma": list(self.sigma),
+        }
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "StageParams":
+        p = cls()
+        for k in ("block_size", "block_step", "group_size", "bm_range", "bm_step", "thMSE"):
+            setattr(p, k, d[k])
+        p.lambda_ = d.get("lambda", 0.0)
+        for i in range(3):
+            p.sigma[i] = d["sigma"][i]
+        return p
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the compiled library; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m isp_mw_b200.build` (no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    vp, cp, ip = ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int
+    sp = ctypes.POINTER(StageParams)
+    lib.bm3d_stage_params_default.argtypes = [cp, ip, ctypes.POINTER(ctypes.c_double), sp]
+    lib.bm3d_stage_params_thmse_default.argtypes = [cp, ip, sp]
+    lib.bm3d_ctx_create.argtypes = [ctypes.POINTER(vp), ip]
+    lib.bm3d_ctx_destroy.argtypes = [vp]
+    lib.bm3d_ctx_destroy.restype = None
+    lib.bm3d_last_error.argtypes = [vp]
+    lib.bm3d_last_error.restype = cp
+    plane = [ip, ip, ctypes.c_size_t, ctypes.c_float, ip, vp]
+    lib.bm3d_stage.argtypes = [vp, sp, ip, vp, vp, vp] + plane
+    lib.bm3d_stage3.argtypes = [vp, sp, ip, vp, vp, vp] + plane
+    lib.bm3d_full.argtypes = [vp, sp, sp, vp, vp] + plane
+    lib.bm3d_full3.argtypes = [vp, sp, sp, vp, vp] + plane
+    lib.bm3d_stage_f64.argtypes = [vp, sp, ip, vp, vp, vp, ip, ip, ctypes.c_size_t,
+                                   ctypes.c_double, ip, vp]
+    lib.bm3d_ref_block_count.argtypes = [sp, ip, ip]
+    lib.bm3d_ref_block_count.restype = ctypes.c_longlong
+    lib.bm3d_debug_groups.argtypes = [vp, sp, ip, vp, ip, ip, ctypes.c_size_t, ctypes.c_float,
+                                      vp, vp, vp]
+    lib.bm3d_last_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
+    lib.bm3d_set_tiling.argtypes = [vp, ip, ip, ip]
+    lib.bm3d_set_kernel_timing.argtypes = [vp, ip]
+    lib.bm3d_kernel_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_longlong)]
+    _lib = lib
+    return lib
+
+
+def stage_params_default(profile: str = "fast", wiener: bool = False,
+                         sigma: Sequence[float] = (10.0, 10.0, 10.0)) -> StageParams:
+    """Profile defaults with sigma applied and thMSE_Default() re-run."""
+    lib = load_library()
+    p = StageParams()
+    s = (ctypes.c_double * 3)(*sigma)
+    rc = lib.bm3d_stage_params_default(profile.encode(), int(wiener), s, ctypes.byref(p))
+    if rc != BM3D_OK:
+        raise ValueError(f"unrecognized profile {profile!r}")
+    return p
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _plane_info(x):
+    """(pointer, mem kind, width, height, stride, dtype name) of a plane."""
+    if _is_torch(x):
+        if x.dim() != 2 or x.stride(1) != 1:
+            raise ValueError("planes must be 2-D with unit column stride")
+        mem = MEM_DEVICE if x.is_cuda else MEM_HOST
+        return x.data_ptr(), mem, x.shape[1], x.shape[0], x.stride(0), str(x.dtype).split(".")[-1]
+    a = x
+    if not isinstance(a, np.ndarray) or a.ndim != 2 or a.strides[1] != a.itemsize:
+        raise ValueError("planes must be 2-D numpy arrays with unit column stride")
+    return a.ctypes.data, MEM_HOST, a.shape[1], a.shape[0], a.strides[0] // a.itemsize, a.dtype.name
+
+
+def _stream_of(x) -> int:
+    if _is_torch(x) and x.is_cuda:
+        import torch
+        return torch.cuda.current_stream(x.device).cuda_stream
+    return 0
+
+
+class Context:
+    """A ``bm3d_ctx`` on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.bm3d_ctx_create(ctypes.byref(h), int(device))
+        if rc != BM3D_OK:
+            raise BM3DError(rc, self.lib.bm3d_last_error(None).decode())
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bm3d_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, allow_copied: bool = True) -> int:
+        if rc == BM3D_OK or (allow_copied and rc == BM3D_COPIED):
+            return rc
+        raise BM3DError(rc, self.lib.bm3d_last_error(self.h).decode())
+
+    def set_tiling(self, tile_x: int = 0, tile_y: int = 0, warps: int = 0):
+        self._check(self.lib.bm3d_set_tiling(self.h, tile_x, tile_y, warps))
+
+    def stage(self, params: StageParams, wiener: bool, dst, src, ref=None,
+              value_range: float = 1.0) -> int:
+        """One stage on one plane (``bm3d_stage`` / ``bm3d_stage_f64``)."""
+        ref = src if ref is None else ref
+        dp, mem, w, h, stride, dt = _plane_info(dst)
+        spp, mem_s, *_ = _plane_info(src)
+        rp, mem_r, *_ = _plane_info(ref)
+        if not (mem == mem_s == mem_r):
+            raise ValueError("dst, src and ref must live in the same memory")
+        stream = _stream_of(dst)
+        if dt == "float64":
+            rc = self.lib.bm3d_stage_f64(self.h, ctypes.byref(params), int(wiener), dp, spp, rp,
+                                         w, h, stride, ctypes.c_double(value_range), mem, stream)
+        else:
+            rc = self.lib.bm3d_stage(self.h, ctypes.byref(params), int(wiener), dp, spp, rp, w,
+                                     h, stride, value_range, mem, stream)
+        return self._check(rc)
+
+    def stage3(self, params: StageParams, wiener: bool, dst, src, ref=None,
+               value_range: float = 1.0) -> int:
+        ref = src if ref is None else ref
+        infos = [_plane_info(x) for x in list(dst) + list(src) + list(ref)]
+        w, h, stride, mem = infos[0][2], infos[0][3], infos[0][4], infos[0][1]
+        arr = ctypes.c_void_p * 3
+        rc = self.lib.bm3d_stage3(self.h, ctypes.byref(params), int(wiener),
+                                  arr(*[i[0] for i in infos[0:3]]),
+                                  arr(*[i[0] for i in infos[3:6]]),
+                                  arr(*[i[0] for i in infos[6:9]]), w, h, stride, value_range,
+                                  mem, _stream_of(dst[0]))
+        return self._check(rc)
+
+    def full(self, basic: StageParams, final: StageParams, dst, src,
+             value_range: float = 1.0) -> int:
+        dp, mem, w, h, stride, _ = _plane_info(dst)
+        spp, *_ = _plane_info(src)
+        rc = self.lib.bm3d_full(self.h, ctypes.byref(basic), ctypes.byref(final), dp, spp, w, h,
+                                stride, value_range, mem, _stream_of(dst))
+        return self._check(rc)
+
+    def full3(self, basic: StageParams, final: StageParams, dst, src,
+              value_range: float = 1.0) -> int:
+        infos = [_plane_info(x) for x in list(dst) + list(src)]
+        w, h, stride, mem = infos[0][2], infos[0][3], infos[0][4], infos[0][1]
+        arr = ctypes.c_void_p * 3
+        rc = self.lib.bm3d_full3(self.h, ctypes.byref(basic), ctypes.byref(final),
+                                 arr(*[i[0] for i in infos[0:3]]),
+                                 arr(*[i[0] for i in infos[3:6]]), w, h, stride, value_range,
+                                 mem, _stream_of(dst[0]))
+        return self._check(rc)
+
+    def ref_block_count(self, params: StageParams, width: int, height: int) -> int:
+        return int(self.lib.bm3d_ref_block_count(ctypes.byref(params), width, height))
+
+    def debug_groups(self, params: StageParams, wiener: bool, ref: np.ndarray,
+                     value_range: float = 1.0):
+        """Group of every reference block: (counts[R], pos[R, 16, 2] (y, x), keys[R, 16])."""
+        ref = np.ascontiguousarray(ref, dtype=np.float32)
+        h, w = ref.shape
+        n = self.ref_block_count(params, w, h)
+        counts = np.zeros(n, np.int32)
+        pos = np.full((n, 16, 2), -1, np.int32)
+        keys = np.zeros((n, 16), np.float32)
+        rc = self.lib.bm3d_debug_groups(self.h, ctypes.byref(params), int(wiener),
+                                        ref.ctypes.data, w, h, w, value_range,
+                                        counts.ctypes.data, pos.ctypes.data, keys.ctypes.data)
+        self._check(rc, allow_copied=False)
+        return counts, pos, keys
+
+    def set_kernel_timing(self, on: bool):
+        self._check(self.lib.bm3d_set_kernel_timing(self.h, int(on)))
+
+    def kernel_time(self, wiener: bool):
+        """(total ms, launches) of the basic / final stage kernel since timing began."""
+        ms, n = ctypes.c_double(), ctypes.c_longlong()
+        self._check(self.lib.bm3d_kernel_time(self.h, int(wiener), ctypes.byref(ms),
+                                              ctypes.byref(n)))
+        return ms.value, n.value
+
+    def last_stats(self):
+        out = (ctypes.c_ulonglong * 4)()
+        self._check(self.lib.bm3d_last_stats(self.h, out))
+        return [int(v) for v in out]
+
+
+# ---------------------------------------------------------------------------
+# Mirror of the reference's parameter and filter classes (include/BM3D.h).
+
+class BM3D_Para_Base:
+    """Fields of BM3D_Para_Base (include/BM3D.h:15-45)."""
+
+    wiener = False
+
+    def __init__(self, profile: str = "fast"):
+        self.profile = profile
+        p = stage_params_default(profile, self.wiener, (10.0, 10.0, 10.0))
+        self.sigma = [10.0, 10.0, 10.0]
+        self.BlockSize = p.block_size
+        self.BlockStep = p.block_step
+        self.GroupSize = p.group_size
+        self.BMrange = p.bm_range
+        self.BMstep = p.bm_step
+        self.thMSE = p.thMSE
+        self.lambda_ = p.lambda_
+
+    def thMSE_Default(self):
+        p = self.to_c()
+        load_library().bm3d_stage_params_thmse_default(self.profile.encode(), int(self.wiener),
+                                                       ctypes.byref(p))
+        self.thMSE = p.thMSE
+
+    def to_c(self) -> StageParams:
+        return StageParams.from_dict({
+            "block_size": self.BlockSize, "block_step": self.BlockStep,
+            "group_size": self.GroupSize, "bm_range": self.BMrange, "bm_step": self.BMstep,
+            "thMSE": self.thMSE, "lambda": self.lambda_, "sigma": self.sigma})
+
+
+class BM3D_Basic_Para(BM3D_Para_Base):
+    """include/BM3D.h:48-98."""
+    wiener = False
+
+
+class BM3D_Final_Para(BM3D_Para_Base):
+    """include/BM3D.h:101-151."""
+    wiener = True
+
+
+class BM3D_Para:
+    """include/BM3D.h:154-168."""
+
+    def __init__(self, profile: str = "fast"):
+        self.basic = BM3D_Basic_Para(profile)
+        self.final = BM3D_Final_Para(profile)
+
+    def thMSE_Default(self):
+        self.basic.thMSE_Default()
+        self.final.thMSE_Default()
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _empty_like(x):
+    if _is_torch(x):
+        import torch
+        return torch.empty_like(x)
+    return np.empty_like(x)
+
+
+class _Stage:
+    wiener = False
+
+    def __init__(self, para: Optional[BM3D_Para_Base] = None, ctx: Optional[Context] = None):
+        self.para = para if para is not None else (
+            BM3D_Final_Para() if self.wiener else BM3D_Basic_Para())
+        self.ctx = ctx
+
+    def process(self, dst, src, ref=None, value_range: float = 1.0):
+        """FilterIF2::process(dst, src[, ref]) (include/Filter.h:174-199)."""
+        ctx = self.ctx or default_context()
+        if isinstance(src, (list, tuple)):
+            ctx.stage3(self.para.to_c(), self.wiener, dst, src, ref, value_range)
+        else:
+            ctx.stage(self.para.to_c(), self.wiener, dst, src, ref, value_range)
+        return dst
+
+    def __call__(self, src, ref=None, value_range: float = 1.0):
+        """FilterIF2::operator()(src[, ref]) (include/Filter.h:189-216)."""
+        if isinstance(src, (list, tuple)):
+            dst = [s.copy() if isinstance(s, np.ndarray) else s.clone() for s in src]
+        else:
+            dst = _empty_like(src)
+        return self.process(dst, src, ref, value_range)
+
+
+class BM3D_Basic(_Stage):
+    """include/BM3D.h:287-309: the hard-threshold basic estimate."""
+    wiener = False
+
+
+class BM3D_Final(_Stage):
+    """include/BM3D.h:312-334: the Wiener final estimate (ref = basic estimate)."""
+    wiener = True
+
+
+class BM3D:
+    """include/BM3D.h:337-357: basic then final."""
+
+    def __init__(self, para: Optional[BM3D_Para] = None, ctx: Optional[Context] = None):
+        self.para = para if para is not None else BM3D_Para()
+        self.ctx = ctx
+
+    def process(self, dst, src, value_range: float = 1.0):
+        ctx = self.ctx or default_context()
+        if isinstance(src, (list, tuple)):
+            ctx.full3(self.para.basic.to_c(), self.para.final.to_c(), dst, src, value_range)
+        else:
+            ctx.full(self.para.basic.to_c(), self.para.final.to_c(), dst, src, value_range)
+        return dst
+
+    def __call__(self, src, value_range: float = 1.0):
+        if isinstance(src, (list, tuple)):
+            dst = [s.copy() if isinstance(s, np.ndarray) else s.clone() for s in src]
+        else:
+            dst = _empty_like(src)
+        return self.process(dst, src, value_range)

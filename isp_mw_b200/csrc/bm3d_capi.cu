@@ -1,0 +1,808 @@
+// C ABI of the B200 BM3D path (declared in include/bm3d_b200.h): parameter
+// mirroring, per-call constant setup, context scratch and kernel launches.
+#include "bm3d_b200.h"
+#include "bm3d_stage.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace bm3d;
+
+// ---------------------------------------------------------------------------
+// Context
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct bm3d_ctx {
+    int device = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
+    std::string err;
+    // scratch
+    DevBuf acc[2 * kMaxPlanes];       // num / den per plane
+    DevBuf basic[kMaxPlanes];         // basic estimate for bm3d_full*
+    DevBuf stage_in[kMaxPlanes];      // host-mode staging of src
+    DevBuf stage_ref[kMaxPlanes];     // host-mode staging of ref
+    DevBuf stage_out[kMaxPlanes];     // host-mode staging of dst
+    DevBuf groups[3];                 // debug group dump
+    unsigned long long *stats = nullptr;
+    float *absmax = nullptr;          // per plane max |src| of the running stage
+    cudaStream_t last_stream = nullptr;
+    int tile_x = 8, tile_y = 8, warps = 16;
+    // optional per-launch timing of the stage kernels: [0] basic, [1] final
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[2];
+    double time_ms[2] = {0, 0};
+    long long launches[2] = {0, 0};
+};
+
+static void drain_timing(bm3d_ctx *ctx)
+{
+    for (int k = 0; k < 2; ++k) {
+        for (auto &ev : ctx->pending[k]) {
+            float ms = 0;
+            if (cudaEventSynchronize(ev.second) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, ev.first, ev.second) == cudaSuccess) {
+                ctx->time_ms[k] += ms;
+                ctx->launches[k] += 1;
+            }
+            cudaEventDestroy(ev.first);
+            cudaEventDestroy(ev.second);
+        }
+        ctx->pending[k].clear();
+    }
+}
+
+static thread_local std::string g_create_error;
+constexpr int kStats = 5;
+
+static int cuda_fail(bm3d_ctx *ctx, cudaError_t e, const char *what)
+{
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+    if (ctx) ctx->err = buf;
+    else g_create_error = buf;
+    return e == cudaErrorMemoryAllocation ? BM3D_ERR_NOMEM : BM3D_ERR_CUDA;
+}
+
+#define CK(ctx, call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);                           \
+    } while (0)
+
+static int ensure(bm3d_ctx *ctx, DevBuf &b, size_t bytes)
+{
+    if (b.bytes >= bytes) return BM3D_OK;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    CK(ctx, cudaMalloc(&b.ptr, bytes));
+    b.bytes = bytes;
+    return BM3D_OK;
+}
+
+static void upload_dct_tables()
+{
+    static std::vector<float> ff, fi;
+    static std::vector<double> df, di;
+    static int off[17];
+    if (ff.empty()) {
+        const long double pi = 3.141592653589793238462643383279502884L;
+        int o = 0;
+        for (int n = 1; n <= 16; ++n) {
+            off[n] = o;
+            for (int k = 0; k < n; ++k)
+                for (int j = 0; j < n; ++j) {
+                    long double cf = 2.0L * cosl(pi * (2 * j + 1) * k / (2.0L * n));
+                    long double ci = j == 0 ? 1.0L : 2.0L * cosl(pi * j * (2 * k + 1) / (2.0L * n));
+                    ff.push_back(static_cast<float>(cf));
+                    fi.push_back(static_cast<float>(ci));
+                    df.push_back(static_cast<double>(cf));
+                    di.push_back(static_cast<double>(ci));
+                }
+            o += n * n;
+        }
+        off[0] = 0;
+    }
+    cudaMemcpyToSymbol(c_dct_fwd_f, ff.data(), ff.size() * sizeof(float));
+    cudaMemcpyToSymbol(c_dct_inv_f, fi.data(), fi.size() * sizeof(float));
+    cudaMemcpyToSymbol(c_dct_fwd_d, df.data(), df.size() * sizeof(double));
+    cudaMemcpyToSymbol(c_dct_inv_d, di.data(), di.size() * sizeof(double));
+    cudaMemcpyToSymbol(c_dct_off, off, sizeof(off));
+}
+
+extern "C" int bm3d_ctx_create(bm3d_ctx **out, int device)
+{
+    if (!out) return BM3D_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
+    if (device < 0 || device >= count) {
+        g_create_error = "bm3d_ctx_create: no such CUDA device";
+        return BM3D_ERR_CUDA;
+    }
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceProperties");
+    if (prop.major < 10) {
+        g_create_error = "bm3d_ctx_create: this build targets sm_100a (B200)";
+        return BM3D_ERR_CUDA;
+    }
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+    bm3d_ctx *ctx = new bm3d_ctx;
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    ctx->smem_optin = prop.sharedMemPerBlockOptin;
+    upload_dct_tables();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        delete ctx;
+        return cuda_fail(nullptr, e, "upload_dct_tables");
+    }
+    e = cudaMalloc(&ctx->stats, kStats * sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        delete ctx;
+        return cuda_fail(nullptr, e, "cudaMalloc(stats)");
+    }
+    cudaMemset(ctx->stats, 0, kStats * sizeof(unsigned long long));
+    e = cudaMalloc(&ctx->absmax, kMaxPlanes * sizeof(float));
+    if (e != cudaSuccess) {
+        cudaFree(ctx->stats);
+        delete ctx;
+        return cuda_fail(nullptr, e, "cudaMalloc(absmax)");
+    }
+    *out = ctx;
+    return BM3D_OK;
+}
+
+extern "C" void bm3d_ctx_destroy(bm3d_ctx *ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    auto fr = [](DevBuf &b) {
+        if (b.ptr) cudaFree(b.ptr);
+        b.ptr = nullptr;
+    };
+    for (auto &b : ctx->acc) fr(b);
+    for (auto &b : ctx->basic) fr(b);
+    for (auto &b : ctx->stage_in) fr(b);
+    for (auto &b : ctx->stage_ref) fr(b);
+    for (auto &b : ctx->stage_out) fr(b);
+    for (auto &b : ctx->groups) fr(b);
+    if (ctx->stats) cudaFree(ctx->stats);
+    if (ctx->absmax) cudaFree(ctx->absmax);
+    drain_timing(ctx);
+    delete ctx;
+}
+
+extern "C" const char *bm3d_last_error(const bm3d_ctx *ctx)
+{
+    if (ctx) return ctx->err.c_str();
+    return g_create_error.c_str();
+}
+
+extern "C" int bm3d_set_tiling(bm3d_ctx *ctx, int tile_x, int tile_y, int warps)
+{
+    if (!ctx || tile_x < 0 || tile_y < 0 || warps < 0 || warps > 16) return BM3D_ERR_INVALID;
+    if (tile_x) ctx->tile_x = tile_x;
+    if (tile_y) ctx->tile_y = tile_y;
+    if (warps) ctx->warps = warps;
+    return BM3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Parameters: the reference's profile constructors (include/BM3D.h:27-151).
+
+static bool known_profile(const std::string &p)
+{
+    return p == "fast" || p == "lc" || p == "np" || p == "high" || p == "vn";
+}
+
+extern "C" int bm3d_stage_params_thmse_default(const char *profile, int wiener,
+                                               bm3d_stage_params *p)
+{
+    if (!profile || !p || !known_profile(profile)) return BM3D_ERR_INVALID;
+    const std::string prof(profile);
+    if (!wiener) p->thMSE = prof == "vn" ? 1000 + p->sigma[0] * 150 : 400 + p->sigma[0] * 80;
+    else p->thMSE = prof == "vn" ? 400 + p->sigma[0] * 40 : 200 + p->sigma[0] * 10;
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_stage_params_default(const char *profile, int wiener, const double sigma[3],
+                                         bm3d_stage_params *out)
+{
+    if (!profile || !out || !known_profile(profile)) return BM3D_ERR_INVALID;
+    const std::string prof(profile);
+    bm3d_stage_params p;
+    p.block_size = 8;
+    p.bm_range = (prof == "fast" || prof == "lc") ? 9 : 16;
+    p.bm_step = 1;
+    if (!wiener) {
+        p.block_step = 4;
+        p.group_size = 16;
+        p.lambda = 2.7;
+        if (prof == "fast") p.block_step = 8;
+        else if (prof == "lc") p.block_step = 6;
+        else if (prof == "high") p.block_step = 3;
+        else if (prof == "vn") {
+            p.block_step = 4;
+            p.group_size = 32;
+            p.lambda = 2.8;
+        }
+    } else {
+        p.block_step = 3;
+        p.group_size = 32;
+        p.lambda = 0;
+        if (prof == "fast") {
+            p.block_step = 7;
+            p.group_size = 16;
+        } else if (prof == "lc") {
+            p.block_step = 5;
+            p.group_size = 16;
+        } else if (prof == "high") {
+            p.block_step = 2;
+        } else if (prof == "vn") {
+            p.block_size = 11;
+            p.block_step = 6;
+        }
+    }
+    for (int i = 0; i < 3; ++i) p.sigma[i] = sigma ? sigma[i] : 10.0;
+    bm3d_stage_params_thmse_default(profile, wiener, &p);
+    *out = p;
+    return BM3D_OK;
+}
+
+extern "C" long long bm3d_ref_block_count(const bm3d_stage_params *p, int width, int height)
+{
+    if (!p || p->block_size <= 0 || p->block_step <= 0 || width < p->block_size ||
+        height < p->block_size)
+        return -1;
+    return static_cast<long long>(ref_count(width - p->block_size, p->block_step)) *
+           ref_count(height - p->block_size, p->block_step);
+}
+
+// ---------------------------------------------------------------------------
+// Stage setup: BM3D_Base ctor (include/BM3D.h:237-259) and BM3D_FilterData
+// ctor (source/BM3D.cpp:9-73), evaluated in double exactly as the reference.
+
+static void opp_norms(double norm[3])
+{
+    const double Yr = static_cast<double>(1.0L / 3.0L), Yg = Yr, Yb = Yr;
+    const double Ur = static_cast<double>(1.0L / 2.0L), Ug = 0.0, Ub = static_cast<double>(-1.0L / 2.0L);
+    const double Vr = static_cast<double>(1.0L / 4.0L), Vg = static_cast<double>(-1.0L / 2.0L),
+                 Vb = static_cast<double>(1.0L / 4.0L);
+    norm[0] = std::sqrt(Yr * Yr + Yg * Yg + Yb * Yb);
+    norm[1] = std::sqrt(Ur * Ur + Ug * Ug + Ub * Ub);
+    norm[2] = std::sqrt(Vr * Vr + Vg * Vg + Vb * Vb);
+}
+
+enum class Guard { Run, Copy, Invalid, Unsupported };
+
+static Guard check_params(const bm3d_stage_params *p, int nplanes)
+{
+    if (!p) return Guard::Invalid;
+    double norm[3];
+    opp_norms(norm);
+    const double thMSE = p->thMSE * norm[0];
+    const bool sig = nplanes == 3 ? (p->sigma[0] <= 0 && p->sigma[1] <= 0 && p->sigma[2] <= 0)
+                                  : (p->sigma[0] <= 0);
+    if (sig || p->group_size == 0 || p->block_size <= 0 || p->bm_range <= 0 ||
+        p->bm_range < p->bm_step || thMSE <= 0)
+        return Guard::Copy;
+    if (p->group_size < 0 || p->block_step <= 0 || p->bm_step <= 0) return Guard::Invalid;
+    if (p->block_size != kBS || p->group_size > kGSMax) return Guard::Unsupported;
+    return Guard::Run;
+}
+
+template <typename T>
+static void fill_tables(StageArgs<T> &a, const bm3d_stage_params *p, bool wiener, int nplanes,
+                        double value_range)
+{
+    double norm[3];
+    opp_norms(norm);
+    const double thMSE = p->thMSE * norm[0];
+    const int GS = p->group_size, BS = p->block_size;
+    a.active = 0;
+    for (int c = 0; c < nplanes; ++c) {
+        if (!(p->sigma[c] > 0)) continue;
+        a.active |= 1 << c;
+        const double sigma = p->sigma[c] / double(255) * norm[c];
+        for (int i = 1; i <= GS; ++i) {
+            const double finalAMP = 2 * i * 2 * BS * 2 * BS;
+            const double forwardAMP = std::sqrt(finalAMP);
+            a.wss[c][i - 1] = static_cast<T>(sigma * forwardAMP * sigma * forwardAMP);
+            const double thrBase = sigma * p->lambda * forwardAMP;
+            a.thr[c][i - 1][0] = static_cast<T>(thrBase);
+            a.thr[c][i - 1][1] = static_cast<T>(thrBase * std::sqrt(double(2)));
+            a.thr[c][i - 1][2] = static_cast<T>(thrBase * double(2));
+            a.thr[c][i - 1][3] = static_cast<T>(thrBase * std::sqrt(double(8)));
+        }
+    }
+    if (nplanes == 1) a.active = 1;
+    for (int i = 1; i <= GS; ++i) a.finalAMP[i - 1] = 2 * i * 2 * BS * 2 * BS;
+    (void)wiener;
+    // Block::BlockMatchingMulti (include/Block.h:582-584); the plane range is
+    // an FLType, promoted to double in the product.
+    const T range = static_cast<T>(value_range);
+    const double MSE2SSE = static_cast<double>(BS * BS) * range * range / double(255 * 255);
+    a.distMul = double(1) / MSE2SSE;
+    a.thSSE = static_cast<T>(thMSE * MSE2SSE);
+    a.match = (GS == 1 || thMSE <= 0) ? 0 : 1;
+}
+
+template <typename T, bool W, int NPL, int KS>
+static int launch_one(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int warps)
+{
+    auto kern = stage_kernel<T, W, NPL, KS>;
+    const SmemPlan sp =
+        plan_smem<T>(NPL, W, a.ref_alias_src, a.region_h, a.region_pitch, a.key_slots, warps);
+    CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sp.total)));
+    const int grid = a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->timing && !a.bm_only) {
+        CK(ctx, cudaEventCreate(&e0));
+        CK(ctx, cudaEventCreate(&e1));
+        CK(ctx, cudaEventRecord(e0, s));
+    }
+    kern<<<grid, warps * kWarp, sp.total, s>>>(a);
+    CK(ctx, cudaGetLastError());
+    if (e0) {
+        CK(ctx, cudaEventRecord(e1, s));
+        ctx->pending[W ? 1 : 0].emplace_back(e0, e1);
+    }
+    return BM3D_OK;
+}
+
+template <typename T, bool W, int NPL>
+static int launch_ks(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int warps)
+{
+    if (a.bm_step == 1) return launch_one<T, W, NPL, 4>(ctx, a, s, warps);
+    return launch_one<T, W, NPL, 1>(ctx, a, s, warps);
+}
+
+template <typename T>
+static int launch_stage(bm3d_ctx *ctx, StageArgs<T> &a, bool wiener, int nplanes, cudaStream_t s,
+                        int warps)
+{
+    if (nplanes == 1)
+        return wiener ? launch_ks<T, true, 1>(ctx, a, s, warps) : launch_ks<T, false, 1>(ctx, a, s, warps);
+    return wiener ? launch_ks<T, true, 3>(ctx, a, s, warps) : launch_ks<T, false, 3>(ctx, a, s, warps);
+}
+
+// Geometry, tiling and shared-memory fit.
+template <typename T>
+static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params *p, bool wiener,
+                         int nplanes, int width, int height, int &warps)
+{
+    a.width = width;
+    a.height = height;
+    a.step = p->block_step;
+    a.group_size = p->group_size;
+    a.bm_step = p->bm_step;
+    a.range = p->bm_range / p->bm_step * p->bm_step;
+    a.nx = ref_count(width - kBS, a.step);
+    a.ny = ref_count(height - kBS, a.step);
+    const int span = 2 * (a.range / a.bm_step) + 1;
+    a.key_slots = span * span + 1;
+    int tx = ctx->tile_x, ty = ctx->tile_y;
+    warps = ctx->warps;
+    for (;;) {
+        const int reach = a.match ? a.range : 0;
+        a.region_w = std::min(width, (tx - 1) * a.step + 2 * reach + kBS);
+        a.region_h = std::min(height, (ty - 1) * a.step + 2 * reach + kBS);
+        a.region_pitch = a.region_w | 1;
+        const SmemPlan sp = plan_smem<T>(nplanes, wiener, a.ref_alias_src, a.region_h,
+                                         a.region_pitch, a.key_slots, warps);
+        if (sp.total <= ctx->smem_optin) break;
+        if (warps > 8) warps /= 2;
+        else if (ty > 1 && ty >= tx) --ty;
+        else if (tx > 1) --tx;
+        else if (warps > 1) warps /= 2;
+        else {
+            ctx->err = "stage does not fit in shared memory";
+            return BM3D_ERR_UNSUPPORTED;
+        }
+    }
+    a.tile_x = std::min(tx, a.nx);
+    a.tile_y = std::min(ty, a.ny);
+    a.tiles_x = (a.nx + a.tile_x - 1) / a.tile_x;
+    return BM3D_OK;
+}
+
+template <typename T>
+static int copy_plane(bm3d_ctx *ctx, T *dst, size_t dpitch, const T *src, size_t spitch, int w,
+                      int h, cudaMemcpyKind kind, cudaStream_t s)
+{
+    CK(ctx, cudaMemcpy2DAsync(dst, dpitch * sizeof(T), src, spitch * sizeof(T), w * sizeof(T), h,
+                              kind, s));
+    return BM3D_OK;
+}
+
+// One stage over device-resident planes (all with row pitch `stride`).
+template <typename T>
+static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wiener, int nplanes,
+                            T *const dst[], const T *const src[], const T *const ref[], int width,
+                            int height, size_t stride, double value_range, cudaStream_t s,
+                            int *gcount = nullptr, int *gpos = nullptr, T *gkey = nullptr,
+                            bool bm_only = false)
+{
+    StageArgs<T> a;
+    std::memset(&a, 0, sizeof(a));
+    fill_tables(a, p, wiener, nplanes, value_range);
+    a.stride = static_cast<long long>(stride);
+    a.ref_alias_src = 0;
+    for (int c = 0; c < nplanes; ++c) {
+        a.src[c] = src[c];
+        a.ref[c] = ref[c];
+        if (src[c] == ref[c]) a.ref_alias_src |= 1 << c;
+    }
+    int warps;
+    int rc = plan_geometry(ctx, a, p, wiener, nplanes, width, height, warps);
+    if (rc != BM3D_OK) return rc;
+    using Acc = typename AccOf<T>::type;
+    const size_t acc_bytes = sizeof(Acc) * static_cast<size_t>(width) * height;
+    const long long npx = static_cast<long long>(width) * height;
+    const int threads = 256;
+    const int blocks = static_cast<int>(std::min<long long>((npx + threads - 1) / threads,
+                                                            static_cast<long long>(ctx->sm_count) * 8));
+    // At most 2 * (reference blocks) * GroupSize terms reach one pixel (block
+    // (0, 0) can sit in every group, twice).
+    const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, p->group_size);
+    a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
+    a.absmax = ctx->absmax;
+    if (!bm_only) CK(ctx, cudaMemsetAsync(ctx->absmax, 0, kMaxPlanes * sizeof(float), s));
+    for (int c = 0; c < nplanes; ++c) {
+        if (!(a.active & (1 << c)) && !bm_only) continue;
+        if ((rc = ensure(ctx, ctx->acc[2 * c], acc_bytes)) != BM3D_OK) return rc;
+        if ((rc = ensure(ctx, ctx->acc[2 * c + 1], acc_bytes)) != BM3D_OK) return rc;
+        a.num[c] = static_cast<Acc *>(ctx->acc[2 * c].ptr);
+        a.den[c] = static_cast<Acc *>(ctx->acc[2 * c + 1].ptr);
+        if (!bm_only) {
+            prep_kernel<T><<<blocks, threads, 0, s>>>(a.num[c], a.den[c], src[c],
+                                                      static_cast<long long>(stride), width,
+                                                      height, ctx->absmax + c);
+            CK(ctx, cudaGetLastError());
+        }
+    }
+    a.group_count = gcount;
+    a.group_pos = gpos;
+    a.group_key = gkey;
+    a.bm_only = bm_only ? 1 : 0;
+    a.stats = ctx->stats;
+    // per-stage counters; the invariant counter (stats[4]) is sticky
+    CK(ctx, cudaMemsetAsync(ctx->stats, 0, 4 * sizeof(unsigned long long), s));
+    if ((rc = launch_stage(ctx, a, wiener, nplanes, s, warps)) != BM3D_OK) return rc;
+    ctx->last_stream = s;
+    if (bm_only) return BM3D_OK;
+    for (int c = 0; c < nplanes; ++c) {
+        if (!(a.active & (1 << c))) continue;
+        normalize_kernel<T><<<blocks, threads, 0, s>>>(dst[c], static_cast<long long>(stride),
+                                                       a.num[c], a.den[c], width, height);
+        CK(ctx, cudaGetLastError());
+    }
+    return BM3D_OK;
+}
+
+// Host-mode calls end synchronised; a nonzero invariant counter means a group
+// member fell outside its tile's staged window and was skipped.
+static int check_invariants(bm3d_ctx *ctx)
+{
+    unsigned long long v[kStats];
+    CK(ctx, cudaMemcpy(v, ctx->stats, sizeof(v), cudaMemcpyDeviceToHost));
+    if (v[4] != 0) {
+        ctx->err = "internal error: " + std::to_string(v[4]) + " group blocks outside the staged window";
+        return BM3D_ERR_CUDA;
+    }
+    return BM3D_OK;
+}
+
+template <typename T>
+static int passthrough(bm3d_ctx *ctx, int nplanes, T *const dst[], const T *const src[], int width,
+                       int height, size_t stride, int mem, cudaStream_t s)
+{
+    for (int c = 0; c < nplanes; ++c) {
+        if (dst[c] == src[c]) continue;
+        int rc = copy_plane(ctx, dst[c], stride, src[c], stride, width, height,
+                            mem == BM3D_MEM_HOST ? cudaMemcpyHostToHost : cudaMemcpyDeviceToDevice, s);
+        if (rc != BM3D_OK) return rc;
+    }
+    if (mem == BM3D_MEM_HOST) CK(ctx, cudaStreamSynchronize(s));
+    return BM3D_COPIED;
+}
+
+static int check_planes(int nplanes, const void *const dst[], const void *const src[],
+                        const void *const ref[], int width, int height, size_t stride, int bs)
+{
+    if (width < bs || height < bs || stride < static_cast<size_t>(width)) return BM3D_ERR_INVALID;
+    for (int c = 0; c < nplanes; ++c)
+        if (!dst[c] || !src[c] || (ref && !ref[c])) return BM3D_ERR_INVALID;
+    return BM3D_OK;
+}
+
+// A stage in either memory kind. In host mode planes go through context
+// staging buffers with pitch = width.
+template <typename T>
+static int stage_any(bm3d_ctx *ctx, const bm3d_stage_params *p, int wiener, int nplanes,
+                     T *const dst[], const T *const src[], const T *const ref[], int width,
+                     int height, size_t stride, double value_range, int mem, void *stream)
+{
+    if (!ctx) return BM3D_ERR_INVALID;
+    if (mem != BM3D_MEM_HOST && mem != BM3D_MEM_DEVICE) return BM3D_ERR_INVALID;
+    const Guard g = check_params(p, nplanes);
+    if (g == Guard::Invalid) return BM3D_ERR_INVALID;
+    int rc = check_planes(nplanes, reinterpret_cast<const void *const *>(dst),
+                          reinterpret_cast<const void *const *>(src),
+                          reinterpret_cast<const void *const *>(ref), width, height, stride,
+                          p->block_size > 0 ? p->block_size : 1);
+    if (rc != BM3D_OK) return rc;
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (g == Guard::Copy) return passthrough(ctx, nplanes, dst, src, width, height, stride, mem, s);
+    if (g == Guard::Unsupported) {
+        ctx->err = "parameters outside this build (BlockSize 8, GroupSize <= 16)";
+        return BM3D_ERR_UNSUPPORTED;
+    }
+    if (mem == BM3D_MEM_DEVICE)
+        return run_stage_device(ctx, p, wiener != 0, nplanes, dst, src, ref, width, height, stride,
+                                value_range, s);
+    const size_t plane_bytes = sizeof(T) * static_cast<size_t>(width) * height;
+    T *dd[kMaxPlanes];
+    const T *ds[kMaxPlanes], *dr[kMaxPlanes];
+    for (int c = 0; c < nplanes; ++c) {
+        if ((rc = ensure(ctx, ctx->stage_in[c], plane_bytes)) != BM3D_OK) return rc;
+        if ((rc = ensure(ctx, ctx->stage_out[c], plane_bytes)) != BM3D_OK) return rc;
+        T *in = static_cast<T *>(ctx->stage_in[c].ptr);
+        if ((rc = copy_plane(ctx, in, width, src[c], stride, width, height,
+                             cudaMemcpyHostToDevice, s)) != BM3D_OK)
+            return rc;
+        ds[c] = in;
+        if (ref[c] == src[c]) {
+            dr[c] = in;
+        } else {
+            if ((rc = ensure(ctx, ctx->stage_ref[c], plane_bytes)) != BM3D_OK) return rc;
+            T *r = static_cast<T *>(ctx->stage_ref[c].ptr);
+            if ((rc = copy_plane(ctx, r, width, ref[c], stride, width, height,
+                                 cudaMemcpyHostToDevice, s)) != BM3D_OK)
+                return rc;
+            dr[c] = r;
+        }
+        dd[c] = static_cast<T *>(ctx->stage_out[c].ptr);
+        // planes this stage leaves alone (sigma <= 0) keep the caller's contents
+        if (nplanes > 1 && !(p->sigma[c] > 0))
+            if ((rc = copy_plane(ctx, dd[c], width, dst[c], stride, width, height,
+                                 cudaMemcpyHostToDevice, s)) != BM3D_OK)
+                return rc;
+    }
+    rc = run_stage_device(ctx, p, wiener != 0, nplanes, dd, ds, dr, width, height, width,
+                          value_range, s);
+    if (rc != BM3D_OK) return rc;
+    for (int c = 0; c < nplanes; ++c)
+        if ((rc = copy_plane(ctx, dst[c], stride, static_cast<const T *>(dd[c]), width, width,
+                             height, cudaMemcpyDeviceToHost, s)) != BM3D_OK)
+            return rc;
+    CK(ctx, cudaStreamSynchronize(s));
+    return check_invariants(ctx);
+}
+
+extern "C" int bm3d_stage(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, float *dst,
+                          const float *src, const float *ref, int width, int height,
+                          size_t stride, float value_range, int mem, void *stream)
+{
+    float *d[1] = {dst};
+    const float *s[1] = {src}, *r[1] = {ref ? ref : src};
+    return stage_any<float>(ctx, params, wiener, 1, d, s, r, width, height, stride, value_range,
+                            mem, stream);
+}
+
+extern "C" int bm3d_stage_f64(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener,
+                              double *dst, const double *src, const double *ref, int width,
+                              int height, size_t stride, double value_range, int mem,
+                              void *stream)
+{
+    double *d[1] = {dst};
+    const double *s[1] = {src}, *r[1] = {ref ? ref : src};
+    return stage_any<double>(ctx, params, wiener, 1, d, s, r, width, height, stride, value_range,
+                             mem, stream);
+}
+
+extern "C" int bm3d_stage3(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener,
+                           float *const dst[3], const float *const src[3],
+                           const float *const ref[3], int width, int height, size_t stride,
+                           float value_range, int mem, void *stream)
+{
+    if (!dst || !src) return BM3D_ERR_INVALID;
+    const float *const *r = ref ? ref : src;
+    return stage_any<float>(ctx, params, wiener, 3, dst, src, r, width, height, stride,
+                            value_range, mem, stream);
+}
+
+template <typename T>
+static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *fin,
+                    int nplanes, T *const dst[], const T *const src[], int width, int height,
+                    size_t stride, double value_range, int mem, void *stream)
+{
+    if (!ctx || !basic || !fin) return BM3D_ERR_INVALID;
+    if (mem != BM3D_MEM_HOST && mem != BM3D_MEM_DEVICE) return BM3D_ERR_INVALID;
+    int rc = check_planes(nplanes, reinterpret_cast<const void *const *>(dst),
+                          reinterpret_cast<const void *const *>(src), nullptr, width, height,
+                          stride, 1);
+    if (rc != BM3D_OK) return rc;
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t plane_bytes = sizeof(T) * static_cast<size_t>(width) * height;
+    const size_t dpitch = mem == BM3D_MEM_HOST ? static_cast<size_t>(width) : stride;
+    // Device-resident src and dst (context staging in host mode) and the basic
+    // estimate, all with row pitch dpitch.
+    const T *ds[kMaxPlanes];
+    T *tmp[kMaxPlanes], *dd[kMaxPlanes];
+    for (int c = 0; c < nplanes; ++c) {
+        if ((rc = ensure(ctx, ctx->basic[c], sizeof(T) * dpitch * height)) != BM3D_OK) return rc;
+        tmp[c] = static_cast<T *>(ctx->basic[c].ptr);
+    }
+    if (mem == BM3D_MEM_HOST) {
+        for (int c = 0; c < nplanes; ++c) {
+            if ((rc = ensure(ctx, ctx->stage_in[c], plane_bytes)) != BM3D_OK) return rc;
+            if ((rc = ensure(ctx, ctx->stage_out[c], plane_bytes)) != BM3D_OK) return rc;
+            T *in = static_cast<T *>(ctx->stage_in[c].ptr);
+            if ((rc = copy_plane(ctx, in, width, src[c], stride, width, height,
+                                 cudaMemcpyHostToDevice, s)) != BM3D_OK)
+                return rc;
+            ds[c] = in;
+            dd[c] = static_cast<T *>(ctx->stage_out[c].ptr);
+        }
+    } else {
+        for (int c = 0; c < nplanes; ++c) {
+            ds[c] = src[c];
+            dd[c] = dst[c];
+        }
+    }
+    // Planes a stage does not filter (sigma <= 0), or a stage whose parameters
+    // the reference's guard rejects, pass src through: the basic estimate and
+    // dst start as copies of src, as in the reference's in-place Frame path
+    // (source/BM3D.cpp:512-521).
+    for (int c = 0; c < nplanes; ++c) {
+        if ((rc = copy_plane(ctx, tmp[c], dpitch, ds[c], dpitch, width, height,
+                             cudaMemcpyDeviceToDevice, s)) != BM3D_OK)
+            return rc;
+        if (nplanes > 1 || check_params(fin, nplanes) != Guard::Run)
+            if ((rc = copy_plane(ctx, dd[c], dpitch, ds[c], dpitch, width, height,
+                                 cudaMemcpyDeviceToDevice, s)) != BM3D_OK)
+                return rc;
+    }
+    {
+        const Guard g = check_params(basic, nplanes);
+        if (g == Guard::Invalid) return BM3D_ERR_INVALID;
+        if (g == Guard::Unsupported) {
+            ctx->err = "parameters outside this build (BlockSize 8, GroupSize <= 16)";
+            return BM3D_ERR_UNSUPPORTED;
+        }
+        if (g == Guard::Run) {
+            rc = run_stage_device(ctx, basic, false, nplanes, tmp, ds, ds, width, height, dpitch,
+                                  value_range, s);
+            if (rc != BM3D_OK) return rc;
+        }
+    }
+    {
+        const Guard g = check_params(fin, nplanes);
+        if (g == Guard::Invalid) return BM3D_ERR_INVALID;
+        if (g == Guard::Unsupported) {
+            ctx->err = "parameters outside this build (BlockSize 8, GroupSize <= 16)";
+            return BM3D_ERR_UNSUPPORTED;
+        }
+        const T *tr[kMaxPlanes];
+        for (int c = 0; c < nplanes; ++c) tr[c] = tmp[c];
+        if (g == Guard::Run) {
+            rc = run_stage_device(ctx, fin, true, nplanes, dd, ds, tr, width, height, dpitch,
+                                  value_range, s);
+            if (rc != BM3D_OK) return rc;
+        }
+    }
+    if (mem == BM3D_MEM_HOST) {
+        for (int c = 0; c < nplanes; ++c)
+            if ((rc = copy_plane(ctx, dst[c], stride, static_cast<const T *>(dd[c]), width, width,
+                                 height, cudaMemcpyDeviceToHost, s)) != BM3D_OK)
+                return rc;
+        CK(ctx, cudaStreamSynchronize(s));
+        return check_invariants(ctx);
+    }
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_full(bm3d_ctx *ctx, const bm3d_stage_params *basic,
+                         const bm3d_stage_params *final_, float *dst, const float *src, int width,
+                         int height, size_t stride, float value_range, int mem, void *stream)
+{
+    float *d[1] = {dst};
+    const float *s[1] = {src};
+    return full_any<float>(ctx, basic, final_, 1, d, s, width, height, stride, value_range, mem,
+                           stream);
+}
+
+extern "C" int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic,
+                          const bm3d_stage_params *final_, float *const dst[3],
+                          const float *const src[3], int width, int height, size_t stride,
+                          float value_range, int mem, void *stream)
+{
+    if (!dst || !src) return BM3D_ERR_INVALID;
+    return full_any<float>(ctx, basic, final_, 3, dst, src, width, height, stride, value_range,
+                           mem, stream);
+}
+
+extern "C" int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *p, int wiener,
+                                 const float *ref, int width, int height, size_t stride,
+                                 float value_range, int *counts, int *pos_yx, float *keys)
+{
+    if (!ctx || !p || !ref || !counts || !pos_yx || !keys) return BM3D_ERR_INVALID;
+    const Guard g = check_params(p, 1);
+    if (g == Guard::Invalid || g == Guard::Copy) return BM3D_ERR_INVALID;
+    if (g == Guard::Unsupported) return BM3D_ERR_UNSUPPORTED;
+    if (width < p->block_size || height < p->block_size || stride < static_cast<size_t>(width))
+        return BM3D_ERR_INVALID;
+    CK(ctx, cudaSetDevice(ctx->device));
+    const long long nref = bm3d_ref_block_count(p, width, height);
+    int rc;
+    const size_t plane_bytes = sizeof(float) * static_cast<size_t>(width) * height;
+    if ((rc = ensure(ctx, ctx->stage_in[0], plane_bytes)) != BM3D_OK) return rc;
+    if ((rc = ensure(ctx, ctx->groups[0], sizeof(int) * nref)) != BM3D_OK) return rc;
+    if ((rc = ensure(ctx, ctx->groups[1], sizeof(int) * nref * kGSMax * 2)) != BM3D_OK) return rc;
+    if ((rc = ensure(ctx, ctx->groups[2], sizeof(float) * nref * kGSMax)) != BM3D_OK) return rc;
+    cudaStream_t s = nullptr;
+    float *in = static_cast<float *>(ctx->stage_in[0].ptr);
+    if ((rc = copy_plane(ctx, in, width, ref, stride, width, height, cudaMemcpyHostToDevice, s)) !=
+        BM3D_OK)
+        return rc;
+    float *d[1] = {in};
+    const float *sp[1] = {in};
+    rc = run_stage_device<float>(ctx, p, wiener != 0, 1, d, sp, sp, width, height, width,
+                                 value_range, s, static_cast<int *>(ctx->groups[0].ptr),
+                                 static_cast<int *>(ctx->groups[1].ptr),
+                                 static_cast<float *>(ctx->groups[2].ptr), true);
+    if (rc != BM3D_OK) return rc;
+    CK(ctx, cudaMemcpyAsync(counts, ctx->groups[0].ptr, sizeof(int) * nref, cudaMemcpyDeviceToHost, s));
+    CK(ctx, cudaMemcpyAsync(pos_yx, ctx->groups[1].ptr, sizeof(int) * nref * kGSMax * 2,
+                            cudaMemcpyDeviceToHost, s));
+    CK(ctx, cudaMemcpyAsync(keys, ctx->groups[2].ptr, sizeof(float) * nref * kGSMax,
+                            cudaMemcpyDeviceToHost, s));
+    CK(ctx, cudaStreamSynchronize(s));
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_set_kernel_timing(bm3d_ctx *ctx, int on)
+{
+    if (!ctx) return BM3D_ERR_INVALID;
+    CK(ctx, cudaSetDevice(ctx->device));
+    drain_timing(ctx);
+    ctx->timing = on != 0;
+    ctx->time_ms[0] = ctx->time_ms[1] = 0;
+    ctx->launches[0] = ctx->launches[1] = 0;
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_kernel_time(bm3d_ctx *ctx, int wiener, double *ms, long long *launches)
+{
+    if (!ctx || !ms || !launches) return BM3D_ERR_INVALID;
+    CK(ctx, cudaSetDevice(ctx->device));
+    drain_timing(ctx);
+    *ms = ctx->time_ms[wiener ? 1 : 0];
+    *launches = ctx->launches[wiener ? 1 : 0];
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_last_stats(bm3d_ctx *ctx, unsigned long long out[4])
+{
+    if (!ctx || !out) return BM3D_ERR_INVALID;
+    CK(ctx, cudaSetDevice(ctx->device));
+    CK(ctx, cudaStreamSynchronize(ctx->last_stream));
+    CK(ctx, cudaMemcpy(out, ctx->stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    return BM3D_OK;
+}

@@ -1,0 +1,241 @@
+// Device-side pieces shared by the BM3D stage kernels: exactly-rounded
+// arithmetic helpers, the search-window geometry of the reference, sort keys
+// and the shared-memory layout of one CTA.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bm3d {
+
+constexpr int kWarp = 32;
+constexpr int kBS = 8;           // block size handled by the register-resident path
+constexpr int kGSMax = 16;       // largest group this path holds in registers
+constexpr int kGroupStride = 72; // floats per block in a warp's group buffer (64 + 8 pad)
+
+// ---------------------------------------------------------------------------
+// Arithmetic that must not be contracted into FMA: the reference accumulates
+// block distances as dist += temp * temp with separate rounding of the product
+// (include/Block.h:600-603; MSVC /fp:precise, msvc/ISP_MW.vcxproj:161,179).
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+// FLType(dist * distMul) with distMul a double (include/Block.h:610).
+__device__ __forceinline__ float key_from_dist(float d, double mul)
+{
+    return __double2float_rn(__dmul_rn(static_cast<double>(d), mul));
+}
+__device__ __forceinline__ double key_from_dist(double d, double mul) { return __dmul_rn(d, mul); }
+
+// ---------------------------------------------------------------------------
+// Block::_SearchBoundary (include/Block.h:716-746) in closed form.
+__host__ __device__ __forceinline__ int search_boundary(int pos, int plane_boundary, int range,
+                                                        int step)
+{
+    range = range / step * step;
+    if (pos == plane_boundary) return plane_boundary;
+    if (pos > plane_boundary) {
+        int b = pos - range;
+        if (b < plane_boundary) b += (plane_boundary - b + step - 1) / step * step;
+        return b;
+    }
+    int b = pos + range;
+    if (b > plane_boundary) b -= (b - plane_boundary + step - 1) / step * step;
+    return b;
+}
+
+// Reference-block position k along one axis: 0, step, 2 step, ... with the
+// last one clamped to the plane border (source/BM3D.cpp:98-120).
+__host__ __device__ __forceinline__ int ref_pos(int k, int step, int last)
+{
+    const int p = k * step;
+    return p > last ? last : p;
+}
+
+__host__ __device__ __forceinline__ int ref_count(int last, int step)
+{
+    return last / step + 1 + (last % step != 0 ? 1 : 0);
+}
+
+// ---------------------------------------------------------------------------
+// Sort keys: (key value, candidate index) compared lexicographically. Valid
+// keys are finite and >= 0, so the IEEE bit pattern orders like the value.
+// The candidate index is the candidate's place in the reference's search list
+// (raster order of the window, then the trailing (0, 0) slot), so ties in the
+// key fall back to that list order, which is std::stable_sort's order
+// (include/Block.h:699).
+template <typename T> struct SortKey;
+
+template <> struct SortKey<float> {
+    unsigned long long v;
+    static __device__ __forceinline__ SortKey invalid() { return SortKey{~0ull}; }
+    static __device__ __forceinline__ SortKey make(float key, unsigned idx)
+    {
+        return SortKey{(static_cast<unsigned long long>(__float_as_uint(key)) << 32) | idx};
+    }
+    __device__ __forceinline__ bool valid() const { return v != ~0ull; }
+    __device__ __forceinline__ float key() const { return __uint_as_float(static_cast<unsigned>(v >> 32)); }
+    __device__ __forceinline__ unsigned idx() const { return static_cast<unsigned>(v); }
+    __device__ __forceinline__ bool operator<(const SortKey &o) const { return v < o.v; }
+    __device__ __forceinline__ bool operator==(const SortKey &o) const { return v == o.v; }
+    __device__ __forceinline__ SortKey shfl_xor(int m) const
+    {
+        return SortKey{__shfl_xor_sync(0xffffffffu, v, m)};
+    }
+};
+
+template <> struct SortKey<double> {
+    unsigned long long k;
+    unsigned long long i;
+    static __device__ __forceinline__ SortKey invalid() { return SortKey{~0ull, ~0ull}; }
+    static __device__ __forceinline__ SortKey make(double key, unsigned idx)
+    {
+        return SortKey{static_cast<unsigned long long>(__double_as_longlong(key)), idx};
+    }
+    __device__ __forceinline__ bool valid() const { return k != ~0ull; }
+    __device__ __forceinline__ double key() const { return __longlong_as_double(static_cast<long long>(k)); }
+    __device__ __forceinline__ unsigned idx() const { return static_cast<unsigned>(i); }
+    __device__ __forceinline__ bool operator<(const SortKey &o) const
+    {
+        return k < o.k || (k == o.k && i < o.i);
+    }
+    __device__ __forceinline__ bool operator==(const SortKey &o) const { return k == o.k && i == o.i; }
+    __device__ __forceinline__ SortKey shfl_xor(int m) const
+    {
+        return SortKey{__shfl_xor_sync(0xffffffffu, k, m), __shfl_xor_sync(0xffffffffu, i, m)};
+    }
+};
+
+template <typename K> __device__ __forceinline__ K warp_min(K v)
+{
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) {
+        K o = v.shfl_xor(m);
+        if (o < v) v = o;
+    }
+    return v;
+}
+
+template <typename T> __device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int m = 16; m >= 1; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    return v;
+}
+
+// Plane position (row, column) of one block of a group.
+struct BlockPos {
+    int y, x;
+};
+
+// ---------------------------------------------------------------------------
+// Aggregation accumulators. FP32 stages accumulate numerator and weight sums
+// in 64-bit fixed point (value * 2^scale rounded to an integer): integer
+// atomics are associative, so the sums -- and everything downstream,
+// including the final stage's block matching on the basic estimate -- are
+// bit-reproducible and independent of tiling and scheduling. FP64 stages
+// accumulate in double.
+template <typename T> struct AccOf { using type = long long; };
+template <> struct AccOf<double> { using type = double; };
+
+// Fixed-point exponent for a plane whose |src| <= absmax when at most
+// 2^log2_bound contributions reach one pixel: every contribution is bounded by
+// 64 * absmax (a filtered block value is bounded by the group's L2 norm,
+// <= 32 * absmax for a 1024-pixel group, times a weight <= 1), so a pixel's
+// sum stays below 2^62.
+__device__ __forceinline__ float fixed_scale(float absmax, int log2_bound)
+{
+    if (!(absmax > 0.0f) || !(absmax < 3.0e38f)) absmax = 1.0f;
+    int e = 0;
+    frexpf(absmax * 64.0f, &e);  // absmax * 64 < 2^e
+    int s = 62 - e - log2_bound;
+    s = s < -60 ? -60 : (s > 60 ? 60 : s);
+    return ldexpf(1.0f, s);
+}
+
+// ---------------------------------------------------------------------------
+// Per-stage launch arguments (one struct, passed by value).
+constexpr int kMaxPlanes = 3;
+
+template <typename T> struct StageArgs {
+    const T *src[kMaxPlanes];   // noisy planes (collaborative filtering input)
+    const T *ref[kMaxPlanes];   // basic: plane 0 drives matching; final: basic estimate
+    typename AccOf<T>::type *num[kMaxPlanes];  // numerator sums, width x height, pitch = width
+    typename AccOf<T>::type *den[kMaxPlanes];  // weight sums, same layout
+    const float *absmax;        // per plane max |src| (device), sets the fixed-point scale
+    int log2_bound;             // ceil(log2(max contributions to one pixel))
+    int active;                 // bit p set: plane p is filtered (sigma[p] > 0)
+    int width, height;
+    long long stride;           // row pitch of src / ref, in elements
+    int step;                   // BlockStep
+    int group_size;             // GroupSize (1..kGSMax)
+    int range;                  // BMrange rounded down to a multiple of bm_step
+    int bm_step;                // BMstep
+    int match;                  // 0 when GroupSize == 1 or thMSE <= 0 (source/BM3D.cpp:226)
+    int nx, ny;                 // reference positions per axis
+    int tile_x, tile_y;         // reference positions per CTA tile
+    int tiles_x;                // tiles per row of the tile grid
+    int region_w, region_h;     // upper bounds of a tile's staged window
+    int region_pitch;           // row pitch of staged windows in shared memory
+    int key_slots;              // per-warp search list capacity
+    int ref_alias_src;          // bit p set: ref[p] == src[p], stage once
+    T thSSE;                    // FLType(thMSE * MSE2SSE)      (include/Block.h:582-584)
+    double distMul;             // 1 / MSE2SSE
+    T thr[kMaxPlanes][kGSMax][4];  // hard thresholds by (#zero indices) (source/BM3D.cpp:35-68)
+    T wss[kMaxPlanes][kGSMax];     // wienerSigmaSqr                     (source/BM3D.cpp:31)
+    double finalAMP[kGSMax];       // 2n * 2BS * 2BS                     (source/BM3D.cpp:26)
+    // optional outputs
+    int *group_count;           // per reference block: group size        (may be null)
+    int *group_pos;             // per reference block: kGSMax x (y, x)   (may be null)
+    T *group_key;               // per reference block: kGSMax keys       (may be null)
+    unsigned long long *stats;  // [0] sum n, [1] sum n^2, [2] candidates, [3] tie fix-ups,
+                                // [4] group members outside the staged window (must be 0)
+    int bm_only;                // skip the collaborative filter (group dump)
+};
+
+// Shared-memory carve-up of one CTA, identical on host and device.
+struct SmemPlan {
+    int n_stage;                 // staged windows (src planes + separate ref planes)
+    size_t region_bytes;         // one staged window
+    size_t acc_bytes;            // one accumulator window
+    size_t off_acc;              // 2 * planes accumulator windows
+    size_t off_origin;           // 64-value copies of block (0, 0) per staged window + accumulators
+    size_t off_warps;
+    size_t warp_bytes;
+    size_t total;
+};
+
+template <typename T>
+__host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alias_mask,
+                                              int region_h, int region_pitch, int key_slots,
+                                              int nwarps)
+{
+    SmemPlan s;
+    int nref = 0;
+    const int nref_planes = wiener ? nplanes : 1;
+    for (int p = 0; p < nref_planes; ++p)
+        if (!(alias_mask & (1 << p))) ++nref;
+    s.n_stage = nplanes + nref;
+    using Acc = typename AccOf<T>::type;
+    s.region_bytes = (static_cast<size_t>(region_h) * region_pitch * sizeof(T) + 15) / 16 * 16;
+    s.acc_bytes = (static_cast<size_t>(region_h) * region_pitch * sizeof(Acc) + 15) / 16 * 16;
+    s.off_acc = s.region_bytes * s.n_stage;
+    s.off_origin = s.off_acc + s.acc_bytes * 2 * nplanes;
+    // block (0, 0) copies: T per staged window, then Acc per accumulator
+    const size_t origin_bytes = sizeof(T) * 64 * s.n_stage + sizeof(Acc) * 64 * 2 * nplanes;
+    s.off_warps = (s.off_origin + origin_bytes + 15) / 16 * 16;
+    const size_t group_bytes = sizeof(T) * kGSMax * kGroupStride;
+    const size_t key_bytes = sizeof(SortKey<T>) * key_slots;
+    const size_t scratch = group_bytes > key_bytes ? group_bytes : key_bytes;
+    // scratch | heap (kGSMax sort keys) | group list (kGSMax BlockPos) | group keys (kGSMax T)
+    s.warp_bytes = (scratch + sizeof(SortKey<T>) * kGSMax + sizeof(BlockPos) * kGSMax +
+                    sizeof(T) * kGSMax + 15) / 16 * 16;
+    s.total = s.off_warps + s.warp_bytes * nwarps;
+    return s;
+}
+
+}  // namespace bm3d

@@ -1,0 +1,748 @@
+// Fused BM3D stage kernel: block matching, 3-D transform, shrinkage, inverse
+// transform and shared-memory aggregation for one tile of reference blocks per
+// CTA, one reference block per warp at a time.
+//
+// Reference: BM3D_Base::Kernel (source/BM3D.cpp:80-136, 139-218),
+// BM3D_Base::BlockMatching (source/BM3D.cpp:221-236),
+// Block::BlockMatchingMulti (include/Block.h:578-615, 658-703),
+// BM3D_Basic::CollaborativeFilter (source/BM3D.cpp:339-385),
+// BM3D_Final::CollaborativeFilter (source/BM3D.cpp:411-457).
+#pragma once
+
+#include "bm3d_device.cuh"
+#include "dct.cuh"
+
+namespace bm3d {
+
+// Cosine matrices for group lengths 1..16 (row k = output k), concatenated;
+// entry n starts at c_dct_off[n]. Filled by the host when a context is made.
+__constant__ float c_dct_fwd_f[1496];
+__constant__ float c_dct_inv_f[1496];
+__constant__ double c_dct_fwd_d[1496];
+__constant__ double c_dct_inv_d[1496];
+__constant__ int c_dct_off[17];
+
+template <typename T> struct DctTab;
+template <> struct DctTab<float> {
+    static __device__ __forceinline__ const float *fwd() { return c_dct_fwd_f; }
+    static __device__ __forceinline__ const float *inv() { return c_dct_inv_f; }
+};
+template <> struct DctTab<double> {
+    static __device__ __forceinline__ const double *fwd() { return c_dct_fwd_d; }
+    static __device__ __forceinline__ const double *inv() { return c_dct_inv_d; }
+};
+
+template <typename T>
+__device__ __forceinline__ void zdct_fwd(T (&a)[kGSMax], int n)
+{
+    if (n == 16) redft10_16(a);
+    else dct_matrix<T, kGSMax>(a, n, DctTab<T>::fwd() + c_dct_off[n]);
+}
+
+template <typename T>
+__device__ __forceinline__ void zdct_inv(T (&a)[kGSMax], int n)
+{
+    if (n == 16) redft01_16(a);
+    else dct_matrix<T, kGSMax>(a, n, DctTab<T>::inv() + c_dct_off[n]);
+}
+
+// ---------------------------------------------------------------------------
+// One CTA's view of its staged windows.
+template <typename T> struct Tile {
+    using Acc = typename AccOf<T>::type;
+    int ry0, rx0, rh, rw;      // staged window origin / size in the plane
+    int pitch;
+    bool origin_inside;        // block (0, 0) lies inside the staged window
+    const T *srcw[kMaxPlanes]; // staged src windows
+    const T *refw[kMaxPlanes]; // staged ref windows (refw[0] drives matching)
+    const T *src0[kMaxPlanes]; // block (0, 0) of src when outside the window
+    const T *ref0[kMaxPlanes];
+    Acc *accN[kMaxPlanes], *accD[kMaxPlanes];
+    Acc *accN0[kMaxPlanes], *accD0[kMaxPlanes];
+};
+
+// One aggregation term: fixed point for FP32 stages, double for FP64.
+__device__ __forceinline__ void acc_add(long long *p, float v, float scale)
+{
+    atomicAdd(reinterpret_cast<unsigned long long *>(p),
+              static_cast<unsigned long long>(__float2ll_rn(v * scale)));
+}
+__device__ __forceinline__ void acc_add(double *p, double v, float) { atomicAdd(p, v); }
+__device__ __forceinline__ void acc_flush(long long *p, long long v)
+{
+    atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
+}
+__device__ __forceinline__ void acc_flush(double *p, double v) { atomicAdd(p, v); }
+
+// Address of pixel (y, x) of the block at plane position (py, px) inside a
+// staged window, or inside the (0, 0) copy when the block is (0, 0) and the
+// window does not contain it.
+template <typename T, typename P>
+__device__ __forceinline__ P *block_ptr(const Tile<T> &t, P *win, P *origin, int py, int px,
+                                        int &pitch)
+{
+    if (py == 0 && px == 0 && !t.origin_inside) {
+        pitch = kBS;
+        return origin;
+    }
+    pitch = t.pitch;
+    return win + (py - t.ry0) * t.pitch + (px - t.rx0);
+}
+
+// True when the block at (py, px) can be addressed: inside the staged window,
+// or the (0, 0) block held in its own copy. Group members always are by
+// construction; the check keeps a violated invariant from touching memory.
+template <typename T>
+__device__ __forceinline__ bool block_in_tile(const Tile<T> &t, int py, int px)
+{
+    if (py == 0 && px == 0 && !t.origin_inside) return true;
+    return py >= t.ry0 && px >= t.rx0 && py + kBS <= t.ry0 + t.rh && px + kBS <= t.rx0 + t.rw;
+}
+
+// ---------------------------------------------------------------------------
+// Block matching for reference block (j0, i0) by one warp. Fills list[0..n)
+// with (y, x) in the reference's group order and returns n.
+template <typename T, int KS>
+__device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int i0, int lane,
+                           SortKey<T> *keys, SortKey<T> *heap, BlockPos *list, T *lkeys,
+                           unsigned long long &n_cand, unsigned long long &n_fix)
+{
+    using K = SortKey<T>;
+    const int GS = a.group_size;
+    if (!a.match) {
+        if (lane == 0) {
+            list[0] = BlockPos{j0, i0};
+            lkeys[0] = T(0);
+        }
+        __syncwarp();
+        return 1;
+    }
+    const int st = a.bm_step, R = a.range;
+    const int right = a.width - kBS, bottom = a.height - kBS;
+    const int l = search_boundary(i0, 0, R, st), r = search_boundary(i0, right, R, st);
+    const int tp = search_boundary(j0, 0, R, st), b = search_boundary(j0, bottom, R, st);
+    const int nr = (b - tp) / st + 1, nc = (r - l) / st + 1;
+    const int ngrid = nr * nc;
+
+    // Reference block in registers.
+    T refv[kBS][kBS];
+    {
+        const T *rb = t.refw[0] + (j0 - t.ry0) * t.pitch + (i0 - t.rx0);
+#pragma unroll
+        for (int y = 0; y < kBS; ++y)
+#pragma unroll
+            for (int x = 0; x < kBS; ++x) refv[y][x] = rb[y * t.pitch + x];
+    }
+
+    // Candidates: column strips of KS consecutive grid rows per task, plus one
+    // task for the trailing (0, 0) slot of the reference's search list.
+    const int nstrips = (nr + KS - 1) / KS;
+    const int ntasks = nstrips * nc;
+    constexpr int ROWS = (KS - 1) + kBS;  // KS > 1 only with BMstep == 1
+    for (int task = lane; task <= ntasks; task += kWarp) {
+        const T *base;
+        int bp, nq, rr0 = 0, cc = 0;
+        if (task < ntasks) {
+            const int strip = task / nc;
+            cc = task - strip * nc;
+            rr0 = strip * KS;
+            nq = min(KS, nr - rr0);
+            bp = t.pitch;
+            base = t.refw[0] + (tp + rr0 * st - t.ry0) * t.pitch + (l + cc * st - t.rx0);
+        } else {
+            nq = 1;
+            base = block_ptr(t, t.refw[0], t.ref0[0], 0, 0, bp);
+        }
+        T acc[KS];
+#pragma unroll
+        for (int q = 0; q < KS; ++q) acc[q] = T(0);
+        if (KS == 1) {
+#pragma unroll
+            for (int y = 0; y < kBS; ++y) {
+                T row[kBS];
+#pragma unroll
+                for (int x = 0; x < kBS; ++x) row[x] = base[y * bp + x];
+#pragma unroll
+                for (int x = 0; x < kBS; ++x) {
+                    const T d = sub_rn(refv[y][x], row[x]);
+                    acc[0] = add_rn(acc[0], mul_rn(d, d));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int w = 0; w < ROWS; ++w) {
+                if (w < nq - 1 + kBS) {
+                    T row[kBS];
+#pragma unroll
+                    for (int x = 0; x < kBS; ++x) row[x] = base[w * bp + x];
+#pragma unroll
+                    for (int q = 0; q < KS; ++q) {
+                        const int y = w - q;
+                        if (y >= 0 && y < kBS && q < nq) {
+#pragma unroll
+                            for (int x = 0; x < kBS; ++x) {
+                                const T d = sub_rn(refv[y < 0 ? 0 : (y >= kBS ? kBS - 1 : y)][x], row[x]);
+                                acc[q] = add_rn(acc[q], mul_rn(d, d));
+                            }
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < KS; ++q) {
+            if (q < nq) {
+                int idx;
+                bool self;
+                if (task < ntasks) {
+                    const int rr = rr0 + q;
+                    idx = rr * nc + cc;
+                    self = (tp + rr * st == j0) && (l + cc * st == i0);
+                } else {
+                    idx = ngrid;
+                    self = false;
+                }
+                const T d = acc[q];
+                const bool ok = !self && d <= a.thSSE && d != T(0);
+                keys[idx] = ok ? K::make(key_from_dist(d, a.distMul), static_cast<unsigned>(idx))
+                               : K::invalid();
+            }
+        }
+    }
+    __syncwarp();
+    n_cand += static_cast<unsigned long long>(ngrid);  // grid minus self, plus (0, 0)
+
+    // Ordered selection of the GS - 1 best candidates: every lane keeps the
+    // minimum of its strided slice; the warp minimum is taken and its owner
+    // advances to the next larger key of its slice.
+    const int nkeys = ngrid + 1;
+    K cur = K::invalid();
+    int nvalid = 0;
+    for (int i = lane; i < nkeys; i += kWarp) {
+        const K v = keys[i];
+        nvalid += v.valid() ? 1 : 0;
+        if (v < cur) cur = v;
+    }
+    const int accepted = __reduce_add_sync(0xffffffffu, nvalid);
+    const int take = min(GS - 1, accepted);
+    // list[0] is the reference block itself (key 0, include/Block.h:685)
+    if (lane == 0) {
+        list[0] = BlockPos{j0, i0};
+        lkeys[0] = T(0);
+    }
+    bool tie = false;
+    T prev_key = T(-1);
+    for (int k = 0; k < take; ++k) {
+        const K m = warp_min(cur);
+        const T mk = m.key();
+        tie |= (mk == prev_key);
+        prev_key = mk;
+        if (lane == 0) {
+            const int idx = static_cast<int>(m.idx());
+            int y = 0, x = 0;
+            if (idx < ngrid) {
+                const int rr = idx / nc;
+                y = tp + rr * st;
+                x = l + (idx - rr * nc) * st;
+            }
+            list[k + 1] = BlockPos{y, x};
+            lkeys[k + 1] = mk;
+        }
+        if (cur == m) {
+            K nxt = K::invalid();
+            for (int i = lane; i < nkeys; i += kWarp) {
+                const K v = keys[i];
+                if (m < v && v < nxt) nxt = v;
+            }
+            cur = nxt;
+        }
+    }
+    // More matches than the group holds: the reference keeps GroupSize of them
+    // with std::partial_sort (include/Block.h:690-696), whose placement of
+    // equal keys is libstdc++'s heap order, not list order. Redo such groups
+    // with that exact algorithm when a tie touches the kept set.
+    if (accepted + 1 > GS && GS > 1) {
+        const K m = warp_min(cur);
+        tie |= (m.valid() && m.key() == prev_key);
+        if (tie) {
+            if (lane == 0) {
+                ++n_fix;
+                // heap[] holds the first GS entries of the reference's match list:
+                // the reference block, then matches in list order.
+                heap[0] = K::make(T(0), 0xffffffffu);
+                int h = 1, i = 0;
+                for (; i < nkeys && h < GS; ++i)
+                    if (keys[i].valid()) heap[h++] = keys[i];
+                auto less = [](const K &p, const K &q) { return p.key() < q.key(); };
+                auto adjust = [&](int hole, int len, K value) {
+                    const int top = hole;
+                    int child = hole;
+                    while (child < (len - 1) / 2) {
+                        child = 2 * (child + 1);
+                        if (less(heap[child], heap[child - 1])) child--;
+                        heap[hole] = heap[child];
+                        hole = child;
+                    }
+                    if ((len & 1) == 0 && child == (len - 2) / 2) {
+                        child = 2 * (child + 1);
+                        heap[hole] = heap[child - 1];
+                        hole = child - 1;
+                    }
+                    int parent = (hole - 1) / 2;
+                    while (hole > top && less(heap[parent], value)) {
+                        heap[hole] = heap[parent];
+                        hole = parent;
+                        parent = (hole - 1) / 2;
+                    }
+                    heap[hole] = value;
+                };
+                for (int parent = (GS - 2) / 2;; --parent) {  // __make_heap
+                    adjust(parent, GS, heap[parent]);
+                    if (parent == 0) break;
+                }
+                for (; i < nkeys; ++i) {  // __heap_select
+                    const K v = keys[i];
+                    if (v.valid() && less(v, heap[0])) adjust(0, GS, v);
+                }
+                for (int last = GS; last > 1;) {  // __sort_heap
+                    --last;
+                    const K v = heap[last];
+                    heap[last] = heap[0];
+                    adjust(0, last, v);
+                }
+                for (int k = 0; k < GS; ++k) {
+                    const unsigned idx = heap[k].idx();
+                    int y = 0, x = 0;
+                    if (idx == 0xffffffffu) {
+                        y = j0;
+                        x = i0;
+                    } else if (static_cast<int>(idx) < ngrid) {
+                        const int rr = static_cast<int>(idx) / nc;
+                        y = tp + rr * st;
+                        x = l + (static_cast<int>(idx) - rr * nc) * st;
+                    }
+                    list[k] = BlockPos{y, x};
+                    lkeys[k] = heap[k].key();
+                }
+            }
+        }
+    }
+    __syncwarp();
+    return take + 1;
+}
+
+// ---------------------------------------------------------------------------
+// Forward 2-D transform (rows then columns) of the n blocks of a group, read
+// from a staged window and left in the warp's group buffer G[z][y][x].
+// Lane (z, h) = (lane / 2, lane % 2) owns rows 4h..4h+3, then columns
+// 4h..4h+3, of block z.
+template <typename T>
+__device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win, const T *origin,
+                                                  const BlockPos *list, int n, int lane, T *G,
+                                                  unsigned long long &n_bad)
+{
+    const int z = lane >> 1, h = lane & 1;
+    T *gz = G + z * kGroupStride;
+    if (z < n) {
+        const BlockPos p = list[z];
+        const bool ok = block_in_tile(t, p.y, p.x);
+        n_bad += ok ? 0 : 1;
+        int pitch;
+        const T *bp = block_ptr(t, win, origin, ok ? p.y : t.ry0, ok ? p.x : t.rx0, pitch);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            T row[8];
+            const int y = 4 * h + r;
+#pragma unroll
+            for (int x = 0; x < 8; ++x) row[x] = ok ? bp[y * pitch + x] : T(0);
+            redft10_8(row);
+#pragma unroll
+            for (int x = 0; x < 8; ++x) gz[y * 8 + x] = row[x];
+        }
+    }
+    __syncwarp();
+    if (z < n) {
+        T col[4][8];
+#pragma unroll
+        for (int y = 0; y < 8; ++y)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) col[c][y] = gz[y * 8 + 4 * h + c];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            redft10_8(col[c]);
+#pragma unroll
+            for (int y = 0; y < 8; ++y) gz[y * 8 + 4 * h + c] = col[c][y];
+        }
+    }
+    __syncwarp();
+}
+
+// Columns then rows of the inverse 2-D transform; returns rows 4h..4h+3 of
+// block z in v.
+template <typename T>
+__device__ __forceinline__ void xy_inverse(const T *G, int n, int lane, T (&v)[4][8])
+{
+    const int z = lane >> 1, h = lane & 1;
+    T *gz = const_cast<T *>(G) + z * kGroupStride;
+    if (z < n) {
+        T col[4][8];
+#pragma unroll
+        for (int y = 0; y < 8; ++y)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) col[c][y] = gz[y * 8 + 4 * h + c];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            redft01_8(col[c]);
+#pragma unroll
+            for (int y = 0; y < 8; ++y) gz[y * 8 + 4 * h + c] = col[c][y];
+        }
+    }
+    __syncwarp();
+    if (z < n) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+#pragma unroll
+            for (int x = 0; x < 8; ++x) v[r][x] = gz[(4 * h + r) * 8 + x];
+            redft01_8(v[r]);
+        }
+    }
+}
+
+// Pencils along the group axis: lane owns positions p = lane and lane + 32.
+template <typename T>
+__device__ __forceinline__ void load_pencils(const T *G, int n, int lane, T (&a)[kGSMax],
+                                             T (&b)[kGSMax])
+{
+#pragma unroll
+    for (int z = 0; z < kGSMax; ++z) {
+        a[z] = z < n ? G[z * kGroupStride + lane] : T(0);
+        b[z] = z < n ? G[z * kGroupStride + lane + 32] : T(0);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_pencils(T *G, int n, int lane, const T (&a)[kGSMax],
+                                              const T (&b)[kGSMax])
+{
+#pragma unroll
+    for (int z = 0; z < kGSMax; ++z)
+        if (z < n) {
+            G[z * kGroupStride + lane] = a[z];
+            G[z * kGroupStride + lane + 32] = b[z];
+        }
+}
+
+// Collaborative filtering of one group on plane p, aggregated into the CTA's
+// accumulator windows.
+template <typename T, bool WIENER>
+__device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
+                             int n, int lane, T *G, float scale, unsigned long long &n_bad)
+{
+    T sa[kGSMax], sb[kGSMax];
+    T ra[kGSMax], rb[kGSMax];
+    if (WIENER) {
+        gather_xy_forward(t, t.refw[p], t.ref0[p], list, n, lane, G, n_bad);
+        load_pencils(G, n, lane, ra, rb);
+        zdct_fwd(ra, n);
+        zdct_fwd(rb, n);
+        __syncwarp();
+    }
+    gather_xy_forward(t, t.srcw[p], t.src0[p], list, n, lane, G, n_bad);
+    load_pencils(G, n, lane, sa, sb);
+    zdct_fwd(sa, n);
+    zdct_fwd(sb, n);
+
+    T denW;
+    if (!WIENER) {
+        // Hard threshold: |x| <= thr -> 0, else retained (source/BM3D.cpp:361-371).
+        // thr depends on how many of (x, y, z) are 0 (source/BM3D.cpp:52-67).
+        const int x = lane & 7, ya = lane >> 3;  // p0 = (ya, x), p1 = (ya + 4, x)
+        const int fa = (x == 0) + (ya == 0), fb = (x == 0);
+        const T *thr = a.thr[p][n - 1];
+        int kept = 0;
+#pragma unroll
+        for (int z = 0; z < kGSMax; ++z) {
+            if (z < n) {
+                const T ta = thr[fa + (z == 0)], tb = thr[fb + (z == 0)];
+                const T va = sa[z], vb = sb[z];
+                const T aa = va < T(0) ? -va : va, ab = vb < T(0) ? -vb : vb;
+                if (aa <= ta) sa[z] = T(0); else ++kept;
+                if (ab <= tb) sb[z] = T(0); else ++kept;
+            }
+        }
+        const int retained = __reduce_add_sync(0xffffffffu, kept);
+        denW = retained < 1 ? T(1) : T(1) / static_cast<T>(retained);
+    } else {
+        // Empirical Wiener shrinkage guided by the basic estimate
+        // (source/BM3D.cpp:435-443).
+        const T s2 = a.wss[p][n - 1];
+        T l2 = T(0);
+#pragma unroll
+        for (int z = 0; z < kGSMax; ++z) {
+            if (z < n) {
+                const T ya2 = ra[z] * ra[z], yb2 = rb[z] * rb[z];
+                const T wa = ya2 / (ya2 + s2), wb = yb2 / (yb2 + s2);
+                sa[z] *= wa;
+                sb[z] *= wb;
+                l2 += wa * wa + wb * wb;
+            }
+        }
+        l2 = warp_sum(l2);
+        denW = l2 <= T(0) ? T(1) : T(1) / l2;
+    }
+    const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
+
+    zdct_inv(sa, n);
+    zdct_inv(sb, n);
+    __syncwarp();
+    store_pencils(G, n, lane, sa, sb);
+    __syncwarp();
+    T v[4][8];
+    xy_inverse(G, n, lane, v);
+
+    // Aggregation: BlockGroup::AddTo / CountTo (include/Block.h:1240-1265, 1334-1357).
+    const int z = lane >> 1, h = lane & 1;
+    if (z < n && block_in_tile(t, list[z].y, list[z].x)) {
+        const BlockPos q = list[z];
+        int pitch;
+        auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
+        auto *dd = block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+                const int o = (4 * h + r) * pitch + x;
+                acc_add(dn + o, v[r][x] * numW, scale);
+                acc_add(dd + o, denW, scale);
+            }
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, bool WIENER, int NPL, int KS>
+__global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+
+    // Tile of reference positions.
+    const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
+    const int kx0 = tx * a.tile_x, ky0 = ty * a.tile_y;
+    const int kx1 = min(kx0 + a.tile_x, a.nx), ky1 = min(ky0 + a.tile_y, a.ny);
+    const int right = a.width - kBS, bottom = a.height - kBS;
+
+    // Staged window: union of the search windows of the tile's blocks.
+    Tile<T> t;
+    {
+        int y0 = 1 << 30, y1 = -1, x0 = 1 << 30, x1 = -1;
+        if (a.match) {
+            for (int k = ky0; k < ky1; ++k) {
+                const int j = ref_pos(k, a.step, bottom);
+                y0 = min(y0, search_boundary(j, 0, a.range, a.bm_step));
+                y1 = max(y1, search_boundary(j, bottom, a.range, a.bm_step));
+            }
+            for (int k = kx0; k < kx1; ++k) {
+                const int i = ref_pos(k, a.step, right);
+                x0 = min(x0, search_boundary(i, 0, a.range, a.bm_step));
+                x1 = max(x1, search_boundary(i, right, a.range, a.bm_step));
+            }
+        } else {
+            y0 = ref_pos(ky0, a.step, bottom);
+            y1 = ref_pos(ky1 - 1, a.step, bottom);
+            x0 = ref_pos(kx0, a.step, right);
+            x1 = ref_pos(kx1 - 1, a.step, right);
+        }
+        t.ry0 = y0;
+        t.rx0 = x0;
+        t.rh = y1 + kBS - y0;
+        t.rw = x1 + kBS - x0;
+        t.pitch = a.region_pitch;
+        t.origin_inside = (y0 == 0 && x0 == 0);
+    }
+
+    const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
+                                     a.key_slots, nwarps);
+    {
+        int s = 0;
+        T *origin = reinterpret_cast<T *>(smem + sp.off_origin);
+        for (int p = 0; p < NPL; ++p) {
+            t.srcw[p] = reinterpret_cast<const T *>(smem + sp.region_bytes * s);
+            t.src0[p] = origin + 64 * s;
+            ++s;
+        }
+        for (int p = 0; p < NPL; ++p) {
+            const bool has_ref = WIENER || p == 0;
+            if (!has_ref) {
+                t.refw[p] = t.srcw[p];
+                t.ref0[p] = t.src0[p];
+            } else if (a.ref_alias_src & (1 << p)) {
+                t.refw[p] = t.srcw[p];
+                t.ref0[p] = t.src0[p];
+            } else {
+                t.refw[p] = reinterpret_cast<const T *>(smem + sp.region_bytes * s);
+                t.ref0[p] = origin + 64 * s;
+                ++s;
+            }
+        }
+        using Acc = typename AccOf<T>::type;
+        Acc *origin_acc = reinterpret_cast<Acc *>(origin + 64 * sp.n_stage);
+        for (int p = 0; p < NPL; ++p) {
+            t.accN[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p));
+            t.accD[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p + 1));
+            t.accN0[p] = origin_acc + 64 * (2 * p);
+            t.accD0[p] = origin_acc + 64 * (2 * p + 1);
+        }
+    }
+
+    // Stage windows, zero accumulators.
+    const int npx = t.rh * t.rw;
+    for (int p = 0; p < NPL; ++p) {
+        const bool need_src = !a.bm_only && (a.active & (1 << p));
+        const bool need_ref = (p == 0) || (WIENER && need_src);
+        const bool ref_sep = need_ref && t.refw[p] != t.srcw[p];
+        for (int i = tid; i < npx; i += blockDim.x) {
+            const int y = i / t.rw, x = i - y * t.rw;
+            const long long g = static_cast<long long>(t.ry0 + y) * a.stride + (t.rx0 + x);
+            const int s = y * t.pitch + x;
+            if (need_src || (p == 0 && !ref_sep)) const_cast<T *>(t.srcw[p])[s] = __ldg(a.src[p] + g);
+            if (ref_sep) const_cast<T *>(t.refw[p])[s] = __ldg(a.ref[p] + g);
+            if (need_src) {
+                t.accN[p][s] = 0;
+                t.accD[p][s] = 0;
+            }
+        }
+        if (!t.origin_inside && (need_src || p == 0)) {
+            for (int i = tid; i < 64; i += blockDim.x) {
+                const long long g = static_cast<long long>(i >> 3) * a.stride + (i & 7);
+                const_cast<T *>(t.src0[p])[i] = __ldg(a.src[p] + g);
+                if (ref_sep) const_cast<T *>(t.ref0[p])[i] = __ldg(a.ref[p] + g);
+                t.accN0[p][i] = 0;
+                t.accD0[p][i] = 0;
+            }
+        }
+    }
+    __syncthreads();
+
+    // Per-warp scratch.
+    unsigned char *wbase = smem + sp.off_warps + sp.warp_bytes * warp;
+    const size_t group_bytes = sizeof(T) * kGSMax * kGroupStride;
+    const size_t key_bytes = sizeof(SortKey<T>) * a.key_slots;
+    const size_t scratch = group_bytes > key_bytes ? group_bytes : key_bytes;
+    T *G = reinterpret_cast<T *>(wbase);
+    SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
+    SortKey<T> *heap = reinterpret_cast<SortKey<T> *>(wbase + scratch);
+    BlockPos *list = reinterpret_cast<BlockPos *>(wbase + scratch + sizeof(SortKey<T>) * kGSMax);
+    T *lkeys = reinterpret_cast<T *>(wbase + scratch + sizeof(SortKey<T>) * kGSMax +
+                                     sizeof(BlockPos) * kGSMax);
+
+    unsigned long long n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
+    float scale[NPL];
+#pragma unroll
+    for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
+    const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
+    for (int r = warp; r < nrefs; r += nwarps) {
+        const int ky = ky0 + r / tw, kx = kx0 + r % tw;
+        const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
+        const int n = match_block<T, KS>(a, t, j0, i0, lane, keys, heap, list, lkeys, n_cand, n_fix);
+        n_sum += n;
+        n_sq += static_cast<unsigned long long>(n) * n;
+        if (a.group_count != nullptr && lane < n) {
+            const long long ridx = static_cast<long long>(ky) * a.nx + kx;
+            if (lane == 0) a.group_count[ridx] = n;
+            a.group_pos[(ridx * kGSMax + lane) * 2 + 0] = list[lane].y;
+            a.group_pos[(ridx * kGSMax + lane) * 2 + 1] = list[lane].x;
+            a.group_key[ridx * kGSMax + lane] = lkeys[lane];
+        }
+        if (!a.bm_only) {
+#pragma unroll
+            for (int p = 0; p < NPL; ++p)
+                if (a.active & (1 << p)) filter_group<T, WIENER>(a, t, p, list, n, lane, G, scale[p], n_bad);
+        }
+        __syncwarp();
+    }
+
+    if (a.stats != nullptr && lane == 0) {
+        atomicAdd(a.stats + 0, n_sum);
+        atomicAdd(a.stats + 1, n_sq);
+        atomicAdd(a.stats + 2, n_cand);
+        atomicAdd(a.stats + 3, n_fix);
+    }
+    if (a.stats != nullptr && n_bad) atomicAdd(a.stats + 4, n_bad);
+    if (a.bm_only) return;
+    __syncthreads();
+
+    // Flush the accumulator windows into the plane-wide num / den.
+    for (int p = 0; p < NPL; ++p) {
+        if (!(a.active & (1 << p))) continue;
+        for (int i = tid; i < npx; i += blockDim.x) {
+            const int y = i / t.rw, x = i - y * t.rw;
+            const int s = y * t.pitch + x;
+            const auto d = t.accD[p][s];
+            if (d != 0) {
+                const long long g = static_cast<long long>(t.ry0 + y) * a.width + (t.rx0 + x);
+                acc_flush(a.num[p] + g, t.accN[p][s]);
+                acc_flush(a.den[p] + g, d);
+            }
+        }
+        if (!t.origin_inside) {
+            for (int i = tid; i < 64; i += blockDim.x) {
+                const auto d = t.accD0[p][i];
+                if (d != 0) {
+                    const long long g = static_cast<long long>(i >> 3) * a.width + (i & 7);
+                    acc_flush(a.num[p] + g, t.accN0[p][i]);
+                    acc_flush(a.den[p] + g, d);
+                }
+            }
+        }
+    }
+}
+
+// dst = num / den (source/BM3D.cpp:130-135, include/Image_Type.hpp:319-332).
+// Both sums carry the same fixed-point scale, which cancels.
+__device__ __forceinline__ float ratio(long long n, long long d)
+{
+    return static_cast<float>(static_cast<double>(n) / static_cast<double>(d));
+}
+__device__ __forceinline__ double ratio(double n, double d) { return n / d; }
+
+template <typename T>
+__global__ void normalize_kernel(T *dst, long long dst_stride,
+                                 const typename AccOf<T>::type *num,
+                                 const typename AccOf<T>::type *den, int width, int height)
+{
+    const long long n = static_cast<long long>(width) * height;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long y = i / width, x = i - y * width;
+        dst[y * dst_stride + x] = ratio(num[i], den[i]);
+    }
+}
+
+// Zero one plane's accumulators and fold max |src| into *absmax (which the
+// caller zeroes first). Non-negative floats order like their bit patterns.
+template <typename T>
+__global__ void prep_kernel(typename AccOf<T>::type *num, typename AccOf<T>::type *den,
+                            const T *src, long long stride, int width, int height, float *absmax)
+{
+    const long long n = static_cast<long long>(width) * height;
+    float m = 0.0f;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        num[i] = 0;
+        den[i] = 0;
+        const long long y = i / width, x = i - y * width;
+        const float v = fabsf(static_cast<float>(src[y * stride + x]));
+        m = v > m ? v : m;  // NaN is skipped
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        const float q = __shfl_xor_sync(0xffffffffu, m, o);
+        m = q > m ? q : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m > 0.0f)
+        atomicMax(reinterpret_cast<int *>(absmax), __float_as_int(fminf(m, 3.0e38f)));
+}
+
+}  // namespace bm3d

@@ -1,0 +1,150 @@
+// Register-resident unnormalised DCTs for the BM3D collaborative filter.
+//
+// They compute exactly the transforms the reference gets from FFTW r2r plans
+// (source/BM3D.cpp:13-23): REDFT10 forward and REDFT01 backward,
+//   REDFT10: Y_k = 2 sum_{j=0}^{n-1} x_j cos(pi (2j+1) k / (2n))
+//   REDFT01: Y_k = x_0 + 2 sum_{j=1}^{n-1} x_j cos(pi j (2k+1) / (2n))
+// so REDFT01(REDFT10(x)) = 2n x, which the reference undoes with finalAMP.
+//
+// Lengths 8 and 16 use an even/odd split (the 8-point even half is split once
+// more); other lengths multiply by a small cosine matrix. All functions are
+// __host__ __device__ so the CPU unit tests can check them against scipy.
+#pragma once
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+
+namespace bm3d {
+
+// 2 cos(k pi / 16), k = 1..7
+#define BM3D_C16_1 1.9615705608064609
+#define BM3D_C16_2 1.8477590650225735
+#define BM3D_C16_3 1.6629392246050905
+#define BM3D_C16_4 1.4142135623730951
+#define BM3D_C16_5 1.1111404660392046
+#define BM3D_C16_6 0.7653668647301797
+#define BM3D_C16_7 0.39018064403225666
+
+// REDFT10 of length 8, in place.
+template <typename T>
+__host__ __device__ __forceinline__ void redft10_8(T (&x)[8])
+{
+    const T C1 = T(BM3D_C16_1), C2 = T(BM3D_C16_2), C3 = T(BM3D_C16_3), C4 = T(BM3D_C16_4);
+    const T C5 = T(BM3D_C16_5), C6 = T(BM3D_C16_6), C7 = T(BM3D_C16_7);
+    const T u0 = x[0] + x[7], u1 = x[1] + x[6], u2 = x[2] + x[5], u3 = x[3] + x[4];
+    const T v0 = x[0] - x[7], v1 = x[1] - x[6], v2 = x[2] - x[5], v3 = x[3] - x[4];
+    const T a = u0 + u3, b = u1 + u2, c = u0 - u3, d = u1 - u2;
+    x[0] = T(2) * (a + b);
+    x[4] = C4 * (a - b);
+    x[2] = C2 * c + C6 * d;
+    x[6] = C6 * c - C2 * d;
+    x[1] = C1 * v0 + C3 * v1 + C5 * v2 + C7 * v3;
+    x[3] = C3 * v0 - C7 * v1 - C1 * v2 - C5 * v3;
+    x[5] = C5 * v0 - C1 * v1 + C7 * v2 + C3 * v3;
+    x[7] = C7 * v0 - C5 * v1 + C3 * v2 - C1 * v3;
+}
+
+// REDFT01 of length 8, in place.
+template <typename T>
+__host__ __device__ __forceinline__ void redft01_8(T (&x)[8])
+{
+    const T C1 = T(BM3D_C16_1), C2 = T(BM3D_C16_2), C3 = T(BM3D_C16_3), C4 = T(BM3D_C16_4);
+    const T C5 = T(BM3D_C16_5), C6 = T(BM3D_C16_6), C7 = T(BM3D_C16_7);
+    const T p = x[0] + C4 * x[4], q = x[0] - C4 * x[4];
+    const T s = C2 * x[2] + C6 * x[6], t = C6 * x[2] - C2 * x[6];
+    const T e0 = p + s, e3 = p - s, e1 = q + t, e2 = q - t;
+    const T o0 = C1 * x[1] + C3 * x[3] + C5 * x[5] + C7 * x[7];
+    const T o1 = C3 * x[1] - C7 * x[3] - C1 * x[5] - C5 * x[7];
+    const T o2 = C5 * x[1] - C1 * x[3] + C7 * x[5] + C3 * x[7];
+    const T o3 = C7 * x[1] - C5 * x[3] + C3 * x[5] - C1 * x[7];
+    x[0] = e0 + o0;
+    x[7] = e0 - o0;
+    x[1] = e1 + o1;
+    x[6] = e1 - o1;
+    x[2] = e2 + o2;
+    x[5] = e2 - o2;
+    x[3] = e3 + o3;
+    x[4] = e3 - o3;
+}
+
+// D16[m][j] = 2 cos(pi (2j+1)(2m+1) / 32): odd half of the 16-point transforms.
+#define BM3D_D16 \
+    {{1.9903694533443939, 1.9138806714644176, 1.76384252869671, 1.546020906725474, 1.268786568327291, 0.9427934736519956, 0.5805693545089247, 0.19603428065912154},\
+     {1.9138806714644176, 1.268786568327291, 0.19603428065912154, -0.9427934736519954, -1.7638425286967099, -1.9903694533443939, -1.5460209067254738, -0.5805693545089265},\
+     {1.76384252869671, 0.19603428065912154, -1.546020906725474, -1.9138806714644179, -0.5805693545089249, 1.2687865683272899, 1.9903694533443936, 0.942793473651996},\
+     {1.546020906725474, -0.9427934736519954, -1.9138806714644179, 0.19603428065912018, 1.9903694533443939, 0.5805693545089268, -1.7638425286967112, -1.2687865683272934},\
+     {1.268786568327291, -1.7638425286967099, -0.5805693545089249, 1.9903694533443939, -0.19603428065911993, -1.9138806714644185, 0.9427934736519947, 1.5460209067254753},\
+     {0.9427934736519956, -1.9903694533443939, 1.2687865683272912, 0.5805693545089251, -1.9138806714644174, 1.5460209067254718, 0.1960342806591181, -1.7638425286967123},\
+     {0.5805693545089247, -1.5460209067254742, 1.9903694533443939, -1.7638425286967097, 0.9427934736519947, 0.19603428065912518, -1.2687865683272912, 1.9138806714644188},\
+     {0.19603428065912154, -0.5805693545089249, 0.942793473651996, -1.2687865683272908, 1.5460209067254753, -1.7638425286967123, 1.9138806714644168, -1.990369453344394}}
+
+// REDFT10 of length 16, in place.
+template <typename T>
+__host__ __device__ __forceinline__ void redft10_16(T (&x)[16])
+{
+    constexpr double D[8][8] = BM3D_D16;
+    T u[8], v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        u[j] = x[j] + x[15 - j];
+        v[j] = x[j] - x[15 - j];
+    }
+    redft10_8(u);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        T acc = T(D[m][0]) * v[0];
+#pragma unroll
+        for (int j = 1; j < 8; ++j) acc += T(D[m][j]) * v[j];
+        x[2 * m + 1] = acc;
+        x[2 * m] = u[m];
+    }
+}
+
+// REDFT01 of length 16, in place.
+template <typename T>
+__host__ __device__ __forceinline__ void redft01_16(T (&x)[16])
+{
+    constexpr double D[8][8] = BM3D_D16;
+    T e[8], o[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) e[m] = x[2 * m];
+    redft01_8(e);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        T acc = T(D[0][k]) * x[1];
+#pragma unroll
+        for (int m = 1; m < 8; ++m) acc += T(D[m][k]) * x[2 * m + 1];
+        o[k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        x[k] = e[k] + o[k];
+        x[15 - k] = e[k] - o[k];
+    }
+}
+
+// Length-n transform with an explicit n x n matrix (row k = output k),
+// for n <= N: entries j >= n of x are ignored, outputs k >= n are untouched.
+template <typename T, int N, typename Mat>
+__host__ __device__ __forceinline__ void dct_matrix(T (&x)[N], int n, const Mat *mat)
+{
+    T y[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        T acc = T(0);
+        if (k < n) {
+#pragma unroll
+            for (int j = 0; j < N; ++j)
+                if (j < n) acc += T(mat[k * n + j]) * x[j];
+        }
+        y[k] = acc;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k)
+        if (k < n) x[k] = y[k];
+}
+
+}  // namespace bm3d

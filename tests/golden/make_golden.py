@@ -1,0 +1,82 @@
+"""Generate tests/golden/*.npz from the reference's own BM3D, compiled in
+place by oracle/Makefile (oracle/_ref/libbm3d_ref_f32.so).
+
+Each fixture holds its inputs (so it does not depend on the generator's
+floating-point behaviour on another machine), the parameters, and the
+reference's basic estimate, final estimate and group lists.
+
+    python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from isp_mw_b200 import synth  # noqa: E402
+
+
+def params(profile, sigma_param):
+    s = [sigma_param] * 3 if np.isscalar(sigma_param) else list(sigma_param)
+    return (oracle.reference_stage_default(profile, False, s),
+            oracle.reference_stage_default(profile, True, s))
+
+
+def tie_plane(h, w):
+    """Sawtooth ramps of exact binary fractions: every candidate at the same
+    horizontal offset has exactly the same block distance, so kept groups are
+    full of equal keys and std::partial_sort's tie placement decides them."""
+    y, x = np.mgrid[0:h, 0:w]
+    return (((x % 32) / 64.0) + ((y // 16) % 2) / 8.0).astype(np.float32)
+
+
+CASES = [
+    ("fast_64x64_s25", "fast", 64, 64, 25.0, 11),
+    ("fast_97x70_s10", "fast", 70, 97, 10.0, 12),
+    ("fast_13x21_s50", "fast", 21, 13, 50.0, 13),
+    ("lc_60x44_s15", "lc", 44, 60, 15.0, 14),
+    ("fast_ties_48x40", "fast", 40, 48, None, 15),
+]
+
+
+def main():
+    oracle.build(reference=True)
+    ref = oracle.backend("reference", np.float32)
+    for name, profile, h, w, s255, seed in CASES:
+        if s255 is None:
+            noisy = tie_plane(h, w)
+            clean = noisy.copy()
+            sp = synth.sigma_param(20.0)
+        else:
+            clean, noisy = synth.pair(h, w, s255, seed)
+            sp = synth.sigma_param(s255)
+        b, f = params(profile, sp)
+        basic, final = ref.full(b, f, noisy)
+        gb = ref.groups(False, b, noisy)
+        gf = ref.groups(True, f, basic)
+        np.savez_compressed(
+            os.path.join(HERE, name + ".npz"), noisy=noisy, basic=basic, final=final,
+            basic_counts=gb[0], basic_pos=gb[1], basic_keys=gb[2],
+            final_counts=gf[0], final_pos=gf[1], final_keys=gf[2],
+            params=json.dumps({"basic": b, "final": f, "profile": profile}))
+        print(name, noisy.shape)
+    # three planes sharing luma groups
+    h, w = 40, 52
+    planes = [synth.pair(h, w, s, 30 + i)[1] for i, s in enumerate((15.0, 10.0, 10.0))]
+    sp = [synth.sigma_param(15.0, 0), synth.sigma_param(10.0, 1), synth.sigma_param(10.0, 2)]
+    b, f = params("fast", sp)
+    basic = ref.stage3(False, b, planes)
+    final = ref.stage3(True, f, planes, basic)
+    np.savez_compressed(os.path.join(HERE, "fast3_52x40.npz"), noisy=np.stack(planes),
+                        basic=np.stack(basic), final=np.stack(final),
+                        params=json.dumps({"basic": b, "final": f, "profile": "fast"}))
+    print("fast3_52x40")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,108 @@
+"""The CPU oracle: the C restatement (oracle/bm3d_oracle_impl.h) is pinned
+bit for bit against the reference's own BM3D compiled in place
+(oracle/_ref), live when that build exists and always against the committed
+golden fixtures that build produced (tests/golden/make_golden.py)."""
+import ctypes
+import glob
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+
+
+def load(path):
+    z = np.load(path)
+    return z, json.loads(str(z["params"]))
+
+
+@pytest.mark.parametrize("path", [p for p in GOLDEN if "fast3" not in p],
+                         ids=lambda p: os.path.basename(p))
+def test_port_matches_golden(oracle_mod, path):
+    z, prm = load(path)
+    port = oracle_mod.backend("port", np.float32)
+    basic, final = port.full(prm["basic"], prm["final"], z["noisy"])
+    assert np.array_equal(basic, z["basic"])
+    assert np.array_equal(final, z["final"])
+    for stage, plane in (("basic", z["noisy"]), ("final", z["basic"])):
+        counts, pos, keys = port.groups(stage == "final", prm[stage], plane)
+        assert np.array_equal(counts, z[f"{stage}_counts"])
+        assert np.array_equal(pos, z[f"{stage}_pos"])
+        assert np.array_equal(keys, z[f"{stage}_keys"])
+
+
+def test_port_matches_golden_three_planes(oracle_mod):
+    z, prm = load(os.path.join(ROOT, "tests", "golden", "fast3_52x40.npz"))
+    port = oracle_mod.backend("port", np.float32)
+    basic = port.stage3(False, prm["basic"], list(z["noisy"]))
+    final = port.stage3(True, prm["final"], list(z["noisy"]), basic)
+    assert np.array_equal(np.stack(basic), z["basic"])
+    assert np.array_equal(np.stack(final), z["final"])
+
+
+def test_golden_covers_ties(oracle_mod):
+    """The tie fixture really has equal keys inside kept groups."""
+    z, _ = load(os.path.join(ROOT, "tests", "golden", "fast_ties_48x40.npz"))
+    keys, counts = z["basic_keys"], z["basic_counts"]
+    ties = sum(int(np.any(np.diff(keys[r, 1:counts[r]]) == 0)) for r in range(len(counts)))
+    assert ties > 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("shape,s255,profile", [((57, 83), 25.0, "fast"), ((40, 31), 5.0, "lc"),
+                                               ((24, 24), 50.0, "fast")])
+def test_port_matches_reference_live(oracle_mod, dtype, shape, s255, profile):
+    if not oracle_mod.reference_available():
+        pytest.skip("reference build absent")
+    from isp_mw_b200 import synth
+    _, noisy = synth.pair(shape[0], shape[1], s255, 77)
+    sp = [synth.sigma_param(s255)] * 3
+    b = oracle_mod.reference_stage_default(profile, False, sp)
+    f = oracle_mod.reference_stage_default(profile, True, sp)
+    ref = oracle_mod.backend("reference", dtype)
+    port = oracle_mod.backend("port", dtype)
+    rb, rf = ref.full(b, f, noisy)
+    pb, pf = port.full(b, f, noisy)
+    assert np.array_equal(rb, pb) and np.array_equal(rf, pf)
+
+
+def test_port_param_guard_copies(oracle_mod):
+    """Rejected parameters copy src (source/BM3D.cpp:82-87)."""
+    from isp_mw_b200 import synth
+    _, noisy = synth.pair(32, 32, 10.0, 5)
+    port = oracle_mod.backend("port", np.float32)
+    p = {"block_size": 8, "block_step": 8, "group_size": 16, "bm_range": 9, "bm_step": 1,
+         "thMSE": 1000.0, "lambda": 2.7, "sigma": [0.0, 0.0, 0.0]}
+    assert np.array_equal(port.stage(False, p, noisy), noisy)
+
+
+@pytest.fixture(scope="module")
+def std_sort():
+    out = os.path.join(ROOT, "tests", "_build")
+    os.makedirs(out, exist_ok=True)
+    so = os.path.join(out, "libpsort.so")
+    src = os.path.join(ROOT, "tests", "cpp", "partial_sort_std.cpp")
+    subprocess.run(["g++", "-O2", "-shared", "-fPIC", src, "-o", so], check=True)
+    return ctypes.CDLL(so)
+
+
+def test_partial_sort_emulation_matches_libstdcxx(oracle_mod, std_sort):
+    """The heap-select emulation (used by the oracle and, for tied groups, by
+    the GPU kernel) reproduces std::partial_sort including its placement of
+    equal keys."""
+    rng = np.random.default_rng(3)
+    for trial in range(400):
+        n = int(rng.integers(2, 400))
+        m = int(rng.integers(1, min(n, 33) + 1))
+        keys = rng.integers(0, max(2, n // int(rng.integers(1, 20))), n).astype(np.float32)
+        payload = np.arange(n, dtype=np.int32)
+        ek, ep = oracle_mod.partial_sort_f32(keys, payload, m)
+        sk, sp = keys.copy(), payload.copy()
+        std_sort.std_partial_sort_f32(sk.ctypes.data_as(ctypes.c_void_p),
+                                      sp.ctypes.data_as(ctypes.c_void_p), m, n)
+        assert np.array_equal(ek[:m], sk[:m]) and np.array_equal(ep[:m], sp[:m]), trial
