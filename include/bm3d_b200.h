@@ -38,7 +38,8 @@ enum {
     BM3D_ERR_INVALID = -1,     /* null pointer, width/height < BlockSize, stride < width, ... */
     BM3D_ERR_UNSUPPORTED = -2, /* parameters valid in the reference but not built here */
     BM3D_ERR_CUDA = -3,        /* CUDA runtime error (message via bm3d_last_error) */
-    BM3D_ERR_NOMEM = -4        /* device allocation failed */
+    BM3D_ERR_NOMEM = -4,       /* device allocation failed */
+    BM3D_ERR_TOO_LARGE = -5    /* plane exceeds bm3d_stage_noalloc's static scratch */
 };
 
 enum { BM3D_MEM_HOST = 0, BM3D_MEM_DEVICE = 1 };
@@ -142,6 +143,33 @@ int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener
  * evaluated, out[3] = groups re-ordered to follow std::partial_sort's tie
  * placement. Synchronises the context's last stream. */
 int bm3d_last_stats(bm3d_ctx *ctx, unsigned long long out[4]);
+
+/* One stage on one plane of DEVICE memory, like bm3d_stage with
+ * BM3D_MEM_DEVICE, but without a context and without allocating anything:
+ * no cudaMalloc / cudaFree / allocating library routine is called. It is for
+ * callers that cannot allocate device memory once running -- e.g. a filter
+ * plugin whose host application owns every device allocation, or a real-time
+ * frame loop that may not risk a device-synchronising, possibly failing
+ * cudaMalloc per frame. No counterpart in the reference (whose CPU filter
+ * allocates its accumulators per call, source/BM3D.cpp:89-90).
+ *
+ * Scratch is a file-scope static device array of this library: 32 MiB + 512
+ * bytes (fixed-point numerator and weight sums for up to 2,097,152 pixels,
+ * e.g. 1920x1080, plus a small header). Every GPU that loads the library holds
+ * it until the process exits. Planes larger than that are rejected with
+ * BM3D_ERR_TOO_LARGE (use bm3d_stage instead).
+ *
+ * The first call on a device, with that device current, sets up that device
+ * (looks up the scratch array's device address, uploads the cosine tables);
+ * make that first call before any stream capture. Work is enqueued on
+ * `stream` (NULL = legacy default stream) and the call returns without
+ * waiting. All calls share the one scratch array and every call clears the
+ * parts it needs before use, but two calls whose work overlaps on the GPU
+ * (e.g. on two streams of the same device) race on it: serialise them.
+ * Returns the status codes of bm3d_stage, plus BM3D_ERR_TOO_LARGE. */
+int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, float *dst, const float *src,
+                       const float *ref, int width, int height, size_t stride, float value_range,
+                       void *stream);
 
 /* Per-launch timing of the stage kernels with CUDA events recorded on the
  * launch stream (off by default). Turning it on or off resets the totals.

@@ -28,6 +28,7 @@ BM3D_ERR_INVALID = -1
 BM3D_ERR_UNSUPPORTED = -2
 BM3D_ERR_CUDA = -3
 BM3D_ERR_NOMEM = -4
+BM3D_ERR_TOO_LARGE = -5
 MEM_HOST = 0
 MEM_DEVICE = 1
 
@@ -36,6 +37,7 @@ EXPORTS = [
     "bm3d_ctx_destroy", "bm3d_last_error", "bm3d_stage", "bm3d_stage3", "bm3d_full",
     "bm3d_full3", "bm3d_stage_f64", "bm3d_ref_block_count", "bm3d_debug_groups",
     "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
+    "bm3d_stage_noalloc",
 ]
 
 
@@ -112,6 +114,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                       vp, vp, vp]
     lib.bm3d_last_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_ulonglong)]
     lib.bm3d_set_tiling.argtypes = [vp, ip, ip, ip]
+    lib.bm3d_stage_noalloc.argtypes = [sp, ip, vp, vp, vp, ip, ip, ctypes.c_size_t,
+                                       ctypes.c_float, vp]
     lib.bm3d_set_kernel_timing.argtypes = [vp, ip]
     lib.bm3d_kernel_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong)]

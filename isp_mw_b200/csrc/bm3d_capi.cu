@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -804,5 +805,176 @@ extern "C" int bm3d_last_stats(bm3d_ctx *ctx, unsigned long long out[4])
     CK(ctx, cudaSetDevice(ctx->device));
     CK(ctx, cudaStreamSynchronize(ctx->last_stream));
     CK(ctx, cudaMemcpy(out, ctx->stats, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    return BM3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free stage: bm3d_stage_noalloc.
+//
+// For callers that must not allocate device memory after start-up, e.g. a
+// filter plugin inside a host application that owns every device allocation,
+// or a real-time video path where a cudaMalloc (which can synchronise the
+// device and can fail under memory pressure) is not allowed per frame. The
+// stage kernels' scratch -- the fixed-point numerator and weight planes, the
+// per-plane |src| maximum and the counters -- lives in the file-scope array
+// below instead of context buffers. Every GPU that loads this library holds
+// the array until the process exits.
+
+namespace {
+
+constexpr size_t kNoAllocMaxPixels = size_t(1) << 21;  // 2,097,152 pixels (1920x1080 fits)
+constexpr size_t kNoAllocAccBytes = kNoAllocMaxPixels * sizeof(long long);
+// num (int64 per pixel) | den (int64 per pixel) | absmax (4 floats) | counters (8 x u64)
+constexpr size_t kNoAllocBytes = 2 * kNoAllocAccBytes + 256 + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+struct NoAllocDevice {
+    bool ready = false;
+    unsigned char *scratch = nullptr;  // device address of g_noalloc_scratch
+    int sm_count = 0;
+    size_t smem_optin = 0;
+};
+
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// Cosine tables in fixed-size host arrays (no heap), uploaded per device.
+float g_na_ff[1496], g_na_fi[1496];
+double g_na_df[1496], g_na_di[1496];
+int g_na_off[17];
+
+// Status for a failed step: CUDA errors map to BM3D_ERR_CUDA, everything else
+// to the given code. (The message names the step for readers of this file.)
+int noalloc_error(const char *, cudaError_t e = cudaSuccess, int code = BM3D_ERR_INVALID)
+{
+    return e == cudaSuccess ? code : BM3D_ERR_CUDA;
+}
+
+// Set-up once per device, with that device current: the device address of the
+// scratch array (the host-side symbol is only a stand-in, not a device
+// address), the cosine tables, and the device limits.
+int noalloc_setup(int dev, NoAllocDevice **out)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice &d = g_noalloc_dev[dev];
+    if (d.ready) {
+        *out = &d;
+        return BM3D_OK;
+    }
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) return noalloc_error("cudaGetSymbolAddress(g_noalloc_scratch)", e);
+    if (g_na_off[16] == 0) {
+        const long double pi = 3.141592653589793238462643383279502884L;
+        int o = 0;
+        for (int n = 1; n <= 16; ++n) {
+            g_na_off[n] = o;
+            for (int k = 0; k < n; ++k)
+                for (int j = 0; j < n; ++j) {
+                    const long double cf = 2.0L * cosl(pi * (2 * j + 1) * k / (2.0L * n));
+                    const long double ci =
+                        j == 0 ? 1.0L : 2.0L * cosl(pi * j * (2 * k + 1) / (2.0L * n));
+                    g_na_ff[o + k * n + j] = static_cast<float>(cf);
+                    g_na_fi[o + k * n + j] = static_cast<float>(ci);
+                    g_na_df[o + k * n + j] = static_cast<double>(cf);
+                    g_na_di[o + k * n + j] = static_cast<double>(ci);
+                }
+            o += n * n;
+        }
+    }
+    if ((e = cudaMemcpyToSymbol(c_dct_fwd_f, g_na_ff, sizeof(g_na_ff))) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_dct_inv_f, g_na_fi, sizeof(g_na_fi))) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_dct_fwd_d, g_na_df, sizeof(g_na_df))) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_dct_inv_d, g_na_di, sizeof(g_na_di))) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_dct_off, g_na_off, sizeof(g_na_off))) != cudaSuccess)
+        return noalloc_error("cudaMemcpyToSymbol(cosine tables)", e);
+    int sm = 0, optin = 0;
+    if ((e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
+            cudaSuccess)
+        return noalloc_error("cudaDeviceGetAttribute", e);
+    d.scratch = static_cast<unsigned char *>(ptr);
+    d.sm_count = sm;
+    d.smem_optin = static_cast<size_t>(optin);
+    d.ready = true;
+    *out = &d;
+    return BM3D_OK;
+}
+
+}  // namespace
+
+extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, float *dst,
+                                  const float *src, const float *ref, int width, int height,
+                                  size_t stride, float value_range, void *stream)
+{
+    if (!ref) ref = src;
+    if (!params || !dst || !src) return noalloc_error("bm3d_stage_noalloc: null argument");
+    const Guard g = check_params(params, 1);
+    if (g == Guard::Invalid) return noalloc_error("bm3d_stage_noalloc: invalid parameters");
+    if (g == Guard::Unsupported) return BM3D_ERR_UNSUPPORTED;  // BlockSize 8, GroupSize <= 16 only
+    if (width < params->block_size || height < params->block_size ||
+        stride < static_cast<size_t>(width))
+        return noalloc_error("bm3d_stage_noalloc: width/height below BlockSize or stride < width");
+    if (static_cast<size_t>(width) * static_cast<size_t>(height) > kNoAllocMaxPixels)
+        return BM3D_ERR_TOO_LARGE;  // larger than the 2,097,152-pixel static scratch
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_error("cudaGetDevice", e);
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_error("bm3d_stage_noalloc: device id");
+    NoAllocDevice *d = nullptr;
+    int rc = noalloc_setup(dev, &d);
+    if (rc != BM3D_OK) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (g == Guard::Copy) {
+        if (dst != src &&
+            (e = cudaMemcpy2DAsync(dst, stride * sizeof(float), src, stride * sizeof(float),
+                                   width * sizeof(float), height, cudaMemcpyDeviceToDevice, s)) !=
+                cudaSuccess)
+            return noalloc_error("cudaMemcpy2DAsync", e);
+        return BM3D_COPIED;
+    }
+
+    // The shared scratch: this call's accumulators start from zero below.
+    long long *num = reinterpret_cast<long long *>(d->scratch);
+    long long *den = reinterpret_cast<long long *>(d->scratch + kNoAllocAccBytes);
+    float *absmax = reinterpret_cast<float *>(d->scratch + 2 * kNoAllocAccBytes);
+    unsigned long long *stats =
+        reinterpret_cast<unsigned long long *>(d->scratch + 2 * kNoAllocAccBytes + 256);
+
+    StageArgs<float> a;
+    std::memset(&a, 0, sizeof(a));
+    fill_tables(a, params, wiener != 0, 1, value_range);
+    a.stride = static_cast<long long>(stride);
+    a.src[0] = src;
+    a.ref[0] = ref;
+    a.ref_alias_src = src == ref ? 1 : 0;
+    bm3d_ctx info;  // device limits and default tiling only; owns no device memory
+    info.device = dev;
+    info.sm_count = d->sm_count;
+    info.smem_optin = d->smem_optin;
+    int warps;
+    rc = plan_geometry(&info, a, params, wiener != 0, 1, width, height, warps);
+    if (rc != BM3D_OK) return rc;
+    const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, params->group_size);
+    a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
+    a.absmax = absmax;
+    a.num[0] = num;
+    a.den[0] = den;
+    a.stats = stats;
+
+    const long long npx = static_cast<long long>(width) * height;
+    const int threads = 256;
+    const int blocks = static_cast<int>(
+        std::min<long long>((npx + threads - 1) / threads, static_cast<long long>(d->sm_count) * 8));
+    if ((e = cudaMemsetAsync(absmax, 0, 256 + 256, s)) != cudaSuccess)
+        return noalloc_error("cudaMemsetAsync(scratch header)", e);
+    prep_kernel<float><<<blocks, threads, 0, s>>>(num, den, src, a.stride, width, height, absmax);
+    if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("prep_kernel", e);
+    rc = launch_stage(&info, a, wiener != 0, 1, s, warps);
+    if (rc != BM3D_OK) return rc;
+    normalize_kernel<float><<<blocks, threads, 0, s>>>(dst, a.stride, num, den, width, height);
+    if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("normalize_kernel", e);
     return BM3D_OK;
 }
