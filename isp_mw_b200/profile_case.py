@@ -1,0 +1,46 @@
+"""A fixed workload for profiler captures: warm-up launches, then `--launches`
+launches of one BM3D stage on one seeded synthetic plane (device memory).
+
+    python -m isp_mw_b200.profile_case --stage final --width 1920 --height 1080
+"""
+from __future__ import annotations
+
+import argparse
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--stage", choices=["basic", "final"], default="final")
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--sigma", type=float, default=25.0)
+    ap.add_argument("--warmup", type=int, default=2)
+    ap.add_argument("--launches", type=int, default=2)
+    args = ap.parse_args()
+
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+
+    _, noisy = synth.pair(args.height, args.width, args.sigma, 2024)
+    sp = [synth.sigma_param(args.sigma)] * 3
+    b = isp_mw_b200.stage_params_default("fast", False, sp)
+    f = isp_mw_b200.stage_params_default("fast", True, sp)
+    ctx = isp_mw_b200.Context(0)
+    src = torch.from_numpy(noisy).cuda()
+    basic = torch.empty_like(src)
+    out = torch.empty_like(src)
+    ctx.stage(b, False, basic, src)
+    for _ in range(args.warmup + args.launches):
+        if args.stage == "basic":
+            ctx.stage(b, False, out, src)
+        else:
+            ctx.stage(f, True, out, src, basic)
+    torch.cuda.synchronize()
+    st = ctx.last_stats()
+    print(f"stage={args.stage} {args.width}x{args.height} groups_sum_n={st[0]} candidates={st[2]}")
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()
