@@ -12,6 +12,7 @@ constexpr int kWarp = 32;
 constexpr int kBS = 8;           // block size handled by the register-resident path
 constexpr int kGSMax = 16;       // largest group this path holds in registers
 constexpr int kGroupStride = 72; // floats per block in a warp's group buffer (64 + 8 pad)
+constexpr int kCand = 64;        // candidates a warp sorts after thresholding
 
 // ---------------------------------------------------------------------------
 // Arithmetic that must not be contracted into FMA: the reference accumulates
@@ -82,9 +83,14 @@ template <> struct SortKey<float> {
     __device__ __forceinline__ unsigned idx() const { return static_cast<unsigned>(v); }
     __device__ __forceinline__ bool operator<(const SortKey &o) const { return v < o.v; }
     __device__ __forceinline__ bool operator==(const SortKey &o) const { return v == o.v; }
+    __device__ __forceinline__ unsigned key_bits() const { return static_cast<unsigned>(v >> 32); }
     __device__ __forceinline__ SortKey shfl_xor(int m) const
     {
         return SortKey{__shfl_xor_sync(0xffffffffu, v, m)};
+    }
+    __device__ __forceinline__ SortKey shfl(int src) const
+    {
+        return SortKey{__shfl_sync(0xffffffffu, v, src)};
     }
 };
 
@@ -104,9 +110,14 @@ template <> struct SortKey<double> {
         return k < o.k || (k == o.k && i < o.i);
     }
     __device__ __forceinline__ bool operator==(const SortKey &o) const { return k == o.k && i == o.i; }
+    __device__ __forceinline__ unsigned long long key_bits() const { return k; }
     __device__ __forceinline__ SortKey shfl_xor(int m) const
     {
         return SortKey{__shfl_xor_sync(0xffffffffu, k, m), __shfl_xor_sync(0xffffffffu, i, m)};
+    }
+    __device__ __forceinline__ SortKey shfl(int src) const
+    {
+        return SortKey{__shfl_sync(0xffffffffu, k, src), __shfl_sync(0xffffffffu, i, src)};
     }
 };
 
@@ -118,6 +129,45 @@ template <typename K> __device__ __forceinline__ K warp_min(K v)
         if (o < v) v = o;
     }
     return v;
+}
+
+// Bitonic sort of one key per lane, ascending by lane.
+template <typename K> __device__ __forceinline__ K bitonic32(K v, int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const K p = v.shfl_xor(j);
+            const bool take_min = ((lane & k) == 0) == ((lane & j) == 0);
+            v = (take_min == (p < v)) ? p : v;
+        }
+    }
+    return v;
+}
+
+// Bitonic sort of two keys per lane (element e = lane + 32 s), ascending by e.
+template <typename K> __device__ __forceinline__ void bitonic64(K &v0, K &v1, int lane)
+{
+#pragma unroll
+    for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j == 32) {
+                if (v1 < v0) {
+                    const K t = v0;
+                    v0 = v1;
+                    v1 = t;
+                }
+            } else {
+                const K p0 = v0.shfl_xor(j), p1 = v1.shfl_xor(j);
+                const bool lower = (lane & j) == 0;
+                const bool up0 = (lane & k) == 0, up1 = ((lane + 32) & k) == 0;
+                v0 = ((up0 == lower) == (p0 < v0)) ? p0 : v0;
+                v1 = ((up1 == lower) == (p1 < v1)) ? p1 : v1;
+            }
+        }
+    }
 }
 
 template <typename T> __device__ __forceinline__ T warp_sum(T v)
@@ -231,8 +281,9 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
     const size_t group_bytes = sizeof(T) * kGSMax * kGroupStride;
     const size_t key_bytes = sizeof(SortKey<T>) * key_slots;
     const size_t scratch = group_bytes > key_bytes ? group_bytes : key_bytes;
-    // scratch | heap (kGSMax sort keys) | group list (kGSMax BlockPos) | group keys (kGSMax T)
-    s.warp_bytes = (scratch + sizeof(SortKey<T>) * kGSMax + sizeof(BlockPos) * kGSMax +
+    // scratch | candidate/heap buffer (kCand sort keys) | group list (kGSMax BlockPos) |
+    // group keys (kGSMax T)
+    s.warp_bytes = (scratch + sizeof(SortKey<T>) * kCand + sizeof(BlockPos) * kGSMax +
                     sizeof(T) * kGSMax + 15) / 16 * 16;
     s.total = s.off_warps + s.warp_bytes * nwarps;
     return s;

@@ -212,16 +212,18 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
     __syncwarp();
     n_cand += static_cast<unsigned long long>(ngrid);  // grid minus self, plus (0, 0)
 
-    // Ordered selection of the GS - 1 best candidates: every lane keeps the
-    // minimum of its strided slice; the warp minimum is taken and its owner
-    // advances to the next larger key of its slice.
+    // Ordered selection of the GS - 1 best candidates by (key, list index).
+    // T = the (take)-th smallest of the lanes' minima bounds the take best
+    // from above (those minima are take distinct candidates). All candidates
+    // whose key value is <= T's -- ties with the cut-off included -- are
+    // compacted and bitonic-sorted; typically 16-24 of ~360.
     const int nkeys = ngrid + 1;
-    K cur = K::invalid();
+    K lmin = K::invalid();
     int nvalid = 0;
     for (int i = lane; i < nkeys; i += kWarp) {
         const K v = keys[i];
         nvalid += v.valid() ? 1 : 0;
-        if (v < cur) cur = v;
+        if (v < lmin) lmin = v;
     }
     const int accepted = __reduce_add_sync(0xffffffffu, nvalid);
     const int take = min(GS - 1, accepted);
@@ -230,40 +232,85 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
         list[0] = BlockPos{j0, i0};
         lkeys[0] = T(0);
     }
-    bool tie = false;
-    T prev_key = T(-1);
-    for (int k = 0; k < take; ++k) {
-        const K m = warp_min(cur);
-        const T mk = m.key();
-        tie |= (mk == prev_key);
-        prev_key = mk;
-        if (lane == 0) {
-            const int idx = static_cast<int>(m.idx());
-            int y = 0, x = 0;
-            if (idx < ngrid) {
-                const int rr = idx / nc;
-                y = tp + rr * st;
-                x = l + (idx - rr * nc) * st;
-            }
-            list[k + 1] = BlockPos{y, x};
-            lkeys[k + 1] = mk;
+    auto put = [&](int rank, const K &m) {  // rank-th best candidate -> list[rank + 1]
+        const int idx = static_cast<int>(m.idx());
+        int y = 0, x = 0;
+        if (idx < ngrid) {
+            const int rr = idx / nc;
+            y = tp + rr * st;
+            x = l + (idx - rr * nc) * st;
         }
-        if (cur == m) {
-            K nxt = K::invalid();
+        list[rank + 1] = BlockPos{y, x};
+        lkeys[rank + 1] = m.key();
+    };
+    bool tie = false;
+    if (take > 0) {
+        const K thr = bitonic32(lmin, lane).shfl(take - 1);
+        const auto tb = thr.key_bits();
+        int cnt = 0;
+        for (int i = lane; i < nkeys; i += kWarp) {
+            const K v = keys[i];
+            cnt += (v.valid() && v.key_bits() <= tb) ? 1 : 0;
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < kWarp; o <<= 1) {
+            const int q = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += q;
+        }
+        const int M = __shfl_sync(0xffffffffu, incl, kWarp - 1);
+        if (M <= kCand) {
+            int pos = incl - cnt;
             for (int i = lane; i < nkeys; i += kWarp) {
                 const K v = keys[i];
-                if (m < v && v < nxt) nxt = v;
+                if (v.valid() && v.key_bits() <= tb) heap[pos++] = v;
             }
-            cur = nxt;
+            __syncwarp();
+            K v0 = lane < M ? heap[lane] : K::invalid();
+            K v1 = lane + kWarp < M ? heap[lane + kWarp] : K::invalid();
+            if (M <= kWarp) v0 = bitonic32(v0, lane);
+            else bitonic64(v0, v1, lane);
+            if (lane < take) put(lane, v0);
+            if (lane + kWarp < take) put(lane + kWarp, v1);
+            // equal keys at adjacent ranks r, r + 1 with r < take
+            // (every shuffle runs on all 32 lanes; only the selects below differ)
+            const K n0 = v0.shfl((lane + 1) & (kWarp - 1));
+            const K nx = v1.shfl((lane + 1) & (kWarp - 1));
+            const K f1 = v1.shfl(0);
+            const K next0 = lane < kWarp - 1 ? n0 : f1;
+            const bool t0 = lane < take && lane + 1 < M && next0.key_bits() == v0.key_bits();
+            const bool t1 = lane + kWarp < take && lane + kWarp + 1 < M && lane < kWarp - 1 &&
+                            nx.key_bits() == v1.key_bits();
+            tie = __any_sync(0xffffffffu, t0 || t1);
+        } else {
+            // Rare (many candidates share the cut-off): repeated warp minimum,
+            // whose owner lane advances to the next key of its slice.
+            K cur = lmin;
+            T prev_key = T(-1);
+            for (int k = 0; k < take; ++k) {
+                const K m = warp_min(cur);
+                tie |= (m.key() == prev_key);
+                prev_key = m.key();
+                if (lane == 0) put(k, m);
+                if (cur == m) {
+                    K nxt = K::invalid();
+                    for (int i = lane; i < nkeys; i += kWarp) {
+                        const K v = keys[i];
+                        if (m < v && v < nxt) nxt = v;
+                    }
+                    cur = nxt;
+                }
+            }
+            const K m = warp_min(cur);
+            tie |= (m.valid() && m.key() == prev_key);
         }
     }
+    __syncwarp();
     // More matches than the group holds: the reference keeps GroupSize of them
     // with std::partial_sort (include/Block.h:690-696), whose placement of
     // equal keys is libstdc++'s heap order, not list order. Redo such groups
     // with that exact algorithm when a tie touches the kept set.
     if (accepted + 1 > GS && GS > 1) {
-        const K m = warp_min(cur);
-        tie |= (m.valid() && m.key() == prev_key);
         if (tie) {
             if (lane == 0) {
                 ++n_fix;
@@ -332,10 +379,61 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
 }
 
 // ---------------------------------------------------------------------------
+// A warp's group buffer G holds block z at G + z * kGroupStride, element
+// (y, x) at y * 8 + x plus a 4-value gap after row 3. The gap puts the two
+// lanes that share a block on different shared-memory banks, so the row,
+// column and pencil accesses below are all conflict-free.
+__device__ __forceinline__ int gidx(int y, int x) { return y * 8 + x + ((y >> 2) << 2); }
+
+template <typename T> struct Vec4;
+template <> struct Vec4<float> {
+    static __device__ __forceinline__ void load(const float *p, float &a, float &b, float &c,
+                                                float &d)
+    {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        a = v.x; b = v.y; c = v.z; d = v.w;
+    }
+    static __device__ __forceinline__ void store(float *p, float a, float b, float c, float d)
+    {
+        *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, d);
+    }
+    static __device__ __forceinline__ void load2(const float *p, float &a, float &b)
+    {
+        const float2 v = *reinterpret_cast<const float2 *>(p);
+        a = v.x; b = v.y;
+    }
+    static __device__ __forceinline__ void store2(float *p, float a, float b)
+    {
+        *reinterpret_cast<float2 *>(p) = make_float2(a, b);
+    }
+};
+template <> struct Vec4<double> {
+    static __device__ __forceinline__ void load(const double *p, double &a, double &b, double &c,
+                                                double &d)
+    {
+        const double2 u = reinterpret_cast<const double2 *>(p)[0];
+        const double2 v = reinterpret_cast<const double2 *>(p)[1];
+        a = u.x; b = u.y; c = v.x; d = v.y;
+    }
+    static __device__ __forceinline__ void store(double *p, double a, double b, double c, double d)
+    {
+        reinterpret_cast<double2 *>(p)[0] = make_double2(a, b);
+        reinterpret_cast<double2 *>(p)[1] = make_double2(c, d);
+    }
+    static __device__ __forceinline__ void load2(const double *p, double &a, double &b)
+    {
+        const double2 v = *reinterpret_cast<const double2 *>(p);
+        a = v.x; b = v.y;
+    }
+    static __device__ __forceinline__ void store2(double *p, double a, double b)
+    {
+        *reinterpret_cast<double2 *>(p) = make_double2(a, b);
+    }
+};
+
 // Forward 2-D transform (rows then columns) of the n blocks of a group, read
-// from a staged window and left in the warp's group buffer G[z][y][x].
-// Lane (z, h) = (lane / 2, lane % 2) owns rows 4h..4h+3, then columns
-// 4h..4h+3, of block z.
+// from a staged window and left in the warp's group buffer. Lane (z, h) =
+// (lane / 2, lane % 2) owns rows 4h..4h+3, then columns 4h..4h+3, of block z.
 template <typename T>
 __device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win, const T *origin,
                                                   const BlockPos *list, int n, int lane, T *G,
@@ -356,8 +454,8 @@ __device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win
 #pragma unroll
             for (int x = 0; x < 8; ++x) row[x] = ok ? bp[y * pitch + x] : T(0);
             redft10_8(row);
-#pragma unroll
-            for (int x = 0; x < 8; ++x) gz[y * 8 + x] = row[x];
+            Vec4<T>::store(gz + gidx(y, 0), row[0], row[1], row[2], row[3]);
+            Vec4<T>::store(gz + gidx(y, 4), row[4], row[5], row[6], row[7]);
         }
     }
     __syncwarp();
@@ -365,14 +463,12 @@ __device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win
         T col[4][8];
 #pragma unroll
         for (int y = 0; y < 8; ++y)
+            Vec4<T>::load(gz + gidx(y, 4 * h), col[0][y], col[1][y], col[2][y], col[3][y]);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) col[c][y] = gz[y * 8 + 4 * h + c];
+        for (int c = 0; c < 4; ++c) redft10_8(col[c]);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            redft10_8(col[c]);
-#pragma unroll
-            for (int y = 0; y < 8; ++y) gz[y * 8 + 4 * h + c] = col[c][y];
-        }
+        for (int y = 0; y < 8; ++y)
+            Vec4<T>::store(gz + gidx(y, 4 * h), col[0][y], col[1][y], col[2][y], col[3][y]);
     }
     __syncwarp();
 }
@@ -380,43 +476,47 @@ __device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win
 // Columns then rows of the inverse 2-D transform; returns rows 4h..4h+3 of
 // block z in v.
 template <typename T>
-__device__ __forceinline__ void xy_inverse(const T *G, int n, int lane, T (&v)[4][8])
+__device__ __forceinline__ void xy_inverse(T *G, int n, int lane, T (&v)[4][8])
 {
     const int z = lane >> 1, h = lane & 1;
-    T *gz = const_cast<T *>(G) + z * kGroupStride;
+    T *gz = G + z * kGroupStride;
     if (z < n) {
         T col[4][8];
 #pragma unroll
         for (int y = 0; y < 8; ++y)
+            Vec4<T>::load(gz + gidx(y, 4 * h), col[0][y], col[1][y], col[2][y], col[3][y]);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) col[c][y] = gz[y * 8 + 4 * h + c];
+        for (int c = 0; c < 4; ++c) redft01_8(col[c]);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            redft01_8(col[c]);
-#pragma unroll
-            for (int y = 0; y < 8; ++y) gz[y * 8 + 4 * h + c] = col[c][y];
-        }
+        for (int y = 0; y < 8; ++y)
+            Vec4<T>::store(gz + gidx(y, 4 * h), col[0][y], col[1][y], col[2][y], col[3][y]);
     }
     __syncwarp();
     if (z < n) {
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-#pragma unroll
-            for (int x = 0; x < 8; ++x) v[r][x] = gz[(4 * h + r) * 8 + x];
+            const int y = 4 * h + r;
+            Vec4<T>::load(gz + gidx(y, 0), v[r][0], v[r][1], v[r][2], v[r][3]);
+            Vec4<T>::load(gz + gidx(y, 4), v[r][4], v[r][5], v[r][6], v[r][7]);
             redft01_8(v[r]);
         }
     }
 }
 
-// Pencils along the group axis: lane owns positions p = lane and lane + 32.
+// Pencils along the group axis: lane owns positions p = 2 lane and 2 lane + 1,
+// i.e. (y, x) = (lane / 4, 2 (lane % 4) + {0, 1}).
+__device__ __forceinline__ int pencil_off(int lane) { return gidx(lane >> 2, 2 * (lane & 3)); }
+
 template <typename T>
 __device__ __forceinline__ void load_pencils(const T *G, int n, int lane, T (&a)[kGSMax],
                                              T (&b)[kGSMax])
 {
+    const int o = pencil_off(lane);
 #pragma unroll
     for (int z = 0; z < kGSMax; ++z) {
-        a[z] = z < n ? G[z * kGroupStride + lane] : T(0);
-        b[z] = z < n ? G[z * kGroupStride + lane + 32] : T(0);
+        a[z] = T(0);
+        b[z] = T(0);
+        if (z < n) Vec4<T>::load2(G + z * kGroupStride + o, a[z], b[z]);
     }
 }
 
@@ -424,13 +524,16 @@ template <typename T>
 __device__ __forceinline__ void store_pencils(T *G, int n, int lane, const T (&a)[kGSMax],
                                               const T (&b)[kGSMax])
 {
+    const int o = pencil_off(lane);
 #pragma unroll
     for (int z = 0; z < kGSMax; ++z)
-        if (z < n) {
-            G[z * kGroupStride + lane] = a[z];
-            G[z * kGroupStride + lane + 32] = b[z];
-        }
+        if (z < n) Vec4<T>::store2(G + z * kGroupStride + o, a[z], b[z]);
 }
+
+// Empirical Wiener weight y^2 / (y^2 + sigma^2) (source/BM3D.cpp:440); the
+// FP32 path uses the fast division (within 2 ulp), FP64 the exact one.
+__device__ __forceinline__ float wiener_weight(float y2, float s2) { return __fdividef(y2, y2 + s2); }
+__device__ __forceinline__ double wiener_weight(double y2, double s2) { return y2 / (y2 + s2); }
 
 // Collaborative filtering of one group on plane p, aggregated into the CTA's
 // accumulator windows.
@@ -456,8 +559,8 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
     if (!WIENER) {
         // Hard threshold: |x| <= thr -> 0, else retained (source/BM3D.cpp:361-371).
         // thr depends on how many of (x, y, z) are 0 (source/BM3D.cpp:52-67).
-        const int x = lane & 7, ya = lane >> 3;  // p0 = (ya, x), p1 = (ya + 4, x)
-        const int fa = (x == 0) + (ya == 0), fb = (x == 0);
+        // pencil a = (lane / 4, 2 (lane % 4)), pencil b = (lane / 4, 2 (lane % 4) + 1)
+        const int fa = ((lane & 3) == 0) + (lane < 4), fb = (lane < 4);
         const T *thr = a.thr[p][n - 1];
         int kept = 0;
 #pragma unroll
@@ -481,7 +584,7 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
         for (int z = 0; z < kGSMax; ++z) {
             if (z < n) {
                 const T ya2 = ra[z] * ra[z], yb2 = rb[z] * rb[z];
-                const T wa = ya2 / (ya2 + s2), wb = yb2 / (yb2 + s2);
+                const T wa = wiener_weight(ya2, s2), wb = wiener_weight(yb2, s2);
                 sa[z] *= wa;
                 sb[z] *= wb;
                 l2 += wa * wa + wb * wb;
@@ -633,8 +736,8 @@ __global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
     T *G = reinterpret_cast<T *>(wbase);
     SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
     SortKey<T> *heap = reinterpret_cast<SortKey<T> *>(wbase + scratch);
-    BlockPos *list = reinterpret_cast<BlockPos *>(wbase + scratch + sizeof(SortKey<T>) * kGSMax);
-    T *lkeys = reinterpret_cast<T *>(wbase + scratch + sizeof(SortKey<T>) * kGSMax +
+    BlockPos *list = reinterpret_cast<BlockPos *>(wbase + scratch + sizeof(SortKey<T>) * kCand);
+    T *lkeys = reinterpret_cast<T *>(wbase + scratch + sizeof(SortKey<T>) * kCand +
                                      sizeof(BlockPos) * kGSMax);
 
     unsigned long long n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;

@@ -25,7 +25,7 @@ def test_cpp_dropin_program(bm3d_lib, oracle_mod, tmp_path):
     noisy.tofile(inp)
     sp = synth.sigma_param(s255)
     r = subprocess.run([str(exe), str(inp), str(w), str(h), repr(sp), str(tmp_path / "b.f32"),
-                        str(tmp_path / "f.f32")], capture_output=True, text=True)
+                        str(tmp_path / "f.f32")], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, (r.returncode, r.stderr)
     basic = np.fromfile(tmp_path / "b.f32", np.float32).reshape(h, w)
     final = np.fromfile(tmp_path / "f.f32", np.float32).reshape(h, w)
