@@ -25,6 +25,37 @@ __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
+// dist += sum_x (r[x] - c[x])^2 over one 8-pixel row, x ascending, as the
+// reference accumulates it (include/Block.h:596-605). FP32: the subtractions
+// and squares run as packed f32x2 pairs (each element rounded exactly like
+// the scalar op, no fused multiply-add), the additions stay scalar and in
+// order, so the result is bit-identical to the sequential form.
+__device__ __forceinline__ float ssd_row8(float acc, const float (&r)[8], const float (&c)[8])
+{
+#pragma unroll
+    for (int x = 0; x < 8; x += 2) {
+        unsigned long long a, b, d, q;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(a) : "f"(r[x]), "f"(r[x + 1]));
+        asm("mov.b64 %0, {%1, %2};" : "=l"(b) : "f"(c[x]), "f"(c[x + 1]));
+        asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(q) : "l"(d), "l"(d));
+        float q0, q1;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(q0), "=f"(q1) : "l"(q));
+        acc = __fadd_rn(acc, q0);
+        acc = __fadd_rn(acc, q1);
+    }
+    return acc;
+}
+__device__ __forceinline__ double ssd_row8(double acc, const double (&r)[8], const double (&c)[8])
+{
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+        const double d = __dsub_rn(r[x], c[x]);
+        acc = __dadd_rn(acc, __dmul_rn(d, d));
+    }
+    return acc;
+}
+
 // FLType(dist * distMul) with distMul a double (include/Block.h:610).
 __device__ __forceinline__ float key_from_dist(float d, double mul)
 {

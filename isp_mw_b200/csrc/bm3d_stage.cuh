@@ -162,11 +162,7 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
                 T row[kBS];
 #pragma unroll
                 for (int x = 0; x < kBS; ++x) row[x] = base[y * bp + x];
-#pragma unroll
-                for (int x = 0; x < kBS; ++x) {
-                    const T d = sub_rn(refv[y][x], row[x]);
-                    acc[0] = add_rn(acc[0], mul_rn(d, d));
-                }
+                acc[0] = ssd_row8(acc[0], refv[y], row);
             }
         } else {
 #pragma unroll
@@ -178,13 +174,8 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
 #pragma unroll
                     for (int q = 0; q < KS; ++q) {
                         const int y = w - q;
-                        if (y >= 0 && y < kBS && q < nq) {
-#pragma unroll
-                            for (int x = 0; x < kBS; ++x) {
-                                const T d = sub_rn(refv[y < 0 ? 0 : (y >= kBS ? kBS - 1 : y)][x], row[x]);
-                                acc[q] = add_rn(acc[q], mul_rn(d, d));
-                            }
-                        }
+                        if (y >= 0 && y < kBS && q < nq)
+                            acc[q] = ssd_row8(acc[q], refv[y < 0 ? 0 : (y >= kBS ? kBS - 1 : y)], row);
                     }
                 }
             }
