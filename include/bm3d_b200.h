@@ -36,7 +36,8 @@ enum {
      * copied to dst unchanged, as source/BM3D.cpp:82-87 and 143-151 do. */
     BM3D_COPIED = 1,
     BM3D_ERR_INVALID = -1,     /* null pointer, width/height < BlockSize, stride < width, ... */
-    BM3D_ERR_UNSUPPORTED = -2, /* parameters valid in the reference but not built here */
+    BM3D_ERR_UNSUPPORTED = -2, /* valid in the reference but not built here: BlockSize > 16 or
+                                  GroupSize > 32 */
     BM3D_ERR_CUDA = -3,        /* CUDA runtime error (message via bm3d_last_error) */
     BM3D_ERR_NOMEM = -4,       /* device allocation failed */
     BM3D_ERR_TOO_LARGE = -5    /* plane exceeds bm3d_stage_noalloc's static scratch */
@@ -130,8 +131,8 @@ int bm3d_stage_f64(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, d
 long long bm3d_ref_block_count(const bm3d_stage_params *params, int width, int height);
 
 /* Group of every reference block, in scan order (ref-block index = row-major
- * over the scan): counts[r], pos_yx[(r * 16 + k) * 2 + {0, 1}] = (y, x) and
- * keys[r * 16 + k] of member k. Arrays are host memory sized from
+ * over the scan): counts[r], pos_yx[(r * 32 + k) * 2 + {0, 1}] = (y, x) and
+ * keys[r * 32 + k] of member k. Arrays are host memory sized from
  * bm3d_ref_block_count. Replaces BM3D_Base::BlockMatching
  * (reference source/BM3D.cpp:221-236) for parity checks. */
 int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, const float *ref,

@@ -31,6 +31,7 @@ BM3D_ERR_NOMEM = -4
 BM3D_ERR_TOO_LARGE = -5
 MEM_HOST = 0
 MEM_DEVICE = 1
+GROUP_STRIDE = 32  # members per reference block in bm3d_debug_groups' arrays
 
 EXPORTS = [
     "bm3d_stage_params_default", "bm3d_stage_params_thmse_default", "bm3d_ctx_create",
@@ -245,13 +246,13 @@ class Context:
 
     def debug_groups(self, params: StageParams, wiener: bool, ref: np.ndarray,
                      value_range: float = 1.0):
-        """Group of every reference block: (counts[R], pos[R, 16, 2] (y, x), keys[R, 16])."""
+        """Group of every reference block: (counts[R], pos[R, 32, 2] (y, x), keys[R, 32])."""
         ref = np.ascontiguousarray(ref, dtype=np.float32)
         h, w = ref.shape
         n = self.ref_block_count(params, w, h)
         counts = np.zeros(n, np.int32)
-        pos = np.full((n, 16, 2), -1, np.int32)
-        keys = np.zeros((n, 16), np.float32)
+        pos = np.full((n, GROUP_STRIDE, 2), -1, np.int32)
+        keys = np.zeros((n, GROUP_STRIDE), np.float32)
         rc = self.lib.bm3d_debug_groups(self.h, ctypes.byref(params), int(wiener),
                                         ref.ctypes.data, w, h, w, value_range,
                                         counts.ctypes.data, pos.ctypes.data, keys.ctypes.data)

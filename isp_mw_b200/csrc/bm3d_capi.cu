@@ -1,7 +1,7 @@
 // C ABI of the B200 BM3D path (declared in include/bm3d_b200.h): parameter
 // mirroring, per-call constant setup, context scratch and kernel launches.
 #include "bm3d_b200.h"
-#include "bm3d_stage.cuh"
+#include "bm3d_generic.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -34,6 +34,8 @@ struct bm3d_ctx {
     DevBuf groups[3];                 // debug group dump
     unsigned long long *stats = nullptr;
     float *absmax = nullptr;          // per plane max |src| of the running stage
+    float *gtab_f = nullptr;          // generic path cosine matrices: fwd | inv (float)
+    double *gtab_d = nullptr;         // same in double
     cudaStream_t last_stream = nullptr;
     int tile_x = 8, tile_y = 8, warps = 16;
     // optional per-launch timing of the stage kernels: [0] basic, [1] final
@@ -161,6 +163,38 @@ extern "C" int bm3d_ctx_create(bm3d_ctx **out, int device)
         delete ctx;
         return cuda_fail(nullptr, e, "cudaMalloc(absmax)");
     }
+    // cosine matrices of lengths 1..32 for the generic path
+    {
+        std::vector<float> tf(2 * kDctTableSize);
+        std::vector<double> td(2 * kDctTableSize);
+        const long double pi = 3.141592653589793238462643383279502884L;
+        for (int n = 1; n <= kGSTab; ++n) {
+            const int o = dct_table_offset(n);
+            for (int k = 0; k < n; ++k)
+                for (int j = 0; j < n; ++j) {
+                    const long double cf = 2.0L * cosl(pi * (2 * j + 1) * k / (2.0L * n));
+                    const long double ci = j == 0 ? 1.0L : 2.0L * cosl(pi * j * (2 * k + 1) / (2.0L * n));
+                    tf[o + k * n + j] = static_cast<float>(cf);
+                    tf[kDctTableSize + o + k * n + j] = static_cast<float>(ci);
+                    td[o + k * n + j] = static_cast<double>(cf);
+                    td[kDctTableSize + o + k * n + j] = static_cast<double>(ci);
+                }
+        }
+        e = cudaMalloc(&ctx->gtab_f, tf.size() * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&ctx->gtab_d, td.size() * sizeof(double));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(ctx->gtab_f, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(ctx->gtab_d, td.data(), td.size() * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(ctx->stats);
+            cudaFree(ctx->absmax);
+            cudaFree(ctx->gtab_f);
+            cudaFree(ctx->gtab_d);
+            delete ctx;
+            return cuda_fail(nullptr, e, "generic cosine tables");
+        }
+    }
     *out = ctx;
     return BM3D_OK;
 }
@@ -181,6 +215,8 @@ extern "C" void bm3d_ctx_destroy(bm3d_ctx *ctx)
     for (auto &b : ctx->groups) fr(b);
     if (ctx->stats) cudaFree(ctx->stats);
     if (ctx->absmax) cudaFree(ctx->absmax);
+    if (ctx->gtab_f) cudaFree(ctx->gtab_f);
+    if (ctx->gtab_d) cudaFree(ctx->gtab_d);
     drain_timing(ctx);
     delete ctx;
 }
@@ -288,6 +324,14 @@ static void opp_norms(double norm[3])
 
 enum class Guard { Run, Copy, Invalid, Unsupported };
 
+// The register-resident kernel covers BlockSize 8 with GroupSize <= 16 (the
+// "fast" and "lc" profiles); everything else up to BlockSize 16 and GroupSize
+// 32 runs on the generic kernel.
+static bool fast_path(const bm3d_stage_params *p)
+{
+    return p->block_size == kBS && p->group_size <= kGSMax;
+}
+
 static Guard check_params(const bm3d_stage_params *p, int nplanes)
 {
     if (!p) return Guard::Invalid;
@@ -300,7 +344,7 @@ static Guard check_params(const bm3d_stage_params *p, int nplanes)
         p->bm_range < p->bm_step || thMSE <= 0)
         return Guard::Copy;
     if (p->group_size < 0 || p->block_step <= 0 || p->bm_step <= 0) return Guard::Invalid;
-    if (p->block_size != kBS || p->group_size > kGSMax) return Guard::Unsupported;
+    if (p->block_size > kBSMax || p->group_size > kGSTab) return Guard::Unsupported;
     return Guard::Run;
 }
 
@@ -371,41 +415,96 @@ static int launch_ks(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int warps)
     return launch_one<T, W, NPL, 1>(ctx, a, s, warps);
 }
 
+template <typename T, bool W, int NPL>
+static int launch_generic(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int warps)
+{
+    auto kern = generic_stage_kernel<T, W, NPL>;
+    const SmemPlan sp = plan_smem<T>(NPL, W, a.ref_alias_src, a.region_h, a.region_pitch,
+                                     a.key_slots, warps, true, a.block_size, a.group_size);
+    CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sp.total)));
+    const int grid = a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (ctx->timing && !a.bm_only) {
+        CK(ctx, cudaEventCreate(&e0));
+        CK(ctx, cudaEventCreate(&e1));
+        CK(ctx, cudaEventRecord(e0, s));
+    }
+    kern<<<grid, warps * kWarp, sp.total, s>>>(a);
+    CK(ctx, cudaGetLastError());
+    if (e0) {
+        CK(ctx, cudaEventRecord(e1, s));
+        ctx->pending[W ? 1 : 0].emplace_back(e0, e1);
+    }
+    return BM3D_OK;
+}
+
+static bool fast_args(int block_size, int group_size)
+{
+    return block_size == kBS && group_size <= kGSMax;
+}
+
 template <typename T>
 static int launch_stage(bm3d_ctx *ctx, StageArgs<T> &a, bool wiener, int nplanes, cudaStream_t s,
                         int warps)
 {
+    if (!fast_args(a.block_size, a.group_size)) {
+        if (nplanes == 1)
+            return wiener ? launch_generic<T, true, 1>(ctx, a, s, warps)
+                          : launch_generic<T, false, 1>(ctx, a, s, warps);
+        return wiener ? launch_generic<T, true, 3>(ctx, a, s, warps)
+                      : launch_generic<T, false, 3>(ctx, a, s, warps);
+    }
     if (nplanes == 1)
         return wiener ? launch_ks<T, true, 1>(ctx, a, s, warps) : launch_ks<T, false, 1>(ctx, a, s, warps);
     return wiener ? launch_ks<T, true, 3>(ctx, a, s, warps) : launch_ks<T, false, 3>(ctx, a, s, warps);
 }
+
+template <typename T> struct GenericTables;
+template <> struct GenericTables<float> {
+    static const float *fwd(const bm3d_ctx *c) { return c->gtab_f; }
+    static const float *inv(const bm3d_ctx *c) { return c->gtab_f ? c->gtab_f + kDctTableSize : nullptr; }
+};
+template <> struct GenericTables<double> {
+    static const double *fwd(const bm3d_ctx *c) { return c->gtab_d; }
+    static const double *inv(const bm3d_ctx *c) { return c->gtab_d ? c->gtab_d + kDctTableSize : nullptr; }
+};
 
 // Geometry, tiling and shared-memory fit.
 template <typename T>
 static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params *p, bool wiener,
                          int nplanes, int width, int height, int &warps)
 {
+    const int BS = p->block_size;
+    const bool generic = !fast_args(BS, p->group_size);
     a.width = width;
     a.height = height;
+    a.block_size = BS;
     a.step = p->block_step;
     a.group_size = p->group_size;
     a.bm_step = p->bm_step;
     a.range = p->bm_range / p->bm_step * p->bm_step;
-    a.nx = ref_count(width - kBS, a.step);
-    a.ny = ref_count(height - kBS, a.step);
+    a.nx = ref_count(width - BS, a.step);
+    a.ny = ref_count(height - BS, a.step);
     const int span = 2 * (a.range / a.bm_step) + 1;
     a.key_slots = span * span + 1;
-    int tx = ctx->tile_x, ty = ctx->tile_y;
-    warps = ctx->warps;
+    // the generic kernel launches at most 8 warps (launch bounds 256) on 4x4 tiles
+    int tx = generic ? 4 : ctx->tile_x, ty = generic ? 4 : ctx->tile_y;
+    warps = generic ? 8 : ctx->warps;
     for (;;) {
         const int reach = a.match ? a.range : 0;
-        a.region_w = std::min(width, (tx - 1) * a.step + 2 * reach + kBS);
-        a.region_h = std::min(height, (ty - 1) * a.step + 2 * reach + kBS);
-        a.region_pitch = a.region_w | 1;
+        a.region_w = std::min(width, (tx - 1) * a.step + 2 * reach + BS);
+        a.region_h = std::min(height, (ty - 1) * a.step + 2 * reach + BS);
+        // pitch = 5 (mod 8): block matching's lanes read window rows 4 apart,
+        // and this residue keeps those lane groups on the fewest shared banks
+        a.region_pitch = a.region_w + ((5 - a.region_w % 8) + 8) % 8;
         const SmemPlan sp = plan_smem<T>(nplanes, wiener, a.ref_alias_src, a.region_h,
-                                         a.region_pitch, a.key_slots, warps);
+                                         a.region_pitch, a.key_slots, warps, generic, BS,
+                                         p->group_size);
         if (sp.total <= ctx->smem_optin) break;
-        if (warps > 8) warps /= 2;
+        // The generic kernel's per-warp group buffers dominate its footprint:
+        // give up warps before tile size there.
+        if (warps > 8 || (generic && warps > 1)) warps /= 2;
         else if (ty > 1 && ty >= tx) --ty;
         else if (tx > 1) --tx;
         else if (warps > 1) warps /= 2;
@@ -450,6 +549,8 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
     int warps;
     int rc = plan_geometry(ctx, a, p, wiener, nplanes, width, height, warps);
     if (rc != BM3D_OK) return rc;
+    a.dct_fwd = GenericTables<T>::fwd(ctx);
+    a.dct_inv = GenericTables<T>::inv(ctx);
     using Acc = typename AccOf<T>::type;
     const size_t acc_bytes = sizeof(Acc) * static_cast<size_t>(width) * height;
     const long long npx = static_cast<long long>(width) * height;
@@ -550,7 +651,7 @@ static int stage_any(bm3d_ctx *ctx, const bm3d_stage_params *p, int wiener, int 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (g == Guard::Copy) return passthrough(ctx, nplanes, dst, src, width, height, stride, mem, s);
     if (g == Guard::Unsupported) {
-        ctx->err = "parameters outside this build (BlockSize 8, GroupSize <= 16)";
+        ctx->err = "parameters outside this build (BlockSize <= 16, GroupSize <= 32)";
         return BM3D_ERR_UNSUPPORTED;
     }
     if (mem == BM3D_MEM_DEVICE)
@@ -684,7 +785,7 @@ static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_st
         const Guard g = check_params(basic, nplanes);
         if (g == Guard::Invalid) return BM3D_ERR_INVALID;
         if (g == Guard::Unsupported) {
-            ctx->err = "parameters outside this build (BlockSize 8, GroupSize <= 16)";
+            ctx->err = "parameters outside this build (BlockSize <= 16, GroupSize <= 32)";
             return BM3D_ERR_UNSUPPORTED;
         }
         if (g == Guard::Run) {
@@ -697,7 +798,7 @@ static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_st
         const Guard g = check_params(fin, nplanes);
         if (g == Guard::Invalid) return BM3D_ERR_INVALID;
         if (g == Guard::Unsupported) {
-            ctx->err = "parameters outside this build (BlockSize 8, GroupSize <= 16)";
+            ctx->err = "parameters outside this build (BlockSize <= 16, GroupSize <= 32)";
             return BM3D_ERR_UNSUPPORTED;
         }
         const T *tr[kMaxPlanes];
@@ -755,8 +856,8 @@ extern "C" int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *p, int 
     const size_t plane_bytes = sizeof(float) * static_cast<size_t>(width) * height;
     if ((rc = ensure(ctx, ctx->stage_in[0], plane_bytes)) != BM3D_OK) return rc;
     if ((rc = ensure(ctx, ctx->groups[0], sizeof(int) * nref)) != BM3D_OK) return rc;
-    if ((rc = ensure(ctx, ctx->groups[1], sizeof(int) * nref * kGSMax * 2)) != BM3D_OK) return rc;
-    if ((rc = ensure(ctx, ctx->groups[2], sizeof(float) * nref * kGSMax)) != BM3D_OK) return rc;
+    if ((rc = ensure(ctx, ctx->groups[1], sizeof(int) * nref * kGSTab * 2)) != BM3D_OK) return rc;
+    if ((rc = ensure(ctx, ctx->groups[2], sizeof(float) * nref * kGSTab)) != BM3D_OK) return rc;
     cudaStream_t s = nullptr;
     float *in = static_cast<float *>(ctx->stage_in[0].ptr);
     if ((rc = copy_plane(ctx, in, width, ref, stride, width, height, cudaMemcpyHostToDevice, s)) !=
@@ -770,9 +871,9 @@ extern "C" int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *p, int 
                                  static_cast<float *>(ctx->groups[2].ptr), true);
     if (rc != BM3D_OK) return rc;
     CK(ctx, cudaMemcpyAsync(counts, ctx->groups[0].ptr, sizeof(int) * nref, cudaMemcpyDeviceToHost, s));
-    CK(ctx, cudaMemcpyAsync(pos_yx, ctx->groups[1].ptr, sizeof(int) * nref * kGSMax * 2,
+    CK(ctx, cudaMemcpyAsync(pos_yx, ctx->groups[1].ptr, sizeof(int) * nref * kGSTab * 2,
                             cudaMemcpyDeviceToHost, s));
-    CK(ctx, cudaMemcpyAsync(keys, ctx->groups[2].ptr, sizeof(float) * nref * kGSMax,
+    CK(ctx, cudaMemcpyAsync(keys, ctx->groups[2].ptr, sizeof(float) * nref * kGSTab,
                             cudaMemcpyDeviceToHost, s));
     CK(ctx, cudaStreamSynchronize(s));
     return BM3D_OK;
@@ -913,7 +1014,8 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     if (!params || !dst || !src) return noalloc_error("bm3d_stage_noalloc: null argument");
     const Guard g = check_params(params, 1);
     if (g == Guard::Invalid) return noalloc_error("bm3d_stage_noalloc: invalid parameters");
-    if (g == Guard::Unsupported) return BM3D_ERR_UNSUPPORTED;  // BlockSize 8, GroupSize <= 16 only
+    // the register-resident kernel only: BlockSize 8, GroupSize <= 16
+    if (g == Guard::Unsupported || !fast_path(params)) return BM3D_ERR_UNSUPPORTED;
     if (width < params->block_size || height < params->block_size ||
         stride < static_cast<size_t>(width))
         return noalloc_error("bm3d_stage_noalloc: width/height below BlockSize or stride < width");

@@ -10,7 +10,9 @@ namespace bm3d {
 
 constexpr int kWarp = 32;
 constexpr int kBS = 8;           // block size handled by the register-resident path
-constexpr int kGSMax = 16;       // largest group this path holds in registers
+constexpr int kGSMax = 16;       // largest group the register-resident path holds
+constexpr int kGSTab = 32;       // largest GroupSize handled at all (generic path)
+constexpr int kBSMax = 16;       // largest BlockSize handled at all (generic path)
 constexpr int kGroupStride = 72; // floats per block in a warp's group buffer (64 + 8 pad)
 constexpr int kCand = 64;        // candidates a warp sorts after thresholding
 
@@ -252,8 +254,9 @@ template <typename T> struct StageArgs {
     int active;                 // bit p set: plane p is filtered (sigma[p] > 0)
     int width, height;
     long long stride;           // row pitch of src / ref, in elements
+    int block_size;             // BlockSize (8 on the register-resident path, <= kBSMax)
     int step;                   // BlockStep
-    int group_size;             // GroupSize (1..kGSMax)
+    int group_size;             // GroupSize (1..kGSMax fast path, 1..kGSTab generic)
     int range;                  // BMrange rounded down to a multiple of bm_step
     int bm_step;                // BMstep
     int match;                  // 0 when GroupSize == 1 or thMSE <= 0 (source/BM3D.cpp:226)
@@ -266,34 +269,47 @@ template <typename T> struct StageArgs {
     int ref_alias_src;          // bit p set: ref[p] == src[p], stage once
     T thSSE;                    // FLType(thMSE * MSE2SSE)      (include/Block.h:582-584)
     double distMul;             // 1 / MSE2SSE
-    T thr[kMaxPlanes][kGSMax][4];  // hard thresholds by (#zero indices) (source/BM3D.cpp:35-68)
-    T wss[kMaxPlanes][kGSMax];     // wienerSigmaSqr                     (source/BM3D.cpp:31)
-    double finalAMP[kGSMax];       // 2n * 2BS * 2BS                     (source/BM3D.cpp:26)
+    T thr[kMaxPlanes][kGSTab][4];  // hard thresholds by (#zero indices) (source/BM3D.cpp:35-68)
+    T wss[kMaxPlanes][kGSTab];     // wienerSigmaSqr                     (source/BM3D.cpp:31)
+    double finalAMP[kGSTab];       // 2n * 2BS * 2BS                     (source/BM3D.cpp:26)
+    const T *dct_fwd;           // generic path: cosine matrices of lengths 1..32 (device),
+    const T *dct_inv;           //   length n at offset (n-1) n (2n-1) / 6
     // optional outputs
     int *group_count;           // per reference block: group size        (may be null)
-    int *group_pos;             // per reference block: kGSMax x (y, x)   (may be null)
-    T *group_key;               // per reference block: kGSMax keys       (may be null)
+    int *group_pos;             // per reference block: kGSTab x (y, x)   (may be null)
+    T *group_key;               // per reference block: kGSTab keys       (may be null)
     unsigned long long *stats;  // [0] sum n, [1] sum n^2, [2] candidates, [3] tie fix-ups,
                                 // [4] group members outside the staged window (must be 0)
     int bm_only;                // skip the collaborative filter (group dump)
 };
 
+// Offset of the length-n matrix in the concatenated cosine tables of the
+// generic path: sum_{m < n} m^2.
+__host__ __device__ __forceinline__ int dct_table_offset(int n) { return (n - 1) * n * (2 * n - 1) / 6; }
+constexpr int kDctTableSize = 32 * 33 * 65 / 6;  // lengths 1..32
+
 // Shared-memory carve-up of one CTA, identical on host and device.
+// `generic` selects the layout of the generic-path kernel (group buffers of
+// gs * bs^2 values, a reference-block copy per warp) instead of the
+// register-resident one (kGSMax blocks of 8x8 in kGroupStride rows).
 struct SmemPlan {
     int n_stage;                 // staged windows (src planes + separate ref planes)
     size_t region_bytes;         // one staged window
     size_t acc_bytes;            // one accumulator window
     size_t off_acc;              // 2 * planes accumulator windows
-    size_t off_origin;           // 64-value copies of block (0, 0) per staged window + accumulators
+    size_t off_origin;           // block (0, 0) copies per staged window + accumulators
     size_t off_warps;
     size_t warp_bytes;
+    size_t scratch_bytes;        // group buffer(s) / search list union at the start of a warp's area
+    size_t refblk_bytes;         // generic path: copy of the reference block
     size_t total;
 };
 
 template <typename T>
 __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alias_mask,
                                               int region_h, int region_pitch, int key_slots,
-                                              int nwarps)
+                                              int nwarps, bool generic = false, int bs = kBS,
+                                              int gs = kGSMax)
 {
     SmemPlan s;
     int nref = 0;
@@ -302,20 +318,25 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
         if (!(alias_mask & (1 << p))) ++nref;
     s.n_stage = nplanes + nref;
     using Acc = typename AccOf<T>::type;
+    const int bsq = bs * bs;
     s.region_bytes = (static_cast<size_t>(region_h) * region_pitch * sizeof(T) + 15) / 16 * 16;
     s.acc_bytes = (static_cast<size_t>(region_h) * region_pitch * sizeof(Acc) + 15) / 16 * 16;
     s.off_acc = s.region_bytes * s.n_stage;
     s.off_origin = s.off_acc + s.acc_bytes * 2 * nplanes;
     // block (0, 0) copies: T per staged window, then Acc per accumulator
-    const size_t origin_bytes = sizeof(T) * 64 * s.n_stage + sizeof(Acc) * 64 * 2 * nplanes;
+    const size_t origin_bytes = sizeof(T) * bsq * s.n_stage + sizeof(Acc) * bsq * 2 * nplanes;
     s.off_warps = (s.off_origin + origin_bytes + 15) / 16 * 16;
-    const size_t group_bytes = sizeof(T) * kGSMax * kGroupStride;
+    const size_t group_bytes = generic
+        ? sizeof(T) * static_cast<size_t>(gs) * bsq * (wiener ? 2 : 1)
+        : sizeof(T) * kGSMax * kGroupStride;
     const size_t key_bytes = sizeof(SortKey<T>) * key_slots;
     const size_t scratch = group_bytes > key_bytes ? group_bytes : key_bytes;
-    // scratch | candidate/heap buffer (kCand sort keys) | group list (kGSMax BlockPos) |
-    // group keys (kGSMax T)
-    s.warp_bytes = (scratch + sizeof(SortKey<T>) * kCand + sizeof(BlockPos) * kGSMax +
-                    sizeof(T) * kGSMax + 15) / 16 * 16;
+    s.scratch_bytes = (scratch + 15) / 16 * 16;
+    s.refblk_bytes = generic ? (sizeof(T) * bsq + 15) / 16 * 16 : 0;
+    // scratch | reference block (generic) | candidate/heap buffer (kCand sort keys) |
+    // group list (kGSTab BlockPos) | group keys (kGSTab T)
+    s.warp_bytes = (s.scratch_bytes + s.refblk_bytes + sizeof(SortKey<T>) * kCand +
+                    sizeof(BlockPos) * kGSTab + sizeof(T) * kGSTab + 15) / 16 * 16;
     s.total = s.off_warps + s.warp_bytes * nwarps;
     return s;
 }

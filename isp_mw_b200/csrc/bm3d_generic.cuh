@@ -1,0 +1,235 @@
+// Generic BM3D stage kernel: any BlockSize <= 16, GroupSize <= 32, BMrange,
+// BMstep -- the reference's other profiles ("np", "high", "vn") and custom
+// parameters. One warp per reference block; the group lives in shared memory
+// and the separable 3-D transforms run one line per lane with cosine matrices
+// from global memory. Block matching keeps the reference's exact distance
+// order; selection, aggregation and the staged windows are shared with the
+// register-resident kernel.
+//
+// Reference: as bm3d_stage.cuh (source/BM3D.cpp:80-457, include/Block.h:578-751).
+#pragma once
+
+#include "bm3d_stage.cuh"
+
+namespace bm3d {
+
+// In-place length-n transform of one strided line, by one lane: out[k] =
+// sum_j mat[k n + j] in[j] (row k = output k), n <= kGSTab.
+template <typename T>
+__device__ __forceinline__ void dct_line(T *base, int stride, int n, const T *mat)
+{
+    T in[kGSTab];
+#pragma unroll
+    for (int j = 0; j < kGSTab; ++j) in[j] = j < n ? base[j * stride] : T(0);
+    for (int k = 0; k < n; ++k) {
+        const T *row = mat + k * n;
+        T acc = T(0);
+#pragma unroll
+        for (int j = 0; j < kGSTab; ++j)
+            if (j < n) acc += __ldg(row + j) * in[j];
+        base[k * stride] = acc;
+    }
+}
+
+// Separable 3-D transform of an n x bs x bs group (row-major [z][y][x]) with
+// the concatenated matrices `tab` (forward REDFT10 or backward REDFT01).
+template <typename T>
+__device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab)
+{
+    const int bsq = bs * bs;
+    const T *mb = tab + dct_table_offset(bs);
+    for (int line = lane; line < n * bs; line += kWarp)  // along x
+        dct_line(G + line * bs, 1, bs, mb);
+    __syncwarp();
+    for (int line = lane; line < n * bs; line += kWarp) {  // along y
+        const int z = line / bs, x = line - z * bs;
+        dct_line(G + z * bsq + x, bs, bs, mb);
+    }
+    __syncwarp();
+    const T *mz = tab + dct_table_offset(n);
+    for (int line = lane; line < bsq; line += kWarp)  // along the group
+        dct_line(G + line, bsq, n, mz);
+    __syncwarp();
+}
+
+// Block matching of (j0, i0) for any block size and search step: one lane per
+// candidate, sequential row-major distances against a copy of the reference
+// block (include/Block.h:589-611), then the shared ordered selection.
+template <typename T>
+__device__ int match_generic(const StageArgs<T> &a, const Tile<T> &t, int j0, int i0, int lane,
+                             SortKey<T> *keys, T *refblk, SortKey<T> *heap, BlockPos *list,
+                             T *lkeys, unsigned long long &n_cand, unsigned long long &n_fix)
+{
+    using K = SortKey<T>;
+    if (!a.match) {
+        if (lane == 0) {
+            list[0] = BlockPos{j0, i0};
+            lkeys[0] = T(0);
+        }
+        __syncwarp();
+        return 1;
+    }
+    const int bs = t.bs, bsq = bs * bs;
+    const int st = a.bm_step, R = a.range;
+    const int right = a.width - bs, bottom = a.height - bs;
+    const int l = search_boundary(i0, 0, R, st), r = search_boundary(i0, right, R, st);
+    const int tp = search_boundary(j0, 0, R, st), b = search_boundary(j0, bottom, R, st);
+    const int nr = (b - tp) / st + 1, nc = (r - l) / st + 1;
+    const int ngrid = nr * nc;
+    {
+        const T *rb = t.refw[0] + (j0 - t.ry0) * t.pitch + (i0 - t.rx0);
+        for (int e = lane; e < bsq; e += kWarp) {
+            const int y = e / bs;
+            refblk[e] = rb[y * t.pitch + (e - y * bs)];
+        }
+    }
+    __syncwarp();
+    for (int c = lane; c <= ngrid; c += kWarp) {
+        const T *cand;
+        int cp;
+        bool self = false;
+        if (c < ngrid) {
+            const int rr = c / nc, cc = c - rr * nc;
+            const int cy = tp + rr * st, cx = l + cc * st;
+            self = (cy == j0 && cx == i0);
+            cand = t.refw[0] + (cy - t.ry0) * t.pitch + (cx - t.rx0);
+            cp = t.pitch;
+        } else {
+            cand = block_ptr(t, t.refw[0], t.ref0[0], 0, 0, cp);  // the trailing (0, 0) slot
+        }
+        T d = T(0);
+        for (int y = 0; y < bs; ++y)
+            for (int x = 0; x < bs; ++x) {
+                const T df = sub_rn(refblk[y * bs + x], cand[y * cp + x]);
+                d = add_rn(d, mul_rn(df, df));
+            }
+        const bool ok = !self && d <= a.thSSE && d != T(0);
+        keys[c] = ok ? K::make(key_from_dist(d, a.distMul), static_cast<unsigned>(c)) : K::invalid();
+    }
+    __syncwarp();
+    n_cand += static_cast<unsigned long long>(ngrid);
+    return select_group<T>(a, keys, ngrid, nc, tp, l, st, j0, i0, lane, heap, list, lkeys, n_fix);
+}
+
+// Collaborative filtering of one group on plane p (generic sizes).
+template <typename T, bool WIENER>
+__device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
+                               int n, int lane, T *Gs, T *Gr, float scale,
+                               unsigned long long &n_bad)
+{
+    const int bs = t.bs, bsq = bs * bs, total = n * bsq;
+    for (int e = lane; e < total; e += kWarp) {
+        const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
+        const BlockPos q = list[z];
+        const bool ok = block_in_tile(t, q.y, q.x);
+        if (!ok && rem == 0) ++n_bad;
+        int pitch;
+        const T *bp = block_ptr(t, t.srcw[p], t.src0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
+        Gs[e] = ok ? bp[y * pitch + x] : T(0);
+        if (WIENER) {
+            const T *rp = block_ptr(t, t.refw[p], t.ref0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
+            Gr[e] = ok ? rp[y * pitch + x] : T(0);
+        }
+    }
+    __syncwarp();
+    dct3_generic(Gs, n, bs, lane, a.dct_fwd);
+    T denW;
+    if (!WIENER) {
+        // hard threshold (source/BM3D.cpp:361-371) with thr by #zero indices
+        const T *thr = a.thr[p][n - 1];
+        int kept = 0;
+        for (int e = lane; e < total; e += kWarp) {
+            const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
+            const T v = Gs[e];
+            const T av = v < T(0) ? -v : v;
+            if (av <= thr[(x == 0) + (y == 0) + (z == 0)]) Gs[e] = T(0);
+            else ++kept;
+        }
+        const int retained = __reduce_add_sync(0xffffffffu, kept);
+        denW = retained < 1 ? T(1) : T(1) / static_cast<T>(retained);
+    } else {
+        dct3_generic(Gr, n, bs, lane, a.dct_fwd);
+        const T s2 = a.wss[p][n - 1];
+        T l2 = T(0);
+        for (int e = lane; e < total; e += kWarp) {
+            const T y2 = Gr[e] * Gr[e];
+            const T w = wiener_weight(y2, s2);
+            Gs[e] *= w;
+            l2 += w * w;
+        }
+        l2 = warp_sum(l2);
+        denW = l2 <= T(0) ? T(1) : T(1) / l2;
+    }
+    const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
+    __syncwarp();
+    dct3_generic(Gs, n, bs, lane, a.dct_inv);
+    for (int e = lane; e < total; e += kWarp) {
+        const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
+        const BlockPos q = list[z];
+        if (!block_in_tile(t, q.y, q.x)) continue;
+        int pitch;
+        auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
+        auto *dd = block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch);
+        acc_add(dn + y * pitch + x, Gs[e] * numW, scale);
+        acc_add(dd + y * pitch + x, denW, scale);
+    }
+    __syncwarp();
+}
+
+template <typename T, bool WIENER, int NPL>
+__global__ void __launch_bounds__(256) generic_stage_kernel(const StageArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int bs = a.block_size;
+    const int right = a.width - bs, bottom = a.height - bs;
+
+    Tile<T> t;
+    int kx0, kx1, ky0, ky1;
+    tile_window(a, bs, t, kx0, kx1, ky0, ky1);
+    const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
+                                     a.key_slots, nwarps, true, bs, a.group_size);
+    carve_tile<T, WIENER, NPL>(a, sp, smem, t);
+    stage_tile<T, WIENER, NPL>(a, t);
+
+    unsigned char *wbase = smem + sp.off_warps + sp.warp_bytes * warp;
+    const size_t scratch = sp.scratch_bytes;
+    const int gvals = a.group_size * bs * bs;
+    T *Gs = reinterpret_cast<T *>(wbase);
+    T *Gr = Gs + gvals;
+    SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
+    T *refblk = reinterpret_cast<T *>(wbase + scratch);
+    unsigned char *after = wbase + scratch + sp.refblk_bytes;
+    SortKey<T> *heap = reinterpret_cast<SortKey<T> *>(after);
+    BlockPos *list = reinterpret_cast<BlockPos *>(after + sizeof(SortKey<T>) * kCand);
+    T *lkeys = reinterpret_cast<T *>(after + sizeof(SortKey<T>) * kCand + sizeof(BlockPos) * kGSTab);
+
+    unsigned long long n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
+    float scale[NPL];
+#pragma unroll
+    for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
+    const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
+    for (int r = warp; r < nrefs; r += nwarps) {
+        const int ky = ky0 + r / tw, kx = kx0 + r % tw;
+        const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
+        const int n = match_generic<T>(a, t, j0, i0, lane, keys, refblk, heap, list, lkeys,
+                                       n_cand, n_fix);
+        n_sum += n;
+        n_sq += static_cast<unsigned long long>(n) * n;
+        dump_group(a, ky, kx, n, lane, list, lkeys);
+        if (!a.bm_only) {
+#pragma unroll
+            for (int p = 0; p < NPL; ++p)
+                if (a.active & (1 << p))
+                    filter_generic<T, WIENER>(a, t, p, list, n, lane, Gs, Gr, scale[p], n_bad);
+        }
+        __syncwarp();
+    }
+    flush_stats(a, lane, n_sum, n_sq, n_cand, n_fix, n_bad);
+    if (a.bm_only) return;
+    __syncthreads();
+    flush_tile<T, NPL>(a, t);
+}
+
+}  // namespace bm3d

@@ -52,6 +52,7 @@ template <typename T> struct Tile {
     using Acc = typename AccOf<T>::type;
     int ry0, rx0, rh, rw;      // staged window origin / size in the plane
     int pitch;
+    int bs;                    // block size
     bool origin_inside;        // block (0, 0) lies inside the staged window
     const T *srcw[kMaxPlanes]; // staged src windows
     const T *refw[kMaxPlanes]; // staged ref windows (refw[0] drives matching)
@@ -82,7 +83,7 @@ __device__ __forceinline__ P *block_ptr(const Tile<T> &t, P *win, P *origin, int
                                         int &pitch)
 {
     if (py == 0 && px == 0 && !t.origin_inside) {
-        pitch = kBS;
+        pitch = t.bs;
         return origin;
     }
     pitch = t.pitch;
@@ -96,113 +97,20 @@ template <typename T>
 __device__ __forceinline__ bool block_in_tile(const Tile<T> &t, int py, int px)
 {
     if (py == 0 && px == 0 && !t.origin_inside) return true;
-    return py >= t.ry0 && px >= t.rx0 && py + kBS <= t.ry0 + t.rh && px + kBS <= t.rx0 + t.rw;
+    return py >= t.ry0 && px >= t.rx0 && py + t.bs <= t.ry0 + t.rh && px + t.bs <= t.rx0 + t.rw;
 }
 
-// ---------------------------------------------------------------------------
-// Block matching for reference block (j0, i0) by one warp. Fills list[0..n)
-// with (y, x) in the reference's group order and returns n.
-template <typename T, int KS>
-__device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int i0, int lane,
-                           SortKey<T> *keys, SortKey<T> *heap, BlockPos *list, T *lkeys,
-                           unsigned long long &n_cand, unsigned long long &n_fix)
+// Ordered group of reference block (j0, i0) from its search list: keys[0,
+// ngrid) are the window grid in raster order, keys[ngrid] the trailing (0, 0)
+// slot (invalid keys = rejected or the block itself). Writes list/lkeys in the
+// reference's group order and returns the group size.
+template <typename T>
+__device__ int select_group(const StageArgs<T> &a, const SortKey<T> *keys, int ngrid, int nc,
+                            int tp, int l, int st, int j0, int i0, int lane, SortKey<T> *heap,
+                            BlockPos *list, T *lkeys, unsigned long long &n_fix)
 {
     using K = SortKey<T>;
     const int GS = a.group_size;
-    if (!a.match) {
-        if (lane == 0) {
-            list[0] = BlockPos{j0, i0};
-            lkeys[0] = T(0);
-        }
-        __syncwarp();
-        return 1;
-    }
-    const int st = a.bm_step, R = a.range;
-    const int right = a.width - kBS, bottom = a.height - kBS;
-    const int l = search_boundary(i0, 0, R, st), r = search_boundary(i0, right, R, st);
-    const int tp = search_boundary(j0, 0, R, st), b = search_boundary(j0, bottom, R, st);
-    const int nr = (b - tp) / st + 1, nc = (r - l) / st + 1;
-    const int ngrid = nr * nc;
-
-    // Reference block in registers.
-    T refv[kBS][kBS];
-    {
-        const T *rb = t.refw[0] + (j0 - t.ry0) * t.pitch + (i0 - t.rx0);
-#pragma unroll
-        for (int y = 0; y < kBS; ++y)
-#pragma unroll
-            for (int x = 0; x < kBS; ++x) refv[y][x] = rb[y * t.pitch + x];
-    }
-
-    // Candidates: column strips of KS consecutive grid rows per task, plus one
-    // task for the trailing (0, 0) slot of the reference's search list.
-    const int nstrips = (nr + KS - 1) / KS;
-    const int ntasks = nstrips * nc;
-    constexpr int ROWS = (KS - 1) + kBS;  // KS > 1 only with BMstep == 1
-    for (int task = lane; task <= ntasks; task += kWarp) {
-        const T *base;
-        int bp, nq, rr0 = 0, cc = 0;
-        if (task < ntasks) {
-            const int strip = task / nc;
-            cc = task - strip * nc;
-            rr0 = strip * KS;
-            nq = min(KS, nr - rr0);
-            bp = t.pitch;
-            base = t.refw[0] + (tp + rr0 * st - t.ry0) * t.pitch + (l + cc * st - t.rx0);
-        } else {
-            nq = 1;
-            base = block_ptr(t, t.refw[0], t.ref0[0], 0, 0, bp);
-        }
-        T acc[KS];
-#pragma unroll
-        for (int q = 0; q < KS; ++q) acc[q] = T(0);
-        if (KS == 1) {
-#pragma unroll
-            for (int y = 0; y < kBS; ++y) {
-                T row[kBS];
-#pragma unroll
-                for (int x = 0; x < kBS; ++x) row[x] = base[y * bp + x];
-                acc[0] = ssd_row8(acc[0], refv[y], row);
-            }
-        } else {
-#pragma unroll
-            for (int w = 0; w < ROWS; ++w) {
-                if (w < nq - 1 + kBS) {
-                    T row[kBS];
-#pragma unroll
-                    for (int x = 0; x < kBS; ++x) row[x] = base[w * bp + x];
-#pragma unroll
-                    for (int q = 0; q < KS; ++q) {
-                        const int y = w - q;
-                        if (y >= 0 && y < kBS && q < nq)
-                            acc[q] = ssd_row8(acc[q], refv[y < 0 ? 0 : (y >= kBS ? kBS - 1 : y)], row);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < KS; ++q) {
-            if (q < nq) {
-                int idx;
-                bool self;
-                if (task < ntasks) {
-                    const int rr = rr0 + q;
-                    idx = rr * nc + cc;
-                    self = (tp + rr * st == j0) && (l + cc * st == i0);
-                } else {
-                    idx = ngrid;
-                    self = false;
-                }
-                const T d = acc[q];
-                const bool ok = !self && d <= a.thSSE && d != T(0);
-                keys[idx] = ok ? K::make(key_from_dist(d, a.distMul), static_cast<unsigned>(idx))
-                               : K::invalid();
-            }
-        }
-    }
-    __syncwarp();
-    n_cand += static_cast<unsigned long long>(ngrid);  // grid minus self, plus (0, 0)
-
     // Ordered selection of the GS - 1 best candidates by (key, list index).
     // T = the (take)-th smallest of the lanes' minima bounds the take best
     // from above (those minima are take distinct candidates). All candidates
@@ -367,6 +275,113 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
     }
     __syncwarp();
     return take + 1;
+}
+
+// ---------------------------------------------------------------------------
+// Block matching for reference block (j0, i0) by one warp. Fills list[0..n)
+// with (y, x) in the reference's group order and returns n.
+template <typename T, int KS>
+__device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int i0, int lane,
+                           SortKey<T> *keys, SortKey<T> *heap, BlockPos *list, T *lkeys,
+                           unsigned long long &n_cand, unsigned long long &n_fix)
+{
+    using K = SortKey<T>;
+    const int GS = a.group_size;
+    if (!a.match) {
+        if (lane == 0) {
+            list[0] = BlockPos{j0, i0};
+            lkeys[0] = T(0);
+        }
+        __syncwarp();
+        return 1;
+    }
+    const int st = a.bm_step, R = a.range;
+    const int right = a.width - kBS, bottom = a.height - kBS;
+    const int l = search_boundary(i0, 0, R, st), r = search_boundary(i0, right, R, st);
+    const int tp = search_boundary(j0, 0, R, st), b = search_boundary(j0, bottom, R, st);
+    const int nr = (b - tp) / st + 1, nc = (r - l) / st + 1;
+    const int ngrid = nr * nc;
+
+    // Reference block in registers.
+    T refv[kBS][kBS];
+    {
+        const T *rb = t.refw[0] + (j0 - t.ry0) * t.pitch + (i0 - t.rx0);
+#pragma unroll
+        for (int y = 0; y < kBS; ++y)
+#pragma unroll
+            for (int x = 0; x < kBS; ++x) refv[y][x] = rb[y * t.pitch + x];
+    }
+
+    // Candidates: column strips of KS consecutive grid rows per task, plus one
+    // task for the trailing (0, 0) slot of the reference's search list.
+    const int nstrips = (nr + KS - 1) / KS;
+    const int ntasks = nstrips * nc;
+    constexpr int ROWS = (KS - 1) + kBS;  // KS > 1 only with BMstep == 1
+    for (int task = lane; task <= ntasks; task += kWarp) {
+        const T *base;
+        int bp, nq, rr0 = 0, cc = 0;
+        if (task < ntasks) {
+            const int strip = task / nc;
+            cc = task - strip * nc;
+            rr0 = strip * KS;
+            nq = min(KS, nr - rr0);
+            bp = t.pitch;
+            base = t.refw[0] + (tp + rr0 * st - t.ry0) * t.pitch + (l + cc * st - t.rx0);
+        } else {
+            nq = 1;
+            base = block_ptr(t, t.refw[0], t.ref0[0], 0, 0, bp);
+        }
+        T acc[KS];
+#pragma unroll
+        for (int q = 0; q < KS; ++q) acc[q] = T(0);
+        if (KS == 1) {
+#pragma unroll
+            for (int y = 0; y < kBS; ++y) {
+                T row[kBS];
+#pragma unroll
+                for (int x = 0; x < kBS; ++x) row[x] = base[y * bp + x];
+                acc[0] = ssd_row8(acc[0], refv[y], row);
+            }
+        } else {
+#pragma unroll
+            for (int w = 0; w < ROWS; ++w) {
+                if (w < nq - 1 + kBS) {
+                    T row[kBS];
+#pragma unroll
+                    for (int x = 0; x < kBS; ++x) row[x] = base[w * bp + x];
+#pragma unroll
+                    for (int q = 0; q < KS; ++q) {
+                        const int y = w - q;
+                        if (y >= 0 && y < kBS && q < nq)
+                            acc[q] = ssd_row8(acc[q], refv[y < 0 ? 0 : (y >= kBS ? kBS - 1 : y)], row);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < KS; ++q) {
+            if (q < nq) {
+                int idx;
+                bool self;
+                if (task < ntasks) {
+                    const int rr = rr0 + q;
+                    idx = rr * nc + cc;
+                    self = (tp + rr * st == j0) && (l + cc * st == i0);
+                } else {
+                    idx = ngrid;
+                    self = false;
+                }
+                const T d = acc[q];
+                const bool ok = !self && d <= a.thSSE && d != T(0);
+                keys[idx] = ok ? K::make(key_from_dist(d, a.distMul), static_cast<unsigned>(idx))
+                               : K::invalid();
+            }
+        }
+    }
+    __syncwarp();
+    n_cand += static_cast<unsigned long long>(ngrid);  // grid minus self, plus (0, 0)
+
+    return select_group<T>(a, keys, ngrid, nc, tp, l, st, j0, i0, lane, heap, list, lkeys, n_fix);
 }
 
 // ---------------------------------------------------------------------------
@@ -614,84 +629,91 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
 }
 
 // ---------------------------------------------------------------------------
-template <typename T, bool WIENER, int NPL, int KS>
-__global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
+// CTA-level pieces shared by the register-resident and the generic kernels.
+
+// The CTA's tile of reference positions and its staged window: the union of
+// the search windows of the tile's blocks (or the blocks themselves when no
+// matching happens).
+template <typename T>
+__device__ __forceinline__ void tile_window(const StageArgs<T> &a, int bs, Tile<T> &t, int &kx0,
+                                            int &kx1, int &ky0, int &ky1)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int tid = threadIdx.x;
-    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-
-    // Tile of reference positions.
     const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
-    const int kx0 = tx * a.tile_x, ky0 = ty * a.tile_y;
-    const int kx1 = min(kx0 + a.tile_x, a.nx), ky1 = min(ky0 + a.tile_y, a.ny);
-    const int right = a.width - kBS, bottom = a.height - kBS;
-
-    // Staged window: union of the search windows of the tile's blocks.
-    Tile<T> t;
-    {
-        int y0 = 1 << 30, y1 = -1, x0 = 1 << 30, x1 = -1;
-        if (a.match) {
-            for (int k = ky0; k < ky1; ++k) {
-                const int j = ref_pos(k, a.step, bottom);
-                y0 = min(y0, search_boundary(j, 0, a.range, a.bm_step));
-                y1 = max(y1, search_boundary(j, bottom, a.range, a.bm_step));
-            }
-            for (int k = kx0; k < kx1; ++k) {
-                const int i = ref_pos(k, a.step, right);
-                x0 = min(x0, search_boundary(i, 0, a.range, a.bm_step));
-                x1 = max(x1, search_boundary(i, right, a.range, a.bm_step));
-            }
-        } else {
-            y0 = ref_pos(ky0, a.step, bottom);
-            y1 = ref_pos(ky1 - 1, a.step, bottom);
-            x0 = ref_pos(kx0, a.step, right);
-            x1 = ref_pos(kx1 - 1, a.step, right);
+    kx0 = tx * a.tile_x;
+    ky0 = ty * a.tile_y;
+    kx1 = min(kx0 + a.tile_x, a.nx);
+    ky1 = min(ky0 + a.tile_y, a.ny);
+    const int right = a.width - bs, bottom = a.height - bs;
+    int y0 = 1 << 30, y1 = -1, x0 = 1 << 30, x1 = -1;
+    if (a.match) {
+        for (int k = ky0; k < ky1; ++k) {
+            const int j = ref_pos(k, a.step, bottom);
+            y0 = min(y0, search_boundary(j, 0, a.range, a.bm_step));
+            y1 = max(y1, search_boundary(j, bottom, a.range, a.bm_step));
         }
-        t.ry0 = y0;
-        t.rx0 = x0;
-        t.rh = y1 + kBS - y0;
-        t.rw = x1 + kBS - x0;
-        t.pitch = a.region_pitch;
-        t.origin_inside = (y0 == 0 && x0 == 0);
+        for (int k = kx0; k < kx1; ++k) {
+            const int i = ref_pos(k, a.step, right);
+            x0 = min(x0, search_boundary(i, 0, a.range, a.bm_step));
+            x1 = max(x1, search_boundary(i, right, a.range, a.bm_step));
+        }
+    } else {
+        y0 = ref_pos(ky0, a.step, bottom);
+        y1 = ref_pos(ky1 - 1, a.step, bottom);
+        x0 = ref_pos(kx0, a.step, right);
+        x1 = ref_pos(kx1 - 1, a.step, right);
     }
+    t.ry0 = y0;
+    t.rx0 = x0;
+    t.rh = y1 + bs - y0;
+    t.rw = x1 + bs - x0;
+    t.pitch = a.region_pitch;
+    t.bs = bs;
+    t.origin_inside = (y0 == 0 && x0 == 0);
+}
 
-    const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
-                                     a.key_slots, nwarps);
-    {
-        int s = 0;
-        T *origin = reinterpret_cast<T *>(smem + sp.off_origin);
-        for (int p = 0; p < NPL; ++p) {
-            t.srcw[p] = reinterpret_cast<const T *>(smem + sp.region_bytes * s);
-            t.src0[p] = origin + 64 * s;
+// Carve the CTA's shared memory into staged windows, accumulators and the
+// (0, 0) copies, following plan_smem.
+template <typename T, bool WIENER, int NPL>
+__device__ __forceinline__ void carve_tile(const StageArgs<T> &a, const SmemPlan &sp,
+                                           unsigned char *smem, Tile<T> &t)
+{
+    using Acc = typename AccOf<T>::type;
+    const int bsq = t.bs * t.bs;
+    int s = 0;
+    T *origin = reinterpret_cast<T *>(smem + sp.off_origin);
+    for (int p = 0; p < NPL; ++p) {
+        t.srcw[p] = reinterpret_cast<const T *>(smem + sp.region_bytes * s);
+        t.src0[p] = origin + bsq * s;
+        ++s;
+    }
+    for (int p = 0; p < NPL; ++p) {
+        const bool has_ref = WIENER || p == 0;
+        if (!has_ref || (a.ref_alias_src & (1 << p))) {
+            t.refw[p] = t.srcw[p];
+            t.ref0[p] = t.src0[p];
+        } else {
+            t.refw[p] = reinterpret_cast<const T *>(smem + sp.region_bytes * s);
+            t.ref0[p] = origin + bsq * s;
             ++s;
         }
-        for (int p = 0; p < NPL; ++p) {
-            const bool has_ref = WIENER || p == 0;
-            if (!has_ref) {
-                t.refw[p] = t.srcw[p];
-                t.ref0[p] = t.src0[p];
-            } else if (a.ref_alias_src & (1 << p)) {
-                t.refw[p] = t.srcw[p];
-                t.ref0[p] = t.src0[p];
-            } else {
-                t.refw[p] = reinterpret_cast<const T *>(smem + sp.region_bytes * s);
-                t.ref0[p] = origin + 64 * s;
-                ++s;
-            }
-        }
-        using Acc = typename AccOf<T>::type;
-        Acc *origin_acc = reinterpret_cast<Acc *>(origin + 64 * sp.n_stage);
-        for (int p = 0; p < NPL; ++p) {
-            t.accN[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p));
-            t.accD[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p + 1));
-            t.accN0[p] = origin_acc + 64 * (2 * p);
-            t.accD0[p] = origin_acc + 64 * (2 * p + 1);
-        }
     }
+    Acc *origin_acc = reinterpret_cast<Acc *>(origin + bsq * sp.n_stage);
+    for (int p = 0; p < NPL; ++p) {
+        t.accN[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p));
+        t.accD[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p + 1));
+        t.accN0[p] = origin_acc + bsq * (2 * p);
+        t.accD0[p] = origin_acc + bsq * (2 * p + 1);
+    }
+}
 
-    // Stage windows, zero accumulators.
+// Load the staged windows (and block (0, 0) when outside) and zero the
+// accumulators. Ends with __syncthreads().
+template <typename T, bool WIENER, int NPL>
+__device__ __forceinline__ void stage_tile(const StageArgs<T> &a, const Tile<T> &t)
+{
+    const int tid = threadIdx.x;
     const int npx = t.rh * t.rw;
+    const int bs = t.bs, bsq = bs * bs;
     for (int p = 0; p < NPL; ++p) {
         const bool need_src = !a.bm_only && (a.active & (1 << p));
         const bool need_ref = (p == 0) || (WIENER && need_src);
@@ -708,8 +730,9 @@ __global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
             }
         }
         if (!t.origin_inside && (need_src || p == 0)) {
-            for (int i = tid; i < 64; i += blockDim.x) {
-                const long long g = static_cast<long long>(i >> 3) * a.stride + (i & 7);
+            for (int i = tid; i < bsq; i += blockDim.x) {
+                const int y = i / bs, x = i - y * bs;
+                const long long g = static_cast<long long>(y) * a.stride + x;
                 const_cast<T *>(t.src0[p])[i] = __ldg(a.src[p] + g);
                 if (ref_sep) const_cast<T *>(t.ref0[p])[i] = __ldg(a.ref[p] + g);
                 t.accN0[p][i] = 0;
@@ -718,56 +741,15 @@ __global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
         }
     }
     __syncthreads();
+}
 
-    // Per-warp scratch.
-    unsigned char *wbase = smem + sp.off_warps + sp.warp_bytes * warp;
-    const size_t group_bytes = sizeof(T) * kGSMax * kGroupStride;
-    const size_t key_bytes = sizeof(SortKey<T>) * a.key_slots;
-    const size_t scratch = group_bytes > key_bytes ? group_bytes : key_bytes;
-    T *G = reinterpret_cast<T *>(wbase);
-    SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
-    SortKey<T> *heap = reinterpret_cast<SortKey<T> *>(wbase + scratch);
-    BlockPos *list = reinterpret_cast<BlockPos *>(wbase + scratch + sizeof(SortKey<T>) * kCand);
-    T *lkeys = reinterpret_cast<T *>(wbase + scratch + sizeof(SortKey<T>) * kCand +
-                                     sizeof(BlockPos) * kGSMax);
-
-    unsigned long long n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
-    float scale[NPL];
-#pragma unroll
-    for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
-    const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
-    for (int r = warp; r < nrefs; r += nwarps) {
-        const int ky = ky0 + r / tw, kx = kx0 + r % tw;
-        const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
-        const int n = match_block<T, KS>(a, t, j0, i0, lane, keys, heap, list, lkeys, n_cand, n_fix);
-        n_sum += n;
-        n_sq += static_cast<unsigned long long>(n) * n;
-        if (a.group_count != nullptr && lane < n) {
-            const long long ridx = static_cast<long long>(ky) * a.nx + kx;
-            if (lane == 0) a.group_count[ridx] = n;
-            a.group_pos[(ridx * kGSMax + lane) * 2 + 0] = list[lane].y;
-            a.group_pos[(ridx * kGSMax + lane) * 2 + 1] = list[lane].x;
-            a.group_key[ridx * kGSMax + lane] = lkeys[lane];
-        }
-        if (!a.bm_only) {
-#pragma unroll
-            for (int p = 0; p < NPL; ++p)
-                if (a.active & (1 << p)) filter_group<T, WIENER>(a, t, p, list, n, lane, G, scale[p], n_bad);
-        }
-        __syncwarp();
-    }
-
-    if (a.stats != nullptr && lane == 0) {
-        atomicAdd(a.stats + 0, n_sum);
-        atomicAdd(a.stats + 1, n_sq);
-        atomicAdd(a.stats + 2, n_cand);
-        atomicAdd(a.stats + 3, n_fix);
-    }
-    if (a.stats != nullptr && n_bad) atomicAdd(a.stats + 4, n_bad);
-    if (a.bm_only) return;
-    __syncthreads();
-
-    // Flush the accumulator windows into the plane-wide num / den.
+// Flush the accumulator windows into the plane-wide num / den sums.
+template <typename T, int NPL>
+__device__ __forceinline__ void flush_tile(const StageArgs<T> &a, const Tile<T> &t)
+{
+    const int tid = threadIdx.x;
+    const int npx = t.rh * t.rw;
+    const int bs = t.bs, bsq = bs * bs;
     for (int p = 0; p < NPL; ++p) {
         if (!(a.active & (1 << p))) continue;
         for (int i = tid; i < npx; i += blockDim.x) {
@@ -781,16 +763,99 @@ __global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
             }
         }
         if (!t.origin_inside) {
-            for (int i = tid; i < 64; i += blockDim.x) {
+            for (int i = tid; i < bsq; i += blockDim.x) {
                 const auto d = t.accD0[p][i];
                 if (d != 0) {
-                    const long long g = static_cast<long long>(i >> 3) * a.width + (i & 7);
+                    const int y = i / bs, x = i - y * bs;
+                    const long long g = static_cast<long long>(y) * a.width + x;
                     acc_flush(a.num[p] + g, t.accN0[p][i]);
                     acc_flush(a.den[p] + g, d);
                 }
             }
         }
     }
+}
+
+template <typename T>
+__device__ __forceinline__ void dump_group(const StageArgs<T> &a, int ky, int kx, int n, int lane,
+                                           const BlockPos *list, const T *lkeys)
+{
+    if (a.group_count == nullptr) return;
+    const long long ridx = static_cast<long long>(ky) * a.nx + kx;
+    if (lane == 0) a.group_count[ridx] = n;
+    for (int k = lane; k < n; k += kWarp) {
+        a.group_pos[(ridx * kGSTab + k) * 2 + 0] = list[k].y;
+        a.group_pos[(ridx * kGSTab + k) * 2 + 1] = list[k].x;
+        a.group_key[ridx * kGSTab + k] = lkeys[k];
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void flush_stats(const StageArgs<T> &a, int lane, unsigned long long n_sum,
+                                            unsigned long long n_sq, unsigned long long n_cand,
+                                            unsigned long long n_fix, unsigned long long n_bad)
+{
+    if (a.stats != nullptr && lane == 0) {
+        atomicAdd(a.stats + 0, n_sum);
+        atomicAdd(a.stats + 1, n_sq);
+        atomicAdd(a.stats + 2, n_cand);
+        atomicAdd(a.stats + 3, n_fix);
+    }
+    if (a.stats != nullptr && n_bad) atomicAdd(a.stats + 4, n_bad);
+}
+
+// ---------------------------------------------------------------------------
+// Register-resident stage kernel: BlockSize 8, GroupSize <= 16.
+template <typename T, bool WIENER, int NPL, int KS>
+__global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int right = a.width - kBS, bottom = a.height - kBS;
+
+    Tile<T> t;
+    int kx0, kx1, ky0, ky1;
+    tile_window(a, kBS, t, kx0, kx1, ky0, ky1);
+    const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
+                                     a.key_slots, nwarps);
+    carve_tile<T, WIENER, NPL>(a, sp, smem, t);
+    stage_tile<T, WIENER, NPL>(a, t);
+
+    // Per-warp scratch.
+    unsigned char *wbase = smem + sp.off_warps + sp.warp_bytes * warp;
+    const size_t scratch = sp.scratch_bytes;
+    T *G = reinterpret_cast<T *>(wbase);
+    SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
+    SortKey<T> *heap = reinterpret_cast<SortKey<T> *>(wbase + scratch);
+    BlockPos *list = reinterpret_cast<BlockPos *>(wbase + scratch + sizeof(SortKey<T>) * kCand);
+    T *lkeys = reinterpret_cast<T *>(wbase + scratch + sizeof(SortKey<T>) * kCand +
+                                     sizeof(BlockPos) * kGSTab);
+
+    unsigned long long n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
+    float scale[NPL];
+#pragma unroll
+    for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
+    const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
+    for (int r = warp; r < nrefs; r += nwarps) {
+        const int ky = ky0 + r / tw, kx = kx0 + r % tw;
+        const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
+        const int n = match_block<T, KS>(a, t, j0, i0, lane, keys, heap, list, lkeys, n_cand, n_fix);
+        n_sum += n;
+        n_sq += static_cast<unsigned long long>(n) * n;
+        dump_group(a, ky, kx, n, lane, list, lkeys);
+        if (!a.bm_only) {
+#pragma unroll
+            for (int p = 0; p < NPL; ++p)
+                if (a.active & (1 << p))
+                    filter_group<T, WIENER>(a, t, p, list, n, lane, G, scale[p], n_bad);
+        }
+        __syncwarp();
+    }
+    flush_stats(a, lane, n_sum, n_sq, n_cand, n_fix, n_bad);
+    if (a.bm_only) return;
+    __syncthreads();
+    flush_tile<T, NPL>(a, t);
 }
 
 // dst = num / den (source/BM3D.cpp:130-135, include/Image_Type.hpp:319-332).

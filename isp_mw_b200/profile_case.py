@@ -16,6 +16,8 @@ def main():
     ap.add_argument("--sigma", type=float, default=25.0)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--launches", type=int, default=2)
+    ap.add_argument("--groups-only", action="store_true",
+                    help="run the stage's block matching alone (bm3d_debug_groups)")
     args = ap.parse_args()
 
     import torch
@@ -31,8 +33,11 @@ def main():
     basic = torch.empty_like(src)
     out = torch.empty_like(src)
     ctx.stage(b, False, basic, src)
+    ref_plane = noisy if args.stage == "basic" else basic.cpu().numpy()
     for _ in range(args.warmup + args.launches):
-        if args.stage == "basic":
+        if args.groups_only:
+            ctx.debug_groups(b if args.stage == "basic" else f, args.stage == "final", ref_plane)
+        elif args.stage == "basic":
             ctx.stage(b, False, out, src)
         else:
             ctx.stage(f, True, out, src, basic)

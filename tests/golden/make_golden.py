@@ -23,8 +23,9 @@ from isp_mw_b200 import synth  # noqa: E402
 
 def params(profile, sigma_param):
     s = [sigma_param] * 3 if np.isscalar(sigma_param) else list(sigma_param)
-    return (oracle.reference_stage_default(profile, False, s),
-            oracle.reference_stage_default(profile, True, s))
+    final = oracle.reference_stage_default(profile, True, s)
+    final["lambda"] = 0.0  # never initialised by the reference (include/BM3D.h:101-151), unused
+    return oracle.reference_stage_default(profile, False, s), final
 
 
 def tie_plane(h, w):
@@ -41,6 +42,9 @@ CASES = [
     ("fast_13x21_s50", "fast", 21, 13, 50.0, 13),
     ("lc_60x44_s15", "lc", 44, 60, 15.0, 14),
     ("fast_ties_48x40", "fast", 40, 48, None, 15),
+    ("np_56x72_s20", "np", 56, 72, 20.0, 16),
+    ("high_48x40_s30", "high", 40, 48, 30.0, 17),
+    ("vn_64x56_s15", "vn", 56, 64, 15.0, 18),
 ]
 
 
