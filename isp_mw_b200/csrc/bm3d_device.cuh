@@ -297,7 +297,8 @@ struct SmemPlan {
     size_t region_bytes;         // one staged window
     size_t acc_bytes;            // one accumulator window
     size_t off_acc;              // 2 * planes accumulator windows
-    size_t off_origin;           // block (0, 0) copies per staged window + accumulators
+    size_t off_origin;           // block (0, 0) copies per staged window
+    size_t off_origin_acc;       // block (0, 0) accumulators
     size_t off_warps;
     size_t warp_bytes;
     size_t scratch_bytes;        // group buffer(s) / search list union at the start of a warp's area
@@ -323,9 +324,9 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
     s.acc_bytes = (static_cast<size_t>(region_h) * region_pitch * sizeof(Acc) + 15) / 16 * 16;
     s.off_acc = s.region_bytes * s.n_stage;
     s.off_origin = s.off_acc + s.acc_bytes * 2 * nplanes;
-    // block (0, 0) copies: T per staged window, then Acc per accumulator
-    const size_t origin_bytes = sizeof(T) * bsq * s.n_stage + sizeof(Acc) * bsq * 2 * nplanes;
-    s.off_warps = (s.off_origin + origin_bytes + 15) / 16 * 16;
+    // block (0, 0) copies: T per staged window, then (16-byte aligned) Acc per accumulator
+    s.off_origin_acc = s.off_origin + (sizeof(T) * bsq * s.n_stage + 15) / 16 * 16;
+    s.off_warps = (s.off_origin_acc + sizeof(Acc) * bsq * 2 * nplanes + 15) / 16 * 16;
     const size_t group_bytes = generic
         ? sizeof(T) * static_cast<size_t>(gs) * bsq * (wiener ? 2 : 1)
         : sizeof(T) * kGSMax * kGroupStride;

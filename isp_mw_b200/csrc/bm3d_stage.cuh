@@ -697,7 +697,7 @@ __device__ __forceinline__ void carve_tile(const StageArgs<T> &a, const SmemPlan
             ++s;
         }
     }
-    Acc *origin_acc = reinterpret_cast<Acc *>(origin + bsq * sp.n_stage);
+    Acc *origin_acc = reinterpret_cast<Acc *>(smem + sp.off_origin_acc);
     for (int p = 0; p < NPL; ++p) {
         t.accN[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p));
         t.accD[p] = reinterpret_cast<Acc *>(smem + sp.off_acc + sp.acc_bytes * (2 * p + 1));

@@ -248,7 +248,8 @@ def test_invalid_and_unsupported(ctx):
     with pytest.raises(isp_mw_b200.BM3DError) as e:
         ctx.stage(p, False, np.empty_like(small), small)
     assert e.value.code == isp_mw_b200.BM3D_ERR_INVALID
-    q = isp_mw_b200.stage_params_default("vn", True, (20.0, 20.0, 20.0))  # BlockSize 11
+    q = isp_mw_b200.stage_params_default("vn", True, (20.0, 20.0, 20.0))
+    q.block_size = 17  # beyond the largest block size built (16)
     x = np.zeros((64, 64), np.float32)
     with pytest.raises(isp_mw_b200.BM3DError) as e:
         ctx.stage(q, True, np.empty_like(x), x, x)
@@ -296,3 +297,29 @@ def test_value_range_scales_matching(ctx, oracle_mod):
     d = np.abs(out - ref).max() / 255.0
     report(test="value_range_255", max_abs_scaled=float(d))
     assert d <= MAX_ABS
+
+
+@pytest.mark.parametrize("profile,shape,s255", [("lc", (200, 256), 15.0), ("np", (128, 160), 20.0),
+                                                ("high", (96, 120), 35.0), ("vn", (128, 160), 15.0)])
+def test_profiles_against_oracle(ctx, oracle_mod, profile, shape, s255):
+    """Every reference profile (include/BM3D.h:27-151): np/high final and both vn
+    stages (GroupSize 32, BlockSize 11, BMrange 16) run on the generic kernel."""
+    from isp_mw_b200 import synth
+    import isp_mw_b200
+    _, noisy = synth.pair(shape[0], shape[1], s255, 50)
+    sp = [synth.sigma_param(s255)] * 3
+    b = isp_mw_b200.stage_params_default(profile, False, sp)
+    f = isp_mw_b200.stage_params_default(profile, True, sp)
+    orc = _oracle(oracle_mod)
+    name = f"{profile}_{shape[1]}x{shape[0]}_s{s255:g}"
+    rb = orc.stage(False, b.as_dict(), noisy)
+    assert group_match(name + ":basic_groups", ctx.debug_groups(b, False, noisy),
+                       orc.groups(False, b.as_dict(), noisy)) >= 0.999
+    basic = np.empty_like(noisy)
+    ctx.stage(b, False, basic, noisy)
+    assert_close(name + ":basic", basic, rb)
+    assert group_match(name + ":final_groups", ctx.debug_groups(f, True, basic),
+                       orc.groups(True, f.as_dict(), basic)) >= 0.999
+    final = np.empty_like(noisy)
+    ctx.stage(f, True, final, noisy, basic)
+    assert_close(name + ":final", final, orc.stage(True, f.as_dict(), noisy, basic))
