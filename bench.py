@@ -108,12 +108,12 @@ class ClockSampler:
 
 
 def make_inputs(rank: int):
-    from isp_mw_b200 import synth
+    from isp_mw_b200 import shard, synth
     sets = []
     for r in range(RING):
         planes = []
         for k, s in enumerate(SIGMAS):
-            seed = 1000 * rank + 100 * r + k
+            seed = shard.plane_seed(rank, r, k)
             _, noisy = synth.pair(H, W, s, seed)
             planes.append(noisy)
         sets.append(planes)
@@ -186,11 +186,8 @@ def run_ours(args):
         step(args.warmup + i)
     ev1.record(stream)
     barrier()
-    ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    from isp_mw_b200 import shard
+    ms_max = shard.max_over_ranks(ev0.elapsed_time(ev1), dev)
     mp_step = len(SIGMAS) * W * H / 1e6
     value = world * mp_step * args.steps / (ms_max / 1e3)
 
@@ -237,11 +234,8 @@ def run_ours(args):
     ev1.record(stream)
     barrier()
     e_wall = (time.perf_counter() - e0) * 1e3
-    e_ms = max(ev0.elapsed_time(ev1), e_wall)
-    te = torch.tensor([e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * mp_step * args.steps / (float(te.item()) / 1e3)
+    e_ms = shard.max_over_ranks(max(ev0.elapsed_time(ev1), e_wall), dev)
+    e2e_value = world * mp_step * args.steps / (e_ms / 1e3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
