@@ -172,6 +172,29 @@ int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, float *dst, 
                        const float *ref, int width, int height, size_t stride, float value_range,
                        void *stream);
 
+/* Batched basic + final over `count` device planes of any sizes and noise
+ * levels: one persistent launch per stage walks a device work queue of
+ * (plane, tile) items, and the whole pipeline (accumulator set-up, basic
+ * stage, normalisation, final stage, normalisation) is captured once in a
+ * CUDA graph that bm3d_batch_run replays. Per plane i: basic[i] / final_[i]
+ * (planes in one batch share BlockSize, BlockStep, GroupSize, BMrange and
+ * BMstep per stage; sigma, thMSE and lambda may differ), src[i] / dst[i]
+ * with width[i] x height[i] and row pitch stride[i]. With `autotune` the
+ * tile shape and warps per CTA of each stage are picked by timing candidate
+ * configurations on this batch. Results equal per-plane bm3d_full bit for bit.
+ * The batch keeps its own device buffers (16 B per pixel of accumulators and
+ * the basic estimates) until bm3d_batch_destroy. Replaces looping the
+ * reference's BM3D over images (no batched form exists there). */
+typedef struct bm3d_batch bm3d_batch;
+int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                      const bm3d_stage_params *final_, float *const dst[],
+                      const float *const src[], const int width[], const int height[],
+                      const size_t stride[], int autotune, bm3d_batch **out);
+int bm3d_batch_run(bm3d_batch *batch, void *stream);
+/* tile_x, tile_y, warps of the basic stage, then of the final stage. */
+int bm3d_batch_tuning(const bm3d_batch *batch, int out[6]);
+void bm3d_batch_destroy(bm3d_batch *batch);
+
 /* Per-launch timing of the stage kernels with CUDA events recorded on the
  * launch stream (off by default). Turning it on or off resets the totals.
  * No counterpart in the reference, which has no timing hooks beyond an

@@ -38,7 +38,8 @@ EXPORTS = [
     "bm3d_ctx_destroy", "bm3d_last_error", "bm3d_stage", "bm3d_stage3", "bm3d_full",
     "bm3d_full3", "bm3d_stage_f64", "bm3d_ref_block_count", "bm3d_debug_groups",
     "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
-    "bm3d_stage_noalloc",
+    "bm3d_stage_noalloc", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
+    "bm3d_batch_destroy",
 ]
 
 
@@ -117,6 +118,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_set_tiling.argtypes = [vp, ip, ip, ip]
     lib.bm3d_stage_noalloc.argtypes = [sp, ip, vp, vp, vp, ip, ip, ctypes.c_size_t,
                                        ctypes.c_float, vp]
+    lib.bm3d_batch_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
+                                      ctypes.POINTER(vp)]
+    lib.bm3d_batch_run.argtypes = [vp, vp]
+    lib.bm3d_batch_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    lib.bm3d_batch_destroy.argtypes = [vp]
+    lib.bm3d_batch_destroy.restype = None
     lib.bm3d_set_kernel_timing.argtypes = [vp, ip]
     lib.bm3d_kernel_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong)]
@@ -273,6 +280,61 @@ class Context:
         out = (ctypes.c_ulonglong * 4)()
         self._check(self.lib.bm3d_last_stats(self.h, out))
         return [int(v) for v in out]
+
+
+class Batch:
+    """``bm3d_batch``: basic + final over many device planes (CUDA torch
+    tensors) of any sizes and noise levels, one persistent launch per stage,
+    replayed from a CUDA graph. The planes are bound at creation."""
+
+    def __init__(self, ctx: "Context", basic: Sequence[StageParams], final: Sequence[StageParams],
+                 dst: Sequence, src: Sequence, autotune: bool = True):
+        n = len(src)
+        if not (len(basic) == len(final) == len(dst) == n) or n == 0:
+            raise ValueError("one basic/final parameter set and dst per src plane")
+        self.ctx = ctx
+        self._keep = (list(dst), list(src))
+        infos_d = [_plane_info(d) for d in dst]
+        infos_s = [_plane_info(x) for x in src]
+        if any(i[1] != MEM_DEVICE for i in infos_d + infos_s):
+            raise ValueError("batches take device (CUDA) planes")
+        for a, b in zip(infos_d, infos_s):
+            if a[2:5] != b[2:5]:
+                raise ValueError("dst and src planes must have the same size and pitch")
+        pb = (StageParams * n)(*basic)
+        pf = (StageParams * n)(*final)
+        vp = ctypes.c_void_p * n
+        w = (ctypes.c_int * n)(*[i[2] for i in infos_s])
+        h = (ctypes.c_int * n)(*[i[3] for i in infos_s])
+        st = (ctypes.c_size_t * n)(*[i[4] for i in infos_s])
+        self.h = ctypes.c_void_p()
+        rc = ctx.lib.bm3d_batch_create(ctx.h, n, pb, pf, vp(*[i[0] for i in infos_d]),
+                                       vp(*[i[0] for i in infos_s]), w, h, st, int(autotune),
+                                       ctypes.byref(self.h))
+        ctx._check(rc, allow_copied=False)
+        self.pixels = sum(i[2] * i[3] for i in infos_s)
+
+    def run(self, stream: Optional[int] = None):
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream
+        self.ctx._check(self.ctx.lib.bm3d_batch_run(self.h, stream))
+
+    def tuning(self):
+        out = (ctypes.c_int * 6)()
+        self.ctx._check(self.ctx.lib.bm3d_batch_tuning(self.h, out))
+        return {"basic": tuple(out[0:3]), "final": tuple(out[3:6])}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.bm3d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

@@ -1,7 +1,7 @@
 // C ABI of the B200 BM3D path (declared in include/bm3d_b200.h): parameter
 // mirroring, per-call constant setup, context scratch and kernel launches.
 #include "bm3d_b200.h"
-#include "bm3d_generic.cuh"
+#include "bm3d_batch.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -1079,4 +1079,404 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     normalize_kernel<float><<<blocks, threads, 0, s>>>(dst, a.stride, num, den, width, height);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("normalize_kernel", e);
     return BM3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches: bm3d_batch_create / bm3d_batch_run / bm3d_batch_destroy.
+
+namespace {
+
+struct StageBuild {
+    int tile_x = 0, tile_y = 0, warps = 0;
+    bool generic = false;
+    int nact = 0;            // planes with work in this stage
+    int total_tiles = 0;
+    size_t smem = 0;         // dynamic shared memory of the persistent launch
+    int grid = 0;
+    DevBuf args, base;       // device StageArgs[nact], int[nact + 1]
+};
+
+}  // namespace
+
+struct bm3d_batch {
+    bm3d_ctx *ctx = nullptr;
+    int n = 0;
+    std::vector<int> w, h;
+    std::vector<size_t> stride;
+    std::vector<const float *> src;
+    std::vector<float *> dst;
+    std::vector<bm3d_stage_params> pb, pf;
+    std::vector<Guard> gb, gf;
+    std::vector<size_t> acc_off, basic_off;  // element offsets into acc (int64) and basic (float)
+    DevBuf acc, basic, absmax, counters, planes_b, planes_f;
+    StageBuild sb, sf;
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int batch_fail(bm3d_ctx *ctx, const char *msg)
+{
+    ctx->err = msg;
+    return BM3D_ERR_INVALID;
+}
+
+// Per-plane stage arguments of one stage at one tiling; uploads them and sizes
+// the persistent launch. Returns BM3D_ERR_UNSUPPORTED when the tiling does
+// not fit in shared memory.
+int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuild &out)
+{
+    bm3d_ctx *ctx = B->ctx;
+    std::vector<StageArgs<float>> args;
+    std::vector<int> base(1, 0);
+    size_t smem = 0;
+    bool generic = false;
+    for (int i = 0; i < B->n; ++i) {
+        const bm3d_stage_params *p = wiener ? &B->pf[i] : &B->pb[i];
+        if ((wiener ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
+        StageArgs<float> a;
+        std::memset(&a, 0, sizeof(a));
+        fill_tables(a, p, wiener, 1, 1.0);
+        generic = !fast_args(p->block_size, p->group_size);
+        const int BS = p->block_size;
+        a.width = B->w[i];
+        a.height = B->h[i];
+        a.block_size = BS;
+        a.step = p->block_step;
+        a.group_size = p->group_size;
+        a.bm_step = p->bm_step;
+        a.range = p->bm_range / p->bm_step * p->bm_step;
+        a.nx = ref_count(a.width - BS, a.step);
+        a.ny = ref_count(a.height - BS, a.step);
+        const int span = 2 * (a.range / a.bm_step) + 1;
+        a.key_slots = span * span + 1;
+        const int reach = a.match ? a.range : 0;
+        a.region_w = std::min(a.width, (tx - 1) * a.step + 2 * reach + BS);
+        a.region_h = std::min(a.height, (ty - 1) * a.step + 2 * reach + BS);
+        a.region_pitch = a.region_w + ((5 - a.region_w % 8) + 8) % 8;
+        a.tile_x = std::min(tx, a.nx);
+        a.tile_y = std::min(ty, a.ny);
+        a.tiles_x = (a.nx + a.tile_x - 1) / a.tile_x;
+        a.stride = static_cast<long long>(B->stride[i]);
+        a.src[0] = B->src[i];
+        a.ref[0] = wiener ? static_cast<const float *>(B->basic.ptr) + B->basic_off[i] : B->src[i];
+        a.ref_alias_src = wiener ? 0 : 1;
+        a.num[0] = static_cast<long long *>(B->acc.ptr) + B->acc_off[i];
+        a.den[0] = a.num[0] + static_cast<size_t>(a.width) * a.height;
+        a.absmax = static_cast<float *>(B->absmax.ptr) + i;
+        const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, p->group_size);
+        a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
+        a.dct_fwd = ctx->gtab_f;
+        a.dct_inv = ctx->gtab_f ? ctx->gtab_f + kDctTableSize : nullptr;
+        const SmemPlan sp = plan_smem<float>(1, wiener, a.ref_alias_src, a.region_h, a.region_pitch,
+                                             a.key_slots, warps, generic, BS, p->group_size);
+        smem = std::max(smem, sp.total + kBatchHeader);
+        args.push_back(a);
+        base.push_back(base.back() + a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y));
+    }
+    if (smem > ctx->smem_optin) return BM3D_ERR_UNSUPPORTED;
+    out.tile_x = tx;
+    out.tile_y = ty;
+    out.warps = warps;
+    out.generic = generic;
+    out.nact = static_cast<int>(args.size());
+    out.total_tiles = base.back();
+    out.smem = smem;
+    int rc;
+    if (out.nact > 0) {
+        if ((rc = ensure(ctx, out.args, sizeof(StageArgs<float>) * args.size())) != BM3D_OK) return rc;
+        if ((rc = ensure(ctx, out.base, sizeof(int) * base.size())) != BM3D_OK) return rc;
+        CK(ctx, cudaMemcpy(out.args.ptr, args.data(), sizeof(StageArgs<float>) * args.size(),
+                           cudaMemcpyHostToDevice));
+        CK(ctx, cudaMemcpy(out.base.ptr, base.data(), sizeof(int) * base.size(),
+                           cudaMemcpyHostToDevice));
+    }
+    return BM3D_OK;
+}
+
+template <bool W>
+int launch_batch_stage(bm3d_batch *B, StageBuild &sbd, int *counter, cudaStream_t s)
+{
+    bm3d_ctx *ctx = B->ctx;
+    if (sbd.nact == 0) return BM3D_OK;
+    CK(ctx, cudaMemsetAsync(counter, 0, sizeof(int), s));
+    const auto *args = static_cast<const StageArgs<float> *>(sbd.args.ptr);
+    const int *base = static_cast<const int *>(sbd.base.ptr);
+    auto go = [&](auto kern) -> int {
+        CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(sbd.smem)));
+        int per_sm = 0;
+        CK(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sbd.warps * kWarp,
+                                                              sbd.smem));
+        sbd.grid = std::max(1, per_sm) * ctx->sm_count;
+        kern<<<sbd.grid, sbd.warps * kWarp, sbd.smem, s>>>(args, base, sbd.nact, counter);
+        CK(ctx, cudaGetLastError());
+        return BM3D_OK;
+    };
+    if (sbd.generic) return go(batch_stage_kernel<float, W, 1, 1, true>);
+    if ((W ? B->pf[0].bm_step : B->pb[0].bm_step) == 1)
+        return go(batch_stage_kernel<float, W, 1, 4, false>);
+    return go(batch_stage_kernel<float, W, 1, 1, false>);
+}
+
+int launch_planes(bm3d_batch *B, const DevBuf &planes, int count, bool prep, cudaStream_t s)
+{
+    if (count == 0) return BM3D_OK;
+    long long maxpx = 0;
+    for (int i = 0; i < B->n; ++i) maxpx = std::max(maxpx, static_cast<long long>(B->w[i]) * B->h[i]);
+    const dim3 grid(static_cast<unsigned>(std::min<long long>((maxpx + 255) / 256, 64)),
+                    static_cast<unsigned>(count));
+    const auto *q = static_cast<const BatchPlane<float> *>(planes.ptr);
+    if (prep) prep_batch_kernel<float><<<grid, 256, 0, s>>>(q);
+    else normalize_batch_kernel<float><<<grid, 256, 0, s>>>(q);
+    CK(B->ctx, cudaGetLastError());
+    return BM3D_OK;
+}
+
+// The whole pipeline, enqueued on s (captured into the graph).
+int enqueue_batch(bm3d_batch *B, cudaStream_t s)
+{
+    bm3d_ctx *ctx = B->ctx;
+    int rc;
+    int *counters = static_cast<int *>(B->counters.ptr);
+    for (int i = 0; i < B->n; ++i) {  // planes a stage passes through unfiltered
+        float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[i];
+        if (B->gb[i] != Guard::Run)
+            CK(ctx, cudaMemcpy2DAsync(bi, B->stride[i] * 4, B->src[i], B->stride[i] * 4, B->w[i] * 4,
+                                      B->h[i], cudaMemcpyDeviceToDevice, s));
+        if (B->gf[i] != Guard::Run && B->dst[i] != B->src[i])
+            CK(ctx, cudaMemcpy2DAsync(B->dst[i], B->stride[i] * 4, B->src[i], B->stride[i] * 4,
+                                      B->w[i] * 4, B->h[i], cudaMemcpyDeviceToDevice, s));
+    }
+    CK(ctx, cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * B->n, s));
+    if ((rc = launch_planes(B, B->planes_b, B->sb.nact, true, s)) != BM3D_OK) return rc;
+    if ((rc = launch_batch_stage<false>(B, B->sb, counters, s)) != BM3D_OK) return rc;
+    if ((rc = launch_planes(B, B->planes_b, B->sb.nact, false, s)) != BM3D_OK) return rc;
+    if ((rc = launch_planes(B, B->planes_f, B->sf.nact, true, s)) != BM3D_OK) return rc;
+    if ((rc = launch_batch_stage<true>(B, B->sf, counters + 1, s)) != BM3D_OK) return rc;
+    if ((rc = launch_planes(B, B->planes_f, B->sf.nact, false, s)) != BM3D_OK) return rc;
+    return BM3D_OK;
+}
+
+// Time one stage launch (after a prep) at the current build.
+template <bool W>
+int time_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, cudaStream_t s, float &ms)
+{
+    bm3d_ctx *ctx = B->ctx;
+    int rc;
+    cudaEvent_t e0, e1;
+    CK(ctx, cudaEventCreate(&e0));
+    CK(ctx, cudaEventCreate(&e1));
+    ms = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+        if ((rc = launch_planes(B, planes, sbd.nact, true, s)) != BM3D_OK) return rc;
+        CK(ctx, cudaEventRecord(e0, s));
+        if ((rc = launch_batch_stage<W>(B, sbd, static_cast<int *>(B->counters.ptr) + (W ? 1 : 0),
+                                        s)) != BM3D_OK)
+            return rc;
+        CK(ctx, cudaEventRecord(e1, s));
+        CK(ctx, cudaEventSynchronize(e1));
+        float t = 0;
+        CK(ctx, cudaEventElapsedTime(&t, e0, e1));
+        if (rep > 0) ms = std::min(ms, t);  // first run warms up
+    }
+    if (!W) {  // leave the basic estimates in place for the final stage's tuning
+        if ((rc = launch_planes(B, planes, sbd.nact, false, s)) != BM3D_OK) return rc;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return BM3D_OK;
+}
+
+// Pick the tiling of one stage: the fastest candidate that fits, or the
+// default when not autotuning.
+template <bool W>
+int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotune, cudaStream_t s)
+{
+    const bm3d_stage_params &p = W ? B->pf[0] : B->pb[0];
+    const bool generic = !fast_args(p.block_size, p.group_size);
+    static const int fast_cand[][3] = {{8, 8, 16}, {7, 7, 16}, {6, 8, 12}, {8, 6, 12},
+                                       {6, 6, 12}, {4, 4, 4}, {4, 4, 2}, {2, 2, 1}};
+    static const int gen_cand[][3] = {{4, 4, 8}, {4, 4, 4}, {2, 2, 4}, {2, 2, 2}, {1, 1, 2}, {1, 1, 1}};
+    const int (*cand)[3] = generic ? gen_cand : fast_cand;
+    const int ncand = generic ? 6 : 8;
+    int best = -1;
+    float best_ms = 1e30f;
+    for (int c = 0; c < ncand; ++c) {
+        int rc = build_stage(B, W, cand[c][0], cand[c][1], cand[c][2], sbd);
+        if (rc == BM3D_ERR_UNSUPPORTED) continue;
+        if (rc != BM3D_OK) return rc;
+        if (!autotune) {
+            best = c;
+            break;
+        }
+        float ms;
+        if ((rc = time_stage<W>(B, sbd, planes, s, ms)) != BM3D_OK) return rc;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    if (best < 0) {
+        B->ctx->err = "batch stage does not fit in shared memory";
+        return BM3D_ERR_UNSUPPORTED;
+    }
+    int rc = build_stage(B, W, cand[best][0], cand[best][1], cand[best][2], sbd);
+    if (rc == BM3D_OK && !W && autotune) {
+        float ms;  // re-run the chosen basic tiling so the final stage tunes on its output
+        rc = time_stage<W>(B, sbd, planes, s, ms);
+    }
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                                 const bm3d_stage_params *final_, float *const dst[],
+                                 const float *const src[], const int width[], const int height[],
+                                 const size_t stride[], int autotune, bm3d_batch **out)
+{
+    if (!ctx || !out || count < 1 || !basic || !final_ || !dst || !src || !width || !height ||
+        !stride)
+        return BM3D_ERR_INVALID;
+    *out = nullptr;
+    CK(ctx, cudaSetDevice(ctx->device));
+    auto *B = new bm3d_batch;
+    B->ctx = ctx;
+    B->n = count;
+    auto fail = [&](int rc) {
+        bm3d_batch_destroy(B);
+        return rc;
+    };
+    size_t acc_total = 0, basic_total = 0;
+    for (int i = 0; i < count; ++i) {
+        const Guard gb = check_params(&basic[i], 1), gf = check_params(&final_[i], 1);
+        if (gb == Guard::Invalid || gf == Guard::Invalid) return fail(batch_fail(ctx, "invalid parameters"));
+        if (gb == Guard::Unsupported || gf == Guard::Unsupported) {
+            ctx->err = "parameters outside this build (BlockSize <= 16, GroupSize <= 32)";
+            return fail(BM3D_ERR_UNSUPPORTED);
+        }
+        for (const auto *pp : {&basic[i], &final_[i]}) {
+            const auto &q0 = pp == &basic[i] ? basic[0] : final_[0];
+            if (pp->block_size != q0.block_size || pp->block_step != q0.block_step ||
+                pp->group_size != q0.group_size || pp->bm_range != q0.bm_range ||
+                pp->bm_step != q0.bm_step)
+                return fail(batch_fail(ctx, "planes of a batch must share the stage geometry"));
+        }
+        const int bs = std::max(basic[i].block_size, final_[i].block_size);
+        if (!src[i] || !dst[i] || width[i] < bs || height[i] < bs ||
+            stride[i] < static_cast<size_t>(width[i]))
+            return fail(batch_fail(ctx, "bad plane"));
+        B->w.push_back(width[i]);
+        B->h.push_back(height[i]);
+        B->stride.push_back(stride[i]);
+        B->src.push_back(src[i]);
+        B->dst.push_back(dst[i]);
+        B->pb.push_back(basic[i]);
+        B->pf.push_back(final_[i]);
+        B->gb.push_back(gb);
+        B->gf.push_back(gf);
+        B->acc_off.push_back(acc_total);
+        B->basic_off.push_back(basic_total);
+        acc_total += 2 * static_cast<size_t>(width[i]) * height[i];
+        basic_total += stride[i] * height[i];
+    }
+    int rc;
+    if ((rc = ensure(ctx, B->acc, sizeof(long long) * acc_total)) != BM3D_OK) return fail(rc);
+    if ((rc = ensure(ctx, B->basic, sizeof(float) * basic_total)) != BM3D_OK) return fail(rc);
+    if ((rc = ensure(ctx, B->absmax, sizeof(float) * count)) != BM3D_OK) return fail(rc);
+    if ((rc = ensure(ctx, B->counters, 2 * sizeof(int))) != BM3D_OK) return fail(rc);
+    // per-pixel kernels' plane tables, active planes of each stage in batch order
+    for (int st = 0; st < 2; ++st) {
+        std::vector<BatchPlane<float>> q;
+        for (int i = 0; i < count; ++i) {
+            if ((st ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
+            BatchPlane<float> bp;
+            bp.num = static_cast<long long *>(B->acc.ptr) + B->acc_off[i];
+            bp.den = bp.num + static_cast<size_t>(width[i]) * height[i];
+            bp.src = src[i];
+            bp.dst = st ? dst[i] : static_cast<float *>(B->basic.ptr) + B->basic_off[i];
+            bp.src_stride = static_cast<long long>(stride[i]);
+            bp.dst_stride = static_cast<long long>(stride[i]);
+            bp.width = width[i];
+            bp.height = height[i];
+            bp.absmax = static_cast<float *>(B->absmax.ptr) + i;
+            q.push_back(bp);
+        }
+        DevBuf &dbuf = st ? B->planes_f : B->planes_b;
+        if (!q.empty()) {
+            if ((rc = ensure(ctx, dbuf, sizeof(BatchPlane<float>) * q.size())) != BM3D_OK) return fail(rc);
+            CK(ctx, cudaMemcpy(dbuf.ptr, q.data(), sizeof(BatchPlane<float>) * q.size(),
+                               cudaMemcpyHostToDevice));
+        }
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaStreamCreate"));
+    // planes whose basic stage is a copy must hold src before the final stage tunes
+    for (int i = 0; i < count; ++i)
+        if (B->gb[i] != Guard::Run) {
+            float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[i];
+            e = cudaMemcpy2DAsync(bi, stride[i] * 4, src[i], stride[i] * 4, width[i] * 4, height[i],
+                                  cudaMemcpyDeviceToDevice, B->cap);
+            if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemcpy2DAsync"));
+        }
+    e = cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * count, B->cap);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemsetAsync"));
+    if ((rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap)) != BM3D_OK) return fail(rc);
+    if ((rc = tune_stage<true>(B, B->sf, B->planes_f, autotune != 0, B->cap)) != BM3D_OK) return fail(rc);
+    e = cudaStreamSynchronize(B->cap);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "batch tuning"));
+    // capture the pipeline once
+    e = cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaStreamBeginCapture"));
+    rc = enqueue_batch(B, B->cap);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(B->cap, &g);
+    if (rc != BM3D_OK) {
+        if (g) cudaGraphDestroy(g);
+        return fail(rc);
+    }
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaStreamEndCapture"));
+    B->graph = g;
+    e = cudaGraphInstantiate(&B->exec, g, 0);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaGraphInstantiate"));
+    *out = B;
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_batch_run(bm3d_batch *B, void *stream)
+{
+    if (!B || !B->exec) return BM3D_ERR_INVALID;
+    CK(B->ctx, cudaSetDevice(B->ctx->device));
+    CK(B->ctx, cudaGraphLaunch(B->exec, static_cast<cudaStream_t>(stream)));
+    B->ctx->last_stream = static_cast<cudaStream_t>(stream);
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_batch_tuning(const bm3d_batch *B, int out[6])
+{
+    if (!B || !out) return BM3D_ERR_INVALID;
+    out[0] = B->sb.tile_x;
+    out[1] = B->sb.tile_y;
+    out[2] = B->sb.warps;
+    out[3] = B->sf.tile_x;
+    out[4] = B->sf.tile_y;
+    out[5] = B->sf.warps;
+    return BM3D_OK;
+}
+
+extern "C" void bm3d_batch_destroy(bm3d_batch *B)
+{
+    if (!B) return;
+    cudaSetDevice(B->ctx->device);
+    if (B->cap) cudaStreamSynchronize(B->cap);
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    if (B->cap) cudaStreamDestroy(B->cap);
+    for (DevBuf *b : {&B->acc, &B->basic, &B->absmax, &B->counters, &B->planes_b, &B->planes_f,
+                      &B->sb.args, &B->sb.base, &B->sf.args, &B->sf.base})
+        if (b->ptr) cudaFree(b->ptr);
+    delete B;
 }

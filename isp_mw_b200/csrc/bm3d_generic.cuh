@@ -177,9 +177,8 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
 }
 
 template <typename T, bool WIENER, int NPL>
-__global__ void __launch_bounds__(256) generic_stage_kernel(const StageArgs<T> a)
+__device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int tile, unsigned char *smem)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     const int bs = a.block_size;
@@ -187,7 +186,7 @@ __global__ void __launch_bounds__(256) generic_stage_kernel(const StageArgs<T> a
 
     Tile<T> t;
     int kx0, kx1, ky0, ky1;
-    tile_window(a, bs, t, kx0, kx1, ky0, ky1);
+    tile_window(a, tile, bs, t, kx0, kx1, ky0, ky1);
     const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
                                      a.key_slots, nwarps, true, bs, a.group_size);
     carve_tile<T, WIENER, NPL>(a, sp, smem, t);
@@ -230,6 +229,13 @@ __global__ void __launch_bounds__(256) generic_stage_kernel(const StageArgs<T> a
     if (a.bm_only) return;
     __syncthreads();
     flush_tile<T, NPL>(a, t);
+}
+
+template <typename T, bool WIENER, int NPL>
+__global__ void __launch_bounds__(256) generic_stage_kernel(const StageArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    generic_tile_body<T, WIENER, NPL>(a, blockIdx.x, smem);
 }
 
 }  // namespace bm3d

@@ -635,10 +635,10 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
 // the search windows of the tile's blocks (or the blocks themselves when no
 // matching happens).
 template <typename T>
-__device__ __forceinline__ void tile_window(const StageArgs<T> &a, int bs, Tile<T> &t, int &kx0,
-                                            int &kx1, int &ky0, int &ky1)
+__device__ __forceinline__ void tile_window(const StageArgs<T> &a, int tile, int bs, Tile<T> &t,
+                                            int &kx0, int &kx1, int &ky0, int &ky1)
 {
-    const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
+    const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
     kx0 = tx * a.tile_x;
     ky0 = ty * a.tile_y;
     kx1 = min(kx0 + a.tile_x, a.nx);
@@ -805,18 +805,17 @@ __device__ __forceinline__ void flush_stats(const StageArgs<T> &a, int lane, uns
 }
 
 // ---------------------------------------------------------------------------
-// Register-resident stage kernel: BlockSize 8, GroupSize <= 16.
+// Register-resident stage: BlockSize 8, GroupSize <= 16. One tile per call.
 template <typename T, bool WIENER, int NPL, int KS>
-__global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
+__device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile, unsigned char *smem)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     const int right = a.width - kBS, bottom = a.height - kBS;
 
     Tile<T> t;
     int kx0, kx1, ky0, ky1;
-    tile_window(a, kBS, t, kx0, kx1, ky0, ky1);
+    tile_window(a, tile, kBS, t, kx0, kx1, ky0, ky1);
     const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
                                      a.key_slots, nwarps);
     carve_tile<T, WIENER, NPL>(a, sp, smem, t);
@@ -856,6 +855,13 @@ __global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
     if (a.bm_only) return;
     __syncthreads();
     flush_tile<T, NPL>(a, t);
+}
+
+template <typename T, bool WIENER, int NPL, int KS>
+__global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    stage_tile_body<T, WIENER, NPL, KS>(a, blockIdx.x, smem);
 }
 
 // dst = num / den (source/BM3D.cpp:130-135, include/Image_Type.hpp:319-332).
