@@ -277,10 +277,12 @@ def run_ours(args):
     outs = [torch.empty((H, W), dtype=torch.float32, device=dev) for _ in SIGMAS]
     stream = torch.cuda.current_stream(dev)
 
+    # One batch (persistent basic + final launches in a CUDA graph) per input set.
+    batches = [isp_mw_b200.Batch(ctx, [p[0] for p in params], [p[1] for p in params], outs,
+                                 planes, autotune=True) for planes in dev_sets]
+
     def step(i):
-        planes = dev_sets[i % RING]
-        for k in range(len(SIGMAS)):
-            ctx.full(params[k][0], params[k][1], outs[k], planes[k])
+        batches[i % RING].run(stream.cuda_stream)
 
     def barrier():
         if world > 1:
@@ -368,16 +370,18 @@ def run_ours(args):
             "dtype": "f32",
             "data": "synthetic (seeded piecewise-smooth planes + Gaussian noise)",
             "config": {"workload": "BM3D basic+final, fast profile, 4 x 1920x1080 f32 luma "
-                                   "planes (sigma 5/10/25/50 per 255) per step",
+                                   "planes (sigma 5/10/25/50 per 255) per step, one batched "
+                                   "graph replay (persistent basic + final launches) per step",
                        "width": W, "height": H, "planes_per_step": len(SIGMAS),
                        "profile": "fast", "sigma_255": list(SIGMAS),
                        "l2": f"inputs rotate over {RING} sets ({RING * len(SIGMAS) * W * H * 4 / 1e6:.0f} MB) "
                              "> 126 MB L2",
+                       "tiling": batches[0].tuning(),
                        "parallelism": f"replicas x{world} (independent planes per GPU)"},
             "e2e": {"value": round(e2e_value, 3), "unit": "MP/s",
                     "h2d_bytes_per_step": len(SIGMAS) * W * H * 4,
                     "d2h_bytes_per_step": len(SIGMAS) * W * H * 4},
-            "gpu_launches": args.steps * len(SIGMAS) * 4,
+            "gpu_launches": args.steps * 6,
             "roofline": {
                 "bound": "fp32",
                 "kernel": "stage_kernel (final)" if dom else "stage_kernel (basic)",
@@ -399,6 +403,8 @@ def run_ours(args):
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
+    for b in batches:
+        b.close()
     ctx.close()
     if world > 1:
         dist.barrier()

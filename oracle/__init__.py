@@ -109,6 +109,10 @@ class _Backend:
             self._stage = self.lib.ref_bm3d_stage
             self._stage3 = self.lib.ref_bm3d_stage3
             self._groups = self.lib.ref_bm3d_groups
+            self._frame = self.lib.ref_bm3d_frame
+            self._plane_int = self.lib.ref_bm3d_plane_int
+            self._stage_int = self.lib.ref_bm3d_stage_int
+            self._stage_frame = self.lib.ref_bm3d_stage_frame
         elif kind == "port":
             path = os.path.join(BUILD_DIR, "libbm3d_oracle.so")
             if not os.path.exists(path):
@@ -117,11 +121,19 @@ class _Backend:
             self._stage = getattr(self.lib, f"oracle_bm3d_stage_{sfx}")
             self._stage3 = getattr(self.lib, f"oracle_bm3d_stage3_{sfx}")
             self._groups = getattr(self.lib, f"oracle_bm3d_groups_{sfx}")
+            self._frame = getattr(self.lib, f"oracle_bm3d_frame_{sfx}")
+            self._plane_int = getattr(self.lib, f"oracle_bm3d_plane_int_{sfx}")
+            self._stage_int = getattr(self.lib, f"oracle_bm3d_stage_int_{sfx}")
+            self._stage_frame = getattr(self.lib, f"oracle_bm3d_stage_frame_{sfx}")
         else:
             raise ValueError(kind)
         self._stage.restype = ctypes.c_int
         self._stage3.restype = ctypes.c_int
         self._groups.restype = ctypes.c_longlong
+        self._frame.restype = ctypes.c_int
+        self._plane_int.restype = ctypes.c_int
+        self._stage_int.restype = ctypes.c_int
+        self._stage_frame.restype = ctypes.c_int
 
     def stage(self, wiener: bool, params: dict, src: np.ndarray, ref: Optional[np.ndarray] = None,
               value_range: float = 1.0) -> np.ndarray:
@@ -162,10 +174,88 @@ class _Backend:
                      int(nrefs), g, _ptr(counts), _ptr(pos), _ptr(keys))
         return counts, pos, keys
 
+    def frame(self, basic: dict, final: dict, rgb: Sequence[np.ndarray], bits: int = 8,
+              pc: bool = True):
+        """BM3D on an RGB frame of int32 planes (bit depth `bits`, full or
+        limited range): OPP conversion, basic, final, conversion back."""
+        src = [np.ascontiguousarray(c, dtype=np.int32) for c in rgb]
+        h, w = src[0].shape
+        dst = [np.empty_like(c) for c in src]
+        arr = ctypes.c_void_p * 3
+        pb, pf = make_params(basic), make_params(final)
+        if self.kind == "reference":
+            tail = (int(bits), int(pc))
+        else:
+            tail = frame_range(bits, pc)
+        rc = self._frame(ctypes.byref(pb), ctypes.byref(pf), arr(*[d.ctypes.data for d in dst]),
+                         arr(*[c.ctypes.data for c in src]), w, h, *tail)
+        if rc != 0:
+            raise RuntimeError(f"frame: {rc}")
+        return dst
+
+    def plane_int(self, basic: dict, final: dict, src: np.ndarray, quant, bits: int = 8):
+        """BM3D on an int32 plane quantised as quant = (floor, neutral, ceil)."""
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        h, w = src.shape
+        dst = np.empty_like(src)
+        q = tuple(int(v) for v in quant)
+        tail = ((int(bits),) if self.kind == "reference" else ()) + q
+        pb, pf = make_params(basic), make_params(final)
+        rc = self._plane_int(ctypes.byref(pb), ctypes.byref(pf), _ptr(dst), _ptr(src), w, h, *tail)
+        if rc != 0:
+            raise RuntimeError(f"plane_int: {rc}")
+        return dst
+
+    def stage_int(self, wiener: bool, params: dict, src: np.ndarray, ref=None, quant=(0, 0, 255),
+                  bits: int = 8):
+        """One stage on an int32 plane quantised as (floor, neutral, ceil)."""
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        rp = None if ref is None else np.ascontiguousarray(ref, dtype=np.int32)
+        h, w = src.shape
+        dst = np.empty_like(src)
+        q = tuple(int(v) for v in quant)
+        tail = ((int(bits),) if self.kind == "reference" else ()) + q
+        p = make_params(params)
+        self._stage_int(int(wiener), ctypes.byref(p), _ptr(dst), _ptr(src),
+                        None if rp is None else _ptr(rp), w, h, *tail)
+        return dst
+
+    def stage_frame(self, wiener: bool, params: dict, rgb, ref=None, bits: int = 8,
+                    pc: bool = True):
+        """One stage on an RGB frame of int32 planes."""
+        src = [np.ascontiguousarray(c, dtype=np.int32) for c in rgb]
+        rf = None if ref is None else [np.ascontiguousarray(c, dtype=np.int32) for c in ref]
+        h, w = src[0].shape
+        dst = [np.empty_like(c) for c in src]
+        arr = ctypes.c_void_p * 3
+        tail = (int(bits), int(pc)) if self.kind == "reference" else frame_range(bits, pc)
+        p = make_params(params)
+        self._stage_frame(int(wiener), ctypes.byref(p), arr(*[d.ctypes.data for d in dst]),
+                          arr(*[c.ctypes.data for c in src]),
+                          None if rf is None else arr(*[c.ctypes.data for c in rf]), w, h, *tail)
+        return dst
+
     def full(self, basic: dict, final: dict, src: np.ndarray, value_range: float = 1.0):
         """Basic then final, tmp sized from src (the working BM3D sequence)."""
         tmp = self.stage(False, basic, src, src, value_range)
         return tmp, self.stage(True, final, src, tmp, value_range)
+
+
+def frame_range(bits: int, pc: bool = True):
+    """Floor and Ceil of an RGB plane (include/Image_Type.hpp:94-109, GetQuanPara):
+    full range [0, 2^bits - 1], limited range [16, 235] << (bits - 8)."""
+    if pc:
+        return 0, (1 << bits) - 1
+    return 16 << (bits - 8), 235 << (bits - 8)
+
+
+def plane_quant(bits: int, pc: bool = True, chroma: bool = False):
+    """(Floor, Neutral, Ceil) of an integer plane (include/Image_Type.hpp:94-109)."""
+    if pc:
+        lo, hi = 0, (1 << bits) - 1
+    else:
+        lo, hi = 16 << (bits - 8), (240 if chroma else 235) << (bits - 8)
+    return lo, (1 << (bits - 1)) if chroma else lo, hi
 
 
 def backend(kind: str = "port", dtype=np.float32) -> _Backend:

@@ -439,6 +439,226 @@ long long FN(oracle_bm3d_groups)(int wiener, const oracle_stage_params *p, const
     return r;
 }
 
+/* ---- integer planes and RGB frames ---------------------------------------
+ * The float planes are the reference's default Plane_FL ranges: luma [0, 1],
+ * chroma [-0.5, 0.5] (include/Image_Type.cpp:407-421, Image_Type.hpp:184-202).
+ */
+
+/* MatrixConvert_RGB2YUV with ColorMatrix::OPP to a float destination, no
+ * clipping (include/Conversion.hpp:518-575); `only_y` is ConvertToY
+ * (include/Conversion.hpp:398-430), whose Y formula is the same. RGB planes
+ * have Floor = Neutral = floor_. */
+static void FN(rgb_to_opp)(FLT *const yuv[3], const int *const rgb[3], size_t npx, int floor_,
+                           int ceil_, int only_y)
+{
+    const int sRange = ceil_ - floor_;
+    const FLT dRangeY = (FLT)1, dRangeC = (FLT)0.5 - (FLT)-0.5, dFloorY = 0, dNeutralC = 0;
+    const FLT gainY = dRangeY / ((FLT)sRange * (FLT)3);
+    const FLT offsetY = -(FLT)floor_ * (FLT)3 * gainY + dFloorY;
+    const FLT gainU = dRangeC / ((FLT)sRange * (FLT)2);
+    const FLT gainV = dRangeC / ((FLT)sRange * (FLT)4);
+    const FLT offsetC = dNeutralC;
+    for (size_t i = 0; i < npx; ++i) {
+        const FLT r = (FLT)rgb[0][i], g = (FLT)rgb[1][i], b = (FLT)rgb[2][i];
+        yuv[0][i] = (r + g + b) * gainY + offsetY;
+        if (only_y) continue;
+        yuv[1][i] = (r - b) * gainU + offsetC;
+        yuv[2][i] = (r - g * (FLT)2 + b) * gainV + offsetC;
+    }
+}
+
+/* MatrixConvert_YUV2RGB with ColorMatrix::OPP from the float planes to
+ * integers in [floor_, ceil_], clipped, +0.5 and truncated
+ * (include/Conversion.hpp:661-748; coefficients include/Specification.h:
+ * 468-484). */
+static void FN(opp_to_rgb)(int *const rgb[3], const FLT *const yuv[3], size_t npx, int floor_,
+                           int ceil_)
+{
+    const int dRange = ceil_ - floor_;
+    const FLT sRangeY = (FLT)1 - (FLT)0, sRangeC = (FLT)0.5 - (FLT)-0.5;
+    const FLT gY = (FLT)dRange / sRangeY, gC = (FLT)dRange / sRangeC;
+    const FLT Ry = (FLT)(1.0L) * gY, Ru = (FLT)(1.0L) * gC, Rv = (FLT)(2.0L / 3.0L) * gC;
+    const FLT Gy = (FLT)(1.0L) * gY, Gu = (FLT)(0.0L) * gC, Gv = (FLT)(-4.0L / 3.0L) * gC;
+    const FLT By = (FLT)(1.0L) * gY, Bu = (FLT)(-1.0L) * gC, Bv = (FLT)(2.0L / 3.0L) * gC;
+    const FLT sFloorY = 0, sNeutralC = 0;
+    const FLT offR = -sFloorY * Ry - sNeutralC * (Ru + Rv) + (FLT)floor_ + (FLT)0.5;
+    const FLT offG = -sFloorY * Gy - sNeutralC * (Gu + Gv) + (FLT)floor_ + (FLT)0.5;
+    const FLT offB = -sFloorY * By - sNeutralC * (Bu + Bv) + (FLT)floor_ + (FLT)0.5;
+    const FLT lo = (FLT)floor_, hi = (FLT)ceil_;
+    for (size_t i = 0; i < npx; ++i) {
+        const FLT y = yuv[0][i], u = yuv[1][i], v = yuv[2][i];
+        FLT t;
+        t = Ry * y + Ru * u + Rv * v + offR;
+        rgb[0][i] = (int)(t <= lo ? lo : t >= hi ? hi : t);
+        t = Gy * y + Gv * v + offG;
+        rgb[1][i] = (int)(t <= lo ? lo : t >= hi ? hi : t);
+        t = By * y + Bu * u + Bv * v + offB;
+        rgb[2][i] = (int)(t <= lo ? lo : t >= hi ? hi : t);
+    }
+}
+
+/* RangeConvert from an integer plane (floor_, neutral, ceil_) to the float
+ * plane of range 1, no clipping except for full-range chroma
+ * (include/Conversion.hpp:134-254, different-range branch). */
+static void FN(int_to_fl)(FLT *dst, const int *src, size_t npx, int floor_, int neutral, int ceil_)
+{
+    const int chroma = floor_ < neutral;
+    const int pc_chroma = chroma && (floor_ + ceil_) % 2 == 1;
+    const FLT fFloor = chroma ? (FLT)-0.5 : (FLT)0, fCeil = chroma ? (FLT)0.5 : (FLT)1;
+    const FLT fNeutral = 0;
+    const int sRange = ceil_ - floor_;
+    const FLT dRange = fCeil - fFloor;
+    const FLT gain = dRange / (FLT)sRange;
+    const FLT offset = -(FLT)neutral * gain + fNeutral;
+    for (size_t i = 0; i < npx; ++i) {
+        const FLT t = (FLT)src[i] * gain + offset;
+        dst[i] = pc_chroma ? (t <= fFloor ? fFloor : t >= fCeil ? fCeil : t) : t;
+    }
+}
+
+/* RangeConvert back: clipped to [floor_, ceil_] after +0.5 (+0.499999 for
+ * full-range chroma), truncated. */
+static void FN(fl_to_int)(int *dst, const FLT *src, size_t npx, int floor_, int neutral, int ceil_)
+{
+    const int chroma = floor_ < neutral;
+    const int pc_chroma = chroma && (floor_ + ceil_) % 2 == 1;
+    const FLT fFloor = chroma ? (FLT)-0.5 : (FLT)0, fCeil = chroma ? (FLT)0.5 : (FLT)1;
+    const FLT fNeutral = 0;
+    const FLT sRange = fCeil - fFloor;
+    const int dRange = ceil_ - floor_;
+    const FLT gain = (FLT)dRange / sRange;
+    const FLT offset = -fNeutral * gain + (FLT)neutral + (pc_chroma ? (FLT)0.499999 : (FLT)0.5);
+    const FLT lo = (FLT)floor_, hi = (FLT)ceil_;
+    for (size_t i = 0; i < npx; ++i) {
+        const FLT t = src[i] * gain + offset;
+        dst[i] = (int)(t <= lo ? lo : t >= hi ? hi : t);
+    }
+}
+
+/* The guard of the stage-level integer and Frame paths
+ * (source/BM3D.cpp:250-256, 286-293): GroupSize == 1 (not 0) copies. */
+static int FN(int_path_rejected)(const oracle_stage_params *p, int nplanes)
+{
+    const int sig = nplanes == 1 ? p->sigma[0] > 0
+                                 : (p->sigma[0] > 0 || p->sigma[1] > 0 || p->sigma[2] > 0);
+    return !sig || p->group_size == 1 || p->block_size <= 0 || p->bm_range <= 0 ||
+           p->bm_range < p->bm_step || p->thMSE <= 0;
+}
+
+static FLT *FN(alloc)(size_t npx) { return (FLT *)malloc(sizeof(FLT) * (npx ? npx : 1)); }
+
+/* BM3D::process_Frame (source/BM3D.cpp:501-527): OPP RGB->YUV, three-plane
+ * basic then final (final in place on the YUV source), YUV->RGB. */
+int FN(oracle_bm3d_frame)(const oracle_stage_params *pb, const oracle_stage_params *pf,
+                          int *const dst[3], const int *const src[3], int width, int height,
+                          int floor_, int ceil_)
+{
+    const size_t npx = (size_t)width * height;
+    FLT *yuv[3], *tmp[3], *out[3];
+    for (int c = 0; c < 3; ++c) {
+        yuv[c] = FN(alloc)(npx);
+        tmp[c] = FN(alloc)(npx);
+        out[c] = FN(alloc)(npx);
+    }
+    FN(rgb_to_opp)(yuv, src, npx, floor_, ceil_, 0);
+    for (int c = 0; c < 3; ++c) {
+        memcpy(tmp[c], yuv[c], sizeof(FLT) * npx);
+        memcpy(out[c], yuv[c], sizeof(FLT) * npx);
+    }
+    const FLT *const yc[3] = {yuv[0], yuv[1], yuv[2]};
+    FN(oracle_bm3d_stage3)(0, pb, tmp, yc, yc, width, height, 1.0);
+    const FLT *const tc[3] = {tmp[0], tmp[1], tmp[2]};
+    FN(oracle_bm3d_stage3)(1, pf, out, yc, tc, width, height, 1.0);
+    FN(opp_to_rgb)(dst, (const FLT *const *)out, npx, floor_, ceil_);
+    for (int c = 0; c < 3; ++c) {
+        free(yuv[c]);
+        free(tmp[c]);
+        free(out[c]);
+    }
+    return 0;
+}
+
+/* BM3D_Base::process_Frame (source/BM3D.cpp:284-313): one stage on an RGB
+ * frame, in place on the YUV source; ref (or src when null) converted by
+ * the stage's RGB2YUV: Y only for the basic stage (320-336), all three
+ * planes for the final stage (392-408). */
+int FN(oracle_bm3d_stage_frame)(int wiener, const oracle_stage_params *p, int *const dst[3],
+                                const int *const src[3], const int *const ref[3], int width,
+                                int height, int floor_, int ceil_)
+{
+    const size_t npx = (size_t)width * height;
+    if (FN(int_path_rejected)(p, 3)) {
+        for (int c = 0; c < 3; ++c) memcpy(dst[c], src[c], sizeof(int) * npx);
+        return 2;
+    }
+    FLT *yuv[3], *ryuv[3] = {0, 0, 0}, *out[3];
+    for (int c = 0; c < 3; ++c) {
+        yuv[c] = FN(alloc)(npx);
+        out[c] = FN(alloc)(npx);
+    }
+    FN(rgb_to_opp)(yuv, src, npx, floor_, ceil_, 0);
+    const FLT *rc3[3] = {yuv[0], yuv[1], yuv[2]};
+    if (ref) {
+        for (int c = 0; c < (wiener ? 3 : 1); ++c) ryuv[c] = FN(alloc)(npx);
+        FN(rgb_to_opp)(ryuv, ref, npx, floor_, ceil_, !wiener);
+        for (int c = 0; c < 3; ++c) rc3[c] = ryuv[wiener ? c : 0];
+    }
+    for (int c = 0; c < 3; ++c) memcpy(out[c], yuv[c], sizeof(FLT) * npx);
+    const FLT *const yc[3] = {yuv[0], yuv[1], yuv[2]};
+    FN(oracle_bm3d_stage3)(wiener, p, out, yc, rc3, width, height, 1.0);
+    FN(opp_to_rgb)(dst, (const FLT *const *)out, npx, floor_, ceil_);
+    for (int c = 0; c < 3; ++c) {
+        free(yuv[c]);
+        free(out[c]);
+        free(ryuv[c]);
+    }
+    return 0;
+}
+
+/* Basic then final on an integer plane: BM3D::process_Plane
+ * (source/BM3D.cpp:475-497) with the basic estimate sized like the source
+ * (the reference's own process_Plane_FL passes a 0x0 one). */
+int FN(oracle_bm3d_plane_int)(const oracle_stage_params *pb, const oracle_stage_params *pf,
+                              int *dst, const int *src, int width, int height, int floor_,
+                              int neutral, int ceil_)
+{
+    const size_t npx = (size_t)width * height;
+    FLT *fsrc = FN(alloc)(npx), *ftmp = FN(alloc)(npx), *fdst = FN(alloc)(npx);
+    FN(int_to_fl)(fsrc, src, npx, floor_, neutral, ceil_);
+    FN(oracle_bm3d_stage)(0, pb, ftmp, fsrc, fsrc, width, height, 1.0);
+    FN(oracle_bm3d_stage)(1, pf, fdst, fsrc, ftmp, width, height, 1.0);
+    FN(fl_to_int)(dst, fdst, npx, floor_, neutral, ceil_);
+    free(fsrc);
+    free(ftmp);
+    free(fdst);
+    return 0;
+}
+
+/* BM3D_Base::process_Plane (source/BM3D.cpp:248-281): one stage on an
+ * integer plane; ref (or src when null) converted the same way. */
+int FN(oracle_bm3d_stage_int)(int wiener, const oracle_stage_params *p, int *dst, const int *src,
+                              const int *ref, int width, int height, int floor_, int neutral,
+                              int ceil_)
+{
+    const size_t npx = (size_t)width * height;
+    if (FN(int_path_rejected)(p, 1)) {
+        memcpy(dst, src, sizeof(int) * npx);
+        return 2;
+    }
+    FLT *fsrc = FN(alloc)(npx), *fref = fsrc, *fdst = FN(alloc)(npx);
+    FN(int_to_fl)(fsrc, src, npx, floor_, neutral, ceil_);
+    if (ref) {
+        fref = FN(alloc)(npx);
+        FN(int_to_fl)(fref, ref, npx, floor_, neutral, ceil_);
+    }
+    FN(oracle_bm3d_stage)(wiener, p, fdst, fsrc, fref, width, height, 1.0);
+    FN(fl_to_int)(dst, fdst, npx, floor_, neutral, ceil_);
+    if (fref != fsrc) free(fref);
+    free(fsrc);
+    free(fdst);
+    return 0;
+}
+
 #undef FN
 #undef CAT
 #undef CAT_

@@ -16,6 +16,7 @@
  * FLType is float when built with -D_CUDA_ and double otherwise
  * (include/Type.h:26-30). */
 #include "BM3D.h"
+#include "Conversion.hpp"
 
 #include <cstring>
 
@@ -207,6 +208,128 @@ long long ref_bm3d_groups(int wiener, const ref_stage_params *s, const FLType *r
     fill_para(p, s);
     BasicProbe probe(p);
     return dump_groups(probe, refP, max_refs, max_group, counts, pos_yx, keys);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+/* BM3D on an RGB Frame: FilterIF2::operator()(Frame) -> BM3D::process_Frame
+ * (source/BM3D.cpp:501-527): OPP RGB->YUV, three-plane basic then final,
+ * YUV->RGB with clipping. Planes are the reference's DType (int32) with the
+ * Frame's quantisation: bit depth `bits`, full (PC) range when `pc`. */
+int ref_bm3d_frame(const ref_stage_params *b, const ref_stage_params *f, int *const dst[3],
+                   const int *const src[3], int width, int height, int bits, int pc)
+{
+    Frame in(0, PixelType::RGB, width, height, bits, pc ? QuantRange::PC : QuantRange::TV);
+    const size_t n = sizeof(int) * (size_t)width * (size_t)height;
+    std::memcpy(in.R().data(), src[0], n);
+    std::memcpy(in.G().data(), src[1], n);
+    std::memcpy(in.B().data(), src[2], n);
+    BM3D_Para para("fast");
+    fill_para(para.basic, b);
+    fill_para(para.final, f);
+    BM3D filter(para);
+    Frame out = filter(in);
+    std::memcpy(dst[0], out.R().data(), n);
+    std::memcpy(dst[1], out.G().data(), n);
+    std::memcpy(dst[2], out.B().data(), n);
+    return 0;
+}
+
+/* BM3D (basic then final) on an integer Plane. BM3D::process_Plane
+ * (source/BM3D.cpp:475-497) converts with RangeConvert to a float plane of
+ * range 1 and back with clipping, but its process_Plane_FL (464-472) hands
+ * the basic stage a default-constructed 0x0 `tmp`, so the reference fails
+ * its size check there. This entry runs the same sequence from the
+ * reference's own pieces with `tmp` sized like the source, the evident
+ * intent. The plane's quantisation is (bits, floor, neutral, ceil);
+ * neutral > floor marks a chroma plane. */
+int ref_bm3d_plane_int(const ref_stage_params *b, const ref_stage_params *f, int *dst,
+                       const int *src, int width, int height, int bits, int floor_, int neutral,
+                       int ceil_)
+{
+    Plane in(0, width, height, bits, floor_, neutral, ceil_, TransferChar::linear, false);
+    std::memcpy(in.data(), src, sizeof(int) * (size_t)width * (size_t)height);
+    Plane out(in, false);
+    BM3D_Para para("fast");
+    fill_para(para.basic, b);
+    fill_para(para.final, f);
+    BM3D_Basic basic(para.basic);
+    BM3D_Final final(para.final);
+    Plane_FL dst_data(out, false);
+    Plane_FL src_data(in, false);
+    RangeConvert(src_data, in, false);
+    Plane_FL tmp(src_data, false);
+    basic.Kernel(tmp, src_data, src_data);
+    final.Kernel(dst_data, src_data, tmp);
+    RangeConvert(out, dst_data, true);
+    std::memcpy(dst, out.data(), sizeof(int) * (size_t)width * (size_t)height);
+    return 0;
+}
+
+/* One stage on an integer Plane: BM3D_Basic or BM3D_Final used as a filter,
+ * BM3D_Base::process_Plane (source/BM3D.cpp:248-281). `ref` may be null
+ * (ref = src). */
+int ref_bm3d_stage_int(int wiener, const ref_stage_params *p, int *dst, const int *src,
+                       const int *ref, int width, int height, int bits, int floor_, int neutral,
+                       int ceil_)
+{
+    const size_t n = sizeof(int) * (size_t)width * (size_t)height;
+    Plane in(0, width, height, bits, floor_, neutral, ceil_, TransferChar::linear, false);
+    std::memcpy(in.data(), src, n);
+    Plane rf(in, false);
+    if (ref) std::memcpy(rf.data(), ref, n);
+    BM3D_Para para("fast");
+    Plane out;
+    if (!wiener) {
+        fill_para(para.basic, p);
+        BM3D_Basic filt(para.basic);
+        out = ref ? filt(in, rf) : filt(in);
+    } else {
+        fill_para(para.final, p);
+        BM3D_Final filt(para.final);
+        out = ref ? filt(in, rf) : filt(in);
+    }
+    std::memcpy(dst, out.data(), n);
+    return 0;
+}
+
+/* One stage on an RGB Frame: BM3D_Basic or BM3D_Final used as a filter,
+ * BM3D_Base::process_Frame (source/BM3D.cpp:284-313) with the stage's
+ * RGB2YUV (320-336 basic: Y of ref only; 392-408 final: all of ref). `ref`
+ * may be null (ref = src). */
+int ref_bm3d_stage_frame(int wiener, const ref_stage_params *p, int *const dst[3],
+                         const int *const src[3], const int *const ref[3], int width, int height,
+                         int bits, int pc)
+{
+    const size_t n = sizeof(int) * (size_t)width * (size_t)height;
+    const QuantRange q = pc ? QuantRange::PC : QuantRange::TV;
+    Frame in(0, PixelType::RGB, width, height, bits, q);
+    Frame rf(0, PixelType::RGB, width, height, bits, q);
+    std::memcpy(in.R().data(), src[0], n);
+    std::memcpy(in.G().data(), src[1], n);
+    std::memcpy(in.B().data(), src[2], n);
+    if (ref) {
+        std::memcpy(rf.R().data(), ref[0], n);
+        std::memcpy(rf.G().data(), ref[1], n);
+        std::memcpy(rf.B().data(), ref[2], n);
+    }
+    BM3D_Para para("fast");
+    Frame out;
+    if (!wiener) {
+        fill_para(para.basic, p);
+        BM3D_Basic filt(para.basic);
+        out = ref ? filt(in, rf) : filt(in);
+    } else {
+        fill_para(para.final, p);
+        BM3D_Final filt(para.final);
+        out = ref ? filt(in, rf) : filt(in);
+    }
+    std::memcpy(dst[0], out.R().data(), n);
+    std::memcpy(dst[1], out.G().data(), n);
+    std::memcpy(dst[2], out.B().data(), n);
+    return 0;
 }
 
 }  // extern "C"
