@@ -23,6 +23,7 @@
 #define BM3D_B200_H_
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -119,6 +120,57 @@ int bm3d_full(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_pa
 int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *final_,
                float *const dst[3], const float *const src[3], int width, int height,
                size_t stride, float value_range, int mem, void *stream);
+
+/* ---- Integer planes and RGB frames ------------------------------------
+ * Planes of the reference's integer pixel type (DType = int32,
+ * include/Type.h:25) with its quantisation: Floor, Neutral and Ceil of the plane
+ * (include/Image_Type.h:77-79); Neutral > Floor marks a chroma plane. RGB
+ * planes have Neutral = Floor. `stride` is in pixels. The float working
+ * planes have the reference's default Plane_FL ranges (luma [0, 1], chroma
+ * [-0.5, 0.5]) and live in context scratch; the filtering itself is
+ * bm3d_stage / bm3d_stage3 / bm3d_full / bm3d_full3 on them. Returns the
+ * status codes of those calls; BM3D_ERR_INVALID also for ceil <= floor. */
+
+/* Basic then final on one integer plane: RangeConvert to float, the two
+ * stages, RangeConvert back clipped to [floor, ceil] (+0.5, or +0.499999 for
+ * full-range chroma, then truncation). Replaces BM3D::process_Plane
+ * (reference source/BM3D.cpp:475-497) through FilterIF2::operator()(Plane)
+ * (include/Filter.h:210-215), with the basic estimate sized from src (the
+ * reference's process_Plane_FL passes an empty plane there). */
+int bm3d_plane_int(bm3d_ctx *ctx, const bm3d_stage_params *basic,
+                   const bm3d_stage_params *final_, int32_t *dst, const int32_t *src, int width,
+                   int height, size_t stride, int floor_, int neutral, int ceil_, int mem,
+                   void *stream);
+
+/* One stage on one integer plane (ref may be NULL: ref = src). Replaces
+ * BM3D_Basic / BM3D_Final used as a filter on a Plane,
+ * BM3D_Base::process_Plane (reference source/BM3D.cpp:248-281), including
+ * its guard: sigma[0] <= 0, GroupSize == 1, BlockSize <= 0, BMrange <= 0,
+ * BMrange < BMstep or thMSE <= 0 copy src (BM3D_COPIED). */
+int bm3d_stage_int(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, int32_t *dst,
+                   const int32_t *src, const int32_t *ref, int width, int height, size_t stride,
+                   int floor_, int neutral, int ceil_, int mem, void *stream);
+
+/* Basic then final on an RGB frame (R, G, B planes with Floor floor_ and
+ * Ceil ceil_): OPP RGB->YUV (MatrixConvert_RGB2YUV, include/Conversion.hpp:
+ * 518-575), three-plane basic and final with groups matched on Y,
+ * YUV->RGB clipped to [floor_, ceil_] (MatrixConvert_YUV2RGB,
+ * include/Conversion.hpp:661-748). Replaces BM3D::process_Frame
+ * (reference source/BM3D.cpp:501-527) through FilterIF2::operator()(Frame). */
+int bm3d_frame(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *final_,
+               int32_t *const dst[3], const int32_t *const src[3], int width, int height,
+               size_t stride, int floor_, int ceil_, int mem, void *stream);
+
+/* One stage on an RGB frame (ref may be NULL: ref = src); the basic stage
+ * converts only Y of a distinct ref, the final stage all of it. Replaces
+ * BM3D_Basic / BM3D_Final used as a filter on a Frame,
+ * BM3D_Base::process_Frame (reference source/BM3D.cpp:284-313) with
+ * RGB2YUV (320-336, 392-408), including its guard (all sigma <= 0,
+ * GroupSize == 1, ... copy src: BM3D_COPIED). */
+int bm3d_stage_frame(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener,
+                     int32_t *const dst[3], const int32_t *const src[3],
+                     const int32_t *const ref[3], int width, int height, size_t stride,
+                     int floor_, int ceil_, int mem, void *stream);
 
 /* FP64 forms of bm3d_stage / bm3d_full: the same kernels instantiated for
  * double (the reference's FLType without _CUDA_, include/Type.h:26-30). */

@@ -39,7 +39,7 @@ EXPORTS = [
     "bm3d_full3", "bm3d_stage_f64", "bm3d_ref_block_count", "bm3d_debug_groups",
     "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
     "bm3d_stage_noalloc", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
-    "bm3d_batch_destroy",
+    "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
 ]
 
 
@@ -124,6 +124,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_batch_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     lib.bm3d_batch_destroy.argtypes = [vp]
     lib.bm3d_batch_destroy.restype = None
+    quant = [ip, ip, ctypes.c_size_t, ip, ip, ip, ip, vp]   # w, h, stride, floor, neutral, ceil, mem, stream
+    lib.bm3d_plane_int.argtypes = [vp, sp, sp, vp, vp] + quant
+    lib.bm3d_stage_int.argtypes = [vp, sp, ip, vp, vp, vp] + quant
+    rgb = [ip, ip, ctypes.c_size_t, ip, ip, ip, vp]         # w, h, stride, floor, ceil, mem, stream
+    lib.bm3d_frame.argtypes = [vp, sp, sp, vp, vp] + rgb
+    lib.bm3d_stage_frame.argtypes = [vp, sp, ip, vp, vp, vp] + rgb
     lib.bm3d_set_kernel_timing.argtypes = [vp, ip]
     lib.bm3d_kernel_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong)]
@@ -246,6 +252,59 @@ class Context:
                                  arr(*[i[0] for i in infos[0:3]]),
                                  arr(*[i[0] for i in infos[3:6]]), w, h, stride, value_range,
                                  mem, _stream_of(dst[0]))
+        return self._check(rc)
+
+    # -- integer planes and RGB frames (int32 numpy arrays or CUDA tensors) --
+
+    @staticmethod
+    def _int_planes(planes):
+        infos = [_plane_info(x) for x in planes]
+        if any(i[5] != "int32" for i in infos):
+            raise ValueError("integer paths take int32 planes")
+        w, h, stride, mem = infos[0][2], infos[0][3], infos[0][4], infos[0][1]
+        if any(i[1:5] != (mem, w, h, stride) for i in infos):
+            raise ValueError("planes must share memory kind, size and stride")
+        return [i[0] for i in infos], w, h, stride, mem
+
+    def plane_int(self, basic: StageParams, final: StageParams, dst, src, quant) -> int:
+        """Basic then final on an int32 plane quantised as quant = (floor, neutral, ceil)."""
+        (dp, spp), w, h, stride, mem = self._int_planes([dst, src])
+        lo, mid, hi = (int(v) for v in quant)
+        rc = self.lib.bm3d_plane_int(self.h, ctypes.byref(basic), ctypes.byref(final), dp, spp,
+                                     w, h, stride, lo, mid, hi, mem, _stream_of(dst))
+        return self._check(rc)
+
+    def stage_int(self, params: StageParams, wiener: bool, dst, src, ref=None,
+                  quant=(0, 0, 255)) -> int:
+        """One stage on an int32 plane (ref None = src)."""
+        planes = [dst, src] + ([] if ref is None else [ref])
+        ptrs, w, h, stride, mem = self._int_planes(planes)
+        lo, mid, hi = (int(v) for v in quant)
+        rc = self.lib.bm3d_stage_int(self.h, ctypes.byref(params), int(wiener), ptrs[0], ptrs[1],
+                                     ptrs[2] if ref is not None else None, w, h, stride, lo, mid,
+                                     hi, mem, _stream_of(dst))
+        return self._check(rc)
+
+    def frame(self, basic: StageParams, final: StageParams, dst, src, floor: int = 0,
+              ceil: int = 255) -> int:
+        """Basic then final on an RGB frame of three int32 planes (R, G, B)."""
+        ptrs, w, h, stride, mem = self._int_planes(list(dst) + list(src))
+        arr = ctypes.c_void_p * 3
+        rc = self.lib.bm3d_frame(self.h, ctypes.byref(basic), ctypes.byref(final),
+                                 arr(*ptrs[0:3]), arr(*ptrs[3:6]), w, h, stride, int(floor),
+                                 int(ceil), mem, _stream_of(dst[0]))
+        return self._check(rc)
+
+    def stage_frame(self, params: StageParams, wiener: bool, dst, src, ref=None, floor: int = 0,
+                    ceil: int = 255) -> int:
+        """One stage on an RGB frame (ref None = src)."""
+        planes = list(dst) + list(src) + ([] if ref is None else list(ref))
+        ptrs, w, h, stride, mem = self._int_planes(planes)
+        arr = ctypes.c_void_p * 3
+        rc = self.lib.bm3d_stage_frame(self.h, ctypes.byref(params), int(wiener), arr(*ptrs[0:3]),
+                                       arr(*ptrs[3:6]),
+                                       arr(*ptrs[6:9]) if ref is not None else None, w, h, stride,
+                                       int(floor), int(ceil), mem, _stream_of(dst[0]))
         return self._check(rc)
 
     def ref_block_count(self, params: StageParams, width: int, height: int) -> int:

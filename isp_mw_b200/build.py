@@ -1,6 +1,6 @@
 """Build the B200 BM3D library (``isp_mw_b200/lib/libisp_mw_b200.so``).
 
-nvcc compiles every ``csrc/*.cu`` for sm_100a only (``-gencode
+nvcc compiles every ``csrc/*.cu`` (in parallel, one process per unit) for sm_100a only (``-gencode
 arch=compute_100a,code=sm_100a``) and links one shared library exporting the C
 ABI declared in ``include/bm3d_b200.h``. The library is built in-tree so it
 ships with the repository snapshot; nothing is installed into site-packages.
@@ -11,6 +11,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -45,7 +46,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if not force and not ptxas_info and not _stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    objs = []
+    jobs = []
     for src in sources():
         obj = os.path.join(LIBDIR, os.path.basename(src)[:-3] + ".o")
         cmd = [NVCC] + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-I", CSRC,
@@ -54,8 +55,21 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             cmd += ["-Xptxas", "-v"]
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append((cmd, obj))
+    # one nvcc per translation unit, in parallel
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(workers) as pool:
+        results = list(pool.map(
+            lambda j: subprocess.run(j[0], stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                     text=True), jobs))
+    failed = False
+    for (cmd, _), r in zip(jobs, results):
+        if r.stdout and (verbose or ptxas_info or r.returncode != 0):
+            print(r.stdout, end="", flush=True)
+        failed |= r.returncode != 0
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc")
+    objs = [obj for _, obj in jobs]
     tmp = LIB + ".tmp"
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "--cudart", "static",
            "-o", tmp] + objs

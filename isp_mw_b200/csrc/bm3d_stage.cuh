@@ -15,12 +15,13 @@
 namespace bm3d {
 
 // Cosine matrices for group lengths 1..16 (row k = output k), concatenated;
-// entry n starts at c_dct_off[n]. Filled by the host when a context is made.
-__constant__ float c_dct_fwd_f[1496];
-__constant__ float c_dct_inv_f[1496];
-__constant__ double c_dct_fwd_d[1496];
-__constant__ double c_dct_inv_d[1496];
-__constant__ int c_dct_off[17];
+// entry n starts at c_dct_off[n]. Every translation unit that launches these
+// kernels has its own copy, filled by the host when a context is made.
+static __constant__ float c_dct_fwd_f[1496];
+static __constant__ float c_dct_inv_f[1496];
+static __constant__ double c_dct_fwd_d[1496];
+static __constant__ double c_dct_inv_d[1496];
+static __constant__ int c_dct_off[17];
 
 template <typename T> struct DctTab;
 template <> struct DctTab<float> {

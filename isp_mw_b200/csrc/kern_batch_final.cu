@@ -1,0 +1,11 @@
+// Persistent batched stage kernels, final stage: register-resident (KS = 4
+// and 1) and generic bodies.
+#include "kern_unit.cuh"
+
+BM3D_KERNEL_UNIT(batch_final)
+
+namespace bm3d {
+template const void *batch_kernel_fn<true, 4, false>();
+template const void *batch_kernel_fn<true, 1, false>();
+template const void *batch_kernel_fn<true, 1, true>();
+}  // namespace bm3d

@@ -75,3 +75,15 @@ def pair(height: int, width: int, sigma_255: float, seed: int):
 def psnr(a: np.ndarray, b: np.ndarray, peak: float = 1.0) -> float:
     mse = float(np.mean((np.asarray(a, np.float64) - np.asarray(b, np.float64)) ** 2))
     return float("inf") if mse == 0 else 10.0 * math.log10(peak * peak / mse)
+
+
+def int_planes(h: int, w: int, s255: float, seed: int, lo: int, hi: int, n: int):
+    """n seeded int32 planes: smooth content spanning [lo, hi] plus Gaussian
+    noise of sigma s255 / 255 of the range, rounded and clipped to [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n):
+        clean = clean_plane(h, w, seed * 7 + c)
+        v = lo + clean * (hi - lo) + rng.normal(0.0, s255 / 255.0 * (hi - lo), (h, w))
+        out.append(np.clip(np.round(v), lo, hi).astype(np.int32))
+    return out

@@ -48,6 +48,16 @@ CASES = [
 ]
 
 
+# (name, kind, height, width, sigma/255, bit depth, full range, chroma, seed)
+INT_CASES = [
+    ("int_rgb8_pc_48x56", "frame", 48, 56, 20.0, 8, True, False, 40),
+    ("int_rgb10_tv_41x37", "frame", 41, 37, 30.0, 10, False, False, 41),
+    ("int_y8_tv_44x60", "plane", 44, 60, 15.0, 8, False, False, 42),
+    ("int_c8_pc_40x52", "plane", 40, 52, 25.0, 8, True, True, 43),
+    ("int_y16_pc_36x40", "plane", 36, 40, 10.0, 16, True, False, 44),
+]
+
+
 def main():
     oracle.build(reference=True)
     ref = oracle.backend("reference", np.float32)
@@ -80,6 +90,28 @@ def main():
                         basic=np.stack(basic), final=np.stack(final),
                         params=json.dumps({"basic": b, "final": f, "profile": "fast"}))
     print("fast3_52x40")
+    # integer planes and RGB frames (int32, the reference's Plane / Frame)
+    for name, kind, h, w, s255, bits, pc, chroma, seed in INT_CASES:
+        b, f = params("fast", synth.sigma_param(s255))
+        if kind == "frame":
+            lo, hi = oracle.frame_range(bits, pc)
+            src = synth.int_planes(h, w, s255, seed, lo, hi, 3)
+            full = ref.frame(b, f, src, bits, pc)
+            basic = ref.stage_frame(False, b, src, None, bits, pc)
+            final = ref.stage_frame(True, f, src, basic, bits, pc)
+            quant = (lo, lo, hi)
+        else:
+            quant = oracle.plane_quant(bits, pc, chroma)
+            src = synth.int_planes(h, w, s255, seed, quant[0], quant[2], 1)
+            full = [ref.plane_int(b, f, src[0], quant, bits)]
+            basic = [ref.stage_int(False, b, src[0], None, quant, bits)]
+            final = [ref.stage_int(True, f, src[0], basic[0], quant, bits)]
+        np.savez_compressed(
+            os.path.join(HERE, name + ".npz"), src=np.stack(src), full=np.stack(full),
+            basic=np.stack(basic), final=np.stack(final), quant=np.array(quant, np.int32),
+            params=json.dumps({"basic": b, "final": f, "profile": "fast", "kind": kind,
+                               "bits": bits, "pc": pc}))
+        print(name, (h, w))
 
 
 if __name__ == "__main__":

@@ -14,6 +14,8 @@ import pytest
 from conftest import ROOT
 
 GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+INT_GOLDEN = [p for p in GOLDEN if os.path.basename(p).startswith("int_")]
+GOLDEN = [p for p in GOLDEN if p not in INT_GOLDEN]  # float planes
 
 
 def load(path):
@@ -106,3 +108,44 @@ def test_partial_sort_emulation_matches_libstdcxx(oracle_mod, std_sort):
         std_sort.std_partial_sort_f32(sk.ctypes.data_as(ctypes.c_void_p),
                                       sp.ctypes.data_as(ctypes.c_void_p), m, n)
         assert np.array_equal(ek[:m], sk[:m]) and np.array_equal(ep[:m], sp[:m]), trial
+
+
+@pytest.mark.parametrize("path", INT_GOLDEN, ids=lambda p: os.path.basename(p))
+def test_port_matches_golden_int(oracle_mod, path):
+    """Integer planes and RGB frames: the restatement against the reference's
+    BM3D on Plane / Frame (conversions, three stages' outputs), bit for bit."""
+    z, prm = load(path)
+    port = oracle_mod.backend("port", np.float32)
+    src = list(z["src"])
+    b, f = prm["basic"], prm["final"]
+    if prm["kind"] == "frame":
+        bits, pc = prm["bits"], prm["pc"]
+        assert np.array_equal(np.stack(port.frame(b, f, src, bits, pc)), z["full"])
+        basic = port.stage_frame(False, b, src, None, bits, pc)
+        assert np.array_equal(np.stack(basic), z["basic"])
+        final = port.stage_frame(True, f, src, list(z["basic"]), bits, pc)
+        assert np.array_equal(np.stack(final), z["final"])
+    else:
+        q = tuple(int(v) for v in z["quant"])
+        assert np.array_equal(port.plane_int(b, f, src[0], q), z["full"][0])
+        assert np.array_equal(port.stage_int(False, b, src[0], None, q), z["basic"][0])
+        assert np.array_equal(port.stage_int(True, f, src[0], z["basic"][0], q), z["final"][0])
+
+
+@pytest.mark.parametrize("group_size", [0, 1])
+def test_port_int_guards(oracle_mod, group_size):
+    """GroupSize 1 trips the integer / Frame filters' own guard (exact copy,
+    source/BM3D.cpp:250-256, 286-293); GroupSize 0 passes it and trips the
+    stage's (a conversion round trip, source/BM3D.cpp:82-87)."""
+    z, prm = load(os.path.join(ROOT, "tests", "golden", "int_rgb8_pc_48x56.npz"))
+    ref = oracle_mod.backend("reference" if oracle_mod.reference_available() else "port")
+    port = oracle_mod.backend("port")
+    b = dict(prm["basic"], group_size=group_size)
+    src = list(z["src"])
+    got = port.stage_frame(False, b, src)
+    assert np.array_equal(np.stack(got), np.stack(ref.stage_frame(False, b, src)))
+    q = (0, 0, 255)
+    assert np.array_equal(port.stage_int(False, b, src[0], None, q),
+                          ref.stage_int(False, b, src[0], None, q))
+    if group_size == 1:
+        assert np.array_equal(np.stack(got), z["src"])
