@@ -46,6 +46,7 @@ template <typename T> struct BatchPlane {
     T *dst;
     long long src_stride, dst_stride;
     int width, height;
+    int block_size;
     float *absmax;
 };
 
@@ -73,16 +74,18 @@ __global__ void prep_batch_kernel(const BatchPlane<T> *planes)
         atomicMax(reinterpret_cast<int *>(q.absmax), __float_as_int(fminf(m, 3.0e38f)));
 }
 
-// dst = num / den for every plane (grid.y = plane).
+// dst = num / den for every plane (grid.y = plane); each CTA walks the
+// plane's 32 x 32 tiles from blockIdx.x in steps of gridDim.x.
 template <typename T>
-__global__ void normalize_batch_kernel(const BatchPlane<T> *planes)
+__global__ void __launch_bounds__(256) normalize_batch_kernel(const BatchPlane<T> *planes)
 {
     const BatchPlane<T> q = planes[blockIdx.y];
-    const long long n = static_cast<long long>(q.width) * q.height;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long y = i / q.width, x = i - y * q.width;
-        q.dst[y * q.dst_stride + x] = ratio(q.num[i], q.den[i]);
+    const int tx = (q.width + kNormTile - 1) / kNormTile;
+    const int ntiles = tx * ((q.height + kNormTile - 1) / kNormTile);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int ty = tile / tx, txi = tile - ty * tx;
+        normalize_tile<T>(q.dst, q.dst_stride, q.num, q.den, q.width, q.height, q.block_size,
+                          ty * kNormTile, txi * kNormTile);
     }
 }
 

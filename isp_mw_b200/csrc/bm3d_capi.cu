@@ -615,8 +615,9 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
     if (bm_only) return BM3D_OK;
     for (int c = 0; c < nplanes; ++c) {
         if (!(a.active & (1 << c))) continue;
-        normalize_kernel<T><<<blocks, threads, 0, s>>>(dst[c], static_cast<long long>(stride),
-                                                       a.num[c], a.den[c], width, height);
+        const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
+        normalize_kernel<T><<<ngrid, 256, 0, s>>>(dst[c], static_cast<long long>(stride), a.num[c],
+                                                  a.den[c], width, height, a.block_size);
         CK(ctx, cudaGetLastError());
     }
     return BM3D_OK;
@@ -1472,7 +1473,9 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("prep_kernel", e);
     rc = launch_stage(&info, a, wiener != 0, 1, s, warps);
     if (rc != BM3D_OK) return rc;
-    normalize_kernel<float><<<blocks, threads, 0, s>>>(dst, a.stride, num, den, width, height);
+    const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
+    normalize_kernel<float><<<ngrid, 256, 0, s>>>(dst, a.stride, num, den, width, height,
+                                                  a.block_size);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("normalize_kernel", e);
     return BM3D_OK;
 }
@@ -1622,7 +1625,8 @@ int launch_planes(bm3d_batch *B, const DevBuf &planes, int count, bool prep, cud
     if (count == 0) return BM3D_OK;
     long long maxpx = 0;
     for (int i = 0; i < B->n; ++i) maxpx = std::max(maxpx, static_cast<long long>(B->w[i]) * B->h[i]);
-    const dim3 grid(static_cast<unsigned>(std::min<long long>((maxpx + 255) / 256, 64)),
+    const long long tiles = (maxpx + kNormTile * kNormTile - 1) / (kNormTile * kNormTile);
+    const dim3 grid(static_cast<unsigned>(std::min<long long>(prep ? (maxpx + 255) / 256 : tiles, 64)),
                     static_cast<unsigned>(count));
     const auto *q = static_cast<const BatchPlane<float> *>(planes.ptr);
     if (prep) prep_batch_kernel<float><<<grid, 256, 0, s>>>(q);
@@ -1798,6 +1802,7 @@ extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_para
             bp.dst_stride = static_cast<long long>(stride[i]);
             bp.width = width[i];
             bp.height = height[i];
+            bp.block_size = st ? final_[i].block_size : basic[i].block_size;
             bp.absmax = static_cast<float *>(B->absmax.ptr) + i;
             q.push_back(bp);
         }

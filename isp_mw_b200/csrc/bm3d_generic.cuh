@@ -163,15 +163,15 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
     __syncwarp();
     dct3_generic(Gs, n, bs, lane, a.dct_inv);
+    // the block weight once per block, at its origin (as the register-resident kernel)
     for (int e = lane; e < total; e += kWarp) {
         const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
         const BlockPos q = list[z];
         if (!block_in_tile(t, q.y, q.x)) continue;
         int pitch;
         auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
-        auto *dd = block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch);
         acc_add(dn + y * pitch + x, Gs[e] * numW, scale);
-        acc_add(dd + y * pitch + x, denW, scale);
+        if (rem == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
     }
     __syncwarp();
 }

@@ -33,18 +33,148 @@ template <> struct DctTab<double> {
     static __device__ __forceinline__ const double *inv() { return c_dct_inv_d; }
 };
 
-template <typename T>
-__device__ __forceinline__ void zdct_fwd(T (&a)[kGSMax], int n)
+// Transforms along the group axis for two pencils at once. Lengths 8 and 16
+// use the butterflies of dct.cuh. Every other length N has its own
+// instantiation, so each cosine is read from the constant bank at a
+// compile-time offset (an instruction operand, no load), and the symmetries
+// of the cosine matrices halve the multiplies:
+//   REDFT10: C[k][N-1-j] = (-1)^k C[k][j] -> sums (even k) and differences
+//            (odd k) of mirrored inputs;
+//   REDFT01: C[N-1-k][j] = (-1)^j C[k][j] -> even and odd input halves give
+//            outputs k and N-1-k together.
+template <typename T, int N>
+__device__ __forceinline__ void zfwd_n(T (&a)[kGSMax], T (&b)[kGSMax])
 {
-    if (n == 16) redft10_16(a);
-    else dct_matrix<T, kGSMax>(a, n, DctTab<T>::fwd() + c_dct_off[n]);
+    constexpr int H = N / 2, O = (N - 1) * N * (2 * N - 1) / 6;
+    const T *M = DctTab<T>::fwd() + O;
+    T ua[H + 1], va[H + 1], ub[H + 1], vb[H + 1];
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        ua[j] = a[j] + a[N - 1 - j];
+        va[j] = a[j] - a[N - 1 - j];
+        ub[j] = b[j] + b[N - 1 - j];
+        vb[j] = b[j] - b[N - 1 - j];
+    }
+    ua[H] = (N & 1) ? a[H] : T(0);
+    ub[H] = (N & 1) ? b[H] : T(0);
+    T ya[N], yb[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        T sa = T(0), sb = T(0);
+        if ((k & 1) == 0) {
+#pragma unroll
+            for (int j = 0; j < H + (N & 1); ++j) {
+                sa += M[k * N + j] * ua[j];
+                sb += M[k * N + j] * ub[j];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < H; ++j) {
+                sa += M[k * N + j] * va[j];
+                sb += M[k * N + j] * vb[j];
+            }
+        }
+        ya[k] = sa;
+        yb[k] = sb;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        a[k] = ya[k];
+        b[k] = yb[k];
+    }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void zinv_n(T (&a)[kGSMax], T (&b)[kGSMax])
+{
+    constexpr int O = (N - 1) * N * (2 * N - 1) / 6;
+    const T *M = DctTab<T>::inv() + O;
+    T ya[N], yb[N];
+#pragma unroll
+    for (int k = 0; k < (N + 1) / 2; ++k) {
+        T ea = T(0), oa = T(0), eb = T(0), ob = T(0);
+#pragma unroll
+        for (int j = 0; j < N; j += 2) {
+            ea += M[k * N + j] * a[j];
+            eb += M[k * N + j] * b[j];
+        }
+#pragma unroll
+        for (int j = 1; j < N; j += 2) {
+            oa += M[k * N + j] * a[j];
+            ob += M[k * N + j] * b[j];
+        }
+        ya[k] = ea + oa;
+        yb[k] = eb + ob;
+        if (N - 1 - k != k) {
+            ya[N - 1 - k] = ea - oa;
+            yb[N - 1 - k] = eb - ob;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        a[k] = ya[k];
+        b[k] = yb[k];
+    }
 }
 
 template <typename T>
-__device__ __forceinline__ void zdct_inv(T (&a)[kGSMax], int n)
+__device__ __forceinline__ void zbfly8(T (&a)[kGSMax], bool inverse)
 {
-    if (n == 16) redft01_16(a);
-    else dct_matrix<T, kGSMax>(a, n, DctTab<T>::inv() + c_dct_off[n]);
+    T t[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) t[i] = a[i];
+    if (inverse) redft01_8(t);
+    else redft10_8(t);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) a[i] = t[i];
+}
+
+// Forward (REDFT10) transform of two pencils of length n <= 16.
+template <typename T>
+__device__ __forceinline__ void zdct_fwd2(T (&a)[kGSMax], T (&b)[kGSMax], int n)
+{
+    switch (n) {
+    case 16: redft10_16(a); redft10_16(b); break;
+    case 8: zbfly8(a, false); zbfly8(b, false); break;
+    case 1: zfwd_n<T, 1>(a, b); break;
+    case 2: zfwd_n<T, 2>(a, b); break;
+    case 3: zfwd_n<T, 3>(a, b); break;
+    case 4: zfwd_n<T, 4>(a, b); break;
+    case 5: zfwd_n<T, 5>(a, b); break;
+    case 6: zfwd_n<T, 6>(a, b); break;
+    case 7: zfwd_n<T, 7>(a, b); break;
+    case 9: zfwd_n<T, 9>(a, b); break;
+    case 10: zfwd_n<T, 10>(a, b); break;
+    case 11: zfwd_n<T, 11>(a, b); break;
+    case 12: zfwd_n<T, 12>(a, b); break;
+    case 13: zfwd_n<T, 13>(a, b); break;
+    case 14: zfwd_n<T, 14>(a, b); break;
+    default: zfwd_n<T, 15>(a, b); break;
+    }
+}
+
+// Backward (REDFT01) transform of two pencils of length n <= 16.
+template <typename T>
+__device__ __forceinline__ void zdct_inv2(T (&a)[kGSMax], T (&b)[kGSMax], int n)
+{
+    switch (n) {
+    case 16: redft01_16(a); redft01_16(b); break;
+    case 8: zbfly8(a, true); zbfly8(b, true); break;
+    case 1: zinv_n<T, 1>(a, b); break;
+    case 2: zinv_n<T, 2>(a, b); break;
+    case 3: zinv_n<T, 3>(a, b); break;
+    case 4: zinv_n<T, 4>(a, b); break;
+    case 5: zinv_n<T, 5>(a, b); break;
+    case 6: zinv_n<T, 6>(a, b); break;
+    case 7: zinv_n<T, 7>(a, b); break;
+    case 9: zinv_n<T, 9>(a, b); break;
+    case 10: zinv_n<T, 10>(a, b); break;
+    case 11: zinv_n<T, 11>(a, b); break;
+    case 12: zinv_n<T, 12>(a, b); break;
+    case 13: zinv_n<T, 13>(a, b); break;
+    case 14: zinv_n<T, 14>(a, b); break;
+    default: zinv_n<T, 15>(a, b); break;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -553,14 +683,12 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
     if (WIENER) {
         gather_xy_forward(t, t.refw[p], t.ref0[p], list, n, lane, G, n_bad);
         load_pencils(G, n, lane, ra, rb);
-        zdct_fwd(ra, n);
-        zdct_fwd(rb, n);
+        zdct_fwd2(ra, rb, n);
         __syncwarp();
     }
     gather_xy_forward(t, t.srcw[p], t.src0[p], list, n, lane, G, n_bad);
     load_pencils(G, n, lane, sa, sb);
-    zdct_fwd(sa, n);
-    zdct_fwd(sb, n);
+    zdct_fwd2(sa, sb, n);
 
     T denW;
     if (!WIENER) {
@@ -602,29 +730,27 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
     }
     const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
 
-    zdct_inv(sa, n);
-    zdct_inv(sb, n);
+    zdct_inv2(sa, sb, n);
     __syncwarp();
     store_pencils(G, n, lane, sa, sb);
     __syncwarp();
     T v[4][8];
     xy_inverse(G, n, lane, v);
 
-    // Aggregation: BlockGroup::AddTo / CountTo (include/Block.h:1240-1265, 1334-1357).
+    // Aggregation: BlockGroup::AddTo / CountTo (include/Block.h:1240-1265,
+    // 1334-1357). The weight is the same over the block, so it is added once,
+    // at the block's origin; the normalisation sums origins over each pixel's
+    // covering blocks. Integer sums make that exactly the per-pixel sum.
     const int z = lane >> 1, h = lane & 1;
     if (z < n && block_in_tile(t, list[z].y, list[z].x)) {
         const BlockPos q = list[z];
         int pitch;
         auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
-        auto *dd = block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch);
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int x = 0; x < 8; ++x) {
-                const int o = (4 * h + r) * pitch + x;
-                acc_add(dn + o, v[r][x] * numW, scale);
-                acc_add(dd + o, denW, scale);
-            }
+            for (int x = 0; x < 8; ++x) acc_add(dn + (4 * h + r) * pitch + x, v[r][x] * numW, scale);
+        if (h == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
     }
     __syncwarp();
 }
@@ -756,22 +882,18 @@ __device__ __forceinline__ void flush_tile(const StageArgs<T> &a, const Tile<T> 
         for (int i = tid; i < npx; i += blockDim.x) {
             const int y = i / t.rw, x = i - y * t.rw;
             const int s = y * t.pitch + x;
-            const auto d = t.accD[p][s];
-            if (d != 0) {
-                const long long g = static_cast<long long>(t.ry0 + y) * a.width + (t.rx0 + x);
-                acc_flush(a.num[p] + g, t.accN[p][s]);
-                acc_flush(a.den[p] + g, d);
-            }
+            const auto nv = t.accN[p][s], d = t.accD[p][s];
+            const long long g = static_cast<long long>(t.ry0 + y) * a.width + (t.rx0 + x);
+            if (nv != 0) acc_flush(a.num[p] + g, nv);
+            if (d != 0) acc_flush(a.den[p] + g, d);
         }
         if (!t.origin_inside) {
             for (int i = tid; i < bsq; i += blockDim.x) {
-                const auto d = t.accD0[p][i];
-                if (d != 0) {
-                    const int y = i / bs, x = i - y * bs;
-                    const long long g = static_cast<long long>(y) * a.width + x;
-                    acc_flush(a.num[p] + g, t.accN0[p][i]);
-                    acc_flush(a.den[p] + g, d);
-                }
+                const auto nv = t.accN0[p][i], d = t.accD0[p][i];
+                const int y = i / bs, x = i - y * bs;
+                const long long g = static_cast<long long>(y) * a.width + x;
+                if (nv != 0) acc_flush(a.num[p] + g, nv);
+                if (d != 0) acc_flush(a.den[p] + g, d);
             }
         }
     }
@@ -873,17 +995,58 @@ __device__ __forceinline__ float ratio(long long n, long long d)
 }
 __device__ __forceinline__ double ratio(double n, double d) { return n / d; }
 
+// Tile of the normalisation: 32 x 32 pixels per CTA.
+constexpr int kNormTile = 32;
+
+// dst = num / den for the kNormTile^2 pixels at (y0, x0), with den(y, x) the
+// sum of the block weights W at the bs x bs origins whose block covers
+// (y, x): y - bs < oy <= y, x - bs < ox <= x. Separable sums over a
+// shared-memory copy of W; exact for integer sums.
 template <typename T>
-__global__ void normalize_kernel(T *dst, long long dst_stride,
-                                 const typename AccOf<T>::type *num,
-                                 const typename AccOf<T>::type *den, int width, int height)
+__device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
+                                               const typename AccOf<T>::type *num,
+                                               const typename AccOf<T>::type *wsum, int width,
+                                               int height, int bs, int y0, int x0)
 {
-    const long long n = static_cast<long long>(width) * height;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long y = i / width, x = i - y * width;
-        dst[y * dst_stride + x] = ratio(num[i], den[i]);
+    using Acc = typename AccOf<T>::type;
+    constexpr int N = kNormTile, E = N + kBSMax - 1;
+    __shared__ Acc w[E][E];
+    __shared__ Acc hs[E][N];
+    const int ext = N + bs - 1;
+    for (int i = threadIdx.x; i < ext * ext; i += blockDim.x) {
+        const int ly = i / ext, lx = i - ly * ext;
+        const int gy = y0 - bs + 1 + ly, gx = x0 - bs + 1 + lx;
+        w[ly][lx] = (gy >= 0 && gx >= 0 && gy < height && gx < width)
+                        ? wsum[static_cast<long long>(gy) * width + gx]
+                        : Acc(0);
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ext * N; i += blockDim.x) {
+        const int ly = i / N, lx = i - ly * N;
+        Acc v = 0;
+        for (int d = 0; d < bs; ++d) v += w[ly][lx + d];
+        hs[ly][lx] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
+        const int ly = i / N, lx = i - ly * N;
+        const int gy = y0 + ly, gx = x0 + lx;
+        if (gy >= height || gx >= width) continue;
+        Acc d = 0;
+        for (int k = 0; k < bs; ++k) d += hs[ly + k][lx];
+        dst[gy * dst_stride + gx] = ratio(num[static_cast<long long>(gy) * width + gx], d);
+    }
+    __syncthreads();  // before the next tile overwrites w / hs
+}
+
+// One plane: grid = (ceil(width / 32), ceil(height / 32)) CTAs.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    normalize_kernel(T *dst, long long dst_stride, const typename AccOf<T>::type *num,
+                     const typename AccOf<T>::type *wsum, int width, int height, int bs)
+{
+    normalize_tile<T>(dst, dst_stride, num, wsum, width, height, bs, blockIdx.y * kNormTile,
+                      blockIdx.x * kNormTile);
 }
 
 // Zero one plane's accumulators and fold max |src| into *absmax (which the
