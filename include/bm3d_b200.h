@@ -108,18 +108,21 @@ int bm3d_stage3(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, floa
                 const float *const src[3], const float *const ref[3], int width, int height,
                 size_t stride, float value_range, int mem, void *stream);
 
-/* Basic then final on one plane, the basic estimate held in context scratch.
- * Replaces BM3D::process_Plane_FL (reference source/BM3D.cpp:464-472) with
- * the intermediate sized from src (the reference passes an empty plane there). */
+/* Basic then final on one plane, the basic estimate held in context scratch:
+ * basic = stage(src, ref), dst = final(src, basic). `ref` may be NULL
+ * (ref = src). Replaces BM3D::process(dst, src[, ref]) on Plane_FL,
+ * BM3D::process_Plane_FL (reference source/BM3D.cpp:464-472), with the
+ * intermediate sized from src (the reference passes an empty plane there). */
 int bm3d_full(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *final_,
-              float *dst, const float *src, int width, int height, size_t stride,
-              float value_range, int mem, void *stream);
+              float *dst, const float *src, const float *ref, int width, int height,
+              size_t stride, float value_range, int mem, void *stream);
 
 /* Three-plane basic then final (reference BM3D::process_Frame's YUV core,
- * source/BM3D.cpp:512-521). */
+ * source/BM3D.cpp:512-521); the basic stage matches on ref[0] (ref may be
+ * NULL: ref = src). */
 int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *final_,
-               float *const dst[3], const float *const src[3], int width, int height,
-               size_t stride, float value_range, int mem, void *stream);
+               float *const dst[3], const float *const src[3], const float *const ref[3],
+               int width, int height, size_t stride, float value_range, int mem, void *stream);
 
 /* ---- Integer planes and RGB frames ------------------------------------
  * Planes of the reference's integer pixel type (DType = int32,
@@ -136,11 +139,12 @@ int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_p
  * full-range chroma, then truncation). Replaces BM3D::process_Plane
  * (reference source/BM3D.cpp:475-497) through FilterIF2::operator()(Plane)
  * (include/Filter.h:210-215), with the basic estimate sized from src (the
- * reference's process_Plane_FL passes an empty plane there). */
+ * reference's process_Plane_FL passes an empty plane there). `ref` may be
+ * NULL (ref = src); the basic stage matches on it. */
 int bm3d_plane_int(bm3d_ctx *ctx, const bm3d_stage_params *basic,
-                   const bm3d_stage_params *final_, int32_t *dst, const int32_t *src, int width,
-                   int height, size_t stride, int floor_, int neutral, int ceil_, int mem,
-                   void *stream);
+                   const bm3d_stage_params *final_, int32_t *dst, const int32_t *src,
+                   const int32_t *ref, int width, int height, size_t stride, int floor_,
+                   int neutral, int ceil_, int mem, void *stream);
 
 /* One stage on one integer plane (ref may be NULL: ref = src). Replaces
  * BM3D_Basic / BM3D_Final used as a filter on a Plane,
@@ -155,11 +159,14 @@ int bm3d_stage_int(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener, i
  * Ceil ceil_): OPP RGB->YUV (MatrixConvert_RGB2YUV, include/Conversion.hpp:
  * 518-575), three-plane basic and final with groups matched on Y,
  * YUV->RGB clipped to [floor_, ceil_] (MatrixConvert_YUV2RGB,
- * include/Conversion.hpp:661-748). Replaces BM3D::process_Frame
- * (reference source/BM3D.cpp:501-527) through FilterIF2::operator()(Frame). */
+ * include/Conversion.hpp:661-748). `ref` may be NULL (ref = src); a
+ * distinct ref frame contributes only its Y, on which the basic stage matches
+ * (BM3D_Basic::RGB2YUV, source/BM3D.cpp:320-336). Replaces BM3D::process_Frame
+ * (reference source/BM3D.cpp:501-527) through FilterIF2::operator()(Frame[, ref]). */
 int bm3d_frame(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *final_,
-               int32_t *const dst[3], const int32_t *const src[3], int width, int height,
-               size_t stride, int floor_, int ceil_, int mem, void *stream);
+               int32_t *const dst[3], const int32_t *const src[3], const int32_t *const ref[3],
+               int width, int height, size_t stride, int floor_, int ceil_, int mem,
+               void *stream);
 
 /* One stage on an RGB frame (ref may be NULL: ref = src); the basic stage
  * converts only Y of a distinct ref, the final stage all of it. Replaces

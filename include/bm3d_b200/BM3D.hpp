@@ -16,9 +16,12 @@
 //   - Errors throw bm3d_b200::Error instead of exiting the process.
 //   - BM3D::process(dst, src) sizes its intermediate from src (the reference's
 //     BM3D::process_Plane_FL passes an empty plane, source/BM3D.cpp:464-472).
-//   - Frame / int Plane / RGB<->OPP conversion are not provided.
+//   - Plane (int32) and Frame are minimal: size, quantisation (Floor, Neutral,
+//     Ceil, bit depth) and data; a Frame here is always RGB, the only kind the
+//     reference's BM3D::process_Frame handles (source/BM3D.cpp:501-527).
 #pragma once
 
+#include <cstdint>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -106,6 +109,103 @@ private:
     PCType w_ = 0, h_ = 0;
     value_type floor_ = 0, neutral_ = 0, ceil_ = 1;
     std::vector<value_type> data_;
+};
+
+// Minimal counterpart of the reference's integer Plane (include/Image_Type.h:
+// 46-173): row-major int32 (DType), stride = width, with its quantisation.
+// Default quantisation: full range of `bits` (include/Image_Type.hpp:94-109);
+// chroma planes have Neutral = 2^(bits-1).
+class Plane {
+public:
+    typedef int32_t value_type;
+
+    Plane() {}
+    explicit Plane(value_type value, PCType width = 1920, PCType height = 1080,
+                   value_type bits = 16, bool init = true)
+        : w_(width), h_(height), bits_(bits), ceil_((1 << bits) - 1),
+          data_(static_cast<size_t>(width) * height)
+    {
+        if (init) for (auto &x : data_) x = value;
+    }
+    Plane(value_type value, PCType width, PCType height, value_type bits, value_type floor,
+          value_type neutral, value_type ceil, bool init = true)
+        : w_(width), h_(height), bits_(bits), floor_(floor), neutral_(neutral), ceil_(ceil),
+          data_(static_cast<size_t>(width) * height)
+    {
+        if (init) for (auto &x : data_) x = value;
+    }
+    // Same size and quantisation as src (include/Image_Type.h:95).
+    Plane(const Plane &src, bool init, value_type value = 0)
+        : w_(src.w_), h_(src.h_), bits_(src.bits_), floor_(src.floor_), neutral_(src.neutral_),
+          ceil_(src.ceil_), data_(src.data_.size())
+    {
+        if (init) for (auto &x : data_) x = value;
+    }
+    Plane(const Plane &) = default;
+    Plane(Plane &&) = default;
+    Plane &operator=(const Plane &) = default;
+    Plane &operator=(Plane &&) = default;
+
+    PCType Width() const { return w_; }
+    PCType Height() const { return h_; }
+    PCType Stride() const { return w_; }
+    PCType PixelCount() const { return w_ * h_; }
+    value_type BitDepth() const { return bits_; }
+    value_type Floor() const { return floor_; }
+    value_type Neutral() const { return neutral_; }
+    value_type Ceil() const { return ceil_; }
+    value_type ValueRange() const { return ceil_ - floor_; }
+    bool isChroma() const { return floor_ < neutral_; }
+    value_type *data() { return data_.data(); }
+    const value_type *data() const { return data_.data(); }
+    value_type &operator[](PCType i) { return data_[i]; }
+    const value_type &operator[](PCType i) const { return data_[i]; }
+    value_type &operator()(PCType j, PCType i) { return data_[static_cast<size_t>(j) * w_ + i]; }
+    const value_type &operator()(PCType j, PCType i) const
+    {
+        return data_[static_cast<size_t>(j) * w_ + i];
+    }
+
+private:
+    PCType w_ = 0, h_ = 0;
+    value_type bits_ = 16, floor_ = 0, neutral_ = 0, ceil_ = 65535;
+    std::vector<value_type> data_;
+};
+
+// Minimal RGB Frame (include/Image_Type.h:294-420 with PixelType::RGB): three
+// Planes of one quantisation; full range (PC) or limited range (TV,
+// [16, 235] << (bits - 8)) as Quantize_Value gives RGB planes.
+class Frame {
+public:
+    Frame() {}
+    Frame(int32_t value, PCType width, PCType height, int32_t bits = 8, bool full_range = true)
+    {
+        const int32_t lo = full_range ? 0 : 16 << (bits - 8);
+        const int32_t hi = full_range ? (1 << bits) - 1 : 235 << (bits - 8);
+        for (auto &p : p_) p = Plane(value, width, height, bits, lo, lo, hi);
+    }
+    Frame(const Frame &src, bool init, int32_t value = 0)
+    {
+        for (int i = 0; i < 3; ++i) p_[i] = Plane(src.p_[i], init, value);
+    }
+    Frame(const Frame &) = default;
+    Frame(Frame &&) = default;
+    Frame &operator=(const Frame &) = default;
+    Frame &operator=(Frame &&) = default;
+
+    Plane &R() { return p_[0]; }
+    Plane &G() { return p_[1]; }
+    Plane &B() { return p_[2]; }
+    const Plane &R() const { return p_[0]; }
+    const Plane &G() const { return p_[1]; }
+    const Plane &B() const { return p_[2]; }
+    Plane &P(int i) { return p_[i]; }
+    const Plane &P(int i) const { return p_[i]; }
+    PCType Width() const { return p_[0].Width(); }
+    PCType Height() const { return p_[0].Height(); }
+
+private:
+    Plane p_[3];
 };
 
 // Shared device context: one per process and device, created on first use.
@@ -237,6 +337,54 @@ public:
         return process(dst, src, src);
     }
 
+    // Integer plane: BM3D_Base::process_Plane (source/BM3D.cpp:248-281).
+    Plane &process(Plane &dst, const Plane &src, const Plane &ref)
+    {
+        if (dst.Width() != src.Width() || dst.Height() != src.Height()) dst = Plane(src, false);
+        bm3d_ctx *c = ctx();
+        check(c, bm3d_stage_int(c, &para_, wiener_, dst.data(), src.data(),
+                                &ref == &src ? nullptr : ref.data(), src.Width(), src.Height(),
+                                static_cast<size_t>(src.Stride()), src.Floor(), src.Neutral(),
+                                src.Ceil(), BM3D_MEM_HOST, nullptr));
+        return dst;
+    }
+    Plane &process(Plane &dst, const Plane &src) { return process(dst, src, src); }
+    Plane operator()(const Plane &src, const Plane &ref)
+    {
+        Plane dst(src, false);
+        return process(dst, src, ref);
+    }
+    Plane operator()(const Plane &src)
+    {
+        Plane dst(src, false);
+        return process(dst, src, src);
+    }
+
+    // RGB frame: BM3D_Base::process_Frame (source/BM3D.cpp:284-313).
+    Frame &process(Frame &dst, const Frame &src, const Frame &ref)
+    {
+        if (dst.Width() != src.Width() || dst.Height() != src.Height()) dst = Frame(src, false);
+        int32_t *d[3] = {dst.R().data(), dst.G().data(), dst.B().data()};
+        const int32_t *s[3] = {src.R().data(), src.G().data(), src.B().data()};
+        const int32_t *r[3] = {ref.R().data(), ref.G().data(), ref.B().data()};
+        bm3d_ctx *c = ctx();
+        check(c, bm3d_stage_frame(c, &para_, wiener_, d, s, r, src.Width(), src.Height(),
+                                  static_cast<size_t>(src.R().Stride()), src.R().Floor(),
+                                  src.R().Ceil(), BM3D_MEM_HOST, nullptr));
+        return dst;
+    }
+    Frame &process(Frame &dst, const Frame &src) { return process(dst, src, src); }
+    Frame operator()(const Frame &src, const Frame &ref)
+    {
+        Frame dst(src, false);
+        return process(dst, src, ref);
+    }
+    Frame operator()(const Frame &src)
+    {
+        Frame dst(src, false);
+        return process(dst, src, src);
+    }
+
     // Three planes sharing luma groups: BM3D_Base::Kernel's 9-plane form
     // (source/BM3D.cpp:139-218).
     void Kernel(Plane_FL &dstY, Plane_FL &dstU, Plane_FL &dstV, const Plane_FL &srcY,
@@ -280,23 +428,79 @@ public:
         : basic_(para.basic.to_c()), final_(para.final.to_c()), ctx_(ctx)
     {}
 
-    Plane_FL &process(Plane_FL &dst, const Plane_FL &src)
+    // BM3D::process_Plane_FL (source/BM3D.cpp:464-472); the basic stage matches on ref.
+    Plane_FL &process(Plane_FL &dst, const Plane_FL &src, const Plane_FL &ref)
     {
         if (dst.Width() != src.Width() || dst.Height() != src.Height())
             dst.ReSize(src.Width(), src.Height());
-        bm3d_ctx *c = ctx_ ? ctx_ : default_context();
-        check(c, bm3d_full(c, &basic_, &final_, dst.data(), src.data(), src.Width(), src.Height(),
-                           static_cast<size_t>(src.Stride()), src.ValueRange(), BM3D_MEM_HOST,
-                           nullptr));
+        bm3d_ctx *c = ctx();
+        check(c, bm3d_full(c, &basic_, &final_, dst.data(), src.data(), ref.data(), src.Width(),
+                           src.Height(), static_cast<size_t>(src.Stride()), src.ValueRange(),
+                           BM3D_MEM_HOST, nullptr));
         return dst;
+    }
+    Plane_FL &process(Plane_FL &dst, const Plane_FL &src) { return process(dst, src, src); }
+    Plane_FL operator()(const Plane_FL &src, const Plane_FL &ref)
+    {
+        Plane_FL dst(src, false);
+        return process(dst, src, ref);
     }
     Plane_FL operator()(const Plane_FL &src)
     {
         Plane_FL dst(src, false);
-        return process(dst, src);
+        return process(dst, src, src);
+    }
+
+    // BM3D::process_Plane (source/BM3D.cpp:475-497).
+    Plane &process(Plane &dst, const Plane &src, const Plane &ref)
+    {
+        if (dst.Width() != src.Width() || dst.Height() != src.Height()) dst = Plane(src, false);
+        bm3d_ctx *c = ctx();
+        check(c, bm3d_plane_int(c, &basic_, &final_, dst.data(), src.data(),
+                                &ref == &src ? nullptr : ref.data(), src.Width(), src.Height(),
+                                static_cast<size_t>(src.Stride()), src.Floor(), src.Neutral(),
+                                src.Ceil(), BM3D_MEM_HOST, nullptr));
+        return dst;
+    }
+    Plane &process(Plane &dst, const Plane &src) { return process(dst, src, src); }
+    Plane operator()(const Plane &src, const Plane &ref)
+    {
+        Plane dst(src, false);
+        return process(dst, src, ref);
+    }
+    Plane operator()(const Plane &src)
+    {
+        Plane dst(src, false);
+        return process(dst, src, src);
+    }
+
+    // BM3D::process_Frame (source/BM3D.cpp:501-527).
+    Frame &process(Frame &dst, const Frame &src, const Frame &ref)
+    {
+        if (dst.Width() != src.Width() || dst.Height() != src.Height()) dst = Frame(src, false);
+        int32_t *d[3] = {dst.R().data(), dst.G().data(), dst.B().data()};
+        const int32_t *s[3] = {src.R().data(), src.G().data(), src.B().data()};
+        const int32_t *r[3] = {ref.R().data(), ref.G().data(), ref.B().data()};
+        bm3d_ctx *c = ctx();
+        check(c, bm3d_frame(c, &basic_, &final_, d, s, r, src.Width(), src.Height(),
+                            static_cast<size_t>(src.R().Stride()), src.R().Floor(),
+                            src.R().Ceil(), BM3D_MEM_HOST, nullptr));
+        return dst;
+    }
+    Frame &process(Frame &dst, const Frame &src) { return process(dst, src, src); }
+    Frame operator()(const Frame &src, const Frame &ref)
+    {
+        Frame dst(src, false);
+        return process(dst, src, ref);
+    }
+    Frame operator()(const Frame &src)
+    {
+        Frame dst(src, false);
+        return process(dst, src, src);
     }
 
 private:
+    bm3d_ctx *ctx() { return ctx_ ? ctx_ : default_context(); }
     bm3d_stage_params basic_, final_;
     bm3d_ctx *ctx_;
 };
@@ -312,6 +516,8 @@ using bm3d_b200::BM3D_Final_Para;
 using bm3d_b200::BM3D_Para;
 using bm3d_b200::BM3D_Para_Base;
 using bm3d_b200::FLType;
+using bm3d_b200::Frame;
 using bm3d_b200::PCType;
+using bm3d_b200::Plane;
 using bm3d_b200::Plane_FL;
 #endif

@@ -106,8 +106,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     plane = [ip, ip, ctypes.c_size_t, ctypes.c_float, ip, vp]
     lib.bm3d_stage.argtypes = [vp, sp, ip, vp, vp, vp] + plane
     lib.bm3d_stage3.argtypes = [vp, sp, ip, vp, vp, vp] + plane
-    lib.bm3d_full.argtypes = [vp, sp, sp, vp, vp] + plane
-    lib.bm3d_full3.argtypes = [vp, sp, sp, vp, vp] + plane
+    lib.bm3d_full.argtypes = [vp, sp, sp, vp, vp, vp] + plane
+    lib.bm3d_full3.argtypes = [vp, sp, sp, vp, vp, vp] + plane
     lib.bm3d_stage_f64.argtypes = [vp, sp, ip, vp, vp, vp, ip, ip, ctypes.c_size_t,
                                    ctypes.c_double, ip, vp]
     lib.bm3d_ref_block_count.argtypes = [sp, ip, ip]
@@ -125,10 +125,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_batch_destroy.argtypes = [vp]
     lib.bm3d_batch_destroy.restype = None
     quant = [ip, ip, ctypes.c_size_t, ip, ip, ip, ip, vp]   # w, h, stride, floor, neutral, ceil, mem, stream
-    lib.bm3d_plane_int.argtypes = [vp, sp, sp, vp, vp] + quant
+    lib.bm3d_plane_int.argtypes = [vp, sp, sp, vp, vp, vp] + quant
     lib.bm3d_stage_int.argtypes = [vp, sp, ip, vp, vp, vp] + quant
     rgb = [ip, ip, ctypes.c_size_t, ip, ip, ip, vp]         # w, h, stride, floor, ceil, mem, stream
-    lib.bm3d_frame.argtypes = [vp, sp, sp, vp, vp] + rgb
+    lib.bm3d_frame.argtypes = [vp, sp, sp, vp, vp, vp] + rgb
     lib.bm3d_stage_frame.argtypes = [vp, sp, ip, vp, vp, vp] + rgb
     lib.bm3d_set_kernel_timing.argtypes = [vp, ip]
     lib.bm3d_kernel_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
@@ -236,22 +236,26 @@ class Context:
         return self._check(rc)
 
     def full(self, basic: StageParams, final: StageParams, dst, src,
-             value_range: float = 1.0) -> int:
+             value_range: float = 1.0, ref=None) -> int:
+        """Basic (matching on ref, default src) then final (``bm3d_full``)."""
         dp, mem, w, h, stride, _ = _plane_info(dst)
         spp, *_ = _plane_info(src)
-        rc = self.lib.bm3d_full(self.h, ctypes.byref(basic), ctypes.byref(final), dp, spp, w, h,
-                                stride, value_range, mem, _stream_of(dst))
+        rp = None if ref is None else _plane_info(ref)[0]
+        rc = self.lib.bm3d_full(self.h, ctypes.byref(basic), ctypes.byref(final), dp, spp, rp, w,
+                                h, stride, value_range, mem, _stream_of(dst))
         return self._check(rc)
 
     def full3(self, basic: StageParams, final: StageParams, dst, src,
-              value_range: float = 1.0) -> int:
-        infos = [_plane_info(x) for x in list(dst) + list(src)]
+              value_range: float = 1.0, ref=None) -> int:
+        planes = list(dst) + list(src) + ([] if ref is None else list(ref))
+        infos = [_plane_info(x) for x in planes]
         w, h, stride, mem = infos[0][2], infos[0][3], infos[0][4], infos[0][1]
         arr = ctypes.c_void_p * 3
         rc = self.lib.bm3d_full3(self.h, ctypes.byref(basic), ctypes.byref(final),
                                  arr(*[i[0] for i in infos[0:3]]),
-                                 arr(*[i[0] for i in infos[3:6]]), w, h, stride, value_range,
-                                 mem, _stream_of(dst[0]))
+                                 arr(*[i[0] for i in infos[3:6]]),
+                                 None if ref is None else arr(*[i[0] for i in infos[6:9]]), w, h,
+                                 stride, value_range, mem, _stream_of(dst[0]))
         return self._check(rc)
 
     # -- integer planes and RGB frames (int32 numpy arrays or CUDA tensors) --
@@ -266,12 +270,14 @@ class Context:
             raise ValueError("planes must share memory kind, size and stride")
         return [i[0] for i in infos], w, h, stride, mem
 
-    def plane_int(self, basic: StageParams, final: StageParams, dst, src, quant) -> int:
+    def plane_int(self, basic: StageParams, final: StageParams, dst, src, quant,
+                  ref=None) -> int:
         """Basic then final on an int32 plane quantised as quant = (floor, neutral, ceil)."""
-        (dp, spp), w, h, stride, mem = self._int_planes([dst, src])
+        ptrs, w, h, stride, mem = self._int_planes([dst, src] + ([] if ref is None else [ref]))
         lo, mid, hi = (int(v) for v in quant)
-        rc = self.lib.bm3d_plane_int(self.h, ctypes.byref(basic), ctypes.byref(final), dp, spp,
-                                     w, h, stride, lo, mid, hi, mem, _stream_of(dst))
+        rc = self.lib.bm3d_plane_int(self.h, ctypes.byref(basic), ctypes.byref(final), ptrs[0],
+                                     ptrs[1], ptrs[2] if ref is not None else None, w, h, stride,
+                                     lo, mid, hi, mem, _stream_of(dst))
         return self._check(rc)
 
     def stage_int(self, params: StageParams, wiener: bool, dst, src, ref=None,
@@ -286,13 +292,15 @@ class Context:
         return self._check(rc)
 
     def frame(self, basic: StageParams, final: StageParams, dst, src, floor: int = 0,
-              ceil: int = 255) -> int:
+              ceil: int = 255, ref=None) -> int:
         """Basic then final on an RGB frame of three int32 planes (R, G, B)."""
-        ptrs, w, h, stride, mem = self._int_planes(list(dst) + list(src))
+        planes = list(dst) + list(src) + ([] if ref is None else list(ref))
+        ptrs, w, h, stride, mem = self._int_planes(planes)
         arr = ctypes.c_void_p * 3
         rc = self.lib.bm3d_frame(self.h, ctypes.byref(basic), ctypes.byref(final),
-                                 arr(*ptrs[0:3]), arr(*ptrs[3:6]), w, h, stride, int(floor),
-                                 int(ceil), mem, _stream_of(dst[0]))
+                                 arr(*ptrs[0:3]), arr(*ptrs[3:6]),
+                                 arr(*ptrs[6:9]) if ref is not None else None, w, h, stride,
+                                 int(floor), int(ceil), mem, _stream_of(dst[0]))
         return self._check(rc)
 
     def stage_frame(self, params: StageParams, wiener: bool, dst, src, ref=None, floor: int = 0,
@@ -511,17 +519,18 @@ class BM3D:
         self.para = para if para is not None else BM3D_Para()
         self.ctx = ctx
 
-    def process(self, dst, src, value_range: float = 1.0):
+    def process(self, dst, src, ref=None, value_range: float = 1.0):
+        """FilterIF2::process(dst, src[, ref]): the basic stage matches on ref."""
         ctx = self.ctx or default_context()
         if isinstance(src, (list, tuple)):
-            ctx.full3(self.para.basic.to_c(), self.para.final.to_c(), dst, src, value_range)
+            ctx.full3(self.para.basic.to_c(), self.para.final.to_c(), dst, src, value_range, ref)
         else:
-            ctx.full(self.para.basic.to_c(), self.para.final.to_c(), dst, src, value_range)
+            ctx.full(self.para.basic.to_c(), self.para.final.to_c(), dst, src, value_range, ref)
         return dst
 
-    def __call__(self, src, value_range: float = 1.0):
+    def __call__(self, src, ref=None, value_range: float = 1.0):
         if isinstance(src, (list, tuple)):
             dst = [s.copy() if isinstance(s, np.ndarray) else s.clone() for s in src]
         else:
             dst = _empty_like(src)
-        return self.process(dst, src, value_range)
+        return self.process(dst, src, ref, value_range)

@@ -18,6 +18,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libisp_mw_b200.so")
+CLI = os.path.join(LIBDIR, "isp_mw")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 NVCC_FLAGS = [
@@ -33,11 +34,13 @@ def sources():
 
 
 def _stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(CLI):
         return True
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(LIB), os.path.getmtime(CLI))
     deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(
-        os.path.join(ROOT, "include", "*.h"))
+        os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h")) + glob.glob(
+        os.path.join(ROOT, "include", "bm3d_b200", "*.hpp")) + glob.glob(
+        os.path.join(PKG, "cli", "*.cpp"))
     return any(os.path.getmtime(d) > t for d in deps)
 
 
@@ -77,7 +80,19 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     os.replace(tmp, LIB)
     for o in objs:
         os.remove(o)
+    build_cli(verbose)
     return LIB
+
+
+def build_cli(verbose: bool = False) -> str:
+    """The command-line front end (``lib/isp_mw``), linked against the library."""
+    src = os.path.join(PKG, "cli", "isp_mw.cpp")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), src,
+           "-L", LIBDIR, "-lisp_mw_b200", "-Wl,-rpath,$ORIGIN", "-o", CLI]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return CLI
 
 
 if __name__ == "__main__":

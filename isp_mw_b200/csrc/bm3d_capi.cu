@@ -758,8 +758,9 @@ extern "C" int bm3d_stage3(bm3d_ctx *ctx, const bm3d_stage_params *params, int w
 
 template <typename T>
 static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *fin,
-                    int nplanes, T *const dst[], const T *const src[], int width, int height,
-                    size_t stride, double value_range, int mem, void *stream)
+                    int nplanes, T *const dst[], const T *const src[], const T *const ref[],
+                    int width, int height, size_t stride, double value_range, int mem,
+                    void *stream)
 {
     if (!ctx || !basic || !fin) return BM3D_ERR_INVALID;
     if (mem != BM3D_MEM_HOST && mem != BM3D_MEM_DEVICE) return BM3D_ERR_INVALID;
@@ -773,12 +774,14 @@ static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_st
     const size_t dpitch = mem == BM3D_MEM_HOST ? static_cast<size_t>(width) : stride;
     // Device-resident src and dst (context staging in host mode) and the basic
     // estimate, all with row pitch dpitch.
-    const T *ds[kMaxPlanes];
+    const T *ds[kMaxPlanes], *dr[kMaxPlanes];
     T *tmp[kMaxPlanes], *dd[kMaxPlanes];
     for (int c = 0; c < nplanes; ++c) {
         if ((rc = ensure(ctx, ctx->basic[c], sizeof(T) * dpitch * height)) != BM3D_OK) return rc;
         tmp[c] = static_cast<T *>(ctx->basic[c].ptr);
     }
+    // a distinct ref (the basic stage matches on it; src when absent)
+    const bool own_ref = ref != nullptr && ref[0] != nullptr && ref[0] != src[0];
     if (mem == BM3D_MEM_HOST) {
         for (int c = 0; c < nplanes; ++c) {
             if ((rc = ensure(ctx, ctx->stage_in[c], plane_bytes)) != BM3D_OK) return rc;
@@ -788,13 +791,24 @@ static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_st
                                  cudaMemcpyHostToDevice, s)) != BM3D_OK)
                 return rc;
             ds[c] = in;
+            dr[c] = in;
             dd[c] = static_cast<T *>(ctx->stage_out[c].ptr);
+        }
+        if (own_ref) {
+            if ((rc = ensure(ctx, ctx->stage_ref[0], plane_bytes)) != BM3D_OK) return rc;
+            T *r = static_cast<T *>(ctx->stage_ref[0].ptr);
+            if ((rc = copy_plane(ctx, r, width, ref[0], stride, width, height,
+                                 cudaMemcpyHostToDevice, s)) != BM3D_OK)
+                return rc;
+            dr[0] = r;
         }
     } else {
         for (int c = 0; c < nplanes; ++c) {
             ds[c] = src[c];
+            dr[c] = src[c];
             dd[c] = dst[c];
         }
+        if (own_ref) dr[0] = ref[0];
     }
     // Planes a stage does not filter (sigma <= 0), or a stage whose parameters
     // the reference's guard rejects, pass src through: the basic estimate and
@@ -817,7 +831,7 @@ static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_st
             return BM3D_ERR_UNSUPPORTED;
         }
         if (g == Guard::Run) {
-            rc = run_stage_device(ctx, basic, false, nplanes, tmp, ds, ds, width, height, dpitch,
+            rc = run_stage_device(ctx, basic, false, nplanes, tmp, ds, dr, width, height, dpitch,
                                   value_range, s);
             if (rc != BM3D_OK) return rc;
         }
@@ -849,23 +863,24 @@ static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_st
 }
 
 extern "C" int bm3d_full(bm3d_ctx *ctx, const bm3d_stage_params *basic,
-                         const bm3d_stage_params *final_, float *dst, const float *src, int width,
-                         int height, size_t stride, float value_range, int mem, void *stream)
+                         const bm3d_stage_params *final_, float *dst, const float *src,
+                         const float *ref, int width, int height, size_t stride,
+                         float value_range, int mem, void *stream)
 {
     float *d[1] = {dst};
-    const float *s[1] = {src};
-    return full_any<float>(ctx, basic, final_, 1, d, s, width, height, stride, value_range, mem,
-                           stream);
+    const float *s[1] = {src}, *r[1] = {ref};
+    return full_any<float>(ctx, basic, final_, 1, d, s, r, width, height, stride, value_range,
+                           mem, stream);
 }
 
 extern "C" int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic,
                           const bm3d_stage_params *final_, float *const dst[3],
-                          const float *const src[3], int width, int height, size_t stride,
-                          float value_range, int mem, void *stream)
+                          const float *const src[3], const float *const ref[3], int width,
+                          int height, size_t stride, float value_range, int mem, void *stream)
 {
     if (!dst || !src) return BM3D_ERR_INVALID;
-    return full_any<float>(ctx, basic, final_, 3, dst, src, width, height, stride, value_range,
-                           mem, stream);
+    return full_any<float>(ctx, basic, final_, 3, dst, src, ref, width, height, stride,
+                           value_range, mem, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -1144,8 +1159,8 @@ extern "C" int bm3d_stage_int(bm3d_ctx *ctx, const bm3d_stage_params *params, in
 
 extern "C" int bm3d_plane_int(bm3d_ctx *ctx, const bm3d_stage_params *basic,
                               const bm3d_stage_params *final_, int32_t *dst, const int32_t *src,
-                              int width, int height, size_t stride, int floor_, int neutral,
-                              int ceil_, int mem, void *stream)
+                              const int32_t *ref, int width, int height, size_t stride,
+                              int floor_, int neutral, int ceil_, int mem, void *stream)
 {
     const void *d[1] = {dst}, *sp[1] = {src};
     const bm3d_stage_params *ps[2] = {basic, final_};
@@ -1157,19 +1172,27 @@ extern "C" int bm3d_plane_int(bm3d_ctx *ctx, const bm3d_stage_params *basic,
     int *dd[1] = {dst};
     const int *ss[1] = {src};
     const Quant q{floor_, neutral, ceil_};
+    const int *rr[1] = {ref && ref != src ? ref : nullptr};
     IntPlanes io;
-    if ((rc = stage_ints_in(ctx, 1, ss, nullptr, width, height, stride, mem, s, io)) != BM3D_OK)
+    if ((rc = stage_ints_in(ctx, 1, ss, rr, width, height, stride, mem, s, io)) != BM3D_OK)
         return rc;
     if ((rc = int_outputs(ctx, 1, dd, width, height, mem, io)) != BM3D_OK) return rc;
-    float *fs[1], *fd[1];
+    float *fs[1], *fd[1], *fr[1];
     if ((rc = conv_planes(ctx, 0, 1, width, height, fs)) != BM3D_OK) return rc;
     if ((rc = conv_planes(ctx, 2, 1, width, height, fd)) != BM3D_OK) return rc;
     const dim3 grid = convert_grid(ctx, width, height);
-    int_to_float_kernel<<<grid, 256, 0, s>>>(io.src[0], io.pitch, fs[0], width, width, height,
-                                             range_to_float(q));
+    const RangeMap in = range_to_float(q);
+    int_to_float_kernel<<<grid, 256, 0, s>>>(io.src[0], io.pitch, fs[0], width, width, height, in);
     CK(ctx, cudaGetLastError());
-    const float *cs[1] = {fs[0]};
-    const int st = full_any<float>(ctx, basic, final_, 1, fd, cs, width, height, width, 1.0,
+    fr[0] = fs[0];
+    if (io.ref[0]) {
+        if ((rc = conv_planes(ctx, 1, 1, width, height, fr)) != BM3D_OK) return rc;
+        int_to_float_kernel<<<grid, 256, 0, s>>>(io.ref[0], io.pitch, fr[0], width, width, height,
+                                                 in);
+        CK(ctx, cudaGetLastError());
+    }
+    const float *cs[1] = {fs[0]}, *cr[1] = {fr[0]};
+    const int st = full_any<float>(ctx, basic, final_, 1, fd, cs, cr, width, height, width, 1.0,
                                    BM3D_MEM_DEVICE, stream);
     if (st < 0) return st;
     float_to_int_kernel<<<grid, 256, 0, s>>>(fd[0], width, io.dst[0], io.pitch, width, height,
@@ -1180,21 +1203,26 @@ extern "C" int bm3d_plane_int(bm3d_ctx *ctx, const bm3d_stage_params *basic,
 
 extern "C" int bm3d_frame(bm3d_ctx *ctx, const bm3d_stage_params *basic,
                           const bm3d_stage_params *final_, int32_t *const dst[3],
-                          const int32_t *const src[3], int width, int height, size_t stride,
-                          int floor_, int ceil_, int mem, void *stream)
+                          const int32_t *const src[3], const int32_t *const ref[3], int width,
+                          int height, size_t stride, int floor_, int ceil_, int mem,
+                          void *stream)
 {
     if (!dst || !src) return BM3D_ERR_INVALID;
     const void *d[3] = {dst[0], dst[1], dst[2]}, *sp[3] = {src[0], src[1], src[2]};
     const bm3d_stage_params *ps[2] = {basic, final_};
     int rc = check_int_call(ctx, 3, d, sp, width, height, stride, floor_, ceil_, mem, ps, 2);
     if (rc != BM3D_OK) return rc;
+    if (ref && (!ref[0] || !ref[1] || !ref[2])) return BM3D_ERR_INVALID;
     CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // a distinct ref frame (the reference compares the three plane pointers)
+    const bool own_ref = ref && !(ref[0] == src[0] && ref[1] == src[1] && ref[2] == src[2]);
     IntPlanes io;
-    if ((rc = stage_ints_in(ctx, 3, src, nullptr, width, height, stride, mem, s, io)) != BM3D_OK)
+    if ((rc = stage_ints_in(ctx, 3, src, own_ref ? ref : nullptr, width, height, stride, mem, s,
+                            io)) != BM3D_OK)
         return rc;
     if ((rc = int_outputs(ctx, 3, dst, width, height, mem, io)) != BM3D_OK) return rc;
-    float *fs[3], *fd[3];
+    float *fs[3], *fd[3], *fr[1];
     if ((rc = conv_planes(ctx, 0, 3, width, height, fs)) != BM3D_OK) return rc;
     if ((rc = conv_planes(ctx, 2, 3, width, height, fd)) != BM3D_OK) return rc;
     const dim3 grid = convert_grid(ctx, width, height);
@@ -1202,8 +1230,16 @@ extern "C" int bm3d_frame(bm3d_ctx *ctx, const bm3d_stage_params *basic,
                                            fs[2], width, width, height, opp_forward(floor_, ceil_),
                                            0);
     CK(ctx, cudaGetLastError());
-    const float *cs[3] = {fs[0], fs[1], fs[2]};
-    const int st = full_any<float>(ctx, basic, final_, 3, fd, cs, width, height, width, 1.0,
+    fr[0] = fs[0];
+    if (own_ref) {  // only Y of ref (BM3D_Basic::RGB2YUV, source/BM3D.cpp:333)
+        if ((rc = conv_planes(ctx, 1, 1, width, height, fr)) != BM3D_OK) return rc;
+        rgb_to_opp_kernel<<<grid, 256, 0, s>>>(io.ref[0], io.ref[1], io.ref[2], io.pitch, fr[0],
+                                               fr[0], fr[0], width, width, height,
+                                               opp_forward(floor_, ceil_), 1);
+        CK(ctx, cudaGetLastError());
+    }
+    const float *cs[3] = {fs[0], fs[1], fs[2]}, *cr[3] = {fr[0], fs[1], fs[2]};
+    const int st = full_any<float>(ctx, basic, final_, 3, fd, cs, cr, width, height, width, 1.0,
                                    BM3D_MEM_DEVICE, stream);
     if (st < 0) return st;
     opp_to_rgb_kernel<<<grid, 256, 0, s>>>(fd[0], fd[1], fd[2], width, io.dst[0], io.dst[1],

@@ -175,10 +175,12 @@ class _Backend:
         return counts, pos, keys
 
     def frame(self, basic: dict, final: dict, rgb: Sequence[np.ndarray], bits: int = 8,
-              pc: bool = True):
+              pc: bool = True, ref=None):
         """BM3D on an RGB frame of int32 planes (bit depth `bits`, full or
-        limited range): OPP conversion, basic, final, conversion back."""
+        limited range): OPP conversion, basic (matching on ref's Y when
+        given), final, conversion back."""
         src = [np.ascontiguousarray(c, dtype=np.int32) for c in rgb]
+        rf = None if ref is None else [np.ascontiguousarray(c, dtype=np.int32) for c in ref]
         h, w = src[0].shape
         dst = [np.empty_like(c) for c in src]
         arr = ctypes.c_void_p * 3
@@ -188,20 +190,24 @@ class _Backend:
         else:
             tail = frame_range(bits, pc)
         rc = self._frame(ctypes.byref(pb), ctypes.byref(pf), arr(*[d.ctypes.data for d in dst]),
-                         arr(*[c.ctypes.data for c in src]), w, h, *tail)
+                         arr(*[c.ctypes.data for c in src]),
+                         None if rf is None else arr(*[c.ctypes.data for c in rf]), w, h, *tail)
         if rc != 0:
             raise RuntimeError(f"frame: {rc}")
         return dst
 
-    def plane_int(self, basic: dict, final: dict, src: np.ndarray, quant, bits: int = 8):
+    def plane_int(self, basic: dict, final: dict, src: np.ndarray, quant, bits: int = 8,
+                  ref=None):
         """BM3D on an int32 plane quantised as quant = (floor, neutral, ceil)."""
         src = np.ascontiguousarray(src, dtype=np.int32)
+        rp = None if ref is None else np.ascontiguousarray(ref, dtype=np.int32)
         h, w = src.shape
         dst = np.empty_like(src)
         q = tuple(int(v) for v in quant)
         tail = ((int(bits),) if self.kind == "reference" else ()) + q
         pb, pf = make_params(basic), make_params(final)
-        rc = self._plane_int(ctypes.byref(pb), ctypes.byref(pf), _ptr(dst), _ptr(src), w, h, *tail)
+        rc = self._plane_int(ctypes.byref(pb), ctypes.byref(pf), _ptr(dst), _ptr(src),
+                             None if rp is None else _ptr(rp), w, h, *tail)
         if rc != 0:
             raise RuntimeError(f"plane_int: {rc}")
         return dst

@@ -47,19 +47,19 @@ long long oracle_bm3d_groups_f64(int wiener, const oracle_stage_params *p, const
 
 /* BM3D::process_Frame on int32 RGB planes with the given Floor / Ceil. */
 int oracle_bm3d_frame_f32(const oracle_stage_params *pb, const oracle_stage_params *pf,
-                          int *const dst[3], const int *const src[3], int width, int height,
-                          int floor_, int ceil_);
+                          int *const dst[3], const int *const src[3], const int *const ref[3],
+                          int width, int height, int floor_, int ceil_);
 int oracle_bm3d_frame_f64(const oracle_stage_params *pb, const oracle_stage_params *pf,
-                          int *const dst[3], const int *const src[3], int width, int height,
-                          int floor_, int ceil_);
+                          int *const dst[3], const int *const src[3], const int *const ref[3],
+                          int width, int height, int floor_, int ceil_);
 
 /* BM3D::process_Plane on an int32 plane quantised as (floor, neutral, ceil). */
 int oracle_bm3d_plane_int_f32(const oracle_stage_params *pb, const oracle_stage_params *pf,
-                              int *dst, const int *src, int width, int height, int floor_,
-                              int neutral, int ceil_);
+                              int *dst, const int *src, const int *ref, int width, int height,
+                              int floor_, int neutral, int ceil_);
 int oracle_bm3d_plane_int_f64(const oracle_stage_params *pb, const oracle_stage_params *pf,
-                              int *dst, const int *src, int width, int height, int floor_,
-                              int neutral, int ceil_);
+                              int *dst, const int *src, const int *ref, int width, int height,
+                              int floor_, int neutral, int ceil_);
 
 /* One stage on an RGB frame (ref may be null) / an integer plane. */
 int oracle_bm3d_stage_frame_f32(int wiener, const oracle_stage_params *p, int *const dst[3],

@@ -548,13 +548,14 @@ static int FN(int_path_rejected)(const oracle_stage_params *p, int nplanes)
 static FLT *FN(alloc)(size_t npx) { return (FLT *)malloc(sizeof(FLT) * (npx ? npx : 1)); }
 
 /* BM3D::process_Frame (source/BM3D.cpp:501-527): OPP RGB->YUV, three-plane
- * basic then final (final in place on the YUV source), YUV->RGB. */
+ * basic then final (final in place on the YUV source), YUV->RGB; a ref frame
+ * (may be null) gives the basic stage its Y to match on. */
 int FN(oracle_bm3d_frame)(const oracle_stage_params *pb, const oracle_stage_params *pf,
-                          int *const dst[3], const int *const src[3], int width, int height,
-                          int floor_, int ceil_)
+                          int *const dst[3], const int *const src[3], const int *const ref[3],
+                          int width, int height, int floor_, int ceil_)
 {
     const size_t npx = (size_t)width * height;
-    FLT *yuv[3], *tmp[3], *out[3];
+    FLT *yuv[3], *tmp[3], *out[3], *ry[1] = {0};
     for (int c = 0; c < 3; ++c) {
         yuv[c] = FN(alloc)(npx);
         tmp[c] = FN(alloc)(npx);
@@ -566,7 +567,13 @@ int FN(oracle_bm3d_frame)(const oracle_stage_params *pb, const oracle_stage_para
         memcpy(out[c], yuv[c], sizeof(FLT) * npx);
     }
     const FLT *const yc[3] = {yuv[0], yuv[1], yuv[2]};
-    FN(oracle_bm3d_stage3)(0, pb, tmp, yc, yc, width, height, 1.0);
+    const FLT *rc3[3] = {yuv[0], yuv[1], yuv[2]};
+    if (ref) {  /* BM3D_Basic::RGB2YUV: only Y of ref (source/BM3D.cpp:333) */
+        ry[0] = FN(alloc)(npx);
+        FN(rgb_to_opp)(ry, ref, npx, floor_, ceil_, 1);
+        rc3[0] = ry[0];
+    }
+    FN(oracle_bm3d_stage3)(0, pb, tmp, yc, rc3, width, height, 1.0);
     const FLT *const tc[3] = {tmp[0], tmp[1], tmp[2]};
     FN(oracle_bm3d_stage3)(1, pf, out, yc, tc, width, height, 1.0);
     FN(opp_to_rgb)(dst, (const FLT *const *)out, npx, floor_, ceil_);
@@ -575,6 +582,7 @@ int FN(oracle_bm3d_frame)(const oracle_stage_params *pb, const oracle_stage_para
         free(tmp[c]);
         free(out[c]);
     }
+    free(ry[0]);
     return 0;
 }
 
@@ -617,15 +625,21 @@ int FN(oracle_bm3d_stage_frame)(int wiener, const oracle_stage_params *p, int *c
 
 /* Basic then final on an integer plane: BM3D::process_Plane
  * (source/BM3D.cpp:475-497) with the basic estimate sized like the source
- * (the reference's own process_Plane_FL passes a 0x0 one). */
+ * (the reference's own process_Plane_FL passes a 0x0 one); the basic stage
+ * matches on ref when given. */
 int FN(oracle_bm3d_plane_int)(const oracle_stage_params *pb, const oracle_stage_params *pf,
-                              int *dst, const int *src, int width, int height, int floor_,
-                              int neutral, int ceil_)
+                              int *dst, const int *src, const int *ref, int width, int height,
+                              int floor_, int neutral, int ceil_)
 {
     const size_t npx = (size_t)width * height;
-    FLT *fsrc = FN(alloc)(npx), *ftmp = FN(alloc)(npx), *fdst = FN(alloc)(npx);
+    FLT *fsrc = FN(alloc)(npx), *ftmp = FN(alloc)(npx), *fdst = FN(alloc)(npx), *fref = fsrc;
     FN(int_to_fl)(fsrc, src, npx, floor_, neutral, ceil_);
-    FN(oracle_bm3d_stage)(0, pb, ftmp, fsrc, fsrc, width, height, 1.0);
+    if (ref) {
+        fref = FN(alloc)(npx);
+        FN(int_to_fl)(fref, ref, npx, floor_, neutral, ceil_);
+    }
+    FN(oracle_bm3d_stage)(0, pb, ftmp, fsrc, fref, width, height, 1.0);
+    if (fref != fsrc) free(fref);
     FN(oracle_bm3d_stage)(1, pf, fdst, fsrc, ftmp, width, height, 1.0);
     FN(fl_to_int)(dst, fdst, npx, floor_, neutral, ceil_);
     free(fsrc);

@@ -217,20 +217,29 @@ extern "C" {
 /* BM3D on an RGB Frame: FilterIF2::operator()(Frame) -> BM3D::process_Frame
  * (source/BM3D.cpp:501-527): OPP RGB->YUV, three-plane basic then final,
  * YUV->RGB with clipping. Planes are the reference's DType (int32) with the
- * Frame's quantisation: bit depth `bits`, full (PC) range when `pc`. */
+ * Frame's quantisation: bit depth `bits`, full (PC) range when `pc`. `ref`
+ * may be null (ref = src). */
 int ref_bm3d_frame(const ref_stage_params *b, const ref_stage_params *f, int *const dst[3],
-                   const int *const src[3], int width, int height, int bits, int pc)
+                   const int *const src[3], const int *const ref[3], int width, int height,
+                   int bits, int pc)
 {
-    Frame in(0, PixelType::RGB, width, height, bits, pc ? QuantRange::PC : QuantRange::TV);
+    const QuantRange q = pc ? QuantRange::PC : QuantRange::TV;
+    Frame in(0, PixelType::RGB, width, height, bits, q);
+    Frame rf(0, PixelType::RGB, width, height, bits, q);
     const size_t n = sizeof(int) * (size_t)width * (size_t)height;
     std::memcpy(in.R().data(), src[0], n);
     std::memcpy(in.G().data(), src[1], n);
     std::memcpy(in.B().data(), src[2], n);
+    if (ref) {
+        std::memcpy(rf.R().data(), ref[0], n);
+        std::memcpy(rf.G().data(), ref[1], n);
+        std::memcpy(rf.B().data(), ref[2], n);
+    }
     BM3D_Para para("fast");
     fill_para(para.basic, b);
     fill_para(para.final, f);
     BM3D filter(para);
-    Frame out = filter(in);
+    Frame out = ref ? filter(in, rf) : filter(in);
     std::memcpy(dst[0], out.R().data(), n);
     std::memcpy(dst[1], out.G().data(), n);
     std::memcpy(dst[2], out.B().data(), n);
@@ -244,10 +253,10 @@ int ref_bm3d_frame(const ref_stage_params *b, const ref_stage_params *f, int *co
  * its size check there. This entry runs the same sequence from the
  * reference's own pieces with `tmp` sized like the source, the evident
  * intent. The plane's quantisation is (bits, floor, neutral, ceil);
- * neutral > floor marks a chroma plane. */
+ * neutral > floor marks a chroma plane. `ref` may be null (ref = src). */
 int ref_bm3d_plane_int(const ref_stage_params *b, const ref_stage_params *f, int *dst,
-                       const int *src, int width, int height, int bits, int floor_, int neutral,
-                       int ceil_)
+                       const int *src, const int *ref, int width, int height, int bits,
+                       int floor_, int neutral, int ceil_)
 {
     Plane in(0, width, height, bits, floor_, neutral, ceil_, TransferChar::linear, false);
     std::memcpy(in.data(), src, sizeof(int) * (size_t)width * (size_t)height);
@@ -261,7 +270,15 @@ int ref_bm3d_plane_int(const ref_stage_params *b, const ref_stage_params *f, int
     Plane_FL src_data(in, false);
     RangeConvert(src_data, in, false);
     Plane_FL tmp(src_data, false);
-    basic.Kernel(tmp, src_data, src_data);
+    if (ref) {
+        Plane rp(in, false);
+        std::memcpy(rp.data(), ref, sizeof(int) * (size_t)width * (size_t)height);
+        Plane_FL ref_data(rp, false);
+        RangeConvert(ref_data, rp, false);
+        basic.Kernel(tmp, src_data, ref_data);
+    } else {
+        basic.Kernel(tmp, src_data, src_data);
+    }
     final.Kernel(dst_data, src_data, tmp);
     RangeConvert(out, dst_data, true);
     std::memcpy(dst, out.data(), sizeof(int) * (size_t)width * (size_t)height);

@@ -207,3 +207,44 @@ def test_invalid_quantisation(ctx):
         ctx.plane_int(b, f, x.copy(), x, (10, 10, 10))
     with pytest.raises(isp_mw_b200.BM3DError):
         ctx.frame(b, f, [x.copy() for _ in range(3)], [x] * 3, 255, 0)
+
+
+def test_combined_entries_with_ref(ctx, oracle_mod):
+    """The combined entries with a separate ref (FilterIF2::process(dst, src,
+    ref)): the basic stage matches on ref. Float planes: bm3d_full / full3
+    equal the two stage calls bit for bit. Integer plane and RGB frame: against
+    the oracle (chained, PSNR bar)."""
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    from isp_mw_b200.synth import int_planes
+    sp = [synth.sigma_param(20.0)] * 3
+    b = isp_mw_b200.stage_params_default("fast", False, sp)
+    f = isp_mw_b200.stage_params_default("fast", True, sp)
+    _, noisy = synth.pair(90, 120, 20.0, 5)
+    _, guide = synth.pair(90, 120, 5.0, 5)
+    full = np.empty_like(noisy)
+    ctx.full(b, f, full, noisy, ref=guide)
+    basic, final = np.empty_like(noisy), np.empty_like(noisy)
+    ctx.stage(b, False, basic, noisy, guide)
+    ctx.stage(f, True, final, noisy, basic)
+    assert np.array_equal(full, final)
+    planes = [synth.pair(90, 120, 20.0, 6 + c)[1] for c in range(3)]
+    full3 = [np.empty_like(p) for p in planes]
+    ctx.full3(b, f, full3, planes, ref=[guide, planes[1], planes[2]])
+    b3 = [p.copy() for p in planes]
+    ctx.stage3(b, False, b3, planes, [guide, planes[1], planes[2]])
+    f3 = [p.copy() for p in planes]
+    ctx.stage3(f, True, f3, planes, b3)
+    for c in range(3):
+        assert np.array_equal(full3[c], f3[c])
+    orc = _oracle(oracle_mod)
+    src = int_planes(96, 112, 20.0, 8, 0, 255, 3)
+    ref = int_planes(96, 112, 6.0, 8, 0, 255, 3)
+    got = [np.empty_like(p) for p in src]
+    ctx.frame(b, f, got, src, 0, 255, ref=ref)
+    want = orc.frame(b.as_dict(), f.as_dict(), src, 8, True, ref)
+    assert psnr_int(np.stack(got), np.stack(want), 255) >= MIN_PSNR
+    one = np.empty_like(src[0])
+    ctx.plane_int(b, f, one, src[0], (0, 0, 255), ref=ref[0])
+    want1 = orc.plane_int(b.as_dict(), f.as_dict(), src[0], (0, 0, 255), 8, ref[0])
+    assert psnr_int(one, want1, 255) >= MIN_PSNR
