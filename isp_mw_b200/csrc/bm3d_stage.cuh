@@ -474,18 +474,20 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
                 acc[0] = ssd_row8(acc[0], refv[y], row);
             }
         } else {
+            // Every strip computes all KS candidates over all ROWS window rows,
+            // with no data-dependent branch; candidates past the window's
+            // last row (q >= nq) are discarded below. Their rows lie at most
+            // KS - 1 rows past a staged window or the (0, 0) copy, which are
+            // always followed by other parts of the CTA's shared memory.
 #pragma unroll
             for (int w = 0; w < ROWS; ++w) {
-                if (w < nq - 1 + kBS) {
-                    T row[kBS];
+                T row[kBS];
 #pragma unroll
-                    for (int x = 0; x < kBS; ++x) row[x] = base[w * bp + x];
+                for (int x = 0; x < kBS; ++x) row[x] = base[w * bp + x];
 #pragma unroll
-                    for (int q = 0; q < KS; ++q) {
-                        const int y = w - q;
-                        if (y >= 0 && y < kBS && q < nq)
-                            acc[q] = ssd_row8(acc[q], refv[y < 0 ? 0 : (y >= kBS ? kBS - 1 : y)], row);
-                    }
+                for (int q = 0; q < KS; ++q) {
+                    const int y = w - q;
+                    if (y >= 0 && y < kBS) acc[q] = ssd_row8(acc[q], refv[y], row);
                 }
             }
         }
