@@ -260,6 +260,13 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+# DRAM bytes per launch of the stage kernels on one 1920x1080 plane, from one
+# ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum); the command
+# and the full figures are in profiles/stage_kernel_{final,basic}_1080p_full.txt.
+TRAFFIC_FINAL_1080P = 46.557e6 + 0.014e6
+TRAFFIC_BASIC_1080P = 37.286e6 + 0.004e6
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -389,7 +396,11 @@ def run_ours(args):
                 "peak": round(peak_fp32, 2),
                 "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4),
-                "traffic": None,
+                "traffic": TRAFFIC_FINAL_1080P if dom else TRAFFIC_BASIC_1080P,
+                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, one "
+                                  "ncu capture of the same kernel on one 1920x1080 plane, "
+                                  "sigma 25 (profiles/stage_kernel_"
+                                  + ("final" if dom else "basic") + "_1080p_full.txt)",
                 "peak_source": "nominal FP32 FMA rate 148 SM x 128 lanes x 2 flop x max SM clock "
                                "(MEASURED_PEAKS.json has no FP32 SIMT figure)",
                 "per_launch_ms": round(per_launch_ms, 4),

@@ -1661,8 +1661,10 @@ int launch_planes(bm3d_batch *B, const DevBuf &planes, int count, bool prep, cud
     if (count == 0) return BM3D_OK;
     long long maxpx = 0;
     for (int i = 0; i < B->n; ++i) maxpx = std::max(maxpx, static_cast<long long>(B->w[i]) * B->h[i]);
+    // enough CTAs in all to fill the GPU a few times over, at least 64 per plane
     const long long tiles = (maxpx + kNormTile * kNormTile - 1) / (kNormTile * kNormTile);
-    const dim3 grid(static_cast<unsigned>(std::min<long long>(prep ? (maxpx + 255) / 256 : tiles, 64)),
+    const long long cap = std::max<long long>(64, 8LL * B->ctx->sm_count / count);
+    const dim3 grid(static_cast<unsigned>(std::min<long long>(prep ? (maxpx + 255) / 256 : tiles, cap)),
                     static_cast<unsigned>(count));
     const auto *q = static_cast<const BatchPlane<float> *>(planes.ptr);
     if (prep) prep_batch_kernel<float><<<grid, 256, 0, s>>>(q);
