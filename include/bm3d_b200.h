@@ -124,6 +124,23 @@ int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_p
                float *const dst[3], const float *const src[3], const float *const ref[3],
                int width, int height, size_t stride, float value_range, int mem, void *stream);
 
+/* Basic then final on `count` planes in HOST memory, each with its own
+ * parameters and size, with the copies overlapped with the filtering: plane
+ * i + 1 is uploaded and plane i - 1 downloaded while plane i is filtered on
+ * `stream` (two copy streams and two device slots owned by the context).
+ * Results equal per-plane bm3d_full bit for bit. With `async` = 0 the call
+ * returns when every result is in dst. With `async` != 0 it returns once the
+ * work is enqueued: `stream` completes after the last download, so the caller
+ * synchronises it (or records an event on it) before reading dst or reusing
+ * src; consecutive async calls overlap one another's copies too. Overlap
+ * needs page-locked host planes; pageable planes still work, with the copies
+ * serialised. Replaces looping BM3D::process over host images
+ * (source/BM3D.cpp:464-472), which has no overlap. */
+int bm3d_full_many(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                   const bm3d_stage_params *final_, float *const dst[], const float *const src[],
+                   const int width[], const int height[], const size_t stride[],
+                   float value_range, int async, void *stream);
+
 /* ---- Integer planes and RGB frames ------------------------------------
  * Planes of the reference's integer pixel type (DType = int32,
  * include/Type.h:25) with its quantisation: Floor, Neutral and Ceil of the plane

@@ -40,6 +40,7 @@ EXPORTS = [
     "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
     "bm3d_stage_noalloc", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
     "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
+    "bm3d_full_many",
 ]
 
 
@@ -130,6 +131,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     rgb = [ip, ip, ctypes.c_size_t, ip, ip, ip, vp]         # w, h, stride, floor, ceil, mem, stream
     lib.bm3d_frame.argtypes = [vp, sp, sp, vp, vp, vp] + rgb
     lib.bm3d_stage_frame.argtypes = [vp, sp, ip, vp, vp, vp] + rgb
+    lib.bm3d_full_many.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ctypes.c_float, ip, vp]
     lib.bm3d_set_kernel_timing.argtypes = [vp, ip]
     lib.bm3d_kernel_time.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong)]
@@ -313,6 +315,41 @@ class Context:
                                        arr(*ptrs[3:6]),
                                        arr(*ptrs[6:9]) if ref is not None else None, w, h, stride,
                                        int(floor), int(ceil), mem, _stream_of(dst[0]))
+        return self._check(rc)
+
+    def full_many(self, basic: Sequence[StageParams], final: Sequence[StageParams], dst, src,
+                  value_range: float = 1.0, asynchronous: bool = False,
+                  stream: Optional[int] = None) -> int:
+        """``bm3d_full_many``: basic then final on host planes (numpy arrays or
+        CPU tensors; page-locked for overlap), copies overlapped with the
+        filtering. With ``asynchronous`` the call returns once enqueued on
+        ``stream`` (default: the current torch stream); synchronise it before
+        reading ``dst``."""
+        n = len(src)
+        if not (len(basic) == len(final) == len(dst) == n):
+            raise ValueError("one basic/final parameter set and dst per src plane")
+        di = [_plane_info(x) for x in dst]
+        si = [_plane_info(x) for x in src]
+        if any(i[1] != MEM_HOST for i in di + si):
+            raise ValueError("full_many takes host planes")
+        for a, b in zip(di, si):
+            if a[2:5] != b[2:5]:
+                raise ValueError("dst and src planes must have the same size and stride")
+        if stream is None:
+            try:
+                import torch
+                stream = torch.cuda.current_stream(self.device).cuda_stream
+            except Exception:
+                stream = 0
+        vp = ctypes.c_void_p * max(1, n)
+        pb = (StageParams * max(1, n))(*basic)
+        pf = (StageParams * max(1, n))(*final)
+        w = (ctypes.c_int * max(1, n))(*[i[2] for i in si])
+        h = (ctypes.c_int * max(1, n))(*[i[3] for i in si])
+        st = (ctypes.c_size_t * max(1, n))(*[i[4] for i in si])
+        rc = self.lib.bm3d_full_many(self.h, n, pb, pf, vp(*[i[0] for i in di]),
+                                     vp(*[i[0] for i in si]), w, h, st, value_range,
+                                     int(asynchronous), stream)
         return self._check(rc)
 
     def ref_block_count(self, params: StageParams, width: int, height: int) -> int:

@@ -42,6 +42,15 @@ struct bm3d_ctx {
     double *gtab_d = nullptr;         // same in double
     cudaStream_t last_stream = nullptr;
     int tile_x = 8, tile_y = 8, warps = 16;
+    // bm3d_full_many's copy pipeline: two slots of device planes, an upload
+    // and a download stream, and the events that order slot reuse
+    struct PipeSlot {
+        DevBuf in, out;
+        cudaEvent_t in_ready = nullptr, computed = nullptr, drained = nullptr;
+        bool used = false;
+    } pipe[2];
+    cudaStream_t up = nullptr, down = nullptr;
+    unsigned long long pipe_count = 0;
     // optional per-launch timing of the stage kernels: [0] basic, [1] final
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[2];
@@ -240,6 +249,14 @@ extern "C" void bm3d_ctx_destroy(bm3d_ctx *ctx)
     for (auto &b : ctx->groups) fr(b);
     for (auto &b : ctx->conv) fr(b);
     for (auto &b : ctx->ints) fr(b);
+    for (auto &sl : ctx->pipe) {
+        fr(sl.in);
+        fr(sl.out);
+        for (cudaEvent_t e : {sl.in_ready, sl.computed, sl.drained})
+            if (e) cudaEventDestroy(e);
+    }
+    if (ctx->up) cudaStreamDestroy(ctx->up);
+    if (ctx->down) cudaStreamDestroy(ctx->down);
     if (ctx->stats) cudaFree(ctx->stats);
     if (ctx->absmax) cudaFree(ctx->absmax);
     if (ctx->gtab_f) cudaFree(ctx->gtab_f);
@@ -1297,6 +1314,96 @@ extern "C" int bm3d_stage_frame(bm3d_ctx *ctx, const bm3d_stage_params *params, 
                                            opp_inverse(floor_, ceil_));
     CK(ctx, cudaGetLastError());
     return finish_ints(ctx, 3, dst, width, height, stride, mem, s, io, st);
+}
+
+// ---------------------------------------------------------------------------
+// Many host planes, copies overlapped with the filtering.
+
+extern "C" int bm3d_full_many(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                              const bm3d_stage_params *final_, float *const dst[],
+                              const float *const src[], const int width[], const int height[],
+                              const size_t stride[], float value_range, int async, void *stream)
+{
+    if (!ctx || count < 0 || (count > 0 && (!basic || !final_ || !dst || !src || !width ||
+                                            !height || !stride)))
+        return BM3D_ERR_INVALID;
+    for (int i = 0; i < count; ++i)
+        if (!dst[i] || !src[i] || width[i] < 1 || height[i] < 1 ||
+            stride[i] < static_cast<size_t>(width[i]))
+            return BM3D_ERR_INVALID;
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!ctx->up) {
+        CK(ctx, cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking));
+        CK(ctx, cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking));
+        for (auto &sl : ctx->pipe) {
+            CK(ctx, cudaEventCreateWithFlags(&sl.in_ready, cudaEventDisableTiming));
+            CK(ctx, cudaEventCreateWithFlags(&sl.computed, cudaEventDisableTiming));
+            CK(ctx, cudaEventCreateWithFlags(&sl.drained, cudaEventDisableTiming));
+        }
+    }
+    // Uploads run one plane ahead on `up`, downloads trail on `down`; a slot's
+    // input is reused once its plane has been filtered, its output once it
+    // has been copied out. `stream` does the filtering.
+    int status = BM3D_OK;
+    auto upload = [&](int i) -> int {
+        auto &sl = ctx->pipe[(ctx->pipe_count + i) & 1];
+        const size_t bytes = sizeof(float) * static_cast<size_t>(width[i]) * height[i];
+        if (sl.used) CK(ctx, cudaStreamWaitEvent(ctx->up, sl.computed, 0));
+        if (sl.in.bytes < bytes) {  // growing a buffer: let every use of it finish first
+            if (sl.used) CK(ctx, cudaEventSynchronize(sl.computed));
+            int rc = ensure(ctx, sl.in, bytes);
+            if (rc != BM3D_OK) return rc;
+        }
+        CK(ctx, cudaMemcpy2DAsync(sl.in.ptr, sizeof(float) * width[i], src[i],
+                                  sizeof(float) * stride[i], sizeof(float) * width[i], height[i],
+                                  cudaMemcpyHostToDevice, ctx->up));
+        CK(ctx, cudaEventRecord(sl.in_ready, ctx->up));
+        return BM3D_OK;
+    };
+    if (count > 0) {
+        int rc = upload(0);
+        if (rc != BM3D_OK) return rc;
+    }
+    for (int i = 0; i < count; ++i) {
+        if (i + 1 < count) {
+            int rc = upload(i + 1);
+            if (rc != BM3D_OK) return rc;
+        }
+        auto &sl = ctx->pipe[(ctx->pipe_count + i) & 1];
+        const size_t bytes = sizeof(float) * static_cast<size_t>(width[i]) * height[i];
+        if (sl.used) CK(ctx, cudaStreamWaitEvent(s, sl.drained, 0));
+        if (sl.out.bytes < bytes) {
+            if (sl.used) CK(ctx, cudaEventSynchronize(sl.drained));
+            int rc = ensure(ctx, sl.out, bytes);
+            if (rc != BM3D_OK) return rc;
+        }
+        CK(ctx, cudaStreamWaitEvent(s, sl.in_ready, 0));
+        float *d[1] = {static_cast<float *>(sl.out.ptr)};
+        const float *x[1] = {static_cast<const float *>(sl.in.ptr)};
+        const int rc = full_any<float>(ctx, &basic[i], &final_[i], 1, d, x, nullptr, width[i],
+                                       height[i], static_cast<size_t>(width[i]), value_range,
+                                       BM3D_MEM_DEVICE, s);
+        if (rc < 0) return rc;
+        if (rc == BM3D_COPIED) status = BM3D_COPIED;
+        CK(ctx, cudaEventRecord(sl.computed, s));
+        CK(ctx, cudaStreamWaitEvent(ctx->down, sl.computed, 0));
+        CK(ctx, cudaMemcpy2DAsync(dst[i], sizeof(float) * stride[i], sl.out.ptr,
+                                  sizeof(float) * width[i], sizeof(float) * width[i], height[i],
+                                  cudaMemcpyDeviceToHost, ctx->down));
+        CK(ctx, cudaEventRecord(sl.drained, ctx->down));
+        sl.used = true;
+    }
+    ctx->pipe_count += static_cast<unsigned long long>(count);
+    if (count > 0) {
+        // `stream` completes after the last download
+        auto &last = ctx->pipe[(ctx->pipe_count - 1) & 1];
+        CK(ctx, cudaStreamWaitEvent(s, last.drained, 0));
+    }
+    if (async) return status;
+    CK(ctx, cudaStreamSynchronize(s));
+    const int rc = check_invariants(ctx);
+    return rc != BM3D_OK ? rc : status;
 }
 
 extern "C" int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *p, int wiener,
