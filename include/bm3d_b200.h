@@ -266,6 +266,16 @@ int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
                       const bm3d_stage_params *final_, float *const dst[],
                       const float *const src[], const int width[], const int height[],
                       const size_t stride[], int autotune, bm3d_batch **out);
+/* The same over `count` images of three planes (Y, U, V) each, sharing the
+ * groups matched on Y (as bm3d_full3): plane c of image i is dst[3 * i + c] /
+ * src[3 * i + c], all three of width[i] x height[i] with row pitch stride[i].
+ * Results equal per-image bm3d_full3 bit for bit. Replaces looping the
+ * reference's 9-plane BM3D_Base::Kernel (source/BM3D.cpp:139-218) over
+ * frames. */
+int bm3d_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                       const bm3d_stage_params *final_, float *const dst[],
+                       const float *const src[], const int width[], const int height[],
+                       const size_t stride[], int autotune, bm3d_batch **out);
 int bm3d_batch_run(bm3d_batch *batch, void *stream);
 /* tile_x, tile_y, warps of the basic stage, then of the final stage. */
 int bm3d_batch_tuning(const bm3d_batch *batch, int out[6]);

@@ -40,7 +40,7 @@ EXPORTS = [
     "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
     "bm3d_stage_noalloc", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
     "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
-    "bm3d_full_many",
+    "bm3d_full_many", "bm3d_batch3_create",
 ]
 
 
@@ -121,6 +121,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                        ctypes.c_float, vp]
     lib.bm3d_batch_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
                                       ctypes.POINTER(vp)]
+    lib.bm3d_batch3_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
+                                       ctypes.POINTER(vp)]
     lib.bm3d_batch_run.argtypes = [vp, vp]
     lib.bm3d_batch_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     lib.bm3d_batch_destroy.argtypes = [vp]
@@ -389,14 +391,27 @@ class Context:
 class Batch:
     """``bm3d_batch``: basic + final over many device planes (CUDA torch
     tensors) of any sizes and noise levels, one persistent launch per stage,
-    replayed from a CUDA graph. The planes are bound at creation."""
+    replayed from a CUDA graph. The planes are bound at creation. When every
+    element of ``src`` / ``dst`` is a triple of planes (Y, U, V), the images
+    are filtered as three planes sharing luma groups (``bm3d_batch3_create``)."""
 
     def __init__(self, ctx: "Context", basic: Sequence[StageParams], final: Sequence[StageParams],
                  dst: Sequence, src: Sequence, autotune: bool = True):
         n = len(src)
         if not (len(basic) == len(final) == len(dst) == n) or n == 0:
-            raise ValueError("one basic/final parameter set and dst per src plane")
+            raise ValueError("one basic/final parameter set and dst per src image")
         self.ctx = ctx
+        three = all(isinstance(x, (list, tuple)) for x in src)
+        if three:
+            if not all(isinstance(x, (list, tuple)) and len(x) == 3 for x in list(src) + list(dst)):
+                raise ValueError("three-plane images take three src and three dst planes each")
+            src = [p for x in src for p in x]
+            dst = [p for x in dst for p in x]
+            for i in range(n):
+                shapes = {tuple(p.shape) for p in src[3 * i:3 * i + 3] + dst[3 * i:3 * i + 3]}
+                if len(shapes) != 1:
+                    raise ValueError("the planes of an image must have one size")
+        npl = 3 if three else 1
         self._keep = (list(dst), list(src))
         infos_d = [_plane_info(d) for d in dst]
         infos_s = [_plane_info(x) for x in src]
@@ -405,18 +420,22 @@ class Batch:
         for a, b in zip(infos_d, infos_s):
             if a[2:5] != b[2:5]:
                 raise ValueError("dst and src planes must have the same size and pitch")
+        if npl == 3 and any(infos_s[3 * i][4] != infos_s[3 * i + c][4]
+                            for i in range(n) for c in range(3)):
+            raise ValueError("the planes of an image must share one row pitch")
         pb = (StageParams * n)(*basic)
         pf = (StageParams * n)(*final)
-        vp = ctypes.c_void_p * n
-        w = (ctypes.c_int * n)(*[i[2] for i in infos_s])
-        h = (ctypes.c_int * n)(*[i[3] for i in infos_s])
-        st = (ctypes.c_size_t * n)(*[i[4] for i in infos_s])
+        vp = ctypes.c_void_p * (n * npl)
+        first = infos_s[::npl]
+        w = (ctypes.c_int * n)(*[i[2] for i in first])
+        h = (ctypes.c_int * n)(*[i[3] for i in first])
+        st = (ctypes.c_size_t * n)(*[i[4] for i in first])
         self.h = ctypes.c_void_p()
-        rc = ctx.lib.bm3d_batch_create(ctx.h, n, pb, pf, vp(*[i[0] for i in infos_d]),
-                                       vp(*[i[0] for i in infos_s]), w, h, st, int(autotune),
-                                       ctypes.byref(self.h))
+        create = ctx.lib.bm3d_batch3_create if npl == 3 else ctx.lib.bm3d_batch_create
+        rc = create(ctx.h, n, pb, pf, vp(*[i[0] for i in infos_d]), vp(*[i[0] for i in infos_s]),
+                    w, h, st, int(autotune), ctypes.byref(self.h))
         ctx._check(rc, allow_copied=False)
-        self.pixels = sum(i[2] * i[3] for i in infos_s)
+        self.pixels = sum(i[2] * i[3] for i in first)  # image pixels (per plane for 3-plane images)
 
     def run(self, stream: Optional[int] = None):
         if stream is None:

@@ -21,6 +21,7 @@ __global__ void __launch_bounds__(GENERIC ? 256 : 512, 1)
     extern __shared__ __align__(16) unsigned char smem[];
     int *item = reinterpret_cast<int *>(smem);
     const int total = tile_base[nimg];
+    const unsigned avail = dynamic_smem_bytes() - kBatchHeader;
     for (;;) {
         if (threadIdx.x == 0) *item = atomicAdd(counter, 1);
         __syncthreads();
@@ -33,8 +34,10 @@ __global__ void __launch_bounds__(GENERIC ? 256 : 512, 1)
             else hi = mid - 1;
         }
         const StageArgs<T> &a = args[lo];
-        if (GENERIC) generic_tile_body<T, WIENER, NPL>(a, it - tile_base[lo], smem + kBatchHeader);
-        else stage_tile_body<T, WIENER, NPL, KS>(a, it - tile_base[lo], smem + kBatchHeader);
+        unsigned char *body = smem + kBatchHeader;
+        if constexpr (GENERIC) generic_tile_body<T, WIENER, NPL>(a, it - tile_base[lo], body, avail);
+        else if constexpr (NPL == 3) stage_tile_body_seq3<T, WIENER, KS>(a, it - tile_base[lo], body, avail);
+        else stage_tile_body<T, WIENER, NPL, KS>(a, it - tile_base[lo], body, avail);
         __syncthreads();  // every thread has read *item before it is replaced
     }
 }

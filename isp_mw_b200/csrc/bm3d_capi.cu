@@ -433,7 +433,8 @@ static int launch_one(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int warps)
 {
     const void *kern = stage_kernel_fn<T, W, NPL, KS>();
     const SmemPlan sp =
-        plan_smem<T>(NPL, W, a.ref_alias_src, a.region_h, a.region_pitch, a.key_slots, warps);
+        plan_smem<T>(NPL, W, a.ref_alias_src, a.region_h, a.region_pitch, a.key_slots, warps,
+                     false, kBS, kGSMax, a.tile_x * a.tile_y);
     CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sp.total)));
     const int grid = a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y);
@@ -544,7 +545,7 @@ static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params
         a.region_pitch = a.region_w + ((5 - a.region_w % 8) + 8) % 8;
         const SmemPlan sp = plan_smem<T>(nplanes, wiener, a.ref_alias_src, a.region_h,
                                          a.region_pitch, a.key_slots, warps, generic, BS,
-                                         p->group_size);
+                                         p->group_size, std::min(tx, a.nx) * std::min(ty, a.ny));
         if (sp.total <= ctx->smem_optin) break;
         // The generic kernel's per-warp group buffers dominate its footprint:
         // give up warps before tile size there.
@@ -646,8 +647,10 @@ static int check_invariants(bm3d_ctx *ctx)
 {
     unsigned long long v[kStats];
     CK(ctx, cudaMemcpy(v, ctx->stats, sizeof(v), cudaMemcpyDeviceToHost));
-    if (v[4] != 0) {
-        ctx->err = "internal error: " + std::to_string(v[4]) + " group blocks outside the staged window";
+    if (v[4] != 0) {  // low 32 bits: group blocks outside the window; high: CTAs short of smem
+        ctx->err = "internal error: " + std::to_string(v[4] & 0xffffffffull) +
+                   " group blocks outside the staged window, " + std::to_string(v[4] >> 32) +
+                   " tiles launched with too little shared memory";
         return BM3D_ERR_CUDA;
     }
     return BM3D_OK;
@@ -1642,15 +1645,17 @@ struct StageBuild {
 
 struct bm3d_batch {
     bm3d_ctx *ctx = nullptr;
-    int n = 0;
+    int n = 0;    // images
+    int npl = 1;  // planes per image (1, or 3 sharing the luma groups)
     std::vector<int> w, h;
     std::vector<size_t> stride;
-    std::vector<const float *> src;
+    std::vector<const float *> src;  // plane c of image i at [i * npl + c]
     std::vector<float *> dst;
     std::vector<bm3d_stage_params> pb, pf;
     std::vector<Guard> gb, gf;
-    std::vector<size_t> acc_off, basic_off;  // element offsets into acc (int64) and basic (float)
+    std::vector<size_t> acc_off, basic_off;  // per plane: offsets into acc (int64) and basic (float)
     DevBuf acc, basic, absmax, counters, planes_b, planes_f;
+    int nq_b = 0, nq_f = 0;  // entries of planes_b / planes_f (planes each stage filters)
     StageBuild sb, sf;
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
@@ -1680,7 +1685,8 @@ int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuil
         if ((wiener ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
         StageArgs<float> a;
         std::memset(&a, 0, sizeof(a));
-        fill_tables(a, p, wiener, 1, 1.0);
+        const int npl = B->npl;
+        fill_tables(a, p, wiener, npl, 1.0);
         generic = !fast_args(p->block_size, p->group_size);
         const int BS = p->block_size;
         a.width = B->w[i];
@@ -1702,18 +1708,23 @@ int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuil
         a.tile_y = std::min(ty, a.ny);
         a.tiles_x = (a.nx + a.tile_x - 1) / a.tile_x;
         a.stride = static_cast<long long>(B->stride[i]);
-        a.src[0] = B->src[i];
-        a.ref[0] = wiener ? static_cast<const float *>(B->basic.ptr) + B->basic_off[i] : B->src[i];
-        a.ref_alias_src = wiener ? 0 : 1;
-        a.num[0] = static_cast<long long *>(B->acc.ptr) + B->acc_off[i];
-        a.den[0] = a.num[0] + static_cast<size_t>(a.width) * a.height;
-        a.absmax = static_cast<float *>(B->absmax.ptr) + i;
+        a.ref_alias_src = wiener ? 0 : (1 << npl) - 1;
+        for (int c = 0; c < npl; ++c) {
+            const int k = i * npl + c;
+            a.src[c] = B->src[k];
+            a.ref[c] = wiener ? static_cast<const float *>(B->basic.ptr) + B->basic_off[k]
+                              : B->src[k];
+            a.num[c] = static_cast<long long *>(B->acc.ptr) + B->acc_off[k];
+            a.den[c] = a.num[c] + static_cast<size_t>(a.width) * a.height;
+        }
+        a.absmax = static_cast<float *>(B->absmax.ptr) + i * npl;
         const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, p->group_size);
         a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
         a.dct_fwd = ctx->gtab_f;
         a.dct_inv = ctx->gtab_f ? ctx->gtab_f + kDctTableSize : nullptr;
-        const SmemPlan sp = plan_smem<float>(1, wiener, a.ref_alias_src, a.region_h, a.region_pitch,
-                                             a.key_slots, warps, generic, BS, p->group_size);
+        const SmemPlan sp = plan_smem<float>(npl, wiener, a.ref_alias_src, a.region_h,
+                                             a.region_pitch, a.key_slots, warps, generic, BS,
+                                             p->group_size, a.tile_x * a.tile_y);
         smem = std::max(smem, sp.total + kBatchHeader);
         args.push_back(a);
         base.push_back(base.back() + a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y));
@@ -1758,13 +1769,18 @@ int launch_batch_stage(bm3d_batch *B, StageBuild &sbd, int *counter, cudaStream_
         CK(ctx, cudaLaunchKernel(kern, dim3(sbd.grid), dim3(sbd.warps * kWarp), kargs, sbd.smem, s));
         return BM3D_OK;
     };
-    if (sbd.generic) return go(batch_kernel_fn<W, 1, true>());
-    if ((W ? B->pf[0].bm_step : B->pb[0].bm_step) == 1) return go(batch_kernel_fn<W, 4, false>());
-    return go(batch_kernel_fn<W, 1, false>());
+    const bool ks4 = (W ? B->pf[0].bm_step : B->pb[0].bm_step) == 1;
+    if (B->npl == 3) {
+        if (sbd.generic) return go(batch_kernel_fn<W, 3, 1, true>());
+        return go(ks4 ? batch_kernel_fn<W, 3, 4, false>() : batch_kernel_fn<W, 3, 1, false>());
+    }
+    if (sbd.generic) return go(batch_kernel_fn<W, 1, 1, true>());
+    return go(ks4 ? batch_kernel_fn<W, 1, 4, false>() : batch_kernel_fn<W, 1, 1, false>());
 }
 
-int launch_planes(bm3d_batch *B, const DevBuf &planes, int count, bool prep, cudaStream_t s)
+int launch_planes(bm3d_batch *B, const DevBuf &planes, bool prep, cudaStream_t s)
 {
+    const int count = &planes == &B->planes_b ? B->nq_b : B->nq_f;
     if (count == 0) return BM3D_OK;
     long long maxpx = 0;
     for (int i = 0; i < B->n; ++i) maxpx = std::max(maxpx, static_cast<long long>(B->w[i]) * B->h[i]);
@@ -1787,21 +1803,26 @@ int enqueue_batch(bm3d_batch *B, cudaStream_t s)
     int rc;
     int *counters = static_cast<int *>(B->counters.ptr);
     for (int i = 0; i < B->n; ++i) {  // planes a stage passes through unfiltered
-        float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[i];
-        if (B->gb[i] != Guard::Run)
-            CK(ctx, cudaMemcpy2DAsync(bi, B->stride[i] * 4, B->src[i], B->stride[i] * 4, B->w[i] * 4,
-                                      B->h[i], cudaMemcpyDeviceToDevice, s));
-        if (B->gf[i] != Guard::Run && B->dst[i] != B->src[i])
-            CK(ctx, cudaMemcpy2DAsync(B->dst[i], B->stride[i] * 4, B->src[i], B->stride[i] * 4,
-                                      B->w[i] * 4, B->h[i], cudaMemcpyDeviceToDevice, s));
+        for (int c = 0; c < B->npl; ++c) {
+            const int k = i * B->npl + c;
+            float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[k];
+            const bool b_off = B->gb[i] != Guard::Run || !(B->pb[i].sigma[c] > 0 || B->npl == 1);
+            const bool f_off = B->gf[i] != Guard::Run || !(B->pf[i].sigma[c] > 0 || B->npl == 1);
+            if (b_off)
+                CK(ctx, cudaMemcpy2DAsync(bi, B->stride[i] * 4, B->src[k], B->stride[i] * 4,
+                                          B->w[i] * 4, B->h[i], cudaMemcpyDeviceToDevice, s));
+            if (f_off && B->dst[k] != B->src[k])
+                CK(ctx, cudaMemcpy2DAsync(B->dst[k], B->stride[i] * 4, B->src[k], B->stride[i] * 4,
+                                          B->w[i] * 4, B->h[i], cudaMemcpyDeviceToDevice, s));
+        }
     }
-    CK(ctx, cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * B->n, s));
-    if ((rc = launch_planes(B, B->planes_b, B->sb.nact, true, s)) != BM3D_OK) return rc;
+    CK(ctx, cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * B->n * B->npl, s));
+    if ((rc = launch_planes(B, B->planes_b, true, s)) != BM3D_OK) return rc;
     if ((rc = launch_batch_stage<false>(B, B->sb, counters, s)) != BM3D_OK) return rc;
-    if ((rc = launch_planes(B, B->planes_b, B->sb.nact, false, s)) != BM3D_OK) return rc;
-    if ((rc = launch_planes(B, B->planes_f, B->sf.nact, true, s)) != BM3D_OK) return rc;
+    if ((rc = launch_planes(B, B->planes_b, false, s)) != BM3D_OK) return rc;
+    if ((rc = launch_planes(B, B->planes_f, true, s)) != BM3D_OK) return rc;
     if ((rc = launch_batch_stage<true>(B, B->sf, counters + 1, s)) != BM3D_OK) return rc;
-    if ((rc = launch_planes(B, B->planes_f, B->sf.nact, false, s)) != BM3D_OK) return rc;
+    if ((rc = launch_planes(B, B->planes_f, false, s)) != BM3D_OK) return rc;
     return BM3D_OK;
 }
 
@@ -1816,7 +1837,7 @@ int time_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, cudaStream_
     CK(ctx, cudaEventCreate(&e1));
     ms = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
-        if ((rc = launch_planes(B, planes, sbd.nact, true, s)) != BM3D_OK) return rc;
+        if ((rc = launch_planes(B, planes, true, s)) != BM3D_OK) return rc;
         CK(ctx, cudaEventRecord(e0, s));
         if ((rc = launch_batch_stage<W>(B, sbd, static_cast<int *>(B->counters.ptr) + (W ? 1 : 0),
                                         s)) != BM3D_OK)
@@ -1828,7 +1849,7 @@ int time_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, cudaStream_
         if (rep > 0) ms = std::min(ms, t);  // first run warms up
     }
     if (!W) {  // leave the basic estimates in place for the final stage's tuning
-        if ((rc = launch_planes(B, planes, sbd.nact, false, s)) != BM3D_OK) return rc;
+        if ((rc = launch_planes(B, planes, false, s)) != BM3D_OK) return rc;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1878,10 +1899,10 @@ int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotu
 
 }  // namespace
 
-extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
-                                 const bm3d_stage_params *final_, float *const dst[],
-                                 const float *const src[], const int width[], const int height[],
-                                 const size_t stride[], int autotune, bm3d_batch **out)
+static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_params *basic,
+                            const bm3d_stage_params *final_, float *const dst[],
+                            const float *const src[], const int width[], const int height[],
+                            const size_t stride[], int autotune, bm3d_batch **out)
 {
     if (!ctx || !out || count < 1 || !basic || !final_ || !dst || !src || !width || !height ||
         !stride)
@@ -1891,13 +1912,14 @@ extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_para
     auto *B = new bm3d_batch;
     B->ctx = ctx;
     B->n = count;
+    B->npl = npl;
     auto fail = [&](int rc) {
         bm3d_batch_destroy(B);
         return rc;
     };
     size_t acc_total = 0, basic_total = 0;
     for (int i = 0; i < count; ++i) {
-        const Guard gb = check_params(&basic[i], 1), gf = check_params(&final_[i], 1);
+        const Guard gb = check_params(&basic[i], npl), gf = check_params(&final_[i], npl);
         if (gb == Guard::Invalid || gf == Guard::Invalid) return fail(batch_fail(ctx, "invalid parameters"));
         if (gb == Guard::Unsupported || gf == Guard::Unsupported) {
             ctx->err = "parameters outside this build (BlockSize <= 16, GroupSize <= 32)";
@@ -1911,47 +1933,56 @@ extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_para
                 return fail(batch_fail(ctx, "planes of a batch must share the stage geometry"));
         }
         const int bs = std::max(basic[i].block_size, final_[i].block_size);
-        if (!src[i] || !dst[i] || width[i] < bs || height[i] < bs ||
-            stride[i] < static_cast<size_t>(width[i]))
+        if (width[i] < bs || height[i] < bs || stride[i] < static_cast<size_t>(width[i]))
             return fail(batch_fail(ctx, "bad plane"));
         B->w.push_back(width[i]);
         B->h.push_back(height[i]);
         B->stride.push_back(stride[i]);
-        B->src.push_back(src[i]);
-        B->dst.push_back(dst[i]);
         B->pb.push_back(basic[i]);
         B->pf.push_back(final_[i]);
         B->gb.push_back(gb);
         B->gf.push_back(gf);
-        B->acc_off.push_back(acc_total);
-        B->basic_off.push_back(basic_total);
-        acc_total += 2 * static_cast<size_t>(width[i]) * height[i];
-        basic_total += stride[i] * height[i];
+        for (int c = 0; c < npl; ++c) {
+            const int k = i * npl + c;
+            if (!src[k] || !dst[k]) return fail(batch_fail(ctx, "bad plane"));
+            B->src.push_back(src[k]);
+            B->dst.push_back(dst[k]);
+            B->acc_off.push_back(acc_total);
+            B->basic_off.push_back(basic_total);
+            acc_total += 2 * static_cast<size_t>(width[i]) * height[i];
+            basic_total += stride[i] * height[i];
+        }
     }
     int rc;
     if ((rc = ensure(ctx, B->acc, sizeof(long long) * acc_total)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->basic, sizeof(float) * basic_total)) != BM3D_OK) return fail(rc);
-    if ((rc = ensure(ctx, B->absmax, sizeof(float) * count)) != BM3D_OK) return fail(rc);
+    if ((rc = ensure(ctx, B->absmax, sizeof(float) * count * npl)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->counters, 2 * sizeof(int))) != BM3D_OK) return fail(rc);
     // per-pixel kernels' plane tables, active planes of each stage in batch order
     for (int st = 0; st < 2; ++st) {
         std::vector<BatchPlane<float>> q;
         for (int i = 0; i < count; ++i) {
             if ((st ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
-            BatchPlane<float> bp;
-            bp.num = static_cast<long long *>(B->acc.ptr) + B->acc_off[i];
-            bp.den = bp.num + static_cast<size_t>(width[i]) * height[i];
-            bp.src = src[i];
-            bp.dst = st ? dst[i] : static_cast<float *>(B->basic.ptr) + B->basic_off[i];
-            bp.src_stride = static_cast<long long>(stride[i]);
-            bp.dst_stride = static_cast<long long>(stride[i]);
-            bp.width = width[i];
-            bp.height = height[i];
-            bp.block_size = st ? final_[i].block_size : basic[i].block_size;
-            bp.absmax = static_cast<float *>(B->absmax.ptr) + i;
-            q.push_back(bp);
+            const bm3d_stage_params &pp = st ? final_[i] : basic[i];
+            for (int c = 0; c < npl; ++c) {
+                if (npl > 1 && !(pp.sigma[c] > 0)) continue;  // plane left alone by the stage
+                const int k = i * npl + c;
+                BatchPlane<float> bp;
+                bp.num = static_cast<long long *>(B->acc.ptr) + B->acc_off[k];
+                bp.den = bp.num + static_cast<size_t>(width[i]) * height[i];
+                bp.src = src[k];
+                bp.dst = st ? dst[k] : static_cast<float *>(B->basic.ptr) + B->basic_off[k];
+                bp.src_stride = static_cast<long long>(stride[i]);
+                bp.dst_stride = static_cast<long long>(stride[i]);
+                bp.width = width[i];
+                bp.height = height[i];
+                bp.block_size = pp.block_size;
+                bp.absmax = static_cast<float *>(B->absmax.ptr) + k;
+                q.push_back(bp);
+            }
         }
         DevBuf &dbuf = st ? B->planes_f : B->planes_b;
+        (st ? B->nq_f : B->nq_b) = static_cast<int>(q.size());
         if (!q.empty()) {
             if ((rc = ensure(ctx, dbuf, sizeof(BatchPlane<float>) * q.size())) != BM3D_OK) return fail(rc);
             CK(ctx, cudaMemcpy(dbuf.ptr, q.data(), sizeof(BatchPlane<float>) * q.size(),
@@ -1962,13 +1993,15 @@ extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_para
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaStreamCreate"));
     // planes whose basic stage is a copy must hold src before the final stage tunes
     for (int i = 0; i < count; ++i)
-        if (B->gb[i] != Guard::Run) {
-            float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[i];
-            e = cudaMemcpy2DAsync(bi, stride[i] * 4, src[i], stride[i] * 4, width[i] * 4, height[i],
+        for (int c = 0; c < npl; ++c) {
+            if (B->gb[i] == Guard::Run && (npl == 1 || basic[i].sigma[c] > 0)) continue;
+            const int k = i * npl + c;
+            float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[k];
+            e = cudaMemcpy2DAsync(bi, stride[i] * 4, src[k], stride[i] * 4, width[i] * 4, height[i],
                                   cudaMemcpyDeviceToDevice, B->cap);
             if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemcpy2DAsync"));
         }
-    e = cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * count, B->cap);
+    e = cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * count * npl, B->cap);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemsetAsync"));
     if ((rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap)) != BM3D_OK) return fail(rc);
     if ((rc = tune_stage<true>(B, B->sf, B->planes_f, autotune != 0, B->cap)) != BM3D_OK) return fail(rc);
@@ -1990,6 +2023,24 @@ extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_para
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaGraphInstantiate"));
     *out = B;
     return BM3D_OK;
+}
+
+extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                                 const bm3d_stage_params *final_, float *const dst[],
+                                 const float *const src[], const int width[], const int height[],
+                                 const size_t stride[], int autotune, bm3d_batch **out)
+{
+    return batch_create_any(ctx, 1, count, basic, final_, dst, src, width, height, stride,
+                            autotune, out);
+}
+
+extern "C" int bm3d_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                                  const bm3d_stage_params *final_, float *const dst[],
+                                  const float *const src[], const int width[], const int height[],
+                                  const size_t stride[], int autotune, bm3d_batch **out)
+{
+    return batch_create_any(ctx, 3, count, basic, final_, dst, src, width, height, stride,
+                            autotune, out);
 }
 
 extern "C" int bm3d_batch_run(bm3d_batch *B, void *stream)

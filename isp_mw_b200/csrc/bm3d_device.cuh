@@ -303,16 +303,34 @@ struct SmemPlan {
     size_t warp_bytes;
     size_t scratch_bytes;        // group buffer(s) / search list union at the start of a warp's area
     size_t refblk_bytes;         // generic path: copy of the reference block
+    size_t off_groups;           // three-plane register-resident path: the tile's group lists
     size_t total;
 };
 
+// Bytes of dynamic shared memory this launch was given.
+__device__ __forceinline__ unsigned dynamic_smem_bytes()
+{
+    unsigned v;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(v));
+    return v;
+}
+
+// Shared-memory layout of one CTA. The register-resident kernel runs three
+// planes one after another through a single plane's windows: it then also
+// keeps the tile's group lists, per reference block kGSMax 16-bit positions
+// relative to the window (windows under 255 x 255) and a count byte.
 template <typename T>
 __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alias_mask,
                                               int region_h, int region_pitch, int key_slots,
                                               int nwarps, bool generic = false, int bs = kBS,
-                                              int gs = kGSMax)
+                                              int gs = kGSMax, int tile_refs = 0)
 {
     SmemPlan s;
+    const bool seq3 = nplanes == 3 && !generic;
+    if (seq3) {
+        nplanes = 1;
+        alias_mask &= 1;
+    }
     int nref = 0;
     const int nref_planes = wiener ? nplanes : 1;
     for (int p = 0; p < nref_planes; ++p)
@@ -338,7 +356,10 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
     // group list (kGSTab BlockPos) | group keys (kGSTab T)
     s.warp_bytes = (s.scratch_bytes + s.refblk_bytes + sizeof(SortKey<T>) * kCand +
                     sizeof(BlockPos) * kGSTab + sizeof(T) * kGSTab + 15) / 16 * 16;
-    s.total = s.off_warps + s.warp_bytes * nwarps;
+    s.off_groups = (s.off_warps + s.warp_bytes * nwarps + 15) / 16 * 16;
+    s.total = seq3 ? s.off_groups + static_cast<size_t>(tile_refs) * (2 * kGSMax + 1)
+                   : s.off_warps + s.warp_bytes * nwarps;
+    if (seq3 && (region_h > 255 || region_pitch > 255)) s.total = ~size_t(0) >> 1;  // too wide
     return s;
 }
 

@@ -58,7 +58,7 @@ __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab)
 template <typename T>
 __device__ int match_generic(const StageArgs<T> &a, const Tile<T> &t, int j0, int i0, int lane,
                              SortKey<T> *keys, T *refblk, SortKey<T> *heap, BlockPos *list,
-                             T *lkeys, unsigned long long &n_cand, unsigned long long &n_fix)
+                             T *lkeys, unsigned &n_cand, unsigned &n_fix)
 {
     using K = SortKey<T>;
     if (!a.match) {
@@ -107,7 +107,7 @@ __device__ int match_generic(const StageArgs<T> &a, const Tile<T> &t, int j0, in
         keys[c] = ok ? K::make(key_from_dist(d, a.distMul), static_cast<unsigned>(c)) : K::invalid();
     }
     __syncwarp();
-    n_cand += static_cast<unsigned long long>(ngrid);
+    n_cand += static_cast<unsigned>(ngrid);
     return select_group<T>(a, keys, ngrid, nc, tp, l, st, j0, i0, lane, heap, list, lkeys, n_fix);
 }
 
@@ -115,7 +115,7 @@ __device__ int match_generic(const StageArgs<T> &a, const Tile<T> &t, int j0, in
 template <typename T, bool WIENER>
 __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
                                int n, int lane, T *Gs, T *Gr, float scale,
-                               unsigned long long &n_bad)
+                               unsigned &n_bad)
 {
     const int bs = t.bs, bsq = bs * bs, total = n * bsq;
     for (int e = lane; e < total; e += kWarp) {
@@ -177,7 +177,8 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
 }
 
 template <typename T, bool WIENER, int NPL>
-__device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int tile, unsigned char *smem)
+__device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int tile, unsigned char *smem,
+                                                  unsigned avail)
 {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -189,6 +190,10 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
     tile_window(a, tile, bs, t, kx0, kx1, ky0, ky1);
     const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
                                      a.key_slots, nwarps, true, bs, a.group_size);
+    if (sp.total > avail) {  // launched with less shared memory than the layout needs
+        smem_shortfall(a);
+        return;
+    }
     carve_tile<T, WIENER, NPL>(a, sp, smem, t);
     stage_tile<T, WIENER, NPL>(a, t);
 
@@ -204,7 +209,8 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
     BlockPos *list = reinterpret_cast<BlockPos *>(after + sizeof(SortKey<T>) * kCand);
     T *lkeys = reinterpret_cast<T *>(after + sizeof(SortKey<T>) * kCand + sizeof(BlockPos) * kGSTab);
 
-    unsigned long long n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
+    // per-tile counters (small: 32 bits suffice), flushed once per tile
+    unsigned n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
     float scale[NPL];
 #pragma unroll
     for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
@@ -215,7 +221,7 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
         const int n = match_generic<T>(a, t, j0, i0, lane, keys, refblk, heap, list, lkeys,
                                        n_cand, n_fix);
         n_sum += n;
-        n_sq += static_cast<unsigned long long>(n) * n;
+        n_sq += static_cast<unsigned>(n * n);
         dump_group(a, ky, kx, n, lane, list, lkeys);
         if (!a.bm_only) {
 #pragma unroll
@@ -235,7 +241,7 @@ template <typename T, bool WIENER, int NPL>
 __global__ void __launch_bounds__(256) generic_stage_kernel(const StageArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    generic_tile_body<T, WIENER, NPL>(a, blockIdx.x, smem);
+    generic_tile_body<T, WIENER, NPL>(a, blockIdx.x, smem, dynamic_smem_bytes());
 }
 
 }  // namespace bm3d

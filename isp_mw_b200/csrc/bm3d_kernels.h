@@ -13,8 +13,8 @@ namespace bm3d {
 template <typename T, bool W, int NPL, int KS> const void *stage_kernel_fn();
 // generic_stage_kernel<T, W, NPL> (bm3d_generic.cuh)
 template <typename T, bool W, int NPL> const void *generic_kernel_fn();
-// batch_stage_kernel<float, W, 1, KS, GENERIC> (bm3d_batch.cuh)
-template <bool W, int KS, bool GENERIC> const void *batch_kernel_fn();
+// batch_stage_kernel<float, W, NPL, KS, GENERIC> (bm3d_batch.cuh)
+template <bool W, int NPL, int KS, bool GENERIC> const void *batch_kernel_fn();
 
 // Cosine matrices for group lengths 1..16 (1496 entries each) and the start
 // of length n at off[n] (17 entries).

@@ -238,7 +238,7 @@ __device__ __forceinline__ bool block_in_tile(const Tile<T> &t, int py, int px)
 template <typename T>
 __device__ int select_group(const StageArgs<T> &a, const SortKey<T> *keys, int ngrid, int nc,
                             int tp, int l, int st, int j0, int i0, int lane, SortKey<T> *heap,
-                            BlockPos *list, T *lkeys, unsigned long long &n_fix)
+                            BlockPos *list, T *lkeys, unsigned &n_fix)
 {
     using K = SortKey<T>;
     const int GS = a.group_size;
@@ -414,7 +414,7 @@ __device__ int select_group(const StageArgs<T> &a, const SortKey<T> *keys, int n
 template <typename T, int KS>
 __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int i0, int lane,
                            SortKey<T> *keys, SortKey<T> *heap, BlockPos *list, T *lkeys,
-                           unsigned long long &n_cand, unsigned long long &n_fix)
+                           unsigned &n_cand, unsigned &n_fix)
 {
     using K = SortKey<T>;
     const int GS = a.group_size;
@@ -512,7 +512,7 @@ __device__ int match_block(const StageArgs<T> &a, const Tile<T> &t, int j0, int 
         }
     }
     __syncwarp();
-    n_cand += static_cast<unsigned long long>(ngrid);  // grid minus self, plus (0, 0)
+    n_cand += static_cast<unsigned>(ngrid);  // grid minus self, plus (0, 0)
 
     return select_group<T>(a, keys, ngrid, nc, tp, l, st, j0, i0, lane, heap, list, lkeys, n_fix);
 }
@@ -576,7 +576,7 @@ template <> struct Vec4<double> {
 template <typename T>
 __device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win, const T *origin,
                                                   const BlockPos *list, int n, int lane, T *G,
-                                                  unsigned long long &n_bad)
+                                                  unsigned &n_bad)
 {
     const int z = lane >> 1, h = lane & 1;
     T *gz = G + z * kGroupStride;
@@ -678,8 +678,11 @@ __device__ __forceinline__ double wiener_weight(double y2, double s2) { return y
 // accumulator windows.
 template <typename T, bool WIENER>
 __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
-                             int n, int lane, T *G, float scale, unsigned long long &n_bad)
+                             int n, int lane, T *G, float scale, unsigned &n_bad, int pt = -1)
 {
+    // p indexes the tile's windows; pt (default p) the plane's threshold /
+    // Wiener tables, which differ when planes share one set of windows
+    if (pt < 0) pt = p;
     T sa[kGSMax], sb[kGSMax];
     T ra[kGSMax], rb[kGSMax];
     if (WIENER) {
@@ -698,7 +701,7 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
         // thr depends on how many of (x, y, z) are 0 (source/BM3D.cpp:52-67).
         // pencil a = (lane / 4, 2 (lane % 4)), pencil b = (lane / 4, 2 (lane % 4) + 1)
         const int fa = ((lane & 3) == 0) + (lane < 4), fb = (lane < 4);
-        const T *thr = a.thr[p][n - 1];
+        const T *thr = a.thr[pt][n - 1];
         int kept = 0;
 #pragma unroll
         for (int z = 0; z < kGSMax; ++z) {
@@ -715,7 +718,7 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
     } else {
         // Empirical Wiener shrinkage guided by the basic estimate
         // (source/BM3D.cpp:435-443).
-        const T s2 = a.wss[p][n - 1];
+        const T s2 = a.wss[pt][n - 1];
         T l2 = T(0);
 #pragma unroll
         for (int z = 0; z < kGSMax; ++z) {
@@ -915,24 +918,35 @@ __device__ __forceinline__ void dump_group(const StageArgs<T> &a, int ky, int kx
     }
 }
 
+// A CTA whose launch gave it less shared memory than its layout needs does
+// no work and counts itself in the invariant counter (host-mode calls then
+// fail with an internal error) instead of touching memory past its share.
 template <typename T>
-__device__ __forceinline__ void flush_stats(const StageArgs<T> &a, int lane, unsigned long long n_sum,
-                                            unsigned long long n_sq, unsigned long long n_cand,
-                                            unsigned long long n_fix, unsigned long long n_bad)
+__device__ __forceinline__ void smem_shortfall(const StageArgs<T> &a)
 {
+    if (a.stats != nullptr && threadIdx.x == 0) atomicAdd(a.stats + 4, 1ull << 32);
+}
+
+template <typename T>
+__device__ __forceinline__ void flush_stats(const StageArgs<T> &a, int lane, unsigned n_sum,
+                                            unsigned n_sq, unsigned n_cand, unsigned n_fix,
+                                            unsigned n_bad)
+{
+    using U = unsigned long long;
     if (a.stats != nullptr && lane == 0) {
-        atomicAdd(a.stats + 0, n_sum);
-        atomicAdd(a.stats + 1, n_sq);
-        atomicAdd(a.stats + 2, n_cand);
-        atomicAdd(a.stats + 3, n_fix);
+        atomicAdd(a.stats + 0, static_cast<U>(n_sum));
+        atomicAdd(a.stats + 1, static_cast<U>(n_sq));
+        atomicAdd(a.stats + 2, static_cast<U>(n_cand));
+        atomicAdd(a.stats + 3, static_cast<U>(n_fix));
     }
-    if (a.stats != nullptr && n_bad) atomicAdd(a.stats + 4, n_bad);
+    if (a.stats != nullptr && n_bad) atomicAdd(a.stats + 4, static_cast<U>(n_bad));
 }
 
 // ---------------------------------------------------------------------------
 // Register-resident stage: BlockSize 8, GroupSize <= 16. One tile per call.
 template <typename T, bool WIENER, int NPL, int KS>
-__device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile, unsigned char *smem)
+__device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile, unsigned char *smem,
+                                                unsigned avail)
 {
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -943,6 +957,10 @@ __device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile,
     tile_window(a, tile, kBS, t, kx0, kx1, ky0, ky1);
     const SmemPlan sp = plan_smem<T>(NPL, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
                                      a.key_slots, nwarps);
+    if (sp.total > avail) {  // launched with less shared memory than the layout needs
+        smem_shortfall(a);
+        return;
+    }
     carve_tile<T, WIENER, NPL>(a, sp, smem, t);
     stage_tile<T, WIENER, NPL>(a, t);
 
@@ -956,7 +974,8 @@ __device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile,
     T *lkeys = reinterpret_cast<T *>(wbase + scratch + sizeof(SortKey<T>) * kCand +
                                      sizeof(BlockPos) * kGSTab);
 
-    unsigned long long n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
+    // per-tile counters (small: 32 bits suffice), flushed once per tile
+    unsigned n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
     float scale[NPL];
 #pragma unroll
     for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
@@ -966,7 +985,7 @@ __device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile,
         const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
         const int n = match_block<T, KS>(a, t, j0, i0, lane, keys, heap, list, lkeys, n_cand, n_fix);
         n_sum += n;
-        n_sq += static_cast<unsigned long long>(n) * n;
+        n_sq += static_cast<unsigned>(n * n);
         dump_group(a, ky, kx, n, lane, list, lkeys);
         if (!a.bm_only) {
 #pragma unroll
@@ -982,11 +1001,160 @@ __device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile,
     flush_tile<T, NPL>(a, t);
 }
 
+// One plane c of a three-plane tile into the single-plane windows: src[c],
+// ref[c] where a stage reads it (matching on plane 0; Wiener on every plane),
+// zeroed sums. Ends with __syncthreads().
+template <typename T, bool WIENER>
+__device__ __forceinline__ void stage_plane(const StageArgs<T> &a, const Tile<T> &t, int c)
+{
+    const int tid = threadIdx.x;
+    const int npx = t.rh * t.rw;
+    const int bs = t.bs, bsq = bs * bs;
+    const bool ref_sep = t.refw[0] != t.srcw[0];
+    const bool need_ref = ref_sep && (WIENER || c == 0);
+    const bool filt = !a.bm_only && (a.active & (1 << c));
+    for (int i = tid; i < npx; i += blockDim.x) {
+        const int y = i / t.rw, x = i - y * t.rw;
+        const long long g = static_cast<long long>(t.ry0 + y) * a.stride + (t.rx0 + x);
+        const int s = y * t.pitch + x;
+        const_cast<T *>(t.srcw[0])[s] = __ldg(a.src[c] + g);
+        if (need_ref) const_cast<T *>(t.refw[0])[s] = __ldg(a.ref[c] + g);
+        if (filt) {
+            t.accN[0][s] = 0;
+            t.accD[0][s] = 0;
+        }
+    }
+    if (!t.origin_inside) {
+        for (int i = tid; i < bsq; i += blockDim.x) {
+            const int y = i / bs, x = i - y * bs;
+            const long long g = static_cast<long long>(y) * a.stride + x;
+            const_cast<T *>(t.src0[0])[i] = __ldg(a.src[c] + g);
+            if (need_ref) const_cast<T *>(t.ref0[0])[i] = __ldg(a.ref[c] + g);
+            t.accN0[0][i] = 0;
+            t.accD0[0][i] = 0;
+        }
+    }
+    __syncthreads();
+}
+
+// Flush plane c's accumulator windows (the single-plane windows) into its sums.
+template <typename T>
+__device__ __forceinline__ void flush_plane(const StageArgs<T> &a, const Tile<T> &t, int c)
+{
+    const int tid = threadIdx.x;
+    const int npx = t.rh * t.rw;
+    const int bs = t.bs, bsq = bs * bs;
+    for (int i = tid; i < npx; i += blockDim.x) {
+        const int y = i / t.rw, x = i - y * t.rw;
+        const int s = y * t.pitch + x;
+        const auto nv = t.accN[0][s], d = t.accD[0][s];
+        const long long g = static_cast<long long>(t.ry0 + y) * a.width + (t.rx0 + x);
+        if (nv != 0) acc_flush(a.num[c] + g, nv);
+        if (d != 0) acc_flush(a.den[c] + g, d);
+    }
+    if (!t.origin_inside) {
+        for (int i = tid; i < bsq; i += blockDim.x) {
+            const auto nv = t.accN0[0][i], d = t.accD0[0][i];
+            const int y = i / bs, x = i - y * bs;
+            const long long g = static_cast<long long>(y) * a.width + x;
+            if (nv != 0) acc_flush(a.num[c] + g, nv);
+            if (d != 0) acc_flush(a.den[c] + g, d);
+        }
+    }
+}
+
+// Three planes sharing the groups matched on plane 0 (BM3D_Base::Kernel's
+// 9-plane form, source/BM3D.cpp:139-218), one plane at a time through a
+// single plane's windows: plane 0 matches and keeps each reference block's
+// group list in shared memory, planes 1 and 2 re-stage their windows and
+// filter with those lists. Per plane the arithmetic is that of the
+// one-plane tile, so results equal the all-planes-resident form bit for bit
+// while the footprint stays that of one plane (full-size tiles).
+template <typename T, bool WIENER, int KS>
+__device__ __forceinline__ void stage_tile_body_seq3(const StageArgs<T> &a, int tile,
+                                                     unsigned char *smem, unsigned avail)
+{
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int right = a.width - kBS, bottom = a.height - kBS;
+
+    Tile<T> t;
+    int kx0, kx1, ky0, ky1;
+    tile_window(a, tile, kBS, t, kx0, kx1, ky0, ky1);
+    const SmemPlan sp = plan_smem<T>(3, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
+                                     a.key_slots, nwarps, false, kBS, kGSMax,
+                                     a.tile_x * a.tile_y);
+    if (sp.total > avail) {  // launched with less shared memory than the layout needs
+        smem_shortfall(a);
+        return;
+    }
+    carve_tile<T, WIENER, 1>(a, sp, smem, t);  // every plane goes through windows [0]
+    // group lists: position (y - ry0) << 8 | (x - rx0), or 0xffff for a
+    // (0, 0) block held outside the window; then one count byte per block
+    unsigned short *gpos = reinterpret_cast<unsigned short *>(smem + sp.off_groups);
+    unsigned char *gn = reinterpret_cast<unsigned char *>(gpos + a.tile_x * a.tile_y * kGSMax);
+
+    unsigned char *wbase = smem + sp.off_warps + sp.warp_bytes * warp;
+    const size_t scratch = sp.scratch_bytes;
+    T *G = reinterpret_cast<T *>(wbase);
+    SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
+    SortKey<T> *heap = reinterpret_cast<SortKey<T> *>(wbase + scratch);
+    BlockPos *list = reinterpret_cast<BlockPos *>(wbase + scratch + sizeof(SortKey<T>) * kCand);
+    T *lkeys = reinterpret_cast<T *>(wbase + scratch + sizeof(SortKey<T>) * kCand +
+                                     sizeof(BlockPos) * kGSTab);
+
+    // per-tile counters (small: 32 bits suffice), flushed once per tile
+    unsigned n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
+    const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
+    for (int c = 0; c < 3; ++c) {
+        const bool filt = !a.bm_only && (a.active & (1 << c));
+        if (c > 0 && !filt) continue;
+        stage_plane<T, WIENER>(a, t, c);
+        const float scale = fixed_scale(a.absmax[c], a.log2_bound);
+        for (int r = warp; r < nrefs; r += nwarps) {
+            int n;
+            if (c == 0) {
+                const int ky = ky0 + r / tw, kx = kx0 + r % tw;
+                const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
+                n = match_block<T, KS>(a, t, j0, i0, lane, keys, heap, list, lkeys, n_cand, n_fix);
+                n_sum += n;
+                n_sq += static_cast<unsigned>(n * n);
+                dump_group(a, ky, kx, n, lane, list, lkeys);
+                if (lane == 0) gn[r] = static_cast<unsigned char>(n);
+                for (int k = lane; k < n; k += kWarp) {
+                    const BlockPos q = list[k];
+                    const bool outside = q.y == 0 && q.x == 0 && !t.origin_inside;
+                    gpos[r * kGSMax + k] = outside ? 0xffff
+                                                   : static_cast<unsigned short>(
+                                                         ((q.y - t.ry0) << 8) | (q.x - t.rx0));
+                }
+            } else {
+                n = gn[r];
+                for (int k = lane; k < n; k += kWarp) {
+                    const unsigned v = gpos[r * kGSMax + k];
+                    list[k] = v == 0xffffu ? BlockPos{0, 0}
+                                           : BlockPos{t.ry0 + static_cast<int>(v >> 8),
+                                                      t.rx0 + static_cast<int>(v & 0xffu)};
+                }
+            }
+            __syncwarp();
+            if (filt) filter_group<T, WIENER>(a, t, 0, list, n, lane, G, scale, n_bad, c);
+            __syncwarp();
+        }
+        __syncthreads();
+        if (filt) flush_plane<T>(a, t, c);
+        __syncthreads();  // the windows are re-staged for the next plane
+    }
+    flush_stats(a, lane, n_sum, n_sq, n_cand, n_fix, n_bad);
+}
+
 template <typename T, bool WIENER, int NPL, int KS>
 __global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    stage_tile_body<T, WIENER, NPL, KS>(a, blockIdx.x, smem);
+    const unsigned avail = dynamic_smem_bytes();
+    if constexpr (NPL == 3) stage_tile_body_seq3<T, WIENER, KS>(a, blockIdx.x, smem, avail);
+    else stage_tile_body<T, WIENER, NPL, KS>(a, blockIdx.x, smem, avail);
 }
 
 // dst = num / den (source/BM3D.cpp:130-135, include/Image_Type.hpp:319-332).

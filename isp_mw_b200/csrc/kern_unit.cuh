@@ -17,9 +17,9 @@ template <typename T, bool W, int NPL> const void *generic_kernel_fn()
     return reinterpret_cast<const void *>(&generic_stage_kernel<T, W, NPL>);
 }
 
-template <bool W, int KS, bool GENERIC> const void *batch_kernel_fn()
+template <bool W, int NPL, int KS, bool GENERIC> const void *batch_kernel_fn()
 {
-    return reinterpret_cast<const void *>(&batch_stage_kernel<float, W, 1, KS, GENERIC>);
+    return reinterpret_cast<const void *>(&batch_stage_kernel<float, W, NPL, KS, GENERIC>);
 }
 
 static cudaError_t upload_dct_tables_here(const DctTableData &t)

@@ -45,3 +45,47 @@ def test_batch_equals_per_plane(bm3d_lib, autotune):
     assert all(v > 0 for v in t["basic"] + t["final"])
     batch.close()
     ctx.close()
+
+
+@pytest.mark.parametrize("autotune", [False, True])
+def test_batch3_equals_per_image(bm3d_lib, autotune):
+    """Three-plane images (groups matched on Y, reused by U and V) in one
+    batch equal per-image bm3d_full3, including an image whose chroma sigma
+    is 0 (that plane passes through) and one whose stages are guarded."""
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    ctx = isp_mw_b200.Context(0)
+    shapes = [(120, 160), (97, 211), (64, 72), (180, 140)]
+    srcs, dsts, pbs, pfs, want = [], [], [], [], []
+    for k, (h, w) in enumerate(shapes):
+        planes = [torch.from_numpy(synth.pair(h, w, s, 500 + 3 * k + c)[1]).cuda()
+                  for c, s in enumerate((15.0, 10.0, 10.0))]
+        sp = [synth.sigma_param(15.0, 0), synth.sigma_param(10.0, 1), synth.sigma_param(10.0, 2)]
+        pb = isp_mw_b200.stage_params_default("fast", False, sp)
+        pf = isp_mw_b200.stage_params_default("fast", True, sp)
+        if k == 1:
+            pb.sigma[2] = pf.sigma[2] = 0.0  # V passes through
+        if k == 2:
+            for c in range(3):  # guard: every sigma 0, all planes copied
+                pb.sigma[c] = pf.sigma[c] = 0.0
+        ref = [torch.empty_like(p) for p in planes]
+        ctx.full3(pb, pf, ref, planes)
+        srcs.append(planes)
+        dsts.append([torch.full_like(p, -1.0) for p in planes])
+        pbs.append(pb)
+        pfs.append(pf)
+        want.append(ref)
+    batch = isp_mw_b200.Batch(ctx, pbs, pfs, dsts, srcs, autotune=autotune)
+    for _ in range(2):
+        for d in dsts:
+            for p in d:
+                p.fill_(-1.0)
+        batch.run()
+        torch.cuda.synchronize()
+        for k in range(len(shapes)):
+            for c in range(3):
+                assert torch.equal(dsts[k][c], want[k][c]), (k, c)
+    assert torch.equal(dsts[1][2], srcs[1][2])
+    batch.close()
+    ctx.close()
