@@ -325,3 +325,42 @@ def test_profiles_against_oracle(ctx, oracle_mod, profile, shape, s255):
     final = np.empty_like(noisy)
     ctx.stage(f, True, final, noisy, basic)
     assert_close(name + ":final", final, orc.stage(True, f.as_dict(), noisy, basic))
+
+
+@pytest.mark.parametrize("shape", [(8, 8), (8, 40), (40, 8), (9, 9), (16, 300), (300, 16),
+                                   (0, 0)], ids=lambda s: f"{s[1]}x{s[0]}")
+def test_edge_sizes_against_oracle(ctx, oracle_mod, shape):
+    """Planes of one block, one block row or column, and thin strips: each
+    stage on identical inputs against the oracle (groups exact, outputs within
+    the bar), one and three planes. An empty plane is rejected."""
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    sp = [synth.sigma_param(25.0)] * 3
+    b = isp_mw_b200.stage_params_default("fast", False, sp)
+    f = isp_mw_b200.stage_params_default("fast", True, sp)
+    h, w = shape
+    if h == 0:  # straight through the C ABI: the Python wrapper refuses empty arrays itself
+        import ctypes
+        buf = np.zeros(64, np.float32)
+        for w0, h0 in ((0, 0), (0, 8), (8, 0)):
+            rc = ctx.lib.bm3d_stage(ctx.h, ctypes.byref(b), 0, buf.ctypes.data, buf.ctypes.data,
+                                    buf.ctypes.data, w0, h0, 8, 1.0, isp_mw_b200.MEM_HOST, None)
+            assert rc == isp_mw_b200.BM3D_ERR_INVALID
+        return
+    orc = _oracle(oracle_mod)
+    _, noisy = synth.pair(h, w, 25.0, 60 + h + w)
+    name = f"edge_{w}x{h}"
+    gb = ctx.debug_groups(b, False, noisy)
+    assert group_match(name + ":basic_groups", gb, orc.groups(False, b.as_dict(), noisy)) == 1.0
+    basic = np.empty_like(noisy)
+    ctx.stage(b, False, basic, noisy)
+    assert_close(name + ":basic", basic, orc.stage(False, b.as_dict(), noisy))
+    final = np.empty_like(noisy)
+    ctx.stage(f, True, final, noisy, basic)
+    assert_close(name + ":final", final, orc.stage(True, f.as_dict(), noisy, basic))
+    planes = [synth.pair(h, w, 25.0, 70 + c)[1] for c in range(3)]
+    b3 = [p.copy() for p in planes]
+    ctx.stage3(b, False, b3, planes)
+    want = orc.stage3(False, b.as_dict(), planes)
+    for c in range(3):
+        assert_close(name + f":basic3_{c}", b3[c], want[c])
