@@ -277,6 +277,30 @@ int bm3d_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
                        const float *const src[], const int width[], const int height[],
                        const size_t stride[], int autotune, bm3d_batch **out);
 int bm3d_batch_run(bm3d_batch *batch, void *stream);
+/* Batches fed from HOST memory: `count` planes (sizes and parameters fixed
+ * at creation; device buffers owned by the batch). Each bm3d_host_batch_run
+ * uploads src, runs the batch graph on `stream` and downloads dst; the batch
+ * keeps two device slots, so with page-locked host planes one run's uploads
+ * and downloads overlap the neighbouring runs' filtering.
+ *   async = 0: returns with dst written.
+ *   async = 1: returns once enqueued; `stream` completes after this run's
+ *              download (which also holds the next run's filtering behind it).
+ *   async = 2: returns once enqueued without tying `stream` to the download,
+ *              so consecutive runs overlap fully; bm3d_host_batch_join then
+ *              makes `stream` wait for every download issued so far.
+ * Synchronise (after joining) before reading dst or reusing src. The first
+ * run on each slot builds its graph (the autotuner times that run's data)
+ * and waits for it. Results equal per-plane bm3d_full bit for bit. No
+ * counterpart in the reference. */
+typedef struct bm3d_host_batch bm3d_host_batch;
+int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                           const bm3d_stage_params *final_, const int width[], const int height[],
+                           int autotune, bm3d_host_batch **out);
+int bm3d_host_batch_run(bm3d_host_batch *batch, float *const dst[], const float *const src[],
+                        const size_t stride[], int async, void *stream);
+int bm3d_host_batch_join(bm3d_host_batch *batch, void *stream);
+void bm3d_host_batch_destroy(bm3d_host_batch *batch);
+
 /* tile_x, tile_y, warps of the basic stage, then of the final stage. */
 int bm3d_batch_tuning(const bm3d_batch *batch, int out[6]);
 void bm3d_batch_destroy(bm3d_batch *batch);

@@ -40,7 +40,8 @@ EXPORTS = [
     "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
     "bm3d_stage_noalloc", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
     "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
-    "bm3d_full_many", "bm3d_batch3_create",
+    "bm3d_full_many", "bm3d_batch3_create", "bm3d_host_batch_create", "bm3d_host_batch_run",
+    "bm3d_host_batch_join", "bm3d_host_batch_destroy",
 ]
 
 
@@ -123,6 +124,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                       ctypes.POINTER(vp)]
     lib.bm3d_batch3_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
                                        ctypes.POINTER(vp)]
+    lib.bm3d_host_batch_create.argtypes = [vp, ip, vp, vp, vp, vp, ip, ctypes.POINTER(vp)]
+    lib.bm3d_host_batch_run.argtypes = [vp, vp, vp, vp, ip, vp]
+    lib.bm3d_host_batch_join.argtypes = [vp, vp]
+    lib.bm3d_host_batch_destroy.argtypes = [vp]
+    lib.bm3d_host_batch_destroy.restype = None
     lib.bm3d_batch_run.argtypes = [vp, vp]
     lib.bm3d_batch_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     lib.bm3d_batch_destroy.argtypes = [vp]
@@ -451,6 +457,77 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             self.ctx.lib.bm3d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class HostBatch:
+    """``bm3d_host_batch``: a batch fed from host planes (numpy arrays or CPU
+    tensors; page-locked for overlap). Sizes and parameters are fixed at
+    creation; each ``run`` uploads ``src``, filters and downloads into ``dst``.
+    With ``asynchronous`` the call returns once enqueued on ``stream``
+    (default: the current torch stream), and consecutive runs overlap their
+    copies with one another's filtering; synchronise before reading ``dst``."""
+
+    def __init__(self, ctx: "Context", basic: Sequence[StageParams], final: Sequence[StageParams],
+                 shapes: Sequence, autotune: bool = True):
+        n = len(shapes)
+        if not (len(basic) == len(final) == n) or n == 0:
+            raise ValueError("one basic/final parameter set per plane")
+        self.ctx = ctx
+        self.shapes = [(int(h), int(w)) for h, w in shapes]
+        pb = (StageParams * n)(*basic)
+        pf = (StageParams * n)(*final)
+        w = (ctypes.c_int * n)(*[s[1] for s in self.shapes])
+        h = (ctypes.c_int * n)(*[s[0] for s in self.shapes])
+        self.h = ctypes.c_void_p()
+        rc = ctx.lib.bm3d_host_batch_create(ctx.h, n, pb, pf, w, h, int(autotune),
+                                            ctypes.byref(self.h))
+        ctx._check(rc, allow_copied=False)
+        self.pixels = sum(a * b for a, b in self.shapes)
+
+    def run(self, dst, src, asynchronous=False, stream: Optional[int] = None):
+        """asynchronous: False (dst written on return), True (enqueued; the
+        stream completes after this run's download) or "overlap" (enqueued,
+        no wait tied to the stream: call join() before synchronising)."""
+        n = len(self.shapes)
+        if len(dst) != n or len(src) != n:
+            raise ValueError("one dst and src plane per batch plane")
+        di = [_plane_info(x) for x in dst]
+        si = [_plane_info(x) for x in src]
+        for k, (a, b) in enumerate(zip(di, si)):
+            if a[1] != MEM_HOST or b[1] != MEM_HOST:
+                raise ValueError("host batches take host planes")
+            if (a[3], a[2]) != self.shapes[k] or (b[3], b[2]) != self.shapes[k] or a[4] != b[4]:
+                raise ValueError("plane size or stride does not match the batch")
+        if stream is None:
+            try:
+                import torch
+                stream = torch.cuda.current_stream(self.ctx.device).cuda_stream
+            except Exception:
+                stream = 0
+        vp = ctypes.c_void_p * n
+        st = (ctypes.c_size_t * n)(*[i[4] for i in si])
+        mode = 2 if asynchronous == "overlap" else int(bool(asynchronous))
+        rc = self.ctx.lib.bm3d_host_batch_run(self.h, vp(*[i[0] for i in di]),
+                                              vp(*[i[0] for i in si]), st, mode, stream)
+        self.ctx._check(rc, allow_copied=False)
+
+    def join(self, stream: Optional[int] = None):
+        """Make ``stream`` wait for every download issued so far."""
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream(self.ctx.device).cuda_stream
+        self.ctx._check(self.ctx.lib.bm3d_host_batch_join(self.h, stream), allow_copied=False)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.bm3d_host_batch_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -1859,8 +1859,10 @@ int time_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, cudaStream_
 // Pick the tiling of one stage: the fastest candidate that fits, or the
 // default when not autotuning.
 template <bool W>
-int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotune, cudaStream_t s)
+int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotune, cudaStream_t s,
+               const int *force = nullptr)
 {
+    if (force) return build_stage(B, W, force[0], force[1], force[2], sbd);  // a known tiling
     const bm3d_stage_params &p = W ? B->pf[0] : B->pb[0];
     const bool generic = !fast_args(p.block_size, p.group_size);
     static const int fast_cand[][3] = {{8, 8, 16}, {7, 7, 16}, {6, 8, 12}, {8, 6, 12},
@@ -1902,7 +1904,8 @@ int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotu
 static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_params *basic,
                             const bm3d_stage_params *final_, float *const dst[],
                             const float *const src[], const int width[], const int height[],
-                            const size_t stride[], int autotune, bm3d_batch **out)
+                            const size_t stride[], int autotune, bm3d_batch **out,
+                            const int *force_tiling = nullptr)
 {
     if (!ctx || !out || count < 1 || !basic || !final_ || !dst || !src || !width || !height ||
         !stride)
@@ -2003,8 +2006,12 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
         }
     e = cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * count * npl, B->cap);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemsetAsync"));
-    if ((rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap)) != BM3D_OK) return fail(rc);
-    if ((rc = tune_stage<true>(B, B->sf, B->planes_f, autotune != 0, B->cap)) != BM3D_OK) return fail(rc);
+    if ((rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap,
+                                force_tiling)) != BM3D_OK)
+        return fail(rc);
+    if ((rc = tune_stage<true>(B, B->sf, B->planes_f, autotune != 0, B->cap,
+                               force_tiling ? force_tiling + 3 : nullptr)) != BM3D_OK)
+        return fail(rc);
     e = cudaStreamSynchronize(B->cap);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "batch tuning"));
     // capture the pipeline once
@@ -2076,4 +2083,168 @@ extern "C" void bm3d_batch_destroy(bm3d_batch *B)
                       &B->sb.args, &B->sb.base, &B->sf.args, &B->sf.base})
         if (b->ptr) cudaFree(b->ptr);
     delete B;
+}
+
+// ---------------------------------------------------------------------------
+// Batches fed from host memory: two device slots, each with its own batch
+// graph; uploads, filtering and downloads of consecutive runs overlap.
+
+struct bm3d_host_batch {
+    bm3d_ctx *ctx = nullptr;
+    int n = 0;
+    std::vector<bm3d_stage_params> pb, pf;
+    std::vector<int> w, h;
+    std::vector<size_t> off;  // element offset of each plane in a slot's buffers
+    size_t total = 0;         // floats per slot buffer
+    int autotune = 1;
+    struct Slot {
+        bm3d_batch *batch = nullptr;
+        DevBuf src, dst;
+        cudaEvent_t uploaded = nullptr, filtered = nullptr, drained = nullptr;
+        bool used = false;
+    } slot[2];
+    cudaStream_t up = nullptr, down = nullptr;
+    unsigned long long runs = 0;
+};
+
+extern "C" void bm3d_host_batch_destroy(bm3d_host_batch *H)
+{
+    if (!H) return;
+    cudaSetDevice(H->ctx->device);
+    if (H->up) cudaStreamSynchronize(H->up);
+    if (H->down) cudaStreamSynchronize(H->down);
+    for (auto &sl : H->slot) {
+        if (sl.batch) bm3d_batch_destroy(sl.batch);
+        if (sl.src.ptr) cudaFree(sl.src.ptr);
+        if (sl.dst.ptr) cudaFree(sl.dst.ptr);
+        for (cudaEvent_t e : {sl.uploaded, sl.filtered, sl.drained})
+            if (e) cudaEventDestroy(e);
+    }
+    if (H->up) cudaStreamDestroy(H->up);
+    if (H->down) cudaStreamDestroy(H->down);
+    delete H;
+}
+
+extern "C" int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                                      const bm3d_stage_params *final_, const int width[],
+                                      const int height[], int autotune, bm3d_host_batch **out)
+{
+    if (!ctx || !out || count < 1 || !basic || !final_ || !width || !height)
+        return BM3D_ERR_INVALID;
+    *out = nullptr;
+    CK(ctx, cudaSetDevice(ctx->device));
+    auto *H = new bm3d_host_batch;
+    H->ctx = ctx;
+    H->n = count;
+    H->autotune = autotune;
+    auto fail = [&](int rc) {
+        bm3d_host_batch_destroy(H);
+        return rc;
+    };
+    for (int i = 0; i < count; ++i) {
+        if (width[i] < 1 || height[i] < 1) return fail(BM3D_ERR_INVALID);
+        H->pb.push_back(basic[i]);
+        H->pf.push_back(final_[i]);
+        H->w.push_back(width[i]);
+        H->h.push_back(height[i]);
+        H->off.push_back(H->total);
+        H->total += static_cast<size_t>(width[i]) * height[i];
+    }
+    int rc;
+    for (auto &sl : H->slot) {
+        if ((rc = ensure(ctx, sl.src, sizeof(float) * H->total)) != BM3D_OK) return fail(rc);
+        if ((rc = ensure(ctx, sl.dst, sizeof(float) * H->total)) != BM3D_OK) return fail(rc);
+        cudaError_t e;
+        if ((e = cudaEventCreateWithFlags(&sl.uploaded, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&sl.filtered, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&sl.drained, cudaEventDisableTiming)) != cudaSuccess)
+            return fail(cuda_fail(ctx, e, "cudaEventCreate"));
+    }
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&H->up, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&H->down, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail(cuda_fail(ctx, e, "cudaStreamCreate"));
+    *out = H;
+    return BM3D_OK;
+}
+
+// The slot's batch graph over its device buffers; built on the first run that
+// uses the slot, so the autotuner times real data (slot 1 reuses slot 0's
+// tiling).
+static int host_batch_bind(bm3d_host_batch *H, int k)
+{
+    auto &sl = H->slot[k];
+    if (sl.batch) return BM3D_OK;
+    std::vector<float *> d(H->n);
+    std::vector<const float *> x(H->n);
+    std::vector<size_t> st(H->n);
+    for (int i = 0; i < H->n; ++i) {
+        d[i] = static_cast<float *>(sl.dst.ptr) + H->off[i];
+        x[i] = static_cast<const float *>(sl.src.ptr) + H->off[i];
+        st[i] = static_cast<size_t>(H->w[i]);
+    }
+    int tiling[6];
+    const int *force = nullptr;
+    if (k == 1 && H->slot[0].batch) {
+        bm3d_batch_tuning(H->slot[0].batch, tiling);
+        force = tiling;
+    }
+    return batch_create_any(H->ctx, 1, H->n, H->pb.data(), H->pf.data(), d.data(), x.data(),
+                            H->w.data(), H->h.data(), st.data(), H->autotune, &sl.batch, force);
+}
+
+extern "C" int bm3d_host_batch_run(bm3d_host_batch *H, float *const dst[],
+                                   const float *const src[], const size_t stride[], int async,
+                                   void *stream)
+{
+    if (!H || !dst || !src || !stride) return BM3D_ERR_INVALID;
+    for (int i = 0; i < H->n; ++i)
+        if (!dst[i] || !src[i] || stride[i] < static_cast<size_t>(H->w[i])) return BM3D_ERR_INVALID;
+    bm3d_ctx *ctx = H->ctx;
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int k = static_cast<int>(H->runs & 1);
+    auto &sl = H->slot[k];
+    // inputs: once this slot's previous run has been filtered
+    if (sl.used) CK(ctx, cudaStreamWaitEvent(H->up, sl.filtered, 0));
+    for (int i = 0; i < H->n; ++i)
+        CK(ctx, cudaMemcpy2DAsync(static_cast<float *>(sl.src.ptr) + H->off[i],
+                                  sizeof(float) * H->w[i], src[i], sizeof(float) * stride[i],
+                                  sizeof(float) * H->w[i], H->h[i], cudaMemcpyHostToDevice, H->up));
+    CK(ctx, cudaEventRecord(sl.uploaded, H->up));
+    if (!sl.batch) {  // first use: build (and tune) the slot's graph on these inputs
+        CK(ctx, cudaEventSynchronize(sl.uploaded));
+        const int rc = host_batch_bind(H, k);
+        if (rc != BM3D_OK) return rc;
+    }
+    CK(ctx, cudaStreamWaitEvent(s, sl.uploaded, 0));
+    if (sl.used) CK(ctx, cudaStreamWaitEvent(s, sl.drained, 0));  // outputs copied out
+    int rc = bm3d_batch_run(sl.batch, s);
+    if (rc != BM3D_OK) return rc;
+    CK(ctx, cudaEventRecord(sl.filtered, s));
+    CK(ctx, cudaStreamWaitEvent(H->down, sl.filtered, 0));
+    for (int i = 0; i < H->n; ++i)
+        CK(ctx, cudaMemcpy2DAsync(dst[i], sizeof(float) * stride[i],
+                                  static_cast<const float *>(sl.dst.ptr) + H->off[i],
+                                  sizeof(float) * H->w[i], sizeof(float) * H->w[i], H->h[i],
+                                  cudaMemcpyDeviceToHost, H->down));
+    CK(ctx, cudaEventRecord(sl.drained, H->down));
+    sl.used = true;
+    ++H->runs;
+    if (async == 2) return BM3D_OK;  // the caller joins later (bm3d_host_batch_join)
+    CK(ctx, cudaStreamWaitEvent(s, sl.drained, 0));  // `stream` completes after the download
+    if (async) return BM3D_OK;
+    CK(ctx, cudaStreamSynchronize(s));
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_host_batch_join(bm3d_host_batch *H, void *stream)
+{
+    if (!H) return BM3D_ERR_INVALID;
+    if (H->runs == 0) return BM3D_OK;
+    CK(H->ctx, cudaSetDevice(H->ctx->device));
+    // downloads run in order on one stream: the last one covers them all
+    CK(H->ctx, cudaStreamWaitEvent(static_cast<cudaStream_t>(stream),
+                                   H->slot[(H->runs - 1) & 1].drained, 0));
+    return BM3D_OK;
 }

@@ -18,7 +18,11 @@ def main():
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--groups-only", action="store_true",
                     help="run the stage's block matching alone (bm3d_debug_groups)")
+    ap.add_argument("--planes", type=int, choices=[1, 3], default=1,
+                    help="3: Y/U/V planes (sigma 15/10/10) sharing luma groups (bm3d_stage3)")
     args = ap.parse_args()
+    if args.planes == 3:
+        return three_planes(args)
 
     import torch
     import isp_mw_b200
@@ -44,6 +48,33 @@ def main():
     torch.cuda.synchronize()
     st = ctx.last_stats()
     print(f"stage={args.stage} {args.width}x{args.height} groups_sum_n={st[0]} candidates={st[2]}")
+    ctx.close()
+
+
+def three_planes(args):
+    """Three seeded planes (sigma 15, 10, 10 on Y, U, V), one basic
+    three-plane stage, then the requested stage `--launches + --warmup` times."""
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+
+    sig = (15.0, 10.0, 10.0)
+    planes = [torch.from_numpy(synth.pair(args.height, args.width, s, 7 + c)[1]).cuda()
+              for c, s in enumerate(sig)]
+    sp = [synth.sigma_param(s, c) for c, s in enumerate(sig)]
+    b = isp_mw_b200.stage_params_default("fast", False, sp)
+    f = isp_mw_b200.stage_params_default("fast", True, sp)
+    ctx = isp_mw_b200.Context(0)
+    basic = [p.clone() for p in planes]
+    out = [p.clone() for p in planes]
+    ctx.stage3(b, False, basic, planes)
+    for _ in range(args.warmup + args.launches):
+        if args.stage == "basic":
+            ctx.stage3(b, False, out, planes)
+        else:
+            ctx.stage3(f, True, out, planes, basic)
+    torch.cuda.synchronize()
+    print(f"stage={args.stage} planes=3 {args.width}x{args.height}")
     ctx.close()
 
 

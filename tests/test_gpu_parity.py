@@ -364,3 +364,28 @@ def test_edge_sizes_against_oracle(ctx, oracle_mod, shape):
     want = orc.stage3(False, b.as_dict(), planes)
     for c in range(3):
         assert_close(name + f":basic3_{c}", b3[c], want[c])
+
+
+@pytest.mark.parametrize("profile", ["fast", "np", "vn"])
+def test_three_planes_against_oracle(ctx, oracle_mod, profile):
+    """Three planes sharing luma groups on the register-resident kernel (fast,
+    planes run one at a time) and the generic kernel (np: GroupSize 32; vn:
+    BlockSize 11), each stage on identical inputs against the oracle."""
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    h, w = 96, 136
+    planes = [synth.pair(h, w, s, 80 + c)[1] for c, s in enumerate((15.0, 10.0, 10.0))]
+    sp = [synth.sigma_param(15.0, 0), synth.sigma_param(10.0, 1), synth.sigma_param(10.0, 2)]
+    b = isp_mw_b200.stage_params_default(profile, False, sp)
+    f = isp_mw_b200.stage_params_default(profile, True, sp)
+    orc = _oracle(oracle_mod)
+    basic = [p.copy() for p in planes]
+    ctx.stage3(b, False, basic, planes)
+    rb = orc.stage3(False, b.as_dict(), planes)
+    for c in range(3):
+        assert_close(f"{profile}3:basic:{c}", basic[c], rb[c])
+    final = [p.copy() for p in planes]
+    ctx.stage3(f, True, final, planes, basic)
+    rf = orc.stage3(True, f.as_dict(), planes, basic)
+    for c in range(3):
+        assert_close(f"{profile}3:final:{c}", final[c], rf[c])
