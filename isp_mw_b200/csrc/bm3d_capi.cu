@@ -122,13 +122,13 @@ cudaError_t upload_dct_tables_all(const DctTableData &t)
 
 }  // namespace bm3d
 
-// Cosine matrices in long double, rounded once to each precision.
-static void make_dct_tables(float *ff, float *fi, double *df, double *di, int *off)
+// Cosine matrices in long double, rounded once to each precision; length n
+// starts at (n-1) n (2n-1) / 6.
+static void make_dct_tables(float *ff, float *fi, double *df, double *di)
 {
     const long double pi = 3.141592653589793238462643383279502884L;
     int o = 0;
     for (int n = 1; n <= 16; ++n) {
-        off[n] = o;
         for (int k = 0; k < n; ++k)
             for (int j = 0; j < n; ++j) {
                 const long double cf = 2.0L * cosl(pi * (2 * j + 1) * k / (2.0L * n));
@@ -140,20 +140,18 @@ static void make_dct_tables(float *ff, float *fi, double *df, double *di, int *o
             }
         o += n * n;
     }
-    off[0] = 0;
 }
 
 static float g_tab_ff[1496], g_tab_fi[1496];
 static double g_tab_df[1496], g_tab_di[1496];
-static int g_tab_off[17];
 static std::once_flag g_tab_once;
 
-static void init_dct_tables() { make_dct_tables(g_tab_ff, g_tab_fi, g_tab_df, g_tab_di, g_tab_off); }
+static void init_dct_tables() { make_dct_tables(g_tab_ff, g_tab_fi, g_tab_df, g_tab_di); }
 
 static cudaError_t upload_dct_tables()
 {
     std::call_once(g_tab_once, init_dct_tables);
-    return upload_dct_tables_all(DctTableData{g_tab_ff, g_tab_fi, g_tab_df, g_tab_di, g_tab_off});
+    return upload_dct_tables_all(DctTableData{g_tab_ff, g_tab_fi, g_tab_df, g_tab_di});
 }
 
 extern "C" int bm3d_ctx_create(bm3d_ctx **out, int device)

@@ -16,12 +16,10 @@ template <typename T, bool W, int NPL> const void *generic_kernel_fn();
 // batch_stage_kernel<float, W, NPL, KS, GENERIC> (bm3d_batch.cuh)
 template <bool W, int NPL, int KS, bool GENERIC> const void *batch_kernel_fn();
 
-// Cosine matrices for group lengths 1..16 (1496 entries each) and the start
-// of length n at off[n] (17 entries).
+// Cosine matrices for group lengths 1..16, concatenated (1496 entries each).
 struct DctTableData {
     const float *fwd_f, *inv_f;
     const double *fwd_d, *inv_d;
-    const int *off;
 };
 cudaError_t upload_dct_tables_all(const DctTableData &t);
 

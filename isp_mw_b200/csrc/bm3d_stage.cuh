@@ -15,13 +15,12 @@
 namespace bm3d {
 
 // Cosine matrices for group lengths 1..16 (row k = output k), concatenated;
-// entry n starts at c_dct_off[n]. Every translation unit that launches these
-// kernels has its own copy, filled by the host when a context is made.
+// length n starts at (n-1) n (2n-1) / 6. Every translation unit that launches
+// these kernels has its own copy, filled by the host when a context is made.
 static __constant__ float c_dct_fwd_f[1496];
 static __constant__ float c_dct_inv_f[1496];
 static __constant__ double c_dct_fwd_d[1496];
 static __constant__ double c_dct_inv_d[1496];
-static __constant__ int c_dct_off[17];
 
 template <typename T> struct DctTab;
 template <> struct DctTab<float> {
@@ -34,87 +33,21 @@ template <> struct DctTab<double> {
 };
 
 // Transforms along the group axis for two pencils at once. Lengths 8 and 16
-// use the butterflies of dct.cuh. Every other length N has its own
-// instantiation, so each cosine is read from the constant bank at a
-// compile-time offset (an instruction operand, no load), and the symmetries
-// of the cosine matrices halve the multiplies:
-//   REDFT10: C[k][N-1-j] = (-1)^k C[k][j] -> sums (even k) and differences
-//            (odd k) of mirrored inputs;
-//   REDFT01: C[N-1-k][j] = (-1)^j C[k][j] -> even and odd input halves give
-//            outputs k and N-1-k together.
+// use the butterflies of dct.cuh; every other length N has its own
+// instantiation of the symmetric matrix form (dct.cuh), reading the
+// constant-bank tables at compile-time offsets.
 template <typename T, int N>
 __device__ __forceinline__ void zfwd_n(T (&a)[kGSMax], T (&b)[kGSMax])
 {
-    constexpr int H = N / 2, O = (N - 1) * N * (2 * N - 1) / 6;
-    const T *M = DctTab<T>::fwd() + O;
-    T ua[H + 1], va[H + 1], ub[H + 1], vb[H + 1];
-#pragma unroll
-    for (int j = 0; j < H; ++j) {
-        ua[j] = a[j] + a[N - 1 - j];
-        va[j] = a[j] - a[N - 1 - j];
-        ub[j] = b[j] + b[N - 1 - j];
-        vb[j] = b[j] - b[N - 1 - j];
-    }
-    ua[H] = (N & 1) ? a[H] : T(0);
-    ub[H] = (N & 1) ? b[H] : T(0);
-    T ya[N], yb[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-        T sa = T(0), sb = T(0);
-        if ((k & 1) == 0) {
-#pragma unroll
-            for (int j = 0; j < H + (N & 1); ++j) {
-                sa += M[k * N + j] * ua[j];
-                sb += M[k * N + j] * ub[j];
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < H; ++j) {
-                sa += M[k * N + j] * va[j];
-                sb += M[k * N + j] * vb[j];
-            }
-        }
-        ya[k] = sa;
-        yb[k] = sb;
-    }
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-        a[k] = ya[k];
-        b[k] = yb[k];
-    }
+    constexpr int O = (N - 1) * N * (2 * N - 1) / 6;  // start of length N: sum of m^2, m < N
+    redft10_pair<T, N>(a, b, DctTab<T>::fwd() + O);
 }
 
 template <typename T, int N>
 __device__ __forceinline__ void zinv_n(T (&a)[kGSMax], T (&b)[kGSMax])
 {
     constexpr int O = (N - 1) * N * (2 * N - 1) / 6;
-    const T *M = DctTab<T>::inv() + O;
-    T ya[N], yb[N];
-#pragma unroll
-    for (int k = 0; k < (N + 1) / 2; ++k) {
-        T ea = T(0), oa = T(0), eb = T(0), ob = T(0);
-#pragma unroll
-        for (int j = 0; j < N; j += 2) {
-            ea += M[k * N + j] * a[j];
-            eb += M[k * N + j] * b[j];
-        }
-#pragma unroll
-        for (int j = 1; j < N; j += 2) {
-            oa += M[k * N + j] * a[j];
-            ob += M[k * N + j] * b[j];
-        }
-        ya[k] = ea + oa;
-        yb[k] = eb + ob;
-        if (N - 1 - k != k) {
-            ya[N - 1 - k] = ea - oa;
-            yb[N - 1 - k] = eb - ob;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-        a[k] = ya[k];
-        b[k] = yb[k];
-    }
+    redft01_pair<T, N>(a, b, DctTab<T>::inv() + O);
 }
 
 template <typename T>

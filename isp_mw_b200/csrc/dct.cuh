@@ -7,8 +7,9 @@
 // so REDFT01(REDFT10(x)) = 2n x, which the reference undoes with finalAMP.
 //
 // Lengths 8 and 16 use an even/odd split (the 8-point even half is split once
-// more); other lengths multiply by a small cosine matrix. All functions are
-// __host__ __device__ so the CPU unit tests can check them against scipy.
+// more); other lengths multiply by a small cosine matrix, halved by its
+// symmetry. All functions are __host__ __device__ so the CPU unit tests can
+// check them against scipy.
 #pragma once
 
 #ifndef __CUDACC__
@@ -126,25 +127,86 @@ __host__ __device__ __forceinline__ void redft01_16(T (&x)[16])
     }
 }
 
-// Length-n transform with an explicit n x n matrix (row k = output k),
-// for n <= N: entries j >= n of x are ignored, outputs k >= n are untouched.
+// Length-N transforms of two pencils at once with an explicit N x N cosine
+// matrix `m` (row k = output k), using the matrices' symmetries to halve the
+// multiplies:
+//   REDFT10: C[k][N-1-j] = (-1)^k C[k][j] -> sums (even k) and differences
+//            (odd k) of mirrored inputs;
+//   REDFT01: C[N-1-k][j] = (-1)^j C[k][j] -> even and odd input halves give
+//            outputs k and N-1-k together.
+// Entries N..15 of the pencils are left alone. On the device `m` is a
+// constant-bank table at a compile-time offset, so every coefficient is an
+// instruction operand.
 template <typename T, int N, typename Mat>
-__host__ __device__ __forceinline__ void dct_matrix(T (&x)[N], int n, const Mat *mat)
+__host__ __device__ __forceinline__ void redft10_pair(T (&a)[16], T (&b)[16], const Mat *m)
 {
-    T y[N];
+    constexpr int H = N / 2;
+    T ua[H + 1], va[H + 1], ub[H + 1], vb[H + 1];
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        ua[j] = a[j] + a[N - 1 - j];
+        va[j] = a[j] - a[N - 1 - j];
+        ub[j] = b[j] + b[N - 1 - j];
+        vb[j] = b[j] - b[N - 1 - j];
+    }
+    ua[H] = (N & 1) ? a[H] : T(0);
+    ub[H] = (N & 1) ? b[H] : T(0);
+    T ya[N], yb[N];
 #pragma unroll
     for (int k = 0; k < N; ++k) {
-        T acc = T(0);
-        if (k < n) {
+        T sa = T(0), sb = T(0);
+        if ((k & 1) == 0) {
 #pragma unroll
-            for (int j = 0; j < N; ++j)
-                if (j < n) acc += T(mat[k * n + j]) * x[j];
+            for (int j = 0; j < H + (N & 1); ++j) {
+                sa += T(m[k * N + j]) * ua[j];
+                sb += T(m[k * N + j]) * ub[j];
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < H; ++j) {
+                sa += T(m[k * N + j]) * va[j];
+                sb += T(m[k * N + j]) * vb[j];
+            }
         }
-        y[k] = acc;
+        ya[k] = sa;
+        yb[k] = sb;
     }
 #pragma unroll
-    for (int k = 0; k < N; ++k)
-        if (k < n) x[k] = y[k];
+    for (int k = 0; k < N; ++k) {
+        a[k] = ya[k];
+        b[k] = yb[k];
+    }
+}
+
+template <typename T, int N, typename Mat>
+__host__ __device__ __forceinline__ void redft01_pair(T (&a)[16], T (&b)[16], const Mat *m)
+{
+    T ya[N], yb[N];
+#pragma unroll
+    for (int k = 0; k < (N + 1) / 2; ++k) {
+        T ea = T(0), oa = T(0), eb = T(0), ob = T(0);
+#pragma unroll
+        for (int j = 0; j < N; j += 2) {
+            ea += T(m[k * N + j]) * a[j];
+            eb += T(m[k * N + j]) * b[j];
+        }
+#pragma unroll
+        for (int j = 1; j < N; j += 2) {
+            oa += T(m[k * N + j]) * a[j];
+            ob += T(m[k * N + j]) * b[j];
+        }
+        ya[k] = ea + oa;
+        yb[k] = eb + ob;
+        if (N - 1 - k != k) {
+            ya[N - 1 - k] = ea - oa;
+            yb[N - 1 - k] = eb - ob;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        a[k] = ya[k];
+        b[k] = yb[k];
+    }
 }
 
 }  // namespace bm3d

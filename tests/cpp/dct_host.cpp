@@ -12,9 +12,27 @@ void host_redft10_8_f64(double *x) { double (&a)[8] = *reinterpret_cast<double(*
 void host_redft01_8_f64(double *x) { double (&a)[8] = *reinterpret_cast<double(*)[8]>(x); bm3d::redft01_8(a); }
 void host_redft10_16_f64(double *x) { double (&a)[16] = *reinterpret_cast<double(*)[16]>(x); bm3d::redft10_16(a); }
 void host_redft01_16_f64(double *x) { double (&a)[16] = *reinterpret_cast<double(*)[16]>(x); bm3d::redft01_16(a); }
-void host_dct_matrix_f64(double *x, int n, const double *mat)
+}
+
+// Length-n symmetric matrix transforms (n in 1..16) of two pencils x and y,
+// with the n x n matrix `mat`; inverse selects REDFT01.
+template <int N>
+static void pair(double *x, double *y, const double *mat, int inverse)
 {
     double (&a)[16] = *reinterpret_cast<double(*)[16]>(x);
-    bm3d::dct_matrix<double, 16>(a, n, mat);
+    double (&b)[16] = *reinterpret_cast<double(*)[16]>(y);
+    if (inverse) bm3d::redft01_pair<double, N>(a, b, mat);
+    else bm3d::redft10_pair<double, N>(a, b, mat);
 }
+
+template <int... Ns> struct PairTable {
+    static void run(int n, double *x, double *y, const double *mat, int inverse)
+    {
+        ((n == Ns ? pair<Ns>(x, y, mat, inverse) : void()), ...);
+    }
+};
+
+extern "C" void host_dct_pair_f64(double *x, double *y, int n, const double *mat, int inverse)
+{
+    PairTable<1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16>::run(n, x, y, mat, inverse);
 }

@@ -53,20 +53,24 @@ def test_fast_transforms_match_scipy(dctlib, n, dtype, tol):
 
 @pytest.mark.parametrize("n", range(1, 17))
 def test_matrix_transform_lengths(dctlib, n):
-    """Every group length 1..16 through the generic matrix path, with the
-    cosine matrices the library uploads (row k = output k)."""
+    """Every group length 1..16 through the symmetric matrix form the kernels
+    instantiate per length (two pencils at once), with the cosine matrices
+    the library uploads (row k = output k), against scipy."""
     k = np.arange(n)[:, None]
     j = np.arange(n)[None, :]
     fwd = 2 * np.cos(np.pi * (2 * j + 1) * k / (2 * n))
     inv = np.where(j == 0, 1.0, 2 * np.cos(np.pi * j * (2 * k + 1) / (2 * n)))
     rng = np.random.default_rng(100 + n)
-    x = np.zeros(16)
-    x[:n] = rng.standard_normal(n)
     for mat, typ in ((fwd, 2), (inv, 3)):
-        y = x.copy()
+        xs = [np.zeros(16), np.zeros(16)]
+        for x in xs:
+            x[:n] = rng.standard_normal(n)
+        a, b = xs[0].copy(), xs[1].copy()
         m = np.ascontiguousarray(mat.ravel())
-        dctlib.host_dct_matrix_f64(y.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(n),
-                                   m.ctypes.data_as(ctypes.c_void_p))
-        ref = scipy.fft.dct(x[:n], type=typ, norm=None)
-        assert np.allclose(y[:n], ref, rtol=0, atol=1e-12 * max(1, np.abs(x).sum()) * 4)
-        assert np.all(y[n:] == x[n:])
+        dctlib.host_dct_pair_f64(a.ctypes.data_as(ctypes.c_void_p),
+                                 b.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(n),
+                                 m.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(typ == 3))
+        for got, x in ((a, xs[0]), (b, xs[1])):
+            ref = scipy.fft.dct(x[:n], type=typ, norm=None)
+            assert np.allclose(got[:n], ref, rtol=0, atol=1e-12 * max(1, np.abs(x).sum()) * 4)
+            assert np.all(got[n:] == x[n:])
