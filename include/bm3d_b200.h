@@ -296,6 +296,13 @@ typedef struct bm3d_host_batch bm3d_host_batch;
 int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
                            const bm3d_stage_params *final_, const int width[], const int height[],
                            int autotune, bm3d_host_batch **out);
+/* The same over `count` images of three planes (Y, U, V) each, sharing the
+ * groups matched on Y (as bm3d_batch3_create): bm3d_host_batch_run then takes
+ * plane c of image i as dst[3 * i + c] / src[3 * i + c], with row pitch
+ * stride[i] for all three. Results equal per-image bm3d_full3 bit for bit. */
+int bm3d_host_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                            const bm3d_stage_params *final_, const int width[],
+                            const int height[], int autotune, bm3d_host_batch **out);
 int bm3d_host_batch_run(bm3d_host_batch *batch, float *const dst[], const float *const src[],
                         const size_t stride[], int async, void *stream);
 int bm3d_host_batch_join(bm3d_host_batch *batch, void *stream);

@@ -40,8 +40,8 @@ EXPORTS = [
     "bm3d_last_stats", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
     "bm3d_stage_noalloc", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
     "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
-    "bm3d_full_many", "bm3d_batch3_create", "bm3d_host_batch_create", "bm3d_host_batch_run",
-    "bm3d_host_batch_join", "bm3d_host_batch_destroy",
+    "bm3d_full_many", "bm3d_batch3_create", "bm3d_host_batch_create", "bm3d_host_batch3_create",
+    "bm3d_host_batch_run", "bm3d_host_batch_join", "bm3d_host_batch_destroy",
 ]
 
 
@@ -125,6 +125,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_batch3_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
                                        ctypes.POINTER(vp)]
     lib.bm3d_host_batch_create.argtypes = [vp, ip, vp, vp, vp, vp, ip, ctypes.POINTER(vp)]
+    lib.bm3d_host_batch3_create.argtypes = [vp, ip, vp, vp, vp, vp, ip, ctypes.POINTER(vp)]
     lib.bm3d_host_batch_run.argtypes = [vp, vp, vp, vp, ip, vp]
     lib.bm3d_host_batch_join.argtypes = [vp, vp]
     lib.bm3d_host_batch_destroy.argtypes = [vp]
@@ -472,38 +473,51 @@ class HostBatch:
     creation; each ``run`` uploads ``src``, filters and downloads into ``dst``.
     With ``asynchronous`` the call returns once enqueued on ``stream``
     (default: the current torch stream), and consecutive runs overlap their
-    copies with one another's filtering; synchronise before reading ``dst``."""
+    copies with one another's filtering; synchronise before reading ``dst``.
+    With ``planes=3`` every image is three planes (Y, U, V) sharing luma
+    groups (``bm3d_host_batch3_create``), and ``run`` takes a triple of
+    planes per image."""
 
     def __init__(self, ctx: "Context", basic: Sequence[StageParams], final: Sequence[StageParams],
-                 shapes: Sequence, autotune: bool = True):
+                 shapes: Sequence, autotune: bool = True, planes: int = 1):
         n = len(shapes)
         if not (len(basic) == len(final) == n) or n == 0:
-            raise ValueError("one basic/final parameter set per plane")
+            raise ValueError("one basic/final parameter set per image")
+        if planes not in (1, 3):
+            raise ValueError("planes must be 1 or 3")
         self.ctx = ctx
+        self.npl = planes
         self.shapes = [(int(h), int(w)) for h, w in shapes]
         pb = (StageParams * n)(*basic)
         pf = (StageParams * n)(*final)
         w = (ctypes.c_int * n)(*[s[1] for s in self.shapes])
         h = (ctypes.c_int * n)(*[s[0] for s in self.shapes])
         self.h = ctypes.c_void_p()
-        rc = ctx.lib.bm3d_host_batch_create(ctx.h, n, pb, pf, w, h, int(autotune),
-                                            ctypes.byref(self.h))
+        create = ctx.lib.bm3d_host_batch3_create if planes == 3 else ctx.lib.bm3d_host_batch_create
+        rc = create(ctx.h, n, pb, pf, w, h, int(autotune), ctypes.byref(self.h))
         ctx._check(rc, allow_copied=False)
-        self.pixels = sum(a * b for a, b in self.shapes)
+        self.pixels = sum(a * b for a, b in self.shapes)  # image pixels
 
     def run(self, dst, src, asynchronous=False, stream: Optional[int] = None):
         """asynchronous: False (dst written on return), True (enqueued; the
         stream completes after this run's download) or "overlap" (enqueued,
         no wait tied to the stream: call join() before synchronising)."""
-        n = len(self.shapes)
+        n, npl = len(self.shapes), self.npl
         if len(dst) != n or len(src) != n:
-            raise ValueError("one dst and src plane per batch plane")
+            raise ValueError("one dst and src image per batch image")
+        if npl == 3:
+            if not all(isinstance(x, (list, tuple)) and len(x) == 3 for x in list(dst) + list(src)):
+                raise ValueError("three-plane batches take three planes per image")
+            dst = [p for x in dst for p in x]
+            src = [p for x in src for p in x]
         di = [_plane_info(x) for x in dst]
         si = [_plane_info(x) for x in src]
-        for k, (a, b) in enumerate(zip(di, si)):
+        for j, (a, b) in enumerate(zip(di, si)):
             if a[1] != MEM_HOST or b[1] != MEM_HOST:
                 raise ValueError("host batches take host planes")
-            if (a[3], a[2]) != self.shapes[k] or (b[3], b[2]) != self.shapes[k] or a[4] != b[4]:
+            k = j // npl
+            if ((a[3], a[2]) != self.shapes[k] or (b[3], b[2]) != self.shapes[k] or a[4] != b[4]
+                    or b[4] != si[k * npl][4]):
                 raise ValueError("plane size or stride does not match the batch")
         if stream is None:
             try:
@@ -511,8 +525,8 @@ class HostBatch:
                 stream = torch.cuda.current_stream(self.ctx.device).cuda_stream
             except Exception:
                 stream = 0
-        vp = ctypes.c_void_p * n
-        st = (ctypes.c_size_t * n)(*[i[4] for i in si])
+        vp = ctypes.c_void_p * (n * npl)
+        st = (ctypes.c_size_t * n)(*[i[4] for i in si[::npl]])
         mode = 2 if asynchronous == "overlap" else int(bool(asynchronous))
         rc = self.ctx.lib.bm3d_host_batch_run(self.h, vp(*[i[0] for i in di]),
                                               vp(*[i[0] for i in si]), st, mode, stream)

@@ -2089,10 +2089,11 @@ extern "C" void bm3d_batch_destroy(bm3d_batch *B)
 
 struct bm3d_host_batch {
     bm3d_ctx *ctx = nullptr;
-    int n = 0;
+    int n = 0;    // images
+    int npl = 1;  // planes per image
     std::vector<bm3d_stage_params> pb, pf;
     std::vector<int> w, h;
-    std::vector<size_t> off;  // element offset of each plane in a slot's buffers
+    std::vector<size_t> off;  // element offset of each plane (npl per image) in a slot's buffers
     size_t total = 0;         // floats per slot buffer
     int autotune = 1;
     struct Slot {
@@ -2123,9 +2124,10 @@ extern "C" void bm3d_host_batch_destroy(bm3d_host_batch *H)
     delete H;
 }
 
-extern "C" int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
-                                      const bm3d_stage_params *final_, const int width[],
-                                      const int height[], int autotune, bm3d_host_batch **out)
+static int host_batch_create_any(bm3d_ctx *ctx, int npl, int count,
+                                 const bm3d_stage_params *basic, const bm3d_stage_params *final_,
+                                 const int width[], const int height[], int autotune,
+                                 bm3d_host_batch **out)
 {
     if (!ctx || !out || count < 1 || !basic || !final_ || !width || !height)
         return BM3D_ERR_INVALID;
@@ -2134,6 +2136,7 @@ extern "C" int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage
     auto *H = new bm3d_host_batch;
     H->ctx = ctx;
     H->n = count;
+    H->npl = npl;
     H->autotune = autotune;
     auto fail = [&](int rc) {
         bm3d_host_batch_destroy(H);
@@ -2145,8 +2148,10 @@ extern "C" int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage
         H->pf.push_back(final_[i]);
         H->w.push_back(width[i]);
         H->h.push_back(height[i]);
-        H->off.push_back(H->total);
-        H->total += static_cast<size_t>(width[i]) * height[i];
+        for (int c = 0; c < npl; ++c) {
+            H->off.push_back(H->total);
+            H->total += static_cast<size_t>(width[i]) * height[i];
+        }
     }
     int rc;
     for (auto &sl : H->slot) {
@@ -2166,6 +2171,20 @@ extern "C" int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage
     return BM3D_OK;
 }
 
+extern "C" int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                                      const bm3d_stage_params *final_, const int width[],
+                                      const int height[], int autotune, bm3d_host_batch **out)
+{
+    return host_batch_create_any(ctx, 1, count, basic, final_, width, height, autotune, out);
+}
+
+extern "C" int bm3d_host_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
+                                       const bm3d_stage_params *final_, const int width[],
+                                       const int height[], int autotune, bm3d_host_batch **out)
+{
+    return host_batch_create_any(ctx, 3, count, basic, final_, width, height, autotune, out);
+}
+
 // The slot's batch graph over its device buffers; built on the first run that
 // uses the slot, so the autotuner times real data (slot 1 reuses slot 0's
 // tiling).
@@ -2173,21 +2192,22 @@ static int host_batch_bind(bm3d_host_batch *H, int k)
 {
     auto &sl = H->slot[k];
     if (sl.batch) return BM3D_OK;
-    std::vector<float *> d(H->n);
-    std::vector<const float *> x(H->n);
+    const size_t planes = H->off.size();
+    std::vector<float *> d(planes);
+    std::vector<const float *> x(planes);
     std::vector<size_t> st(H->n);
-    for (int i = 0; i < H->n; ++i) {
-        d[i] = static_cast<float *>(sl.dst.ptr) + H->off[i];
-        x[i] = static_cast<const float *>(sl.src.ptr) + H->off[i];
-        st[i] = static_cast<size_t>(H->w[i]);
+    for (size_t j = 0; j < planes; ++j) {
+        d[j] = static_cast<float *>(sl.dst.ptr) + H->off[j];
+        x[j] = static_cast<const float *>(sl.src.ptr) + H->off[j];
     }
+    for (int i = 0; i < H->n; ++i) st[i] = static_cast<size_t>(H->w[i]);
     int tiling[6];
     const int *force = nullptr;
     if (k == 1 && H->slot[0].batch) {
         bm3d_batch_tuning(H->slot[0].batch, tiling);
         force = tiling;
     }
-    return batch_create_any(H->ctx, 1, H->n, H->pb.data(), H->pf.data(), d.data(), x.data(),
+    return batch_create_any(H->ctx, H->npl, H->n, H->pb.data(), H->pf.data(), d.data(), x.data(),
                             H->w.data(), H->h.data(), st.data(), H->autotune, &sl.batch, force);
 }
 
@@ -2196,8 +2216,12 @@ extern "C" int bm3d_host_batch_run(bm3d_host_batch *H, float *const dst[],
                                    void *stream)
 {
     if (!H || !dst || !src || !stride) return BM3D_ERR_INVALID;
-    for (int i = 0; i < H->n; ++i)
-        if (!dst[i] || !src[i] || stride[i] < static_cast<size_t>(H->w[i])) return BM3D_ERR_INVALID;
+    const int np = H->npl;
+    for (int i = 0; i < H->n; ++i) {
+        if (stride[i] < static_cast<size_t>(H->w[i])) return BM3D_ERR_INVALID;
+        for (int c = 0; c < np; ++c)
+            if (!dst[np * i + c] || !src[np * i + c]) return BM3D_ERR_INVALID;
+    }
     bm3d_ctx *ctx = H->ctx;
     CK(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -2205,10 +2229,12 @@ extern "C" int bm3d_host_batch_run(bm3d_host_batch *H, float *const dst[],
     auto &sl = H->slot[k];
     // inputs: once this slot's previous run has been filtered
     if (sl.used) CK(ctx, cudaStreamWaitEvent(H->up, sl.filtered, 0));
-    for (int i = 0; i < H->n; ++i)
-        CK(ctx, cudaMemcpy2DAsync(static_cast<float *>(sl.src.ptr) + H->off[i],
-                                  sizeof(float) * H->w[i], src[i], sizeof(float) * stride[i],
+    for (int j = 0; j < np * H->n; ++j) {
+        const int i = j / np;
+        CK(ctx, cudaMemcpy2DAsync(static_cast<float *>(sl.src.ptr) + H->off[j],
+                                  sizeof(float) * H->w[i], src[j], sizeof(float) * stride[i],
                                   sizeof(float) * H->w[i], H->h[i], cudaMemcpyHostToDevice, H->up));
+    }
     CK(ctx, cudaEventRecord(sl.uploaded, H->up));
     if (!sl.batch) {  // first use: build (and tune) the slot's graph on these inputs
         CK(ctx, cudaEventSynchronize(sl.uploaded));
@@ -2221,11 +2247,13 @@ extern "C" int bm3d_host_batch_run(bm3d_host_batch *H, float *const dst[],
     if (rc != BM3D_OK) return rc;
     CK(ctx, cudaEventRecord(sl.filtered, s));
     CK(ctx, cudaStreamWaitEvent(H->down, sl.filtered, 0));
-    for (int i = 0; i < H->n; ++i)
-        CK(ctx, cudaMemcpy2DAsync(dst[i], sizeof(float) * stride[i],
-                                  static_cast<const float *>(sl.dst.ptr) + H->off[i],
+    for (int j = 0; j < np * H->n; ++j) {
+        const int i = j / np;
+        CK(ctx, cudaMemcpy2DAsync(dst[j], sizeof(float) * stride[i],
+                                  static_cast<const float *>(sl.dst.ptr) + H->off[j],
                                   sizeof(float) * H->w[i], sizeof(float) * H->w[i], H->h[i],
                                   cudaMemcpyDeviceToHost, H->down));
+    }
     CK(ctx, cudaEventRecord(sl.drained, H->down));
     sl.used = true;
     ++H->runs;
