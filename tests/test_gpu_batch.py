@@ -89,3 +89,59 @@ def test_batch3_equals_per_image(bm3d_lib, autotune):
     assert torch.equal(dsts[1][2], srcs[1][2])
     batch.close()
     ctx.close()
+
+
+def _custom(profile, wiener, sp, bm_step):
+    import isp_mw_b200
+    p = isp_mw_b200.stage_params_default(profile, wiener, sp)
+    if bm_step:
+        p.bm_step = bm_step
+    return p
+
+
+@pytest.mark.parametrize("profile,bm_step", [("lc", 0), ("np", 0), ("high", 0), ("vn", 0),
+                                             ("fast", 2), ("np", 3)])
+def test_batch_other_profiles_equal_per_plane(bm3d_lib, profile, bm_step):
+    """Batches of the other profiles (generic kernel for GroupSize 32 and
+    BlockSize 11) and of matching steps above 1 (single-row matching
+    strips), one and three planes per image, equal per-plane bm3d_full /
+    per-image bm3d_full3 bit for bit."""
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    ctx = isp_mw_b200.Context(0)
+    shapes = [(70, 96), (101, 83), (64, 130)]
+    srcs, dsts, pbs, pfs, want = [], [], [], [], []
+    srcs3, dsts3, want3 = [], [], []
+    for k, (h, w) in enumerate(shapes):
+        s255 = (12.0, 30.0, 45.0)[k]
+        src = torch.from_numpy(synth.pair(h, w, s255, 610 + k)[1]).cuda()
+        sp = [synth.sigma_param(s255)] * 3
+        pb, pf = _custom(profile, False, sp, bm_step), _custom(profile, True, sp, bm_step)
+        ref = torch.empty_like(src)
+        ctx.full(pb, pf, ref, src)
+        srcs.append(src)
+        dsts.append(torch.full_like(src, -1.0))
+        pbs.append(pb)
+        pfs.append(pf)
+        want.append(ref)
+        planes = [src] + [torch.from_numpy(synth.pair(h, w, 10.0, 640 + 3 * k + c)[1]).cuda()
+                          for c in (1, 2)]
+        r3 = [torch.empty_like(p) for p in planes]
+        ctx.full3(pb, pf, r3, planes)
+        srcs3.append(planes)
+        dsts3.append([torch.full_like(p, -1.0) for p in planes])
+        want3.append(r3)
+    batch = isp_mw_b200.Batch(ctx, pbs, pfs, dsts, srcs, autotune=True)
+    batch3 = isp_mw_b200.Batch(ctx, pbs, pfs, dsts3, srcs3, autotune=False)
+    for _ in range(2):
+        batch.run()
+        batch3.run()
+        torch.cuda.synchronize()
+        for k in range(len(shapes)):
+            assert torch.equal(dsts[k], want[k]), k
+            for c in range(3):
+                assert torch.equal(dsts3[k][c], want3[k][c]), (k, c)
+    batch.close()
+    batch3.close()
+    ctx.close()
