@@ -69,9 +69,16 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()  # nvidia-smi takes a moment to start: have a sample before timing
+            while not self.lines and self.proc.poll() is None and time.time() - t0 < 5.0:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self
+
+    def mark(self) -> int:
+        """Index of the next sample (bracket a timed region with two marks)."""
+        return len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -86,10 +93,13 @@ class ClockSampler:
                 self.proc.kill()
             self.thread.join(timeout=2)
 
-    def summary(self):
+    def summary(self, lo: int = 0, hi: int | None = None):
+        """Median SM clock and active throttle reasons over samples [lo, hi)
+        (all samples when that range holds none)."""
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines[lo:hi] or self.lines
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -222,11 +232,13 @@ def run_yuv(args):
         batch.run()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0 = clk.mark()
     ev0.record(stream)
     for _ in range(args.steps):
         batch.run()
     ev1.record(stream)
     barrier()
+    m1 = clk.mark()
     clk.__exit__(None, None, None)
     ms = shard.max_over_ranks(ev0.elapsed_time(ev1), dev)
     mp = YUV_FRAMES * YUV_W * YUV_H / 1e6
@@ -279,7 +291,7 @@ def run_yuv(args):
             "e2e": {"value": round(world * mp * args.steps / (e_ms / 1e3), 3), "unit": "MP/s",
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "gpu_launches": args.steps * 6,
-            "clocks": clk.summary(),
+            "clocks": clk.summary(m0, m1),
         }
         print(json.dumps(line), flush=True)
     batch.close()
@@ -326,11 +338,13 @@ def run_batch(args):
         batch.run()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0 = clk.mark()
     ev0.record(stream)
     for _ in range(args.steps):
         batch.run()
     ev1.record(stream)
     barrier()
+    m1 = clk.mark()
     clk.__exit__(None, None, None)
     ms = shard.max_over_ranks(ev0.elapsed_time(ev1), dev)
     mp = batch.pixels / 1e6
@@ -377,7 +391,7 @@ def run_batch(args):
             "e2e": {"value": round(world * mp * args.steps / (e_ms / 1e3), 3), "unit": "MP/s",
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
             "gpu_launches": args.steps * 6,
-            "clocks": clk.summary(),
+            "clocks": clk.summary(m0, m1),
         }
         print(json.dumps(line), flush=True)
     batch.close()
@@ -428,11 +442,13 @@ def run_ours(args):
         step(i)
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    m0 = clk.mark()
     ev0.record(stream)
     for i in range(args.steps):
         step(args.warmup + i)
     ev1.record(stream)
     barrier()
+    m1 = clk.mark()
     from isp_mw_b200 import shard
     ms_max = shard.max_over_ranks(ev0.elapsed_time(ev1), dev)
     mp_step = len(SIGMAS) * W * H / 1e6
@@ -458,7 +474,7 @@ def run_ours(args):
     t_dom, n_dom = (t_final, n_final) if dom else (t_basic, n_basic)
     per_launch_ms = t_dom / max(1, n_dom)
     achieved = flops[dom] / max(1, n_dom) / (per_launch_ms / 1e3) / 1e12
-    clocks = clk.summary()
+    clocks = clk.summary(m0, m1)
     sm_max = clocks.get("sm_max_mhz") or 1965.0
     peak_fp32 = 148 * 128 * 2 * sm_max * 1e6 / 1e12
 
@@ -682,7 +698,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
