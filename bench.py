@@ -513,6 +513,11 @@ def run_ours(args):
 
     if rank == 0:
         peaks = load_peaks()
+        if peaks.get("hbm_gbs"):
+            hbm_peak, hbm_source = float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+        else:  # an earlier STREAM-style copy measurement on these B200s
+            hbm_peak, hbm_source = 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+        traffic = TRAFFIC_FINAL_1080P if dom else TRAFFIC_BASIC_1080P
         line = {
             "metric": METRIC,
             "value": round(value, 3),
@@ -546,7 +551,7 @@ def run_ours(args):
                 "peak": round(peak_fp32, 2),
                 "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4),
-                "traffic": TRAFFIC_FINAL_1080P if dom else TRAFFIC_BASIC_1080P,
+                "traffic": traffic,
                 "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, one "
                                   "ncu capture of the same kernel on one 1920x1080 plane, "
                                   "sigma 25 (profiles/stage_kernel_"
@@ -555,7 +560,10 @@ def run_ours(args):
                                "(MEASURED_PEAKS.json has no FP32 SIMT figure)",
                 "per_launch_ms": round(per_launch_ms, 4),
                 "algorithmic_gflop_per_launch": round(flops[dom] / max(1, n_dom) / 1e9, 3),
-                "hbm_peak_gbs": peaks.get("hbm_gbs"),
+                "hbm_peak_gbs": hbm_peak,
+                "hbm_peak_source": hbm_source,
+                "dram_gbs": round(traffic / (per_launch_ms / 1e3) / 1e9, 1),
+                "dram_frac": round(traffic / (per_launch_ms / 1e3) / 1e9 / hbm_peak, 4),
             },
             "stage_ms_per_plane": {"basic": round(t_basic / max(1, n_basic), 4),
                                    "final": round(t_final / max(1, n_final), 4)},

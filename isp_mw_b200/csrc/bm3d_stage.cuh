@@ -771,6 +771,18 @@ __device__ __forceinline__ void carve_tile(const StageArgs<T> &a, const SmemPlan
     }
 }
 
+// One element global -> shared without a register round trip (cp.async;
+// element-sized, so no alignment beyond the element's own). Completed by
+// cp_async_wait_all before the CTA barrier that publishes the windows.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(sizeof(T))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Load the staged windows (and block (0, 0) when outside) and zero the
 // accumulators. Ends with __syncthreads().
 template <typename T, bool WIENER, int NPL>
@@ -787,8 +799,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs<T> &a, const Tile<T> 
             const int y = i / t.rw, x = i - y * t.rw;
             const long long g = static_cast<long long>(t.ry0 + y) * a.stride + (t.rx0 + x);
             const int s = y * t.pitch + x;
-            if (need_src || (p == 0 && !ref_sep)) const_cast<T *>(t.srcw[p])[s] = __ldg(a.src[p] + g);
-            if (ref_sep) const_cast<T *>(t.refw[p])[s] = __ldg(a.ref[p] + g);
+            if (need_src || (p == 0 && !ref_sep)) cp_async_elem(const_cast<T *>(t.srcw[p]) + s, a.src[p] + g);
+            if (ref_sep) cp_async_elem(const_cast<T *>(t.refw[p]) + s, a.ref[p] + g);
             if (need_src) {
                 t.accN[p][s] = 0;
                 t.accD[p][s] = 0;
@@ -805,6 +817,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs<T> &a, const Tile<T> 
             }
         }
     }
+    cp_async_wait_all();
     __syncthreads();
 }
 
@@ -950,8 +963,8 @@ __device__ __forceinline__ void stage_plane(const StageArgs<T> &a, const Tile<T>
         const int y = i / t.rw, x = i - y * t.rw;
         const long long g = static_cast<long long>(t.ry0 + y) * a.stride + (t.rx0 + x);
         const int s = y * t.pitch + x;
-        const_cast<T *>(t.srcw[0])[s] = __ldg(a.src[c] + g);
-        if (need_ref) const_cast<T *>(t.refw[0])[s] = __ldg(a.ref[c] + g);
+        cp_async_elem(const_cast<T *>(t.srcw[0]) + s, a.src[c] + g);
+        if (need_ref) cp_async_elem(const_cast<T *>(t.refw[0]) + s, a.ref[c] + g);
         if (filt) {
             t.accN[0][s] = 0;
             t.accD[0][s] = 0;
@@ -967,6 +980,7 @@ __device__ __forceinline__ void stage_plane(const StageArgs<T> &a, const Tile<T>
             t.accD0[0][i] = 0;
         }
     }
+    cp_async_wait_all();
     __syncthreads();
 }
 
