@@ -143,15 +143,30 @@ static void make_dct_tables(float *ff, float *fi, double *df, double *di)
 }
 
 static float g_tab_ff[1496], g_tab_fi[1496];
+static float g_pad_f[bm3d::kPadTable], g_pad_i[bm3d::kPadTable];
 static double g_tab_df[1496], g_tab_di[1496];
 static std::once_flag g_tab_once;
 
-static void init_dct_tables() { make_dct_tables(g_tab_ff, g_tab_fi, g_tab_df, g_tab_di); }
+static void init_dct_tables()
+{
+    make_dct_tables(g_tab_ff, g_tab_fi, g_tab_df, g_tab_di);
+    // column-major, 16 rows, zero past row n: the same FP32 values
+    for (int n = 1; n <= 15; ++n) {
+        if (n == 8) continue;
+        const int src = (n - 1) * n * (2 * n - 1) / 6, dst = bm3d::pad_table_offset(n);
+        for (int j = 0; j < n; ++j)
+            for (int k = 0; k < 16; ++k) {
+                g_pad_f[dst + 16 * j + k] = k < n ? g_tab_ff[src + k * n + j] : 0.0f;
+                g_pad_i[dst + 16 * j + k] = k < n ? g_tab_fi[src + k * n + j] : 0.0f;
+            }
+    }
+}
 
 static cudaError_t upload_dct_tables()
 {
     std::call_once(g_tab_once, init_dct_tables);
-    return upload_dct_tables_all(DctTableData{g_tab_ff, g_tab_fi, g_tab_df, g_tab_di});
+    return upload_dct_tables_all(
+        DctTableData{g_tab_ff, g_tab_fi, g_tab_df, g_tab_di, g_pad_f, g_pad_i});
 }
 
 extern "C" int bm3d_ctx_create(bm3d_ctx **out, int device)

@@ -14,7 +14,13 @@ constexpr int kGSMax = 16;       // largest group the register-resident path hol
 constexpr int kGSTab = 32;       // largest GroupSize handled at all (generic path)
 constexpr int kBSMax = 16;       // largest BlockSize handled at all (generic path)
 constexpr int kGroupStride = 72; // floats per block in a warp's group buffer (64 + 8 pad)
-constexpr int kCand = 64;        // candidates a warp sorts after thresholding
+constexpr int kCand = 64;
+// FP32 group-axis matrices of lengths 1..15 except 8, 16 rows per column
+constexpr int kPadTable = 16 * (15 * 16 / 2 - 8);
+__host__ __device__ constexpr int pad_table_offset(int n)
+{
+    return 16 * ((n - 1) * n / 2 - (n > 8 ? 8 : 0));
+}        // candidates a warp sorts after thresholding
 
 // ---------------------------------------------------------------------------
 // Arithmetic that must not be contracted into FMA: the reference accumulates

@@ -20,6 +20,7 @@ template <bool W, int NPL, int KS, bool GENERIC> const void *batch_kernel_fn();
 struct DctTableData {
     const float *fwd_f, *inv_f;
     const double *fwd_d, *inv_d;
+    const float *pad_fwd, *pad_inv;  // kPadTable entries each (bm3d_device.cuh)
 };
 cudaError_t upload_dct_tables_all(const DctTableData &t);
 

@@ -21,6 +21,11 @@ static __constant__ float c_dct_fwd_f[1496];
 static __constant__ float c_dct_inv_f[1496];
 static __constant__ double c_dct_fwd_d[1496];
 static __constant__ double c_dct_inv_d[1496];
+// FP32 cosine matrices of the lengths other than 8 and 16, column by column:
+// length n starts at 16 * (sum of the lengths m < n, m != 8), and entry
+// (row k, column j) sits at + 16 j + k, zero for k >= n.
+static __constant__ float c_dct_pad_fwd[kPadTable];
+static __constant__ float c_dct_pad_inv[kPadTable];
 
 template <typename T> struct DctTab;
 template <> struct DctTab<float> {
@@ -33,9 +38,10 @@ template <> struct DctTab<double> {
 };
 
 // Transforms along the group axis for two pencils at once. Lengths 8 and 16
-// use the butterflies of dct.cuh; every other length N has its own
+// use the butterflies of dct.cuh. In FP64 every other length N has its own
 // instantiation of the symmetric matrix form (dct.cuh), reading the
-// constant-bank tables at compile-time offsets.
+// constant-bank tables at compile-time offsets; FP32 runs those lengths
+// through one compact loop instead (zgen, below).
 template <typename T, int N>
 __device__ __forceinline__ void zfwd_n(T (&a)[kGSMax], T (&b)[kGSMax])
 {
@@ -602,6 +608,79 @@ __device__ __forceinline__ void store_pencils(T *G, int n, int lane, const T (&a
         if (z < n) Vec4<T>::store2(G + z * kGroupStride + o, a[z], b[z]);
 }
 
+// Group-axis transform of the lane's two pencils for the FP32 lengths other
+// than 8 and 16: y_k = sum_j m[k][j] x_j, x read from the group buffer, j in
+// order, one runtime loop for every such length (a compact body: groups of
+// varied lengths would otherwise run many unrolled bodies at once).
+__device__ __forceinline__ void zgen(const float *G, int n, int lane, const float *m,
+                                     float (&a)[kGSMax], float (&b)[kGSMax])
+{
+    const int o = pencil_off(lane);
+#pragma unroll
+    for (int k = 0; k < kGSMax; ++k) {
+        a[k] = 0.0f;
+        b[k] = 0.0f;
+    }
+#pragma unroll 1
+    for (int j = 0; j < n; ++j) {
+        float xa, xb;
+        Vec4<float>::load2(G + j * kGroupStride + o, xa, xb);
+        const float *mj = m + 16 * j;
+#pragma unroll
+        for (int k = 0; k < kGSMax; ++k) {
+            a[k] = fmaf(mj[k], xa, a[k]);
+            b[k] = fmaf(mj[k], xb, b[k]);
+        }
+    }
+}
+
+// Forward group-axis transform of the pencils held in the group buffer.
+template <typename T>
+__device__ __forceinline__ void group_fwd(T *G, int n, int lane, T (&a)[kGSMax], T (&b)[kGSMax])
+{
+    if constexpr (sizeof(T) == 4) {
+        if (n != 16 && n != 8) {
+            zgen(G, n, lane, c_dct_pad_fwd + pad_table_offset(n), a, b);
+            return;
+        }
+        load_pencils(G, n, lane, a, b);
+        if (n == 16) {
+            redft10_16(a);
+            redft10_16(b);
+        } else {
+            zbfly8(a, false);
+            zbfly8(b, false);
+        }
+    } else {
+        load_pencils(G, n, lane, a, b);
+        zdct_fwd2(a, b, n);
+    }
+}
+
+// Inverse group-axis transform; the result is left in the group buffer.
+template <typename T>
+__device__ __forceinline__ void group_inv(T *G, int n, int lane, T (&a)[kGSMax], T (&b)[kGSMax])
+{
+    if constexpr (sizeof(T) == 4) {
+        if (n != 16 && n != 8) {
+            store_pencils(G, n, lane, a, b);
+            __syncwarp();
+            zgen(G, n, lane, c_dct_pad_inv + pad_table_offset(n), a, b);
+            __syncwarp();
+        } else if (n == 16) {
+            redft01_16(a);
+            redft01_16(b);
+        } else {
+            zbfly8(a, true);
+            zbfly8(b, true);
+        }
+    } else {
+        zdct_inv2(a, b, n);
+    }
+    __syncwarp();
+    store_pencils(G, n, lane, a, b);
+}
+
 // Empirical Wiener weight y^2 / (y^2 + sigma^2) (source/BM3D.cpp:440); the
 // FP32 path uses the fast division (within 2 ulp), FP64 the exact one.
 __device__ __forceinline__ float wiener_weight(float y2, float s2) { return __fdividef(y2, y2 + s2); }
@@ -620,13 +699,11 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
     T ra[kGSMax], rb[kGSMax];
     if (WIENER) {
         gather_xy_forward(t, t.refw[p], t.ref0[p], list, n, lane, G, n_bad);
-        load_pencils(G, n, lane, ra, rb);
-        zdct_fwd2(ra, rb, n);
+        group_fwd(G, n, lane, ra, rb);
         __syncwarp();
     }
     gather_xy_forward(t, t.srcw[p], t.src0[p], list, n, lane, G, n_bad);
-    load_pencils(G, n, lane, sa, sb);
-    zdct_fwd2(sa, sb, n);
+    group_fwd(G, n, lane, sa, sb);
 
     T denW;
     if (!WIENER) {
@@ -668,9 +745,7 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
     }
     const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
 
-    zdct_inv2(sa, sb, n);
-    __syncwarp();
-    store_pencils(G, n, lane, sa, sb);
+    group_inv(G, n, lane, sa, sb);
     __syncwarp();
     T v[4][8];
     xy_inverse(G, n, lane, v);

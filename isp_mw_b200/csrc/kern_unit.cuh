@@ -28,6 +28,8 @@ static cudaError_t upload_dct_tables_here(const DctTableData &t)
     if ((e = cudaMemcpyToSymbol(c_dct_fwd_f, t.fwd_f, sizeof(c_dct_fwd_f))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_dct_inv_f, t.inv_f, sizeof(c_dct_inv_f))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_dct_fwd_d, t.fwd_d, sizeof(c_dct_fwd_d))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_dct_pad_fwd, t.pad_fwd, sizeof(c_dct_pad_fwd))) != cudaSuccess) return e;
+    if ((e = cudaMemcpyToSymbol(c_dct_pad_inv, t.pad_inv, sizeof(c_dct_pad_inv))) != cudaSuccess) return e;
     return cudaMemcpyToSymbol(c_dct_inv_d, t.inv_d, sizeof(c_dct_inv_d));
 }
 
