@@ -525,7 +525,7 @@ __device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win
         n_bad += ok ? 0 : 1;
         int pitch;
         const T *bp = block_ptr(t, win, origin, ok ? p.y : t.ry0, ok ? p.x : t.rx0, pitch);
-#pragma unroll
+#pragma unroll 1
         for (int r = 0; r < 4; ++r) {
             T row[8];
             const int y = 4 * h + r;
@@ -551,10 +551,9 @@ __device__ __forceinline__ void gather_xy_forward(const Tile<T> &t, const T *win
     __syncwarp();
 }
 
-// Columns then rows of the inverse 2-D transform; returns rows 4h..4h+3 of
-// block z in v.
+// Columns of the inverse 2-D transform, in place in the group buffer.
 template <typename T>
-__device__ __forceinline__ void xy_inverse(T *G, int n, int lane, T (&v)[4][8])
+__device__ __forceinline__ void xy_inverse_cols(T *G, int n, int lane)
 {
     const int z = lane >> 1, h = lane & 1;
     T *gz = G + z * kGroupStride;
@@ -570,15 +569,6 @@ __device__ __forceinline__ void xy_inverse(T *G, int n, int lane, T (&v)[4][8])
             Vec4<T>::store(gz + gidx(y, 4 * h), col[0][y], col[1][y], col[2][y], col[3][y]);
     }
     __syncwarp();
-    if (z < n) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int y = 4 * h + r;
-            Vec4<T>::load(gz + gidx(y, 0), v[r][0], v[r][1], v[r][2], v[r][3]);
-            Vec4<T>::load(gz + gidx(y, 4), v[r][4], v[r][5], v[r][6], v[r][7]);
-            redft01_8(v[r]);
-        }
-    }
 }
 
 // Pencils along the group axis: lane owns positions p = 2 lane and 2 lane + 1,
@@ -747,10 +737,10 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
 
     group_inv(G, n, lane, sa, sb);
     __syncwarp();
-    T v[4][8];
-    xy_inverse(G, n, lane, v);
+    xy_inverse_cols(G, n, lane);
 
-    // Aggregation: BlockGroup::AddTo / CountTo (include/Block.h:1240-1265,
+    // Rows of the inverse 2-D transform, each aggregated as soon as it is
+    // ready: BlockGroup::AddTo / CountTo (include/Block.h:1240-1265,
     // 1334-1357). The weight is the same over the block, so it is added once,
     // at the block's origin; the normalisation sums origins over each pixel's
     // covering blocks. Integer sums make that exactly the per-pixel sum.
@@ -759,10 +749,17 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
         const BlockPos q = list[z];
         int pitch;
         auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
+        const T *gz = G + z * kGroupStride;
+#pragma unroll 1
+        for (int r = 0; r < 4; ++r) {
+            const int y = 4 * h + r;
+            T v[8];
+            Vec4<T>::load(gz + gidx(y, 0), v[0], v[1], v[2], v[3]);
+            Vec4<T>::load(gz + gidx(y, 4), v[4], v[5], v[6], v[7]);
+            redft01_8(v);
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int x = 0; x < 8; ++x) acc_add(dn + (4 * h + r) * pitch + x, v[r][x] * numW, scale);
+            for (int x = 0; x < 8; ++x) acc_add(dn + y * pitch + x, v[x] * numW, scale);
+        }
         if (h == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
     }
     __syncwarp();
