@@ -404,7 +404,7 @@ def run_batch(args):
 # DRAM bytes per launch of the stage kernels on one 1920x1080 plane, from one
 # ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum); the command
 # and the full figures are in profiles/stage_kernel_{final,basic}_1080p_full.txt.
-TRAFFIC_FINAL_1080P = 46.518e6 + 0.007e6
+TRAFFIC_FINAL_1080P = 46.487e6 + 0.0e6
 TRAFFIC_BASIC_1080P = 37.286e6 + 0.004e6
 
 
