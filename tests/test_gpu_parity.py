@@ -389,3 +389,29 @@ def test_three_planes_against_oracle(ctx, oracle_mod, profile):
     rf = orc.stage3(True, f.as_dict(), planes, basic)
     for c in range(3):
         assert_close(f"{profile}3:final:{c}", final[c], rf[c])
+
+
+def test_every_group_length_against_oracle(ctx, oracle_mod):
+    """Groups of every length 1..16 (σ 50 on a 256x192 plane makes them all,
+    in both stages) through the FP32 group-axis transforms: butterflies for 8
+    and 16, one runtime-length loop for the others. Both stages on identical
+    inputs meet the strict bar, and the group lists are the oracle's."""
+    from isp_mw_b200 import synth
+    import isp_mw_b200
+    s255 = 50.0
+    _, noisy = synth.pair(192, 256, s255, 77)
+    sp = [synth.sigma_param(s255)] * 3
+    b = isp_mw_b200.stage_params_default("fast", False, sp)
+    f = isp_mw_b200.stage_params_default("fast", True, sp)
+    orc = _oracle(oracle_mod)
+    rb = orc.stage(False, b.as_dict(), noisy)
+    for wiener, p, ref in ((False, b, noisy), (True, f, rb)):
+        name = "every_length:" + ("final" if wiener else "basic")
+        g = ctx.debug_groups(p, wiener, ref)
+        lengths = set(np.unique(g[0]).tolist())
+        assert lengths == set(range(1, 17)), sorted(lengths)
+        assert group_match(name + "_groups", g, orc.groups(wiener, p.as_dict(), ref)) == 1.0
+        want = orc.stage(wiener, p.as_dict(), noisy, ref if wiener else None)
+        got = np.empty_like(noisy)
+        ctx.stage(p, wiener, got, noisy, ref if wiener else None)
+        assert_close(name, got, want)
