@@ -31,19 +31,41 @@ __device__ __forceinline__ void dct_line(T *base, int stride, int n, const T *ma
     }
 }
 
-// Separable 3-D transform of an n x bs x bs group (row-major [z][y][x]) with
-// the concatenated matrices `tab` (forward REDFT10 or backward REDFT01).
+// One 8-point line of an 8 x 8 block, in place, by the butterflies of dct.cuh.
 template <typename T>
-__device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab)
+__device__ __forceinline__ void dct_line8(T *base, int stride, bool inverse)
+{
+    T v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = base[j * stride];
+    if (inverse) redft01_8(v);
+    else redft10_8(v);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) base[j * stride] = v[j];
+}
+
+// Separable 3-D transform of an n x bs x bs group (row-major [z][y][x]) with
+// the concatenated matrices `tab` (forward REDFT10 or backward REDFT01, as
+// `inverse` says). BlockSize 8 runs its rows and columns as butterflies.
+template <typename T>
+__device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool inverse)
 {
     const int bsq = bs * bs;
-    const T *mb = tab + dct_table_offset(bs);
-    for (int line = lane; line < n * bs; line += kWarp)  // along x
-        dct_line(G + line * bs, 1, bs, mb);
-    __syncwarp();
-    for (int line = lane; line < n * bs; line += kWarp) {  // along y
-        const int z = line / bs, x = line - z * bs;
-        dct_line(G + z * bsq + x, bs, bs, mb);
+    if (bs == 8) {
+        for (int line = lane; line < n * 8; line += kWarp)  // along x
+            dct_line8(G + line * 8, 1, inverse);
+        __syncwarp();
+        for (int line = lane; line < n * 8; line += kWarp)  // along y
+            dct_line8(G + (line >> 3) * 64 + (line & 7), 8, inverse);
+    } else {
+        const T *mb = tab + dct_table_offset(bs);
+        for (int line = lane; line < n * bs; line += kWarp)  // along x
+            dct_line(G + line * bs, 1, bs, mb);
+        __syncwarp();
+        for (int line = lane; line < n * bs; line += kWarp) {  // along y
+            const int z = line / bs, x = line - z * bs;
+            dct_line(G + z * bsq + x, bs, bs, mb);
+        }
     }
     __syncwarp();
     const T *mz = tab + dct_table_offset(n);
@@ -132,7 +154,7 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         }
     }
     __syncwarp();
-    dct3_generic(Gs, n, bs, lane, a.dct_fwd);
+    dct3_generic(Gs, n, bs, lane, a.dct_fwd, false);
     T denW;
     if (!WIENER) {
         // hard threshold (source/BM3D.cpp:361-371) with thr by #zero indices
@@ -148,7 +170,7 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         const int retained = __reduce_add_sync(0xffffffffu, kept);
         denW = retained < 1 ? T(1) : T(1) / static_cast<T>(retained);
     } else {
-        dct3_generic(Gr, n, bs, lane, a.dct_fwd);
+        dct3_generic(Gr, n, bs, lane, a.dct_fwd, false);
         const T s2 = a.wss[p][n - 1];
         T l2 = T(0);
         for (int e = lane; e < total; e += kWarp) {
@@ -162,7 +184,7 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     }
     const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
     __syncwarp();
-    dct3_generic(Gs, n, bs, lane, a.dct_inv);
+    dct3_generic(Gs, n, bs, lane, a.dct_inv, true);
     // the block weight once per block, at its origin (as the register-resident kernel)
     for (int e = lane; e < total; e += kWarp) {
         const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
@@ -218,8 +240,13 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
     for (int r = warp; r < nrefs; r += nwarps) {
         const int ky = ky0 + r / tw, kx = kx0 + r % tw;
         const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
-        const int n = match_generic<T>(a, t, j0, i0, lane, keys, refblk, heap, list, lkeys,
-                                       n_cand, n_fix);
+        // BlockSize 8 with step 1: the register-resident kernel's strips of
+        // four candidates; otherwise one lane per candidate
+        const int n = (bs == kBS && a.bm_step == 1)
+                          ? match_block<T, 4>(a, t, j0, i0, lane, keys, heap, list, lkeys, n_cand,
+                                              n_fix)
+                          : match_generic<T>(a, t, j0, i0, lane, keys, refblk, heap, list, lkeys,
+                                             n_cand, n_fix);
         n_sum += n;
         n_sq += static_cast<unsigned>(n * n);
         dump_group(a, ky, kx, n, lane, list, lkeys);
@@ -238,7 +265,7 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
 }
 
 template <typename T, bool WIENER, int NPL>
-__global__ void __launch_bounds__(256) generic_stage_kernel(const StageArgs<T> a)
+__global__ void __launch_bounds__(256, 1) generic_stage_kernel(const StageArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     generic_tile_body<T, WIENER, NPL>(a, blockIdx.x, smem, dynamic_smem_bytes());
