@@ -13,6 +13,12 @@
 
 namespace bm3d {
 
+// FP32 cosine matrices of length 32 (row k = output k), for full groups of
+// GroupSize 32: every coefficient a constant-bank operand. Each translation
+// unit has its own copy, filled by the host when a context is made.
+static __constant__ float c_dct32_fwd[32 * 32];
+static __constant__ float c_dct32_inv[32 * 32];
+
 // In-place length-n transform of one strided line, by one lane: out[k] =
 // sum_j mat[k n + j] in[j] (row k = output k), n <= kGSTab.
 template <typename T>
@@ -68,6 +74,21 @@ __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool i
         }
     }
     __syncwarp();
+    if constexpr (sizeof(T) == 4) {
+        if (n == 32) {  // full GroupSize-32 groups: unrolled, halved by symmetry
+            for (int line = lane; line < bsq; line += kWarp) {
+                T v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) v[j] = G[line + j * bsq];
+                if (inverse) redft01_line<T, 32>(v, c_dct32_inv);
+                else redft10_line<T, 32>(v, c_dct32_fwd);
+#pragma unroll
+                for (int k = 0; k < 32; ++k) G[line + k * bsq] = v[k];
+            }
+            __syncwarp();
+            return;
+        }
+    }
     const T *mz = tab + dct_table_offset(n);
     for (int line = lane; line < bsq; line += kWarp)  // along the group
         dct_line(G + line, bsq, n, mz);

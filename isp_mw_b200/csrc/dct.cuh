@@ -209,4 +209,52 @@ __host__ __device__ __forceinline__ void redft01_pair(T (&a)[16], T (&b)[16], co
     }
 }
 
+// The same symmetric forms for one line of N values (N up to the group
+// size limit, 32), in place.
+template <typename T, int N, typename Mat>
+__host__ __device__ __forceinline__ void redft10_line(T (&a)[N], const Mat *m)
+{
+    constexpr int H = N / 2;
+    T u[H + 1], v[H + 1];
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+        u[j] = a[j] + a[N - 1 - j];
+        v[j] = a[j] - a[N - 1 - j];
+    }
+    u[H] = (N & 1) ? a[H] : T(0);
+    T y[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        T s = T(0);
+        if ((k & 1) == 0) {
+#pragma unroll
+            for (int j = 0; j < H + (N & 1); ++j) s += T(m[k * N + j]) * u[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < H; ++j) s += T(m[k * N + j]) * v[j];
+        }
+        y[k] = s;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) a[k] = y[k];
+}
+
+template <typename T, int N, typename Mat>
+__host__ __device__ __forceinline__ void redft01_line(T (&a)[N], const Mat *m)
+{
+    T y[N];
+#pragma unroll
+    for (int k = 0; k < (N + 1) / 2; ++k) {
+        T e = T(0), o = T(0);
+#pragma unroll
+        for (int j = 0; j < N; j += 2) e += T(m[k * N + j]) * a[j];
+#pragma unroll
+        for (int j = 1; j < N; j += 2) o += T(m[k * N + j]) * a[j];
+        y[k] = e + o;
+        if (N - 1 - k != k) y[N - 1 - k] = e - o;
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) a[k] = y[k];
+}
+
 }  // namespace bm3d

@@ -36,3 +36,11 @@ extern "C" void host_dct_pair_f64(double *x, double *y, int n, const double *mat
 {
     PairTable<1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16>::run(n, x, y, mat, inverse);
 }
+
+// One line of length 32 through the symmetric forms, with the 32 x 32 matrix.
+extern "C" void host_dct_line32_f64(double *x, const double *mat, int inverse)
+{
+    double (&a)[32] = *reinterpret_cast<double(*)[32]>(x);
+    if (inverse) bm3d::redft01_line<double, 32>(a, mat);
+    else bm3d::redft10_line<double, 32>(a, mat);
+}

@@ -74,3 +74,22 @@ def test_matrix_transform_lengths(dctlib, n):
             ref = scipy.fft.dct(x[:n], type=typ, norm=None)
             assert np.allclose(got[:n], ref, rtol=0, atol=1e-12 * max(1, np.abs(x).sum()) * 4)
             assert np.all(got[n:] == x[n:])
+
+
+def test_line_transform_32(dctlib):
+    """The length-32 symmetric line forms (full GroupSize-32 groups) against
+    scipy's DCT-II / DCT-III."""
+    n = 32
+    k = np.arange(n)[:, None]
+    j = np.arange(n)[None, :]
+    fwd = 2 * np.cos(np.pi * (2 * j + 1) * k / (2 * n))
+    inv = np.where(j == 0, 1.0, 2 * np.cos(np.pi * j * (2 * k + 1) / (2 * n)))
+    rng = np.random.default_rng(32)
+    for mat, typ in ((fwd, 2), (inv, 3)):
+        x = rng.standard_normal(n)
+        a = x.copy()
+        m = np.ascontiguousarray(mat.ravel())
+        dctlib.host_dct_line32_f64(a.ctypes.data_as(ctypes.c_void_p),
+                                   m.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(typ == 3))
+        ref = scipy.fft.dct(x, type=typ, norm=None)
+        assert np.allclose(a, ref, rtol=0, atol=1e-12 * np.abs(x).sum() * 8)
