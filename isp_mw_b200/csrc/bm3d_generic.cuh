@@ -154,6 +154,22 @@ __device__ int match_generic(const StageArgs<T> &a, const Tile<T> &t, int j0, in
     return select_group<T>(a, keys, ngrid, nc, tp, l, st, j0, i0, lane, heap, list, lkeys, n_fix);
 }
 
+// Element e of a group stored [z][y][x]: shifts for BlockSize 8, divisions
+// otherwise.
+__device__ __forceinline__ void group_index(int e, int bs, int bsq, int &z, int &y, int &x)
+{
+    if (bs == 8) {
+        z = e >> 6;
+        y = (e >> 3) & 7;
+        x = e & 7;
+    } else {
+        z = e / bsq;
+        const int rem = e - z * bsq;
+        y = rem / bs;
+        x = rem - y * bs;
+    }
+}
+
 // Collaborative filtering of one group on plane p (generic sizes).
 template <typename T, bool WIENER>
 __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
@@ -162,10 +178,11 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
 {
     const int bs = t.bs, bsq = bs * bs, total = n * bsq;
     for (int e = lane; e < total; e += kWarp) {
-        const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
+        int z, y, x;
+        group_index(e, bs, bsq, z, y, x);
         const BlockPos q = list[z];
         const bool ok = block_in_tile(t, q.y, q.x);
-        if (!ok && rem == 0) ++n_bad;
+        if (!ok && y == 0 && x == 0) ++n_bad;
         int pitch;
         const T *bp = block_ptr(t, t.srcw[p], t.src0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
         Gs[e] = ok ? bp[y * pitch + x] : T(0);
@@ -182,7 +199,8 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         const T *thr = a.thr[p][n - 1];
         int kept = 0;
         for (int e = lane; e < total; e += kWarp) {
-            const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
+            int z, y, x;
+            group_index(e, bs, bsq, z, y, x);
             const T v = Gs[e];
             const T av = v < T(0) ? -v : v;
             if (av <= thr[(x == 0) + (y == 0) + (z == 0)]) Gs[e] = T(0);
@@ -208,13 +226,14 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     dct3_generic(Gs, n, bs, lane, a.dct_inv, true);
     // the block weight once per block, at its origin (as the register-resident kernel)
     for (int e = lane; e < total; e += kWarp) {
-        const int z = e / bsq, rem = e - z * bsq, y = rem / bs, x = rem - y * bs;
+        int z, y, x;
+        group_index(e, bs, bsq, z, y, x);
         const BlockPos q = list[z];
         if (!block_in_tile(t, q.y, q.x)) continue;
         int pitch;
         auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
         acc_add(dn + y * pitch + x, Gs[e] * numW, scale);
-        if (rem == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
+        if (y == 0 && x == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
     }
     __syncwarp();
 }
