@@ -185,14 +185,30 @@ __device__ int select_group(const StageArgs<T> &a, const SortKey<T> *keys, int n
     // T = the (take)-th smallest of the lanes' minima bounds the take best
     // from above (those minima are take distinct candidates). All candidates
     // whose key value is <= T's -- ties with the cut-off included -- are
-    // compacted and bitonic-sorted; typically 16-24 of ~360.
+    // compacted and bitonic-sorted; typically 16-24 of ~360. Groups of more
+    // than 17 blocks take T from the lanes' two smallest keys (64 distinct
+    // candidates), which keeps the compacted set within the 64-wide sort.
     const int nkeys = ngrid + 1;
-    K lmin = K::invalid();
+    const bool two = GS - 1 > kWarp / 2;
+    K lmin = K::invalid(), lmin2 = K::invalid();
     int nvalid = 0;
-    for (int i = lane; i < nkeys; i += kWarp) {
-        const K v = keys[i];
-        nvalid += v.valid() ? 1 : 0;
-        if (v < lmin) lmin = v;
+    if (two) {
+        for (int i = lane; i < nkeys; i += kWarp) {
+            const K v = keys[i];
+            nvalid += v.valid() ? 1 : 0;
+            if (v < lmin) {
+                lmin2 = lmin;
+                lmin = v;
+            } else if (v < lmin2) {
+                lmin2 = v;
+            }
+        }
+    } else {
+        for (int i = lane; i < nkeys; i += kWarp) {
+            const K v = keys[i];
+            nvalid += v.valid() ? 1 : 0;
+            if (v < lmin) lmin = v;
+        }
     }
     const int accepted = __reduce_add_sync(0xffffffffu, nvalid);
     const int take = min(GS - 1, accepted);
@@ -214,7 +230,14 @@ __device__ int select_group(const StageArgs<T> &a, const SortKey<T> *keys, int n
     };
     bool tie = false;
     if (take > 0) {
-        const K thr = bitonic32(lmin, lane).shfl(take - 1);
+        K thr;
+        if (two) {  // element take - 1 (< 32) of the 64 sorted sits in lane take - 1's v0
+            K s0 = lmin, s1 = lmin2;
+            bitonic64(s0, s1, lane);
+            thr = s0.shfl(take - 1);
+        } else {
+            thr = bitonic32(lmin, lane).shfl(take - 1);
+        }
         const auto tb = thr.key_bits();
         int cnt = 0;
         for (int i = lane; i < nkeys; i += kWarp) {
