@@ -2,6 +2,9 @@
 launches of one BM3D stage on one seeded synthetic plane (device memory).
 
     python -m isp_mw_b200.profile_case --stage final --width 1920 --height 1080
+
+With `--time`, the launches are timed with CUDA events instead (for the
+profile tables): `--profile np --time` prints ms per launch of each stage.
 """
 from __future__ import annotations
 
@@ -20,7 +23,12 @@ def main():
                     help="run the stage's block matching alone (bm3d_debug_groups)")
     ap.add_argument("--planes", type=int, choices=[1, 3], default=1,
                     help="3: Y/U/V planes (sigma 15/10/10) sharing luma groups (bm3d_stage3)")
+    ap.add_argument("--profile", default="fast", choices=["fast", "lc", "np", "high", "vn"])
+    ap.add_argument("--time", action="store_true",
+                    help="time both stages (CUDA events, --launches each) and print ms and MP/s")
     args = ap.parse_args()
+    if args.time:
+        return time_stages(args)
     if args.planes == 3:
         return three_planes(args)
 
@@ -30,8 +38,8 @@ def main():
 
     _, noisy = synth.pair(args.height, args.width, args.sigma, 2024)
     sp = [synth.sigma_param(args.sigma)] * 3
-    b = isp_mw_b200.stage_params_default("fast", False, sp)
-    f = isp_mw_b200.stage_params_default("fast", True, sp)
+    b = isp_mw_b200.stage_params_default(args.profile, False, sp)
+    f = isp_mw_b200.stage_params_default(args.profile, True, sp)
     ctx = isp_mw_b200.Context(0)
     src = torch.from_numpy(noisy).cuda()
     basic = torch.empty_like(src)
@@ -49,6 +57,43 @@ def main():
     st = ctx.last_stats()
     print(f"stage={args.stage} {args.width}x{args.height} groups_sum_n={st[0]} candidates={st[2]}")
     ctx.close()
+
+
+def time_stages(args):
+    """Basic then final of the chosen profile on one seeded plane, each timed
+    over `--launches` launches after `--warmup`."""
+    import json
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+
+    _, noisy = synth.pair(args.height, args.width, args.sigma, 2024)
+    sp = [synth.sigma_param(args.sigma)] * 3
+    b = isp_mw_b200.stage_params_default(args.profile, False, sp)
+    f = isp_mw_b200.stage_params_default(args.profile, True, sp)
+    ctx = isp_mw_b200.Context(0)
+    src = torch.from_numpy(noisy).cuda()
+    basic = torch.empty_like(src)
+    out = torch.empty_like(src)
+    ms = {}
+    for name, run in (("basic", lambda: ctx.stage(b, False, basic, src)),
+                      ("final", lambda: ctx.stage(f, True, out, src, basic))):
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(max(1, args.launches)):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms[name] = e0.elapsed_time(e1) / max(1, args.launches)
+    ctx.close()
+    mp = args.width * args.height / 1e6
+    print(json.dumps({"profile": args.profile, "plane": f"{args.width}x{args.height}",
+                      "sigma_255": args.sigma, "basic_ms": round(ms["basic"], 4),
+                      "final_ms": round(ms["final"], 4),
+                      "mp_per_s": round(mp / ((ms["basic"] + ms["final"]) / 1e3), 1)}))
 
 
 def three_planes(args):
