@@ -1,10 +1,12 @@
 // Generic BM3D stage kernel: any BlockSize <= 16, GroupSize <= 32, BMrange,
 // BMstep -- the reference's other profiles ("np", "high", "vn") and custom
 // parameters. One warp per reference block; the group lives in shared memory
-// and the separable 3-D transforms run one line per lane with cosine matrices
-// from global memory. Block matching keeps the reference's exact distance
-// order; selection, aggregation and the staged windows are shared with the
-// register-resident kernel.
+// and the separable 3-D transforms run one line per lane: 8-point butterflies
+// for BlockSize 8, an unrolled 32-point form for full GroupSize-32 groups,
+// cosine matrices from global memory otherwise. Block matching keeps the
+// reference's exact distance order (BlockSize 8 with step 1 uses the
+// register-resident kernel's strips); selection, aggregation and the staged
+// windows are shared with the register-resident kernel.
 //
 // Reference: as bm3d_stage.cuh (source/BM3D.cpp:80-457, include/Block.h:578-751).
 #pragma once
