@@ -20,6 +20,9 @@ namespace bm3d {
 // unit has its own copy, filled by the host when a context is made.
 static __constant__ float c_dct32_fwd[32 * 32];
 static __constant__ float c_dct32_inv[32 * 32];
+// The same for BlockSize 11 rows and columns (the "vn" final stage).
+static __constant__ float c_dct11_fwd[11 * 11];
+static __constant__ float c_dct11_inv[11 * 11];
 
 // In-place length-n transform of one strided line, by one lane: out[k] =
 // sum_j mat[k n + j] in[j] (row k = output k), n <= kGSTab.
@@ -52,6 +55,22 @@ __device__ __forceinline__ void dct_line8(T *base, int stride, bool inverse)
     for (int j = 0; j < 8; ++j) base[j * stride] = v[j];
 }
 
+// One 11-point line (FP32), in place, by the symmetric form with
+// constant-bank cosines; other precisions never reach it.
+template <typename T>
+__device__ __forceinline__ void dct_line11(T *base, int stride, bool inverse)
+{
+    if constexpr (sizeof(T) == 4) {
+        T v[11];
+#pragma unroll
+        for (int j = 0; j < 11; ++j) v[j] = base[j * stride];
+        if (inverse) redft01_line<T, 11>(v, c_dct11_inv);
+        else redft10_line<T, 11>(v, c_dct11_fwd);
+#pragma unroll
+        for (int j = 0; j < 11; ++j) base[j * stride] = v[j];
+    }
+}
+
 // Separable 3-D transform of an n x bs x bs group (row-major [z][y][x]) with
 // the concatenated matrices `tab` (forward REDFT10 or backward REDFT01, as
 // `inverse` says). BlockSize 8 runs its rows and columns as butterflies.
@@ -65,6 +84,14 @@ __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool i
         __syncwarp();
         for (int line = lane; line < n * 8; line += kWarp)  // along y
             dct_line8(G + (line >> 3) * 64 + (line & 7), 8, inverse);
+    } else if (sizeof(T) == 4 && bs == 11) {
+        for (int line = lane; line < n * 11; line += kWarp)  // along x
+            dct_line11(G + line * 11, 1, inverse);
+        __syncwarp();
+        for (int line = lane; line < n * 11; line += kWarp) {  // along y
+            const int z = line / 11, x = line - z * 11;
+            dct_line11(G + z * 121 + x, 11, inverse);
+        }
     } else {
         const T *mb = tab + dct_table_offset(bs);
         for (int line = lane; line < n * bs; line += kWarp)  // along x
@@ -143,11 +170,21 @@ __device__ int match_generic(const StageArgs<T> &a, const Tile<T> &t, int j0, in
             cand = block_ptr(t, t.refw[0], t.ref0[0], 0, 0, cp);  // the trailing (0, 0) slot
         }
         T d = T(0);
-        for (int y = 0; y < bs; ++y)
-            for (int x = 0; x < bs; ++x) {
-                const T df = sub_rn(refblk[y * bs + x], cand[y * cp + x]);
-                d = add_rn(d, mul_rn(df, df));
-            }
+        if (bs == 11) {  // the same order, unrolled
+#pragma unroll
+            for (int y = 0; y < 11; ++y)
+#pragma unroll
+                for (int x = 0; x < 11; ++x) {
+                    const T df = sub_rn(refblk[y * 11 + x], cand[y * cp + x]);
+                    d = add_rn(d, mul_rn(df, df));
+                }
+        } else {
+            for (int y = 0; y < bs; ++y)
+                for (int x = 0; x < bs; ++x) {
+                    const T df = sub_rn(refblk[y * bs + x], cand[y * cp + x]);
+                    d = add_rn(d, mul_rn(df, df));
+                }
+        }
         const bool ok = !self && d <= a.thSSE && d != T(0);
         keys[c] = ok ? K::make(key_from_dist(d, a.distMul), static_cast<unsigned>(c)) : K::invalid();
     }
@@ -164,6 +201,11 @@ __device__ __forceinline__ void group_index(int e, int bs, int bsq, int &z, int 
         z = e >> 6;
         y = (e >> 3) & 7;
         x = e & 7;
+    } else if (bs == 11) {  // constant divisors
+        z = e / 121;
+        const int rem = e - z * 121;
+        y = rem / 11;
+        x = rem - y * 11;
     } else {
         z = e / bsq;
         const int rem = e - z * bsq;
