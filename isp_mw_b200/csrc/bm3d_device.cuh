@@ -321,6 +321,12 @@ __device__ __forceinline__ unsigned dynamic_smem_bytes()
     return v;
 }
 
+// Generic kernel's group buffers, [z][y][x]: BlockSize 8 pads rows to 9 and
+// blocks to 72 values, which keeps the row, column and group-axis passes of
+// a warp on 32 distinct banks; other sizes are dense.
+__host__ __device__ __forceinline__ int generic_block_stride(int bs) { return bs == 8 ? 72 : bs * bs; }
+__host__ __device__ __forceinline__ int generic_row_stride(int bs) { return bs == 8 ? 9 : bs; }
+
 // Shared-memory layout of one CTA. The register-resident kernel runs three
 // planes one after another through a single plane's windows: it then also
 // keeps the tile's group lists, per reference block kGSMax 16-bit positions
@@ -352,7 +358,7 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
     s.off_origin_acc = s.off_origin + (sizeof(T) * bsq * s.n_stage + 15) / 16 * 16;
     s.off_warps = (s.off_origin_acc + sizeof(Acc) * bsq * 2 * nplanes + 15) / 16 * 16;
     const size_t group_bytes = generic
-        ? sizeof(T) * static_cast<size_t>(gs) * bsq * (wiener ? 2 : 1)
+        ? sizeof(T) * static_cast<size_t>(gs) * generic_block_stride(bs) * (wiener ? 2 : 1)
         : sizeof(T) * kGSMax * kGroupStride;
     const size_t key_bytes = sizeof(SortKey<T>) * key_slots;
     const size_t scratch = group_bytes > key_bytes ? group_bytes : key_bytes;

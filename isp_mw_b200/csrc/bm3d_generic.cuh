@@ -78,12 +78,12 @@ template <typename T>
 __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool inverse)
 {
     const int bsq = bs * bs;
-    if (bs == 8) {
+    if (bs == 8) {  // padded layout: row stride 9, block stride 72
         for (int line = lane; line < n * 8; line += kWarp)  // along x
-            dct_line8(G + line * 8, 1, inverse);
+            dct_line8(G + (line >> 3) * 72 + (line & 7) * 9, 1, inverse);
         __syncwarp();
         for (int line = lane; line < n * 8; line += kWarp)  // along y
-            dct_line8(G + (line >> 3) * 64 + (line & 7), 8, inverse);
+            dct_line8(G + (line >> 3) * 72 + (line & 7), 9, inverse);
     } else if (sizeof(T) == 4 && bs == 11) {
         for (int line = lane; line < n * 11; line += kWarp)  // along x
             dct_line11(G + line * 11, 1, inverse);
@@ -103,24 +103,30 @@ __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool i
         }
     }
     __syncwarp();
+    // along the group: pencil p = (y, x) of every block
+    const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
     if constexpr (sizeof(T) == 4) {
         if (n == 32) {  // full GroupSize-32 groups: unrolled, halved by symmetry
             for (int line = lane; line < bsq; line += kWarp) {
+                const int py = line / bs;
+                T *g = G + py * rs + (line - py * bs);
                 T v[32];
 #pragma unroll
-                for (int j = 0; j < 32; ++j) v[j] = G[line + j * bsq];
+                for (int j = 0; j < 32; ++j) v[j] = g[j * zs];
                 if (inverse) redft01_line<T, 32>(v, c_dct32_inv);
                 else redft10_line<T, 32>(v, c_dct32_fwd);
 #pragma unroll
-                for (int k = 0; k < 32; ++k) G[line + k * bsq] = v[k];
+                for (int k = 0; k < 32; ++k) g[k * zs] = v[k];
             }
             __syncwarp();
             return;
         }
     }
     const T *mz = tab + dct_table_offset(n);
-    for (int line = lane; line < bsq; line += kWarp)  // along the group
-        dct_line(G + line, bsq, n, mz);
+    for (int line = lane; line < bsq; line += kWarp) {
+        const int py = line / bs;
+        dct_line(G + py * rs + (line - py * bs), zs, n, mz);
+    }
     __syncwarp();
 }
 
@@ -221,18 +227,20 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
                                unsigned &n_bad)
 {
     const int bs = t.bs, bsq = bs * bs, total = n * bsq;
+    const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
     for (int e = lane; e < total; e += kWarp) {
         int z, y, x;
         group_index(e, bs, bsq, z, y, x);
+        const int g = z * zs + y * rs + x;
         const BlockPos q = list[z];
         const bool ok = block_in_tile(t, q.y, q.x);
         if (!ok && y == 0 && x == 0) ++n_bad;
         int pitch;
         const T *bp = block_ptr(t, t.srcw[p], t.src0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
-        Gs[e] = ok ? bp[y * pitch + x] : T(0);
+        Gs[g] = ok ? bp[y * pitch + x] : T(0);
         if (WIENER) {
             const T *rp = block_ptr(t, t.refw[p], t.ref0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
-            Gr[e] = ok ? rp[y * pitch + x] : T(0);
+            Gr[g] = ok ? rp[y * pitch + x] : T(0);
         }
     }
     __syncwarp();
@@ -245,9 +253,10 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         for (int e = lane; e < total; e += kWarp) {
             int z, y, x;
             group_index(e, bs, bsq, z, y, x);
-            const T v = Gs[e];
+            const int g = z * zs + y * rs + x;
+            const T v = Gs[g];
             const T av = v < T(0) ? -v : v;
-            if (av <= thr[(x == 0) + (y == 0) + (z == 0)]) Gs[e] = T(0);
+            if (av <= thr[(x == 0) + (y == 0) + (z == 0)]) Gs[g] = T(0);
             else ++kept;
         }
         const int retained = __reduce_add_sync(0xffffffffu, kept);
@@ -257,9 +266,11 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         const T s2 = a.wss[p][n - 1];
         T l2 = T(0);
         for (int e = lane; e < total; e += kWarp) {
-            const T y2 = Gr[e] * Gr[e];
+            // any one-to-one order works here; the padded layout needs its address
+            const int g = bs == 8 ? (e >> 6) * 72 + ((e >> 3) & 7) * 9 + (e & 7) : e;
+            const T y2 = Gr[g] * Gr[g];
             const T w = wiener_weight(y2, s2);
-            Gs[e] *= w;
+            Gs[g] *= w;
             l2 += w * w;
         }
         l2 = warp_sum(l2);
@@ -276,7 +287,7 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         if (!block_in_tile(t, q.y, q.x)) continue;
         int pitch;
         auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
-        acc_add(dn + y * pitch + x, Gs[e] * numW, scale);
+        acc_add(dn + y * pitch + x, Gs[z * zs + y * rs + x] * numW, scale);
         if (y == 0 && x == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
     }
     __syncwarp();
@@ -305,7 +316,7 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
 
     unsigned char *wbase = smem + sp.off_warps + sp.warp_bytes * warp;
     const size_t scratch = sp.scratch_bytes;
-    const int gvals = a.group_size * bs * bs;
+    const int gvals = a.group_size * generic_block_stride(bs);
     T *Gs = reinterpret_cast<T *>(wbase);
     T *Gr = Gs + gvals;
     SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
