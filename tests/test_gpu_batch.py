@@ -145,3 +145,27 @@ def test_batch_other_profiles_equal_per_plane(bm3d_lib, profile, bm_step):
     batch.close()
     batch3.close()
     ctx.close()
+
+
+def test_batch_rejects_bad_planes(bm3d_lib):
+    """A plane smaller than a block, or stages whose geometry differs between
+    planes, make batch creation fail with BM3D_ERR_INVALID (no launch)."""
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    ctx = isp_mw_b200.Context(0)
+    sp = [synth.sigma_param(20.0)] * 3
+    pb = isp_mw_b200.stage_params_default("fast", False, sp)
+    pf = isp_mw_b200.stage_params_default("fast", True, sp)
+    ok = torch.from_numpy(synth.pair(64, 64, 20.0, 1)[1]).cuda()
+    tiny = torch.zeros((7, 40), dtype=torch.float32, device="cuda")
+    for planes in ([ok, tiny], [tiny]):
+        dsts = [torch.empty_like(p) for p in planes]
+        with pytest.raises(isp_mw_b200.BM3DError) as e:
+            isp_mw_b200.Batch(ctx, [pb] * len(planes), [pf] * len(planes), dsts, planes)
+        assert e.value.code == isp_mw_b200.BM3D_ERR_INVALID
+    other = isp_mw_b200.stage_params_default("lc", False, sp)  # another block step
+    with pytest.raises(isp_mw_b200.BM3DError) as e:
+        isp_mw_b200.Batch(ctx, [pb, other], [pf, pf], [torch.empty_like(ok)] * 2, [ok, ok])
+    assert e.value.code == isp_mw_b200.BM3D_ERR_INVALID
+    ctx.close()
