@@ -1,62 +1,10 @@
 // C ABI of the B200 BM3D path (declared in include/bm3d_b200.h): parameter
 // mirroring, per-call constant setup, context scratch and kernel launches.
-#include "bm3d_b200.h"
-#include "bm3d_batch.cuh"
-#include "bm3d_convert.cuh"
-#include "bm3d_kernels.h"
+// The integer / Frame entry points are in bm3d_capi_convert.cu, the batches
+// in bm3d_capi_batch.cu.
+#include "bm3d_capi_internal.h"
 
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <mutex>
-#include <string>
-#include <vector>
-
-using namespace bm3d;
-
-// ---------------------------------------------------------------------------
-// Context
-
-struct DevBuf {
-    void *ptr = nullptr;
-    size_t bytes = 0;
-};
-
-struct bm3d_ctx {
-    int device = 0;
-    int sm_count = 0;
-    size_t smem_optin = 0;
-    std::string err;
-    // scratch
-    DevBuf acc[2 * kMaxPlanes];       // num / den per plane
-    DevBuf basic[kMaxPlanes];         // basic estimate for bm3d_full*
-    DevBuf stage_in[kMaxPlanes];      // host-mode staging of src
-    DevBuf stage_ref[kMaxPlanes];     // host-mode staging of ref
-    DevBuf stage_out[kMaxPlanes];     // host-mode staging of dst
-    DevBuf groups[3];                 // debug group dump
-    DevBuf conv[3 * kMaxPlanes];      // float working planes of the integer paths: src, ref, dst
-    DevBuf ints[3 * kMaxPlanes];      // host-mode staging of integer planes: src, ref, dst
-    unsigned long long *stats = nullptr;
-    float *absmax = nullptr;          // per plane max |src| of the running stage
-    float *gtab_f = nullptr;          // generic path cosine matrices: fwd | inv (float)
-    double *gtab_d = nullptr;         // same in double
-    cudaStream_t last_stream = nullptr;
-    int tile_x = 8, tile_y = 8, warps = 16;
-    // bm3d_full_many's copy pipeline: two slots of device planes, an upload
-    // and a download stream, and the events that order slot reuse
-    struct PipeSlot {
-        DevBuf in, out;
-        cudaEvent_t in_ready = nullptr, computed = nullptr, drained = nullptr;
-        bool used = false;
-    } pipe[2];
-    cudaStream_t up = nullptr, down = nullptr;
-    unsigned long long pipe_count = 0;
-    // optional per-launch timing of the stage kernels: [0] basic, [1] final
-    bool timing = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[2];
-    double time_ms[2] = {0, 0};
-    long long launches[2] = {0, 0};
-};
+static thread_local std::string g_create_error;
 
 static void drain_timing(bm3d_ctx *ctx)
 {
@@ -75,10 +23,7 @@ static void drain_timing(bm3d_ctx *ctx)
     }
 }
 
-static thread_local std::string g_create_error;
-constexpr int kStats = 5;
-
-static int cuda_fail(bm3d_ctx *ctx, cudaError_t e, const char *what)
+int bm3d::cuda_fail(bm3d_ctx *ctx, cudaError_t e, const char *what)
 {
     char buf[256];
     std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
@@ -87,13 +32,7 @@ static int cuda_fail(bm3d_ctx *ctx, cudaError_t e, const char *what)
     return e == cudaErrorMemoryAllocation ? BM3D_ERR_NOMEM : BM3D_ERR_CUDA;
 }
 
-#define CK(ctx, call)                                                                       \
-    do {                                                                                     \
-        cudaError_t e_ = (call);                                                             \
-        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call);                           \
-    } while (0)
-
-static int ensure(bm3d_ctx *ctx, DevBuf &b, size_t bytes)
+int bm3d::ensure(bm3d_ctx *ctx, DevBuf &b, size_t bytes)
 {
     if (b.bytes >= bytes) return BM3D_OK;
     if (b.ptr) cudaFree(b.ptr);
@@ -395,8 +334,6 @@ static void opp_norms(double norm[3])
     norm[2] = std::sqrt(Vr * Vr + Vg * Vg + Vb * Vb);
 }
 
-enum class Guard { Run, Copy, Invalid, Unsupported };
-
 // The register-resident kernel covers BlockSize 8 with GroupSize <= 16 (the
 // "fast" and "lc" profiles); everything else up to BlockSize 16 and GroupSize
 // 32 runs on the generic kernel.
@@ -405,7 +342,7 @@ static bool fast_path(const bm3d_stage_params *p)
     return p->block_size == kBS && p->group_size <= kGSMax;
 }
 
-static Guard check_params(const bm3d_stage_params *p, int nplanes)
+Guard bm3d::check_params(const bm3d_stage_params *p, int nplanes)
 {
     if (!p) return Guard::Invalid;
     double norm[3];
@@ -422,8 +359,8 @@ static Guard check_params(const bm3d_stage_params *p, int nplanes)
 }
 
 template <typename T>
-static void fill_tables(StageArgs<T> &a, const bm3d_stage_params *p, bool wiener, int nplanes,
-                        double value_range)
+void bm3d::fill_tables(StageArgs<T> &a, const bm3d_stage_params *p, bool wiener, int nplanes,
+                       double value_range)
 {
     double norm[3];
     opp_norms(norm);
@@ -513,7 +450,7 @@ static int launch_generic(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int wa
     return BM3D_OK;
 }
 
-static bool fast_args(int block_size, int group_size)
+bool bm3d::fast_args(int block_size, int group_size)
 {
     return block_size == kBS && group_size <= kGSMax;
 }
@@ -593,15 +530,6 @@ static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params
     return BM3D_OK;
 }
 
-template <typename T>
-static int copy_plane(bm3d_ctx *ctx, T *dst, size_t dpitch, const T *src, size_t spitch, int w,
-                      int h, cudaMemcpyKind kind, cudaStream_t s)
-{
-    CK(ctx, cudaMemcpy2DAsync(dst, dpitch * sizeof(T), src, spitch * sizeof(T), w * sizeof(T), h,
-                              kind, s));
-    return BM3D_OK;
-}
-
 // One stage over device-resident planes (all with row pitch `stride`).
 template <typename T>
 static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wiener, int nplanes,
@@ -672,7 +600,7 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
 
 // Host-mode calls end synchronised; a nonzero invariant counter means a group
 // member fell outside its tile's staged window and was skipped.
-static int check_invariants(bm3d_ctx *ctx)
+int bm3d::check_invariants(bm3d_ctx *ctx)
 {
     unsigned long long v[kStats];
     CK(ctx, cudaMemcpy(v, ctx->stats, sizeof(v), cudaMemcpyDeviceToHost));
@@ -711,9 +639,9 @@ static int check_planes(int nplanes, const void *const dst[], const void *const 
 // A stage in either memory kind. In host mode planes go through context
 // staging buffers with pitch = width.
 template <typename T>
-static int stage_any(bm3d_ctx *ctx, const bm3d_stage_params *p, int wiener, int nplanes,
-                     T *const dst[], const T *const src[], const T *const ref[], int width,
-                     int height, size_t stride, double value_range, int mem, void *stream)
+int bm3d::stage_any(bm3d_ctx *ctx, const bm3d_stage_params *p, int wiener, int nplanes,
+              T *const dst[], const T *const src[], const T *const ref[], int width, int height,
+              size_t stride, double value_range, int mem, void *stream)
 {
     if (!ctx) return BM3D_ERR_INVALID;
     if (mem != BM3D_MEM_HOST && mem != BM3D_MEM_DEVICE) return BM3D_ERR_INVALID;
@@ -806,10 +734,9 @@ extern "C" int bm3d_stage3(bm3d_ctx *ctx, const bm3d_stage_params *params, int w
 }
 
 template <typename T>
-static int full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *fin,
-                    int nplanes, T *const dst[], const T *const src[], const T *const ref[],
-                    int width, int height, size_t stride, double value_range, int mem,
-                    void *stream)
+int bm3d::full_any(bm3d_ctx *ctx, const bm3d_stage_params *basic, const bm3d_stage_params *fin,
+             int nplanes, T *const dst[], const T *const src[], const T *const ref[], int width,
+             int height, size_t stride, double value_range, int mem, void *stream)
 {
     if (!ctx || !basic || !fin) return BM3D_ERR_INVALID;
     if (mem != BM3D_MEM_HOST && mem != BM3D_MEM_DEVICE) return BM3D_ERR_INVALID;
@@ -932,511 +859,16 @@ extern "C" int bm3d_full3(bm3d_ctx *ctx, const bm3d_stage_params *basic,
                            value_range, mem, stream);
 }
 
-// ---------------------------------------------------------------------------
-// Integer planes and RGB frames: conversion kernels around the float paths.
 
-namespace {
-
-// Quantisation of an integer plane (Floor, Neutral, Ceil) and of the float
-// plane it maps to (the reference's default Plane_FL ranges,
-// include/Image_Type.hpp:184-202): luma [0, 1], chroma [-0.5, 0.5].
-struct Quant {
-    int floor_, neutral, ceil_;
-    bool chroma() const { return floor_ < neutral; }
-    // isPCChroma (include/Image_Type.hpp:152-155)
-    bool pc_chroma() const { return chroma() && (floor_ + ceil_) % 2 == 1; }
-    float ffloor() const { return chroma() ? -0.5f : 0.0f; }
-    float fceil() const { return chroma() ? 0.5f : 1.0f; }
-};
-
-// RangeConvert(float plane, int plane, clip = false)
-// (include/Conversion.hpp:231-253): full-range chroma is clipped anyway.
-RangeMap range_to_float(const Quant &q)
-{
-    const int sRange = q.ceil_ - q.floor_;
-    const float dRange = q.fceil() - q.ffloor();
-    const float dNeutral = 0.0f;
-    RangeMap m;
-    m.gain = dRange / static_cast<float>(sRange);
-    m.offset = -static_cast<float>(q.neutral) * m.gain + dNeutral;
-    m.lo = q.ffloor();
-    m.hi = q.fceil();
-    m.clip = q.pc_chroma() ? 1 : 0;
-    return m;
-}
-
-// RangeConvert(int plane, float plane, clip = true): +0.5 (+0.499999 for
-// full-range chroma) before truncation.
-RangeMap range_to_int(const Quant &q)
-{
-    const float sRange = q.fceil() - q.ffloor();
-    const int dRange = q.ceil_ - q.floor_;
-    const float sNeutral = 0.0f;
-    RangeMap m;
-    m.gain = static_cast<float>(dRange) / sRange;
-    m.offset = -sNeutral * m.gain + static_cast<float>(q.neutral);
-    m.offset += q.pc_chroma() ? 0.499999f : 0.5f;
-    m.lo = static_cast<float>(q.floor_);
-    m.hi = static_cast<float>(q.ceil_);
-    m.clip = 1;
-    return m;
-}
-
-// MatrixConvert_RGB2YUV, ColorMatrix::OPP, float destination
-// (include/Conversion.hpp:537-546): source Floor floor_, Ceil ceil_.
-OppForward opp_forward(int floor_, int ceil_)
-{
-    const int sRange = ceil_ - floor_;
-    const float dRangeY = 1.0f - 0.0f, dRangeC = 0.5f - -0.5f, dFloorY = 0.0f, dNeutralC = 0.0f;
-    OppForward c;
-    c.gainY = dRangeY / (static_cast<float>(sRange) * 3.0f);
-    c.offsetY = -static_cast<float>(floor_) * 3.0f * c.gainY + dFloorY;
-    c.gainU = dRangeC / (static_cast<float>(sRange) * 2.0f);
-    c.gainV = dRangeC / (static_cast<float>(sRange) * 4.0f);
-    c.offsetC = dNeutralC;
-    return c;
-}
-
-// MatrixConvert_YUV2RGB, ColorMatrix::OPP, integer destination, clipping
-// (include/Conversion.hpp:690-712, coefficients include/Specification.h:
-// 468-484).
-OppInverse opp_inverse(int floor_, int ceil_)
-{
-    const int dRange = ceil_ - floor_;
-    const float sRangeY = 1.0f - 0.0f, sRangeC = 0.5f - -0.5f, sFloorY = 0.0f, sNeutralC = 0.0f;
-    const float gainY = static_cast<float>(dRange) / sRangeY;
-    const float gainC = static_cast<float>(dRange) / sRangeC;
-    OppInverse c;
-    c.Ry = static_cast<float>(1.0L) * gainY;
-    c.Ru = static_cast<float>(1.0L) * gainC;
-    c.Rv = static_cast<float>(2.0L / 3.0L) * gainC;
-    c.Gy = static_cast<float>(1.0L) * gainY;
-    const float Gu = static_cast<float>(0.0L) * gainC;
-    c.Gv = static_cast<float>(-4.0L / 3.0L) * gainC;
-    c.By = static_cast<float>(1.0L) * gainY;
-    c.Bu = static_cast<float>(-1.0L) * gainC;
-    c.Bv = static_cast<float>(2.0L / 3.0L) * gainC;
-    const float dFloor = static_cast<float>(floor_);
-    c.offR = -sFloorY * c.Ry - sNeutralC * (c.Ru + c.Rv) + dFloor;
-    c.offR += 0.5f;
-    c.offG = -sFloorY * c.Gy - sNeutralC * (Gu + c.Gv) + dFloor;
-    c.offG += 0.5f;
-    c.offB = -sFloorY * c.By - sNeutralC * (c.Bu + c.Bv) + dFloor;
-    c.offB += 0.5f;
-    c.lo = static_cast<float>(floor_);
-    c.hi = static_cast<float>(ceil_);
-    return c;
-}
-
-dim3 convert_grid(const bm3d_ctx *ctx, int width, int height)
-{
-    const int bx = (width + 255) / 256;
-    const int rows = std::max(1, std::min(height, (ctx->sm_count * 16 + bx - 1) / bx));
-    return dim3(static_cast<unsigned>(bx), static_cast<unsigned>(std::min(rows, 65535)));
-}
-
-// The guard of the stage-level integer and Frame filters
-// (source/BM3D.cpp:250-256, 286-293): unlike BM3D_Base::Kernel's, it copies
-// for GroupSize == 1, not 0.
-bool int_path_rejected(const bm3d_stage_params *p, int nplanes)
-{
-    const bool sig = nplanes == 1 ? p->sigma[0] > 0
-                                  : (p->sigma[0] > 0 || p->sigma[1] > 0 || p->sigma[2] > 0);
-    return !sig || p->group_size == 1 || p->block_size <= 0 || p->bm_range <= 0 ||
-           p->bm_range < p->bm_step || p->thMSE <= 0;
-}
-
-// Device-side integer planes of one call: the caller's (device mode) or the
-// context's staging (host mode, pitch = width).
-struct IntPlanes {
-    const int *src[kMaxPlanes] = {nullptr, nullptr, nullptr};
-    const int *ref[kMaxPlanes] = {nullptr, nullptr, nullptr};
-    int *dst[kMaxPlanes] = {nullptr, nullptr, nullptr};
-    size_t pitch = 0;
-};
-
-int stage_ints_in(bm3d_ctx *ctx, int nplanes, const int *const src[], const int *const ref[],
-                  int width, int height, size_t stride, int mem, cudaStream_t s, IntPlanes &io)
-{
-    int rc;
-    if (mem == BM3D_MEM_DEVICE) {
-        io.pitch = stride;
-        for (int c = 0; c < nplanes; ++c) {
-            io.src[c] = src[c];
-            io.ref[c] = ref ? ref[c] : nullptr;
-        }
-        return BM3D_OK;
-    }
-    io.pitch = static_cast<size_t>(width);
-    const size_t bytes = sizeof(int) * static_cast<size_t>(width) * height;
-    for (int c = 0; c < nplanes; ++c) {
-        if ((rc = ensure(ctx, ctx->ints[c], bytes)) != BM3D_OK) return rc;
-        int *d = static_cast<int *>(ctx->ints[c].ptr);
-        if ((rc = copy_plane(ctx, d, io.pitch, src[c], stride, width, height,
-                             cudaMemcpyHostToDevice, s)) != BM3D_OK)
-            return rc;
-        io.src[c] = d;
-        if (ref && ref[c]) {
-            if ((rc = ensure(ctx, ctx->ints[kMaxPlanes + c], bytes)) != BM3D_OK) return rc;
-            int *r = static_cast<int *>(ctx->ints[kMaxPlanes + c].ptr);
-            if ((rc = copy_plane(ctx, r, io.pitch, ref[c], stride, width, height,
-                                 cudaMemcpyHostToDevice, s)) != BM3D_OK)
-                return rc;
-            io.ref[c] = r;
-        }
-    }
-    return BM3D_OK;
-}
-
-int int_outputs(bm3d_ctx *ctx, int nplanes, int *const dst[], int width, int height, int mem,
-                IntPlanes &io)
-{
-    int rc;
-    const size_t bytes = sizeof(int) * static_cast<size_t>(width) * height;
-    for (int c = 0; c < nplanes; ++c) {
-        if (mem == BM3D_MEM_DEVICE) {
-            io.dst[c] = dst[c];
-        } else {
-            if ((rc = ensure(ctx, ctx->ints[2 * kMaxPlanes + c], bytes)) != BM3D_OK) return rc;
-            io.dst[c] = static_cast<int *>(ctx->ints[2 * kMaxPlanes + c].ptr);
-        }
-    }
-    return BM3D_OK;
-}
-
-int finish_ints(bm3d_ctx *ctx, int nplanes, int *const dst[], int width, int height,
-                size_t stride, int mem, cudaStream_t s, const IntPlanes &io, int status)
-{
-    if (mem == BM3D_MEM_DEVICE) return status;
-    int rc;
-    for (int c = 0; c < nplanes; ++c)
-        if ((rc = copy_plane(ctx, dst[c], stride, static_cast<const int *>(io.dst[c]), io.pitch,
-                             width, height, cudaMemcpyDeviceToHost, s)) != BM3D_OK)
-            return rc;
-    CK(ctx, cudaStreamSynchronize(s));
-    rc = check_invariants(ctx);
-    return rc != BM3D_OK ? rc : status;
-}
-
-// Float working planes (pitch = width): kind 0 = src, 1 = ref, 2 = dst.
-int conv_planes(bm3d_ctx *ctx, int kind, int nplanes, int width, int height, float *out[])
-{
-    int rc;
-    const size_t bytes = sizeof(float) * static_cast<size_t>(width) * height;
-    for (int c = 0; c < nplanes; ++c) {
-        if ((rc = ensure(ctx, ctx->conv[kind * kMaxPlanes + c], bytes)) != BM3D_OK) return rc;
-        out[c] = static_cast<float *>(ctx->conv[kind * kMaxPlanes + c].ptr);
-    }
-    return BM3D_OK;
-}
-
-int check_int_call(bm3d_ctx *ctx, int nplanes, const void *const dst[], const void *const src[],
-                   int width, int height, size_t stride, int floor_, int ceil_, int mem,
-                   const bm3d_stage_params *const ps[], int nps)
-{
-    if (!ctx) return BM3D_ERR_INVALID;
-    if (mem != BM3D_MEM_HOST && mem != BM3D_MEM_DEVICE) return BM3D_ERR_INVALID;
-    for (int k = 0; k < nps; ++k)
-        if (!ps[k]) return BM3D_ERR_INVALID;
-    if (ceil_ <= floor_) return BM3D_ERR_INVALID;
-    if (width < 1 || height < 1 || stride < static_cast<size_t>(width)) return BM3D_ERR_INVALID;
-    for (int c = 0; c < nplanes; ++c)
-        if (!dst[c] || !src[c]) return BM3D_ERR_INVALID;
-    return BM3D_OK;
-}
-
-int copy_ints(bm3d_ctx *ctx, int nplanes, int *const dst[], const int *const src[], int width,
-              int height, size_t stride, int mem, cudaStream_t s)
-{
-    int rc;
-    for (int c = 0; c < nplanes; ++c) {
-        if (dst[c] == src[c]) continue;
-        if ((rc = copy_plane(ctx, dst[c], stride, src[c], stride, width, height,
-                             mem == BM3D_MEM_HOST ? cudaMemcpyHostToHost : cudaMemcpyDeviceToDevice,
-                             s)) != BM3D_OK)
-            return rc;
-    }
-    if (mem == BM3D_MEM_HOST) CK(ctx, cudaStreamSynchronize(s));
-    return BM3D_COPIED;
-}
-
-}  // namespace
-
-extern "C" int bm3d_stage_int(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener,
-                              int32_t *dst, const int32_t *src, const int32_t *ref, int width,
-                              int height, size_t stride, int floor_, int neutral, int ceil_,
-                              int mem, void *stream)
-{
-    const void *d[1] = {dst}, *sp[1] = {src};
-    const bm3d_stage_params *ps[1] = {params};
-    int rc = check_int_call(ctx, 1, d, sp, width, height, stride, floor_, ceil_, mem, ps, 1);
-    if (rc != BM3D_OK) return rc;
-    if (neutral < floor_ || neutral > ceil_) return BM3D_ERR_INVALID;
-    CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int *dd[1] = {dst};
-    const int *ss[1] = {src};
-    if (int_path_rejected(params, 1)) return copy_ints(ctx, 1, dd, ss, width, height, stride, mem, s);
-    const Quant q{floor_, neutral, ceil_};
-    const int *rr[1] = {ref && ref != src ? ref : nullptr};
-    IntPlanes io;
-    if ((rc = stage_ints_in(ctx, 1, ss, rr, width, height, stride, mem, s, io)) != BM3D_OK) return rc;
-    if ((rc = int_outputs(ctx, 1, dd, width, height, mem, io)) != BM3D_OK) return rc;
-    float *fs[1], *fr[1], *fd[1];
-    if ((rc = conv_planes(ctx, 0, 1, width, height, fs)) != BM3D_OK) return rc;
-    if ((rc = conv_planes(ctx, 2, 1, width, height, fd)) != BM3D_OK) return rc;
-    const dim3 grid = convert_grid(ctx, width, height);
-    const RangeMap in = range_to_float(q);
-    int_to_float_kernel<<<grid, 256, 0, s>>>(io.src[0], io.pitch, fs[0], width, width, height, in);
-    CK(ctx, cudaGetLastError());
-    fr[0] = fs[0];
-    if (io.ref[0]) {
-        if ((rc = conv_planes(ctx, 1, 1, width, height, fr)) != BM3D_OK) return rc;
-        int_to_float_kernel<<<grid, 256, 0, s>>>(io.ref[0], io.pitch, fr[0], width, width, height,
-                                                 in);
-        CK(ctx, cudaGetLastError());
-    }
-    const float *cs[1] = {fs[0]}, *cr[1] = {fr[0]};
-    const int st = stage_any<float>(ctx, params, wiener, 1, fd, cs, cr, width, height, width, 1.0,
-                                    BM3D_MEM_DEVICE, stream);
-    if (st < 0) return st;
-    float_to_int_kernel<<<grid, 256, 0, s>>>(fd[0], width, io.dst[0], io.pitch, width, height,
-                                             range_to_int(q));
-    CK(ctx, cudaGetLastError());
-    return finish_ints(ctx, 1, dd, width, height, stride, mem, s, io, st);
-}
-
-extern "C" int bm3d_plane_int(bm3d_ctx *ctx, const bm3d_stage_params *basic,
-                              const bm3d_stage_params *final_, int32_t *dst, const int32_t *src,
-                              const int32_t *ref, int width, int height, size_t stride,
-                              int floor_, int neutral, int ceil_, int mem, void *stream)
-{
-    const void *d[1] = {dst}, *sp[1] = {src};
-    const bm3d_stage_params *ps[2] = {basic, final_};
-    int rc = check_int_call(ctx, 1, d, sp, width, height, stride, floor_, ceil_, mem, ps, 2);
-    if (rc != BM3D_OK) return rc;
-    if (neutral < floor_ || neutral > ceil_) return BM3D_ERR_INVALID;
-    CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int *dd[1] = {dst};
-    const int *ss[1] = {src};
-    const Quant q{floor_, neutral, ceil_};
-    const int *rr[1] = {ref && ref != src ? ref : nullptr};
-    IntPlanes io;
-    if ((rc = stage_ints_in(ctx, 1, ss, rr, width, height, stride, mem, s, io)) != BM3D_OK)
-        return rc;
-    if ((rc = int_outputs(ctx, 1, dd, width, height, mem, io)) != BM3D_OK) return rc;
-    float *fs[1], *fd[1], *fr[1];
-    if ((rc = conv_planes(ctx, 0, 1, width, height, fs)) != BM3D_OK) return rc;
-    if ((rc = conv_planes(ctx, 2, 1, width, height, fd)) != BM3D_OK) return rc;
-    const dim3 grid = convert_grid(ctx, width, height);
-    const RangeMap in = range_to_float(q);
-    int_to_float_kernel<<<grid, 256, 0, s>>>(io.src[0], io.pitch, fs[0], width, width, height, in);
-    CK(ctx, cudaGetLastError());
-    fr[0] = fs[0];
-    if (io.ref[0]) {
-        if ((rc = conv_planes(ctx, 1, 1, width, height, fr)) != BM3D_OK) return rc;
-        int_to_float_kernel<<<grid, 256, 0, s>>>(io.ref[0], io.pitch, fr[0], width, width, height,
-                                                 in);
-        CK(ctx, cudaGetLastError());
-    }
-    const float *cs[1] = {fs[0]}, *cr[1] = {fr[0]};
-    const int st = full_any<float>(ctx, basic, final_, 1, fd, cs, cr, width, height, width, 1.0,
-                                   BM3D_MEM_DEVICE, stream);
-    if (st < 0) return st;
-    float_to_int_kernel<<<grid, 256, 0, s>>>(fd[0], width, io.dst[0], io.pitch, width, height,
-                                             range_to_int(q));
-    CK(ctx, cudaGetLastError());
-    return finish_ints(ctx, 1, dd, width, height, stride, mem, s, io, st);
-}
-
-extern "C" int bm3d_frame(bm3d_ctx *ctx, const bm3d_stage_params *basic,
-                          const bm3d_stage_params *final_, int32_t *const dst[3],
-                          const int32_t *const src[3], const int32_t *const ref[3], int width,
-                          int height, size_t stride, int floor_, int ceil_, int mem,
-                          void *stream)
-{
-    if (!dst || !src) return BM3D_ERR_INVALID;
-    const void *d[3] = {dst[0], dst[1], dst[2]}, *sp[3] = {src[0], src[1], src[2]};
-    const bm3d_stage_params *ps[2] = {basic, final_};
-    int rc = check_int_call(ctx, 3, d, sp, width, height, stride, floor_, ceil_, mem, ps, 2);
-    if (rc != BM3D_OK) return rc;
-    if (ref && (!ref[0] || !ref[1] || !ref[2])) return BM3D_ERR_INVALID;
-    CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // a distinct ref frame (the reference compares the three plane pointers)
-    const bool own_ref = ref && !(ref[0] == src[0] && ref[1] == src[1] && ref[2] == src[2]);
-    IntPlanes io;
-    if ((rc = stage_ints_in(ctx, 3, src, own_ref ? ref : nullptr, width, height, stride, mem, s,
-                            io)) != BM3D_OK)
-        return rc;
-    if ((rc = int_outputs(ctx, 3, dst, width, height, mem, io)) != BM3D_OK) return rc;
-    float *fs[3], *fd[3], *fr[1];
-    if ((rc = conv_planes(ctx, 0, 3, width, height, fs)) != BM3D_OK) return rc;
-    if ((rc = conv_planes(ctx, 2, 3, width, height, fd)) != BM3D_OK) return rc;
-    const dim3 grid = convert_grid(ctx, width, height);
-    rgb_to_opp_kernel<<<grid, 256, 0, s>>>(io.src[0], io.src[1], io.src[2], io.pitch, fs[0], fs[1],
-                                           fs[2], width, width, height, opp_forward(floor_, ceil_),
-                                           0);
-    CK(ctx, cudaGetLastError());
-    fr[0] = fs[0];
-    if (own_ref) {  // only Y of ref (BM3D_Basic::RGB2YUV, source/BM3D.cpp:333)
-        if ((rc = conv_planes(ctx, 1, 1, width, height, fr)) != BM3D_OK) return rc;
-        rgb_to_opp_kernel<<<grid, 256, 0, s>>>(io.ref[0], io.ref[1], io.ref[2], io.pitch, fr[0],
-                                               fr[0], fr[0], width, width, height,
-                                               opp_forward(floor_, ceil_), 1);
-        CK(ctx, cudaGetLastError());
-    }
-    const float *cs[3] = {fs[0], fs[1], fs[2]}, *cr[3] = {fr[0], fs[1], fs[2]};
-    const int st = full_any<float>(ctx, basic, final_, 3, fd, cs, cr, width, height, width, 1.0,
-                                   BM3D_MEM_DEVICE, stream);
-    if (st < 0) return st;
-    opp_to_rgb_kernel<<<grid, 256, 0, s>>>(fd[0], fd[1], fd[2], width, io.dst[0], io.dst[1],
-                                           io.dst[2], io.pitch, width, height,
-                                           opp_inverse(floor_, ceil_));
-    CK(ctx, cudaGetLastError());
-    return finish_ints(ctx, 3, dst, width, height, stride, mem, s, io, st);
-}
-
-extern "C" int bm3d_stage_frame(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener,
-                                int32_t *const dst[3], const int32_t *const src[3],
-                                const int32_t *const ref[3], int width, int height, size_t stride,
-                                int floor_, int ceil_, int mem, void *stream)
-{
-    if (!dst || !src) return BM3D_ERR_INVALID;
-    const void *d[3] = {dst[0], dst[1], dst[2]}, *sp[3] = {src[0], src[1], src[2]};
-    const bm3d_stage_params *ps[1] = {params};
-    int rc = check_int_call(ctx, 3, d, sp, width, height, stride, floor_, ceil_, mem, ps, 1);
-    if (rc != BM3D_OK) return rc;
-    if (ref && (!ref[0] || !ref[1] || !ref[2])) return BM3D_ERR_INVALID;
-    CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (int_path_rejected(params, 3)) return copy_ints(ctx, 3, dst, src, width, height, stride, mem, s);
-    // a distinct ref frame (the reference compares the three plane pointers)
-    const bool own_ref = ref && !(ref[0] == src[0] && ref[1] == src[1] && ref[2] == src[2]);
-    IntPlanes io;
-    if ((rc = stage_ints_in(ctx, 3, src, own_ref ? ref : nullptr, width, height, stride, mem, s,
-                            io)) != BM3D_OK)
-        return rc;
-    if ((rc = int_outputs(ctx, 3, dst, width, height, mem, io)) != BM3D_OK) return rc;
-    float *fs[3], *fr[3];
-    if ((rc = conv_planes(ctx, 0, 3, width, height, fs)) != BM3D_OK) return rc;
-    const dim3 grid = convert_grid(ctx, width, height);
-    rgb_to_opp_kernel<<<grid, 256, 0, s>>>(io.src[0], io.src[1], io.src[2], io.pitch, fs[0], fs[1],
-                                           fs[2], width, width, height, opp_forward(floor_, ceil_),
-                                           0);
-    CK(ctx, cudaGetLastError());
-    for (int c = 0; c < 3; ++c) fr[c] = fs[c];
-    if (own_ref) {
-        if ((rc = conv_planes(ctx, 1, wiener ? 3 : 1, width, height, fr)) != BM3D_OK) return rc;
-        if (!wiener) fr[1] = fr[2] = fr[0];  // the basic stage reads only Y of ref
-        rgb_to_opp_kernel<<<grid, 256, 0, s>>>(io.ref[0], io.ref[1], io.ref[2], io.pitch, fr[0],
-                                               fr[1], fr[2], width, width, height,
-                                               opp_forward(floor_, ceil_), wiener ? 0 : 1);
-        CK(ctx, cudaGetLastError());
-    }
-    // in place on the YUV source, as the reference (planes a stage leaves
-    // alone keep their converted values)
-    const float *cs[3] = {fs[0], fs[1], fs[2]}, *cr[3] = {fr[0], fr[1], fr[2]};
-    const int st = stage_any<float>(ctx, params, wiener, 3, fs, cs, cr, width, height, width, 1.0,
-                                    BM3D_MEM_DEVICE, stream);
-    if (st < 0) return st;
-    opp_to_rgb_kernel<<<grid, 256, 0, s>>>(fs[0], fs[1], fs[2], width, io.dst[0], io.dst[1],
-                                           io.dst[2], io.pitch, width, height,
-                                           opp_inverse(floor_, ceil_));
-    CK(ctx, cudaGetLastError());
-    return finish_ints(ctx, 3, dst, width, height, stride, mem, s, io, st);
-}
-
-// ---------------------------------------------------------------------------
-// Many host planes, copies overlapped with the filtering.
-
-extern "C" int bm3d_full_many(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
-                              const bm3d_stage_params *final_, float *const dst[],
-                              const float *const src[], const int width[], const int height[],
-                              const size_t stride[], float value_range, int async, void *stream)
-{
-    if (!ctx || count < 0 || (count > 0 && (!basic || !final_ || !dst || !src || !width ||
-                                            !height || !stride)))
-        return BM3D_ERR_INVALID;
-    for (int i = 0; i < count; ++i)
-        if (!dst[i] || !src[i] || width[i] < 1 || height[i] < 1 ||
-            stride[i] < static_cast<size_t>(width[i]))
-            return BM3D_ERR_INVALID;
-    CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (!ctx->up) {
-        CK(ctx, cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking));
-        CK(ctx, cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking));
-        for (auto &sl : ctx->pipe) {
-            CK(ctx, cudaEventCreateWithFlags(&sl.in_ready, cudaEventDisableTiming));
-            CK(ctx, cudaEventCreateWithFlags(&sl.computed, cudaEventDisableTiming));
-            CK(ctx, cudaEventCreateWithFlags(&sl.drained, cudaEventDisableTiming));
-        }
-    }
-    // Uploads run one plane ahead on `up`, downloads trail on `down`; a slot's
-    // input is reused once its plane has been filtered, its output once it
-    // has been copied out. `stream` does the filtering.
-    int status = BM3D_OK;
-    auto upload = [&](int i) -> int {
-        auto &sl = ctx->pipe[(ctx->pipe_count + i) & 1];
-        const size_t bytes = sizeof(float) * static_cast<size_t>(width[i]) * height[i];
-        if (sl.used) CK(ctx, cudaStreamWaitEvent(ctx->up, sl.computed, 0));
-        if (sl.in.bytes < bytes) {  // growing a buffer: let every use of it finish first
-            if (sl.used) CK(ctx, cudaEventSynchronize(sl.computed));
-            int rc = ensure(ctx, sl.in, bytes);
-            if (rc != BM3D_OK) return rc;
-        }
-        CK(ctx, cudaMemcpy2DAsync(sl.in.ptr, sizeof(float) * width[i], src[i],
-                                  sizeof(float) * stride[i], sizeof(float) * width[i], height[i],
-                                  cudaMemcpyHostToDevice, ctx->up));
-        CK(ctx, cudaEventRecord(sl.in_ready, ctx->up));
-        return BM3D_OK;
-    };
-    if (count > 0) {
-        int rc = upload(0);
-        if (rc != BM3D_OK) return rc;
-    }
-    for (int i = 0; i < count; ++i) {
-        if (i + 1 < count) {
-            int rc = upload(i + 1);
-            if (rc != BM3D_OK) return rc;
-        }
-        auto &sl = ctx->pipe[(ctx->pipe_count + i) & 1];
-        const size_t bytes = sizeof(float) * static_cast<size_t>(width[i]) * height[i];
-        if (sl.used) CK(ctx, cudaStreamWaitEvent(s, sl.drained, 0));
-        if (sl.out.bytes < bytes) {
-            if (sl.used) CK(ctx, cudaEventSynchronize(sl.drained));
-            int rc = ensure(ctx, sl.out, bytes);
-            if (rc != BM3D_OK) return rc;
-        }
-        CK(ctx, cudaStreamWaitEvent(s, sl.in_ready, 0));
-        float *d[1] = {static_cast<float *>(sl.out.ptr)};
-        const float *x[1] = {static_cast<const float *>(sl.in.ptr)};
-        const int rc = full_any<float>(ctx, &basic[i], &final_[i], 1, d, x, nullptr, width[i],
-                                       height[i], static_cast<size_t>(width[i]), value_range,
-                                       BM3D_MEM_DEVICE, s);
-        if (rc < 0) return rc;
-        if (rc == BM3D_COPIED) status = BM3D_COPIED;
-        CK(ctx, cudaEventRecord(sl.computed, s));
-        CK(ctx, cudaStreamWaitEvent(ctx->down, sl.computed, 0));
-        CK(ctx, cudaMemcpy2DAsync(dst[i], sizeof(float) * stride[i], sl.out.ptr,
-                                  sizeof(float) * width[i], sizeof(float) * width[i], height[i],
-                                  cudaMemcpyDeviceToHost, ctx->down));
-        CK(ctx, cudaEventRecord(sl.drained, ctx->down));
-        sl.used = true;
-    }
-    ctx->pipe_count += static_cast<unsigned long long>(count);
-    if (count > 0) {
-        // `stream` completes after the last download
-        auto &last = ctx->pipe[(ctx->pipe_count - 1) & 1];
-        CK(ctx, cudaStreamWaitEvent(s, last.drained, 0));
-    }
-    if (async) return status;
-    CK(ctx, cudaStreamSynchronize(s));
-    const int rc = check_invariants(ctx);
-    return rc != BM3D_OK ? rc : status;
-}
+// The float drivers the other translation units call.
+template void bm3d::fill_tables<float>(StageArgs<float> &, const bm3d_stage_params *, bool, int,
+                                 double);
+template int bm3d::stage_any<float>(bm3d_ctx *, const bm3d_stage_params *, int, int, float *const[],
+                              const float *const[], const float *const[], int, int, size_t,
+                              double, int, void *);
+template int bm3d::full_any<float>(bm3d_ctx *, const bm3d_stage_params *, const bm3d_stage_params *,
+                             int, float *const[], const float *const[], const float *const[],
+                             int, int, size_t, double, int, void *);
 
 extern "C" int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *p, int wiener,
                                  const float *ref, int width, int height, size_t stride,
@@ -1655,653 +1087,3 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     return BM3D_OK;
 }
 
-// ---------------------------------------------------------------------------
-// Batches: bm3d_batch_create / bm3d_batch_run / bm3d_batch_destroy.
-
-namespace {
-
-struct StageBuild {
-    int tile_x = 0, tile_y = 0, warps = 0;
-    bool generic = false;
-    int nact = 0;            // planes with work in this stage
-    int total_tiles = 0;
-    size_t smem = 0;         // dynamic shared memory of the persistent launch
-    int grid = 0;
-    DevBuf args, base;       // device StageArgs[nact], int[nact + 1]
-};
-
-}  // namespace
-
-struct bm3d_batch {
-    bm3d_ctx *ctx = nullptr;
-    int n = 0;    // images
-    int npl = 1;  // planes per image (1, or 3 sharing the luma groups)
-    std::vector<int> w, h;
-    std::vector<size_t> stride;
-    std::vector<const float *> src;  // plane c of image i at [i * npl + c]
-    std::vector<float *> dst;
-    std::vector<bm3d_stage_params> pb, pf;
-    std::vector<Guard> gb, gf;
-    std::vector<size_t> acc_off, basic_off;  // per plane: offsets into acc (int64) and basic (float)
-    DevBuf acc, basic, absmax, counters, planes_b, planes_f;
-    int nq_b = 0, nq_f = 0;  // entries of planes_b / planes_f (planes each stage filters)
-    StageBuild sb, sf;
-    cudaStream_t cap = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-};
-
-namespace {
-
-int batch_fail(bm3d_ctx *ctx, const char *msg)
-{
-    ctx->err = msg;
-    return BM3D_ERR_INVALID;
-}
-
-// Per-plane stage arguments of one stage at one tiling; uploads them and sizes
-// the persistent launch. Returns BM3D_ERR_UNSUPPORTED when the tiling does
-// not fit in shared memory.
-int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuild &out)
-{
-    bm3d_ctx *ctx = B->ctx;
-    std::vector<StageArgs<float>> args;
-    std::vector<int> base(1, 0);
-    size_t smem = 0;
-    bool generic = false;
-    for (int i = 0; i < B->n; ++i) {
-        const bm3d_stage_params *p = wiener ? &B->pf[i] : &B->pb[i];
-        if ((wiener ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
-        StageArgs<float> a;
-        std::memset(&a, 0, sizeof(a));
-        const int npl = B->npl;
-        fill_tables(a, p, wiener, npl, 1.0);
-        generic = !fast_args(p->block_size, p->group_size);
-        const int BS = p->block_size;
-        a.width = B->w[i];
-        a.height = B->h[i];
-        a.block_size = BS;
-        a.step = p->block_step;
-        a.group_size = p->group_size;
-        a.bm_step = p->bm_step;
-        a.range = p->bm_range / p->bm_step * p->bm_step;
-        a.nx = ref_count(a.width - BS, a.step);
-        a.ny = ref_count(a.height - BS, a.step);
-        const int span = 2 * (a.range / a.bm_step) + 1;
-        a.key_slots = span * span + 1;
-        const int reach = a.match ? a.range : 0;
-        a.region_w = std::min(a.width, (tx - 1) * a.step + 2 * reach + BS);
-        a.region_h = std::min(a.height, (ty - 1) * a.step + 2 * reach + BS);
-        a.region_pitch = a.region_w + ((5 - a.region_w % 8) + 8) % 8;
-        a.tile_x = std::min(tx, a.nx);
-        a.tile_y = std::min(ty, a.ny);
-        a.tiles_x = (a.nx + a.tile_x - 1) / a.tile_x;
-        a.stride = static_cast<long long>(B->stride[i]);
-        a.ref_alias_src = wiener ? 0 : (1 << npl) - 1;
-        for (int c = 0; c < npl; ++c) {
-            const int k = i * npl + c;
-            a.src[c] = B->src[k];
-            a.ref[c] = wiener ? static_cast<const float *>(B->basic.ptr) + B->basic_off[k]
-                              : B->src[k];
-            a.num[c] = static_cast<long long *>(B->acc.ptr) + B->acc_off[k];
-            a.den[c] = a.num[c] + static_cast<size_t>(a.width) * a.height;
-        }
-        a.absmax = static_cast<float *>(B->absmax.ptr) + i * npl;
-        const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, p->group_size);
-        a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
-        a.dct_fwd = ctx->gtab_f;
-        a.dct_inv = ctx->gtab_f ? ctx->gtab_f + kDctTableSize : nullptr;
-        const SmemPlan sp = plan_smem<float>(npl, wiener, a.ref_alias_src, a.region_h,
-                                             a.region_pitch, a.key_slots, warps, generic, BS,
-                                             p->group_size, a.tile_x * a.tile_y);
-        smem = std::max(smem, sp.total + kBatchHeader);
-        args.push_back(a);
-        base.push_back(base.back() + a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y));
-    }
-    if (smem > ctx->smem_optin) return BM3D_ERR_UNSUPPORTED;
-    out.tile_x = tx;
-    out.tile_y = ty;
-    out.warps = warps;
-    out.generic = generic;
-    out.nact = static_cast<int>(args.size());
-    out.total_tiles = base.back();
-    out.smem = smem;
-    int rc;
-    if (out.nact > 0) {
-        if ((rc = ensure(ctx, out.args, sizeof(StageArgs<float>) * args.size())) != BM3D_OK) return rc;
-        if ((rc = ensure(ctx, out.base, sizeof(int) * base.size())) != BM3D_OK) return rc;
-        CK(ctx, cudaMemcpy(out.args.ptr, args.data(), sizeof(StageArgs<float>) * args.size(),
-                           cudaMemcpyHostToDevice));
-        CK(ctx, cudaMemcpy(out.base.ptr, base.data(), sizeof(int) * base.size(),
-                           cudaMemcpyHostToDevice));
-    }
-    return BM3D_OK;
-}
-
-template <bool W>
-int launch_batch_stage(bm3d_batch *B, StageBuild &sbd, int *counter, cudaStream_t s)
-{
-    bm3d_ctx *ctx = B->ctx;
-    if (sbd.nact == 0) return BM3D_OK;
-    CK(ctx, cudaMemsetAsync(counter, 0, sizeof(int), s));
-    const auto *args = static_cast<const StageArgs<float> *>(sbd.args.ptr);
-    const int *base = static_cast<const int *>(sbd.base.ptr);
-    int nimg = sbd.nact;
-    auto go = [&](const void *kern) -> int {
-        CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(sbd.smem)));
-        int per_sm = 0;
-        CK(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sbd.warps * kWarp,
-                                                              sbd.smem));
-        sbd.grid = std::max(1, per_sm) * ctx->sm_count;
-        void *kargs[] = {&args, &base, &nimg, &counter};
-        CK(ctx, cudaLaunchKernel(kern, dim3(sbd.grid), dim3(sbd.warps * kWarp), kargs, sbd.smem, s));
-        return BM3D_OK;
-    };
-    const bool ks4 = (W ? B->pf[0].bm_step : B->pb[0].bm_step) == 1;
-    if (B->npl == 3) {
-        if (sbd.generic) return go(batch_kernel_fn<W, 3, 1, true>());
-        return go(ks4 ? batch_kernel_fn<W, 3, 4, false>() : batch_kernel_fn<W, 3, 1, false>());
-    }
-    if (sbd.generic) return go(batch_kernel_fn<W, 1, 1, true>());
-    return go(ks4 ? batch_kernel_fn<W, 1, 4, false>() : batch_kernel_fn<W, 1, 1, false>());
-}
-
-int launch_planes(bm3d_batch *B, const DevBuf &planes, bool prep, cudaStream_t s)
-{
-    const int count = &planes == &B->planes_b ? B->nq_b : B->nq_f;
-    if (count == 0) return BM3D_OK;
-    long long maxpx = 0;
-    for (int i = 0; i < B->n; ++i) maxpx = std::max(maxpx, static_cast<long long>(B->w[i]) * B->h[i]);
-    // enough CTAs in all to fill the GPU a few times over, at least 64 per plane
-    const long long tiles = (maxpx + kNormTile * kNormTile - 1) / (kNormTile * kNormTile);
-    const long long cap = std::max<long long>(64, 8LL * B->ctx->sm_count / count);
-    const dim3 grid(static_cast<unsigned>(std::min<long long>(prep ? (maxpx + 255) / 256 : tiles, cap)),
-                    static_cast<unsigned>(count));
-    const auto *q = static_cast<const BatchPlane<float> *>(planes.ptr);
-    if (prep) prep_batch_kernel<float><<<grid, 256, 0, s>>>(q);
-    else normalize_batch_kernel<float><<<grid, 256, 0, s>>>(q);
-    CK(B->ctx, cudaGetLastError());
-    return BM3D_OK;
-}
-
-// The whole pipeline, enqueued on s (captured into the graph).
-int enqueue_batch(bm3d_batch *B, cudaStream_t s)
-{
-    bm3d_ctx *ctx = B->ctx;
-    int rc;
-    int *counters = static_cast<int *>(B->counters.ptr);
-    for (int i = 0; i < B->n; ++i) {  // planes a stage passes through unfiltered
-        for (int c = 0; c < B->npl; ++c) {
-            const int k = i * B->npl + c;
-            float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[k];
-            const bool b_off = B->gb[i] != Guard::Run || !(B->pb[i].sigma[c] > 0 || B->npl == 1);
-            const bool f_off = B->gf[i] != Guard::Run || !(B->pf[i].sigma[c] > 0 || B->npl == 1);
-            if (b_off)
-                CK(ctx, cudaMemcpy2DAsync(bi, B->stride[i] * 4, B->src[k], B->stride[i] * 4,
-                                          B->w[i] * 4, B->h[i], cudaMemcpyDeviceToDevice, s));
-            if (f_off && B->dst[k] != B->src[k])
-                CK(ctx, cudaMemcpy2DAsync(B->dst[k], B->stride[i] * 4, B->src[k], B->stride[i] * 4,
-                                          B->w[i] * 4, B->h[i], cudaMemcpyDeviceToDevice, s));
-        }
-    }
-    CK(ctx, cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * B->n * B->npl, s));
-    if ((rc = launch_planes(B, B->planes_b, true, s)) != BM3D_OK) return rc;
-    if ((rc = launch_batch_stage<false>(B, B->sb, counters, s)) != BM3D_OK) return rc;
-    if ((rc = launch_planes(B, B->planes_b, false, s)) != BM3D_OK) return rc;
-    if ((rc = launch_planes(B, B->planes_f, true, s)) != BM3D_OK) return rc;
-    if ((rc = launch_batch_stage<true>(B, B->sf, counters + 1, s)) != BM3D_OK) return rc;
-    if ((rc = launch_planes(B, B->planes_f, false, s)) != BM3D_OK) return rc;
-    return BM3D_OK;
-}
-
-// Time one stage launch (after a prep) at the current build.
-template <bool W>
-int time_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, cudaStream_t s, float &ms)
-{
-    bm3d_ctx *ctx = B->ctx;
-    int rc;
-    cudaEvent_t e0, e1;
-    CK(ctx, cudaEventCreate(&e0));
-    CK(ctx, cudaEventCreate(&e1));
-    ms = 1e30f;
-    for (int rep = 0; rep < 3; ++rep) {
-        if ((rc = launch_planes(B, planes, true, s)) != BM3D_OK) return rc;
-        CK(ctx, cudaEventRecord(e0, s));
-        if ((rc = launch_batch_stage<W>(B, sbd, static_cast<int *>(B->counters.ptr) + (W ? 1 : 0),
-                                        s)) != BM3D_OK)
-            return rc;
-        CK(ctx, cudaEventRecord(e1, s));
-        CK(ctx, cudaEventSynchronize(e1));
-        float t = 0;
-        CK(ctx, cudaEventElapsedTime(&t, e0, e1));
-        if (rep > 0) ms = std::min(ms, t);  // first run warms up
-    }
-    if (!W) {  // leave the basic estimates in place for the final stage's tuning
-        if ((rc = launch_planes(B, planes, false, s)) != BM3D_OK) return rc;
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    return BM3D_OK;
-}
-
-// Pick the tiling of one stage: the fastest candidate that fits, or the
-// default when not autotuning.
-template <bool W>
-int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotune, cudaStream_t s,
-               const int *force = nullptr)
-{
-    if (force) return build_stage(B, W, force[0], force[1], force[2], sbd);  // a known tiling
-    const bm3d_stage_params &p = W ? B->pf[0] : B->pb[0];
-    const bool generic = !fast_args(p.block_size, p.group_size);
-    static const int fast_cand[][3] = {{8, 8, 16}, {7, 7, 16}, {6, 8, 12}, {8, 6, 12},
-                                       {6, 6, 12}, {4, 4, 4}, {4, 4, 2}, {2, 2, 1}};
-    static const int gen_cand[][3] = {{4, 4, 8}, {4, 4, 4}, {2, 2, 4}, {2, 2, 2}, {1, 1, 2}, {1, 1, 1}};
-    const int (*cand)[3] = generic ? gen_cand : fast_cand;
-    const int ncand = generic ? 6 : 8;
-    int best = -1;
-    float best_ms = 1e30f;
-    for (int c = 0; c < ncand; ++c) {
-        int rc = build_stage(B, W, cand[c][0], cand[c][1], cand[c][2], sbd);
-        if (rc == BM3D_ERR_UNSUPPORTED) continue;
-        if (rc != BM3D_OK) return rc;
-        if (!autotune) {
-            best = c;
-            break;
-        }
-        float ms;
-        if ((rc = time_stage<W>(B, sbd, planes, s, ms)) != BM3D_OK) return rc;
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = c;
-        }
-    }
-    if (best < 0) {
-        B->ctx->err = "batch stage does not fit in shared memory";
-        return BM3D_ERR_UNSUPPORTED;
-    }
-    int rc = build_stage(B, W, cand[best][0], cand[best][1], cand[best][2], sbd);
-    if (rc == BM3D_OK && !W && autotune) {
-        float ms;  // re-run the chosen basic tiling so the final stage tunes on its output
-        rc = time_stage<W>(B, sbd, planes, s, ms);
-    }
-    return rc;
-}
-
-}  // namespace
-
-static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_params *basic,
-                            const bm3d_stage_params *final_, float *const dst[],
-                            const float *const src[], const int width[], const int height[],
-                            const size_t stride[], int autotune, bm3d_batch **out,
-                            const int *force_tiling = nullptr)
-{
-    if (!ctx || !out || count < 1 || !basic || !final_ || !dst || !src || !width || !height ||
-        !stride)
-        return BM3D_ERR_INVALID;
-    *out = nullptr;
-    CK(ctx, cudaSetDevice(ctx->device));
-    auto *B = new bm3d_batch;
-    B->ctx = ctx;
-    B->n = count;
-    B->npl = npl;
-    auto fail = [&](int rc) {
-        bm3d_batch_destroy(B);
-        return rc;
-    };
-    size_t acc_total = 0, basic_total = 0;
-    for (int i = 0; i < count; ++i) {
-        const Guard gb = check_params(&basic[i], npl), gf = check_params(&final_[i], npl);
-        if (gb == Guard::Invalid || gf == Guard::Invalid) return fail(batch_fail(ctx, "invalid parameters"));
-        if (gb == Guard::Unsupported || gf == Guard::Unsupported) {
-            ctx->err = "parameters outside this build (BlockSize <= 16, GroupSize <= 32)";
-            return fail(BM3D_ERR_UNSUPPORTED);
-        }
-        for (const auto *pp : {&basic[i], &final_[i]}) {
-            const auto &q0 = pp == &basic[i] ? basic[0] : final_[0];
-            if (pp->block_size != q0.block_size || pp->block_step != q0.block_step ||
-                pp->group_size != q0.group_size || pp->bm_range != q0.bm_range ||
-                pp->bm_step != q0.bm_step)
-                return fail(batch_fail(ctx, "planes of a batch must share the stage geometry"));
-        }
-        const int bs = std::max(basic[i].block_size, final_[i].block_size);
-        if (width[i] < bs || height[i] < bs || stride[i] < static_cast<size_t>(width[i]))
-            return fail(batch_fail(ctx, "bad plane"));
-        B->w.push_back(width[i]);
-        B->h.push_back(height[i]);
-        B->stride.push_back(stride[i]);
-        B->pb.push_back(basic[i]);
-        B->pf.push_back(final_[i]);
-        B->gb.push_back(gb);
-        B->gf.push_back(gf);
-        for (int c = 0; c < npl; ++c) {
-            const int k = i * npl + c;
-            if (!src[k] || !dst[k]) return fail(batch_fail(ctx, "bad plane"));
-            B->src.push_back(src[k]);
-            B->dst.push_back(dst[k]);
-            B->acc_off.push_back(acc_total);
-            B->basic_off.push_back(basic_total);
-            acc_total += 2 * static_cast<size_t>(width[i]) * height[i];
-            basic_total += stride[i] * height[i];
-        }
-    }
-    int rc;
-    if ((rc = ensure(ctx, B->acc, sizeof(long long) * acc_total)) != BM3D_OK) return fail(rc);
-    if ((rc = ensure(ctx, B->basic, sizeof(float) * basic_total)) != BM3D_OK) return fail(rc);
-    if ((rc = ensure(ctx, B->absmax, sizeof(float) * count * npl)) != BM3D_OK) return fail(rc);
-    if ((rc = ensure(ctx, B->counters, 2 * sizeof(int))) != BM3D_OK) return fail(rc);
-    // per-pixel kernels' plane tables, active planes of each stage in batch order
-    for (int st = 0; st < 2; ++st) {
-        std::vector<BatchPlane<float>> q;
-        for (int i = 0; i < count; ++i) {
-            if ((st ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
-            const bm3d_stage_params &pp = st ? final_[i] : basic[i];
-            for (int c = 0; c < npl; ++c) {
-                if (npl > 1 && !(pp.sigma[c] > 0)) continue;  // plane left alone by the stage
-                const int k = i * npl + c;
-                BatchPlane<float> bp;
-                bp.num = static_cast<long long *>(B->acc.ptr) + B->acc_off[k];
-                bp.den = bp.num + static_cast<size_t>(width[i]) * height[i];
-                bp.src = src[k];
-                bp.dst = st ? dst[k] : static_cast<float *>(B->basic.ptr) + B->basic_off[k];
-                bp.src_stride = static_cast<long long>(stride[i]);
-                bp.dst_stride = static_cast<long long>(stride[i]);
-                bp.width = width[i];
-                bp.height = height[i];
-                bp.block_size = pp.block_size;
-                bp.absmax = static_cast<float *>(B->absmax.ptr) + k;
-                q.push_back(bp);
-            }
-        }
-        DevBuf &dbuf = st ? B->planes_f : B->planes_b;
-        (st ? B->nq_f : B->nq_b) = static_cast<int>(q.size());
-        if (!q.empty()) {
-            if ((rc = ensure(ctx, dbuf, sizeof(BatchPlane<float>) * q.size())) != BM3D_OK) return fail(rc);
-            CK(ctx, cudaMemcpy(dbuf.ptr, q.data(), sizeof(BatchPlane<float>) * q.size(),
-                               cudaMemcpyHostToDevice));
-        }
-    }
-    cudaError_t e = cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaStreamCreate"));
-    // planes whose basic stage is a copy must hold src before the final stage tunes
-    for (int i = 0; i < count; ++i)
-        for (int c = 0; c < npl; ++c) {
-            if (B->gb[i] == Guard::Run && (npl == 1 || basic[i].sigma[c] > 0)) continue;
-            const int k = i * npl + c;
-            float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[k];
-            e = cudaMemcpy2DAsync(bi, stride[i] * 4, src[k], stride[i] * 4, width[i] * 4, height[i],
-                                  cudaMemcpyDeviceToDevice, B->cap);
-            if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemcpy2DAsync"));
-        }
-    e = cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * count * npl, B->cap);
-    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemsetAsync"));
-    if ((rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap,
-                                force_tiling)) != BM3D_OK)
-        return fail(rc);
-    if ((rc = tune_stage<true>(B, B->sf, B->planes_f, autotune != 0, B->cap,
-                               force_tiling ? force_tiling + 3 : nullptr)) != BM3D_OK)
-        return fail(rc);
-    e = cudaStreamSynchronize(B->cap);
-    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "batch tuning"));
-    // capture the pipeline once
-    e = cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal);
-    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaStreamBeginCapture"));
-    rc = enqueue_batch(B, B->cap);
-    cudaGraph_t g = nullptr;
-    e = cudaStreamEndCapture(B->cap, &g);
-    if (rc != BM3D_OK) {
-        if (g) cudaGraphDestroy(g);
-        return fail(rc);
-    }
-    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaStreamEndCapture"));
-    B->graph = g;
-    e = cudaGraphInstantiate(&B->exec, g, 0);
-    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaGraphInstantiate"));
-    *out = B;
-    return BM3D_OK;
-}
-
-extern "C" int bm3d_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
-                                 const bm3d_stage_params *final_, float *const dst[],
-                                 const float *const src[], const int width[], const int height[],
-                                 const size_t stride[], int autotune, bm3d_batch **out)
-{
-    return batch_create_any(ctx, 1, count, basic, final_, dst, src, width, height, stride,
-                            autotune, out);
-}
-
-extern "C" int bm3d_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
-                                  const bm3d_stage_params *final_, float *const dst[],
-                                  const float *const src[], const int width[], const int height[],
-                                  const size_t stride[], int autotune, bm3d_batch **out)
-{
-    return batch_create_any(ctx, 3, count, basic, final_, dst, src, width, height, stride,
-                            autotune, out);
-}
-
-extern "C" int bm3d_batch_run(bm3d_batch *B, void *stream)
-{
-    if (!B || !B->exec) return BM3D_ERR_INVALID;
-    CK(B->ctx, cudaSetDevice(B->ctx->device));
-    CK(B->ctx, cudaGraphLaunch(B->exec, static_cast<cudaStream_t>(stream)));
-    B->ctx->last_stream = static_cast<cudaStream_t>(stream);
-    return BM3D_OK;
-}
-
-extern "C" int bm3d_batch_tuning(const bm3d_batch *B, int out[6])
-{
-    if (!B || !out) return BM3D_ERR_INVALID;
-    out[0] = B->sb.tile_x;
-    out[1] = B->sb.tile_y;
-    out[2] = B->sb.warps;
-    out[3] = B->sf.tile_x;
-    out[4] = B->sf.tile_y;
-    out[5] = B->sf.warps;
-    return BM3D_OK;
-}
-
-extern "C" void bm3d_batch_destroy(bm3d_batch *B)
-{
-    if (!B) return;
-    cudaSetDevice(B->ctx->device);
-    if (B->cap) cudaStreamSynchronize(B->cap);
-    if (B->exec) cudaGraphExecDestroy(B->exec);
-    if (B->graph) cudaGraphDestroy(B->graph);
-    if (B->cap) cudaStreamDestroy(B->cap);
-    for (DevBuf *b : {&B->acc, &B->basic, &B->absmax, &B->counters, &B->planes_b, &B->planes_f,
-                      &B->sb.args, &B->sb.base, &B->sf.args, &B->sf.base})
-        if (b->ptr) cudaFree(b->ptr);
-    delete B;
-}
-
-// ---------------------------------------------------------------------------
-// Batches fed from host memory: two device slots, each with its own batch
-// graph; uploads, filtering and downloads of consecutive runs overlap.
-
-struct bm3d_host_batch {
-    bm3d_ctx *ctx = nullptr;
-    int n = 0;    // images
-    int npl = 1;  // planes per image
-    std::vector<bm3d_stage_params> pb, pf;
-    std::vector<int> w, h;
-    std::vector<size_t> off;  // element offset of each plane (npl per image) in a slot's buffers
-    size_t total = 0;         // floats per slot buffer
-    int autotune = 1;
-    struct Slot {
-        bm3d_batch *batch = nullptr;
-        DevBuf src, dst;
-        cudaEvent_t uploaded = nullptr, filtered = nullptr, drained = nullptr;
-        bool used = false;
-    } slot[2];
-    cudaStream_t up = nullptr, down = nullptr;
-    unsigned long long runs = 0;
-};
-
-extern "C" void bm3d_host_batch_destroy(bm3d_host_batch *H)
-{
-    if (!H) return;
-    cudaSetDevice(H->ctx->device);
-    if (H->up) cudaStreamSynchronize(H->up);
-    if (H->down) cudaStreamSynchronize(H->down);
-    for (auto &sl : H->slot) {
-        if (sl.batch) bm3d_batch_destroy(sl.batch);
-        if (sl.src.ptr) cudaFree(sl.src.ptr);
-        if (sl.dst.ptr) cudaFree(sl.dst.ptr);
-        for (cudaEvent_t e : {sl.uploaded, sl.filtered, sl.drained})
-            if (e) cudaEventDestroy(e);
-    }
-    if (H->up) cudaStreamDestroy(H->up);
-    if (H->down) cudaStreamDestroy(H->down);
-    delete H;
-}
-
-static int host_batch_create_any(bm3d_ctx *ctx, int npl, int count,
-                                 const bm3d_stage_params *basic, const bm3d_stage_params *final_,
-                                 const int width[], const int height[], int autotune,
-                                 bm3d_host_batch **out)
-{
-    if (!ctx || !out || count < 1 || !basic || !final_ || !width || !height)
-        return BM3D_ERR_INVALID;
-    *out = nullptr;
-    CK(ctx, cudaSetDevice(ctx->device));
-    auto *H = new bm3d_host_batch;
-    H->ctx = ctx;
-    H->n = count;
-    H->npl = npl;
-    H->autotune = autotune;
-    auto fail = [&](int rc) {
-        bm3d_host_batch_destroy(H);
-        return rc;
-    };
-    for (int i = 0; i < count; ++i) {
-        if (width[i] < 1 || height[i] < 1) return fail(BM3D_ERR_INVALID);
-        H->pb.push_back(basic[i]);
-        H->pf.push_back(final_[i]);
-        H->w.push_back(width[i]);
-        H->h.push_back(height[i]);
-        for (int c = 0; c < npl; ++c) {
-            H->off.push_back(H->total);
-            H->total += static_cast<size_t>(width[i]) * height[i];
-        }
-    }
-    int rc;
-    for (auto &sl : H->slot) {
-        if ((rc = ensure(ctx, sl.src, sizeof(float) * H->total)) != BM3D_OK) return fail(rc);
-        if ((rc = ensure(ctx, sl.dst, sizeof(float) * H->total)) != BM3D_OK) return fail(rc);
-        cudaError_t e;
-        if ((e = cudaEventCreateWithFlags(&sl.uploaded, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&sl.filtered, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&sl.drained, cudaEventDisableTiming)) != cudaSuccess)
-            return fail(cuda_fail(ctx, e, "cudaEventCreate"));
-    }
-    cudaError_t e;
-    if ((e = cudaStreamCreateWithFlags(&H->up, cudaStreamNonBlocking)) != cudaSuccess ||
-        (e = cudaStreamCreateWithFlags(&H->down, cudaStreamNonBlocking)) != cudaSuccess)
-        return fail(cuda_fail(ctx, e, "cudaStreamCreate"));
-    *out = H;
-    return BM3D_OK;
-}
-
-extern "C" int bm3d_host_batch_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
-                                      const bm3d_stage_params *final_, const int width[],
-                                      const int height[], int autotune, bm3d_host_batch **out)
-{
-    return host_batch_create_any(ctx, 1, count, basic, final_, width, height, autotune, out);
-}
-
-extern "C" int bm3d_host_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
-                                       const bm3d_stage_params *final_, const int width[],
-                                       const int height[], int autotune, bm3d_host_batch **out)
-{
-    return host_batch_create_any(ctx, 3, count, basic, final_, width, height, autotune, out);
-}
-
-// The slot's batch graph over its device buffers; built on the first run that
-// uses the slot, so the autotuner times real data (slot 1 reuses slot 0's
-// tiling).
-static int host_batch_bind(bm3d_host_batch *H, int k)
-{
-    auto &sl = H->slot[k];
-    if (sl.batch) return BM3D_OK;
-    const size_t planes = H->off.size();
-    std::vector<float *> d(planes);
-    std::vector<const float *> x(planes);
-    std::vector<size_t> st(H->n);
-    for (size_t j = 0; j < planes; ++j) {
-        d[j] = static_cast<float *>(sl.dst.ptr) + H->off[j];
-        x[j] = static_cast<const float *>(sl.src.ptr) + H->off[j];
-    }
-    for (int i = 0; i < H->n; ++i) st[i] = static_cast<size_t>(H->w[i]);
-    int tiling[6];
-    const int *force = nullptr;
-    if (k == 1 && H->slot[0].batch) {
-        bm3d_batch_tuning(H->slot[0].batch, tiling);
-        force = tiling;
-    }
-    return batch_create_any(H->ctx, H->npl, H->n, H->pb.data(), H->pf.data(), d.data(), x.data(),
-                            H->w.data(), H->h.data(), st.data(), H->autotune, &sl.batch, force);
-}
-
-extern "C" int bm3d_host_batch_run(bm3d_host_batch *H, float *const dst[],
-                                   const float *const src[], const size_t stride[], int async,
-                                   void *stream)
-{
-    if (!H || !dst || !src || !stride) return BM3D_ERR_INVALID;
-    const int np = H->npl;
-    for (int i = 0; i < H->n; ++i) {
-        if (stride[i] < static_cast<size_t>(H->w[i])) return BM3D_ERR_INVALID;
-        for (int c = 0; c < np; ++c)
-            if (!dst[np * i + c] || !src[np * i + c]) return BM3D_ERR_INVALID;
-    }
-    bm3d_ctx *ctx = H->ctx;
-    CK(ctx, cudaSetDevice(ctx->device));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int k = static_cast<int>(H->runs & 1);
-    auto &sl = H->slot[k];
-    // inputs: once this slot's previous run has been filtered
-    if (sl.used) CK(ctx, cudaStreamWaitEvent(H->up, sl.filtered, 0));
-    for (int j = 0; j < np * H->n; ++j) {
-        const int i = j / np;
-        CK(ctx, cudaMemcpy2DAsync(static_cast<float *>(sl.src.ptr) + H->off[j],
-                                  sizeof(float) * H->w[i], src[j], sizeof(float) * stride[i],
-                                  sizeof(float) * H->w[i], H->h[i], cudaMemcpyHostToDevice, H->up));
-    }
-    CK(ctx, cudaEventRecord(sl.uploaded, H->up));
-    if (!sl.batch) {  // first use: build (and tune) the slot's graph on these inputs
-        CK(ctx, cudaEventSynchronize(sl.uploaded));
-        const int rc = host_batch_bind(H, k);
-        if (rc != BM3D_OK) return rc;
-    }
-    CK(ctx, cudaStreamWaitEvent(s, sl.uploaded, 0));
-    if (sl.used) CK(ctx, cudaStreamWaitEvent(s, sl.drained, 0));  // outputs copied out
-    int rc = bm3d_batch_run(sl.batch, s);
-    if (rc != BM3D_OK) return rc;
-    CK(ctx, cudaEventRecord(sl.filtered, s));
-    CK(ctx, cudaStreamWaitEvent(H->down, sl.filtered, 0));
-    for (int j = 0; j < np * H->n; ++j) {
-        const int i = j / np;
-        CK(ctx, cudaMemcpy2DAsync(dst[j], sizeof(float) * stride[i],
-                                  static_cast<const float *>(sl.dst.ptr) + H->off[j],
-                                  sizeof(float) * H->w[i], sizeof(float) * H->w[i], H->h[i],
-                                  cudaMemcpyDeviceToHost, H->down));
-    }
-    CK(ctx, cudaEventRecord(sl.drained, H->down));
-    sl.used = true;
-    ++H->runs;
-    if (async == 2) return BM3D_OK;  // the caller joins later (bm3d_host_batch_join)
-    CK(ctx, cudaStreamWaitEvent(s, sl.drained, 0));  // `stream` completes after the download
-    if (async) return BM3D_OK;
-    CK(ctx, cudaStreamSynchronize(s));
-    return BM3D_OK;
-}
-
-extern "C" int bm3d_host_batch_join(bm3d_host_batch *H, void *stream)
-{
-    if (!H) return BM3D_ERR_INVALID;
-    if (H->runs == 0) return BM3D_OK;
-    CK(H->ctx, cudaSetDevice(H->ctx->device));
-    // downloads run in order on one stream: the last one covers them all
-    CK(H->ctx, cudaStreamWaitEvent(static_cast<cudaStream_t>(stream),
-                                   H->slot[(H->runs - 1) & 1].drained, 0));
-    return BM3D_OK;
-}
