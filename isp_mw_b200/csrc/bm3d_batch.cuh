@@ -35,7 +35,8 @@ __global__ void __launch_bounds__(GENERIC ? 256 : 512, 1)
         }
         const StageArgs<T> &a = args[lo];
         unsigned char *body = smem + kBatchHeader;
-        if constexpr (GENERIC) generic_tile_body<T, WIENER, NPL>(a, it - tile_base[lo], body, avail);
+        if constexpr (GENERIC && NPL == 3) generic_tile_body_seq3<T, WIENER>(a, it - tile_base[lo], body, avail);
+        else if constexpr (GENERIC) generic_tile_body<T, WIENER, NPL>(a, it - tile_base[lo], body, avail);
         else if constexpr (NPL == 3) stage_tile_body_seq3<T, WIENER, KS>(a, it - tile_base[lo], body, avail);
         else stage_tile_body<T, WIENER, NPL, KS>(a, it - tile_base[lo], body, avail);
         __syncthreads();  // every thread has read *item before it is replaced

@@ -431,7 +431,8 @@ static int launch_generic(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int wa
 {
     const void *kern = generic_kernel_fn<T, W, NPL>();
     const SmemPlan sp = plan_smem<T>(NPL, W, a.ref_alias_src, a.region_h, a.region_pitch,
-                                     a.key_slots, warps, true, a.block_size, a.group_size);
+                                     a.key_slots, warps, true, a.block_size, a.group_size,
+                                     a.tile_x * a.tile_y);
     CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(sp.total)));
     const int grid = a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y);

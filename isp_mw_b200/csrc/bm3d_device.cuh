@@ -338,7 +338,7 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
                                               int gs = kGSMax, int tile_refs = 0)
 {
     SmemPlan s;
-    const bool seq3 = nplanes == 3 && !generic;
+    const bool seq3 = nplanes == 3;
     if (seq3) {
         nplanes = 1;
         alias_mask &= 1;
@@ -369,7 +369,8 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
     s.warp_bytes = (s.scratch_bytes + s.refblk_bytes + sizeof(SortKey<T>) * kCand +
                     sizeof(BlockPos) * kGSTab + sizeof(T) * kGSTab + 15) / 16 * 16;
     s.off_groups = (s.off_warps + s.warp_bytes * nwarps + 15) / 16 * 16;
-    s.total = seq3 ? s.off_groups + static_cast<size_t>(tile_refs) * (2 * kGSMax + 1)
+    const int glist = generic ? gs : kGSMax;  // group-list entries per reference block
+    s.total = seq3 ? s.off_groups + static_cast<size_t>(tile_refs) * (2 * glist + 1)
                    : s.off_warps + s.warp_bytes * nwarps;
     if (seq3 && (region_h > 255 || region_pitch > 255)) s.total = ~size_t(0) >> 1;  // too wide
     return s;

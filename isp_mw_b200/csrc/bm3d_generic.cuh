@@ -224,8 +224,11 @@ __device__ __forceinline__ void group_index(int e, int bs, int bsq, int &z, int 
 template <typename T, bool WIENER>
 __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
                                int n, int lane, T *Gs, T *Gr, float scale,
-                               unsigned &n_bad)
+                               unsigned &n_bad, int pt = -1)
 {
+    // p indexes the tile's windows; pt (default p) the plane's threshold /
+    // Wiener tables, which differ when planes share one set of windows
+    if (pt < 0) pt = p;
     const int bs = t.bs, bsq = bs * bs, total = n * bsq;
     const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
     for (int e = lane; e < total; e += kWarp) {
@@ -248,7 +251,7 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     T denW;
     if (!WIENER) {
         // hard threshold (source/BM3D.cpp:361-371) with thr by #zero indices
-        const T *thr = a.thr[p][n - 1];
+        const T *thr = a.thr[pt][n - 1];
         int kept = 0;
         for (int e = lane; e < total; e += kWarp) {
             int z, y, x;
@@ -263,7 +266,7 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         denW = retained < 1 ? T(1) : T(1) / static_cast<T>(retained);
     } else {
         dct3_generic(Gr, n, bs, lane, a.dct_fwd, false);
-        const T s2 = a.wss[p][n - 1];
+        const T s2 = a.wss[pt][n - 1];
         T l2 = T(0);
         for (int e = lane; e < total; e += kWarp) {
             // any one-to-one order works here; the padded layout needs its address
@@ -359,11 +362,100 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
     flush_tile<T, NPL>(a, t);
 }
 
+// Three planes sharing the groups matched on plane 0, one plane at a time
+// through a single plane's windows (as stage_tile_body_seq3): plane 0 matches
+// and keeps each reference block's group list in shared memory, planes 1 and
+// 2 re-stage their windows and filter with those lists.
+template <typename T, bool WIENER>
+__device__ __forceinline__ void generic_tile_body_seq3(const StageArgs<T> &a, int tile,
+                                                       unsigned char *smem, unsigned avail)
+{
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int bs = a.block_size, GS = a.group_size;
+    const int right = a.width - bs, bottom = a.height - bs;
+
+    Tile<T> t;
+    int kx0, kx1, ky0, ky1;
+    tile_window(a, tile, bs, t, kx0, kx1, ky0, ky1);
+    const SmemPlan sp = plan_smem<T>(3, WIENER, a.ref_alias_src, a.region_h, a.region_pitch,
+                                     a.key_slots, nwarps, true, bs, GS, a.tile_x * a.tile_y);
+    if (sp.total > avail) {  // launched with less shared memory than the layout needs
+        smem_shortfall(a);
+        return;
+    }
+    carve_tile<T, WIENER, 1>(a, sp, smem, t);  // every plane goes through windows [0]
+    // group lists: position (y - ry0) << 8 | (x - rx0), or 0xffff for a
+    // (0, 0) block held outside the window; then one count byte per block
+    unsigned short *gpos = reinterpret_cast<unsigned short *>(smem + sp.off_groups);
+    unsigned char *gn = reinterpret_cast<unsigned char *>(gpos + a.tile_x * a.tile_y * GS);
+
+    unsigned char *wbase = smem + sp.off_warps + sp.warp_bytes * warp;
+    const size_t scratch = sp.scratch_bytes;
+    T *Gs = reinterpret_cast<T *>(wbase);
+    T *Gr = Gs + GS * generic_block_stride(bs);
+    SortKey<T> *keys = reinterpret_cast<SortKey<T> *>(wbase);
+    T *refblk = reinterpret_cast<T *>(wbase + scratch);
+    unsigned char *after = wbase + scratch + sp.refblk_bytes;
+    SortKey<T> *heap = reinterpret_cast<SortKey<T> *>(after);
+    BlockPos *list = reinterpret_cast<BlockPos *>(after + sizeof(SortKey<T>) * kCand);
+    T *lkeys = reinterpret_cast<T *>(after + sizeof(SortKey<T>) * kCand + sizeof(BlockPos) * kGSTab);
+
+    // per-tile counters (small: 32 bits suffice), flushed once per tile
+    unsigned n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
+    const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
+    for (int c = 0; c < 3; ++c) {
+        const bool filt = !a.bm_only && (a.active & (1 << c));
+        if (c > 0 && !filt) continue;
+        stage_plane<T, WIENER>(a, t, c);
+        const float scale = fixed_scale(a.absmax[c], a.log2_bound);
+        for (int r = warp; r < nrefs; r += nwarps) {
+            int n;
+            if (c == 0) {
+                const int ky = ky0 + r / tw, kx = kx0 + r % tw;
+                const int j0 = ref_pos(ky, a.step, bottom), i0 = ref_pos(kx, a.step, right);
+                n = (bs == kBS && a.bm_step == 1)
+                        ? match_block<T, 4>(a, t, j0, i0, lane, keys, heap, list, lkeys, n_cand,
+                                            n_fix)
+                        : match_generic<T>(a, t, j0, i0, lane, keys, refblk, heap, list, lkeys,
+                                           n_cand, n_fix);
+                n_sum += n;
+                n_sq += static_cast<unsigned>(n * n);
+                dump_group(a, ky, kx, n, lane, list, lkeys);
+                if (lane == 0) gn[r] = static_cast<unsigned char>(n);
+                for (int k = lane; k < n; k += kWarp) {
+                    const BlockPos q = list[k];
+                    const bool outside = q.y == 0 && q.x == 0 && !t.origin_inside;
+                    gpos[r * GS + k] = outside ? 0xffff
+                                               : static_cast<unsigned short>(
+                                                     ((q.y - t.ry0) << 8) | (q.x - t.rx0));
+                }
+            } else {
+                n = gn[r];
+                for (int k = lane; k < n; k += kWarp) {
+                    const unsigned v = gpos[r * GS + k];
+                    list[k] = v == 0xffffu ? BlockPos{0, 0}
+                                           : BlockPos{t.ry0 + static_cast<int>(v >> 8),
+                                                      t.rx0 + static_cast<int>(v & 0xffu)};
+                }
+            }
+            __syncwarp();
+            if (filt) filter_generic<T, WIENER>(a, t, 0, list, n, lane, Gs, Gr, scale, n_bad, c);
+            __syncwarp();
+        }
+        __syncthreads();
+        if (filt) flush_plane<T>(a, t, c);
+        __syncthreads();  // the windows are re-staged for the next plane
+    }
+    flush_stats(a, lane, n_sum, n_sq, n_cand, n_fix, n_bad);
+}
+
 template <typename T, bool WIENER, int NPL>
 __global__ void __launch_bounds__(256, 1) generic_stage_kernel(const StageArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    generic_tile_body<T, WIENER, NPL>(a, blockIdx.x, smem, dynamic_smem_bytes());
+    if constexpr (NPL == 3) generic_tile_body_seq3<T, WIENER>(a, blockIdx.x, smem, dynamic_smem_bytes());
+    else generic_tile_body<T, WIENER, NPL>(a, blockIdx.x, smem, dynamic_smem_bytes());
 }
 
 }  // namespace bm3d
