@@ -60,24 +60,35 @@ def main():
 
 
 def time_stages(args):
-    """Basic then final of the chosen profile on one seeded plane, each timed
-    over `--launches` launches after `--warmup`."""
+    """Basic then final of the chosen profile on one seeded plane (or, with
+    `--planes 3`, three Y/U/V planes at sigma 15/10/10 sharing luma groups),
+    each timed over `--launches` launches after `--warmup`."""
     import json
     import torch
     import isp_mw_b200
     from isp_mw_b200 import synth
 
-    _, noisy = synth.pair(args.height, args.width, args.sigma, 2024)
-    sp = [synth.sigma_param(args.sigma)] * 3
+    ctx = isp_mw_b200.Context(0)
+    if args.planes == 3:
+        sig = (15.0, 10.0, 10.0)
+        src = [torch.from_numpy(synth.pair(args.height, args.width, s, 50 + c)[1]).cuda()
+               for c, s in enumerate(sig)]
+        sp = [synth.sigma_param(s, c) for c, s in enumerate(sig)]
+        basic = [torch.empty_like(p) for p in src]
+        out = [torch.empty_like(p) for p in src]
+        stage = ctx.stage3
+    else:
+        _, noisy = synth.pair(args.height, args.width, args.sigma, 2024)
+        sp = [synth.sigma_param(args.sigma)] * 3
+        src = torch.from_numpy(noisy).cuda()
+        basic = torch.empty_like(src)
+        out = torch.empty_like(src)
+        stage = ctx.stage
     b = isp_mw_b200.stage_params_default(args.profile, False, sp)
     f = isp_mw_b200.stage_params_default(args.profile, True, sp)
-    ctx = isp_mw_b200.Context(0)
-    src = torch.from_numpy(noisy).cuda()
-    basic = torch.empty_like(src)
-    out = torch.empty_like(src)
     ms = {}
-    for name, run in (("basic", lambda: ctx.stage(b, False, basic, src)),
-                      ("final", lambda: ctx.stage(f, True, out, src, basic))):
+    for name, run in (("basic", lambda: stage(b, False, basic, src)),
+                      ("final", lambda: stage(f, True, out, src, basic))):
         for _ in range(args.warmup):
             run()
         torch.cuda.synchronize()
@@ -91,7 +102,9 @@ def time_stages(args):
     ctx.close()
     mp = args.width * args.height / 1e6
     print(json.dumps({"profile": args.profile, "plane": f"{args.width}x{args.height}",
-                      "sigma_255": args.sigma, "basic_ms": round(ms["basic"], 4),
+                      "planes": args.planes,
+                      "sigma_255": [15.0, 10.0, 10.0] if args.planes == 3 else args.sigma,
+                      "basic_ms": round(ms["basic"], 4),
                       "final_ms": round(ms["final"], 4),
                       "mp_per_s": round(mp / ((ms["basic"] + ms["final"]) / 1e3), 1)}))
 
