@@ -221,6 +221,17 @@ int bm3d_debug_groups(bm3d_ctx *ctx, const bm3d_stage_params *params, int wiener
  * placement. Synchronises the context's last stream. */
 int bm3d_last_stats(bm3d_ctx *ctx, unsigned long long out[4]);
 
+/* Device-memory calls return once their work is enqueued, so the kernels'
+ * internal consistency counter (group blocks found outside their tile's
+ * staged window, tiles launched with less shared memory than their layout
+ * needs; both skipped, never touched) is checked only by host-memory calls.
+ * bm3d_check waits for the context's last stream and returns BM3D_ERR_CUDA,
+ * with the counts in bm3d_last_error, if the counter has moved since the
+ * context was made; BM3D_OK otherwise. It covers the stage and combined
+ * entries (batches keep no counter). No counterpart in the reference, which
+ * has no asynchronous calls. */
+int bm3d_check(bm3d_ctx *ctx);
+
 /* One stage on one plane of DEVICE memory, like bm3d_stage with
  * BM3D_MEM_DEVICE, but without a context and without allocating anything:
  * no cudaMalloc / cudaFree / allocating library routine is called. It is for

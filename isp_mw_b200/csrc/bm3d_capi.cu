@@ -940,6 +940,14 @@ extern "C" int bm3d_last_stats(bm3d_ctx *ctx, unsigned long long out[4])
     return BM3D_OK;
 }
 
+extern "C" int bm3d_check(bm3d_ctx *ctx)
+{
+    if (!ctx) return BM3D_ERR_INVALID;
+    CK(ctx, cudaSetDevice(ctx->device));
+    CK(ctx, cudaStreamSynchronize(ctx->last_stream));
+    return check_invariants(ctx);
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free stage: bm3d_stage_noalloc.
 //

@@ -231,6 +231,7 @@ def test_device_mode_matches_host_mode(ctx):
     got = dst.cpu().numpy()
     assert np.abs(got - host).max() <= 1e-5
     assert torch.all(dst_big[:, 333:] == -7.0)
+    ctx.check()  # bm3d_check: the asynchronous calls' consistency counter stayed 0
 
 
 def test_param_guard_copies_src(ctx):
