@@ -288,6 +288,13 @@ int bm3d_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
                        const float *const src[], const int width[], const int height[],
                        const size_t stride[], int autotune, bm3d_batch **out);
 int bm3d_batch_run(bm3d_batch *batch, void *stream);
+/* Waits for `stream` and returns BM3D_ERR_CUDA (counts in bm3d_last_error of
+ * the batch's context) if the batch kernels' consistency counter has moved
+ * since creation -- group blocks outside their tile's staged window, or tiles
+ * launched with too little shared memory, both skipped -- else BM3D_OK (as
+ * bm3d_check does for the single-call entries). No counterpart in the
+ * reference. */
+int bm3d_batch_check(bm3d_batch *batch, void *stream);
 /* Batches fed from HOST memory: `count` planes (sizes and parameters fixed
  * at creation; device buffers owned by the batch). Each bm3d_host_batch_run
  * uploads src, runs the batch graph on `stream` and downloads dst; the batch

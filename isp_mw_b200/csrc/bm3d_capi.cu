@@ -584,6 +584,7 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
     a.group_key = gkey;
     a.bm_only = bm_only ? 1 : 0;
     a.stats = ctx->stats;
+    a.bad = ctx->stats + 4;
     // per-stage counters; the invariant counter (stats[4]) is sticky
     CK(ctx, cudaMemsetAsync(ctx->stats, 0, 4 * sizeof(unsigned long long), s));
     if ((rc = launch_stage(ctx, a, wiener, nplanes, s, warps)) != BM3D_OK) return rc;
@@ -1078,6 +1079,7 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     a.num[0] = num;
     a.den[0] = den;
     a.stats = stats;
+    a.bad = stats + 4;
 
     const long long npx = static_cast<long long>(width) * height;
     const int threads = 256;

@@ -122,6 +122,7 @@ struct bm3d_batch {
     std::vector<Guard> gb, gf;
     std::vector<size_t> acc_off, basic_off;  // per plane: offsets into acc (int64) and basic (float)
     DevBuf acc, basic, absmax, counters, planes_b, planes_f;
+    DevBuf bad;  // the kernels' consistency counter (bm3d_batch_check)
     int nq_b = 0, nq_f = 0;  // entries of planes_b / planes_f (planes each stage filters)
     StageBuild sb, sf;
     cudaStream_t cap = nullptr;
@@ -152,6 +153,7 @@ int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuil
         if ((wiener ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
         StageArgs<float> a;
         std::memset(&a, 0, sizeof(a));
+        a.bad = static_cast<unsigned long long *>(B->bad.ptr);
         const int npl = B->npl;
         fill_tables(a, p, wiener, npl, 1.0);
         generic = !fast_args(p->block_size, p->group_size);
@@ -428,6 +430,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
     if ((rc = ensure(ctx, B->basic, sizeof(float) * basic_total)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->absmax, sizeof(float) * count * npl)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->counters, 2 * sizeof(int))) != BM3D_OK) return fail(rc);
+    if ((rc = ensure(ctx, B->bad, sizeof(unsigned long long))) != BM3D_OK) return fail(rc);
+    CK(ctx, cudaMemset(B->bad.ptr, 0, sizeof(unsigned long long)));
     // per-pixel kernels' plane tables, active planes of each stage in batch order
     for (int st = 0; st < 2; ++st) {
         std::vector<BatchPlane<float>> q;
@@ -526,6 +530,23 @@ extern "C" int bm3d_batch_run(bm3d_batch *B, void *stream)
     return BM3D_OK;
 }
 
+extern "C" int bm3d_batch_check(bm3d_batch *B, void *stream)
+{
+    if (!B) return BM3D_ERR_INVALID;
+    bm3d_ctx *ctx = B->ctx;
+    CK(ctx, cudaSetDevice(ctx->device));
+    CK(ctx, cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    unsigned long long v = 0;
+    CK(ctx, cudaMemcpy(&v, B->bad.ptr, sizeof(v), cudaMemcpyDeviceToHost));
+    if (v != 0) {
+        ctx->err = "internal error: " + std::to_string(v & 0xffffffffull) +
+                   " group blocks outside the staged window, " + std::to_string(v >> 32) +
+                   " tiles launched with too little shared memory";
+        return BM3D_ERR_CUDA;
+    }
+    return BM3D_OK;
+}
+
 extern "C" int bm3d_batch_tuning(const bm3d_batch *B, int out[6])
 {
     if (!B || !out) return BM3D_ERR_INVALID;
@@ -546,7 +567,7 @@ extern "C" void bm3d_batch_destroy(bm3d_batch *B)
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     if (B->cap) cudaStreamDestroy(B->cap);
-    for (DevBuf *b : {&B->acc, &B->basic, &B->absmax, &B->counters, &B->planes_b, &B->planes_f,
+    for (DevBuf *b : {&B->acc, &B->basic, &B->absmax, &B->counters, &B->bad, &B->planes_b, &B->planes_f,
                       &B->sb.args, &B->sb.base, &B->sf.args, &B->sf.base})
         if (b->ptr) cudaFree(b->ptr);
     delete B;

@@ -284,8 +284,11 @@ template <typename T> struct StageArgs {
     int *group_count;           // per reference block: group size        (may be null)
     int *group_pos;             // per reference block: kGSTab x (y, x)   (may be null)
     T *group_key;               // per reference block: kGSTab keys       (may be null)
-    unsigned long long *stats;  // [0] sum n, [1] sum n^2, [2] candidates, [3] tie fix-ups,
-                                // [4] group members outside the staged window (must be 0)
+    unsigned long long *stats;  // [0] sum n, [1] sum n^2, [2] candidates, [3] tie fix-ups
+                                // (may be null)
+    unsigned long long *bad;    // consistency counter, must stay 0: low 32 bits group members
+                                // outside the staged window, high 32 bits CTAs launched with
+                                // too little shared memory (may be null)
     int bm_only;                // skip the collaborative filter (group dump)
 };
 

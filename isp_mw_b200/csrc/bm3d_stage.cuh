@@ -965,7 +965,7 @@ __device__ __forceinline__ void dump_group(const StageArgs<T> &a, int ky, int kx
 template <typename T>
 __device__ __forceinline__ void smem_shortfall(const StageArgs<T> &a)
 {
-    if (a.stats != nullptr && threadIdx.x == 0) atomicAdd(a.stats + 4, 1ull << 32);
+    if (a.bad != nullptr && threadIdx.x == 0) atomicAdd(a.bad, 1ull << 32);
 }
 
 template <typename T>
@@ -980,7 +980,7 @@ __device__ __forceinline__ void flush_stats(const StageArgs<T> &a, int lane, uns
         atomicAdd(a.stats + 2, static_cast<U>(n_cand));
         atomicAdd(a.stats + 3, static_cast<U>(n_fix));
     }
-    if (a.stats != nullptr && n_bad) atomicAdd(a.stats + 4, static_cast<U>(n_bad));
+    if (a.bad != nullptr && n_bad) atomicAdd(a.bad, static_cast<U>(n_bad));
 }
 
 // ---------------------------------------------------------------------------

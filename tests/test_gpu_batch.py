@@ -41,6 +41,7 @@ def test_batch_equals_per_plane(bm3d_lib, autotune):
         for k, (d, r) in enumerate(zip(dsts, want)):
             assert torch.equal(d, r), k
     assert torch.equal(dsts[2], srcs[2])
+    batch.check()  # bm3d_batch_check: the kernels' consistency counter stayed 0
     t = batch.tuning()
     assert all(v > 0 for v in t["basic"] + t["final"])
     batch.close()
