@@ -22,7 +22,9 @@ MIN_PSNR = 60.0
 GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
 INT_GOLDEN = [p for p in GOLDEN if os.path.basename(p).startswith("int_")]
 GOLDEN = [p for p in GOLDEN if p not in INT_GOLDEN]  # float planes
-REPORT = os.path.join(ROOT, "gpurun_out", "parity_report.jsonl")
+# one JSON line per comparison; PARITY_REPORT chooses the file
+REPORT = os.environ.get("PARITY_REPORT",
+                        os.path.join(ROOT, "tests", "_build", "parity_report.jsonl"))
 
 
 def report(**kw):
