@@ -85,7 +85,9 @@ typedef struct bm3d_ctx bm3d_ctx;
 int bm3d_ctx_create(bm3d_ctx **out, int device);
 void bm3d_ctx_destroy(bm3d_ctx *ctx);
 
-/* Last error message of this context (or of the last failed create), never NULL. */
+/* Last error message of this context; with ctx == NULL, of this thread's last
+ * failed bm3d_ctx_create or context-free call (bm3d_stage_noalloc,
+ * bm3d_noalloc_check). Never NULL. */
 const char *bm3d_last_error(const bm3d_ctx *ctx);
 
 /* One BM3D stage on one plane: dst = stage(src, ref).
@@ -254,10 +256,24 @@ int bm3d_check(bm3d_ctx *ctx);
  * waiting. All calls share the one scratch array and every call clears the
  * parts it needs before use, but two calls whose work overlaps on the GPU
  * (e.g. on two streams of the same device) race on it: serialise them.
- * Returns the status codes of bm3d_stage, plus BM3D_ERR_TOO_LARGE. */
+ * Returns the status codes of bm3d_stage, plus BM3D_ERR_TOO_LARGE; the
+ * message of a failed call is bm3d_last_error(NULL) on the calling thread.
+ * Like a device-memory bm3d_stage, the call returns before the kernels run,
+ * so their consistency counter is read by bm3d_noalloc_check. */
 int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, float *dst, const float *src,
                        const float *ref, int width, int height, size_t stride, float value_range,
                        void *stream);
+
+/* The consistency check of bm3d_stage_noalloc (as bm3d_check is for a
+ * context): waits for `stream`, then reads the kernels' consistency counter
+ * of the current device's static scratch -- group blocks found outside their
+ * tile's staged window, tiles launched with less shared memory than their
+ * layout needs, both skipped -- which covers every bm3d_stage_noalloc call on
+ * the device since the library loaded or since the last check. Returns BM3D_OK
+ * if it is zero; otherwise clears it and returns BM3D_ERR_CUDA with the counts
+ * in bm3d_last_error(NULL). Allocates nothing. No counterpart in the
+ * reference. */
+int bm3d_noalloc_check(void *stream);
 
 /* Batched basic + final over `count` device planes of any sizes and noise
  * levels: one persistent launch per stage walks a device work queue of

@@ -38,7 +38,7 @@ EXPORTS = [
     "bm3d_ctx_destroy", "bm3d_last_error", "bm3d_stage", "bm3d_stage3", "bm3d_full",
     "bm3d_full3", "bm3d_stage_f64", "bm3d_ref_block_count", "bm3d_debug_groups",
     "bm3d_last_stats", "bm3d_check", "bm3d_batch_check", "bm3d_set_tiling", "bm3d_set_kernel_timing", "bm3d_kernel_time",
-    "bm3d_stage_noalloc", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
+    "bm3d_stage_noalloc", "bm3d_noalloc_check", "bm3d_batch_create", "bm3d_batch_run", "bm3d_batch_tuning",
     "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
     "bm3d_full_many", "bm3d_batch3_create", "bm3d_host_batch_create", "bm3d_host_batch3_create",
     "bm3d_host_batch_run", "bm3d_host_batch_join", "bm3d_host_batch_destroy",
@@ -122,6 +122,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_set_tiling.argtypes = [vp, ip, ip, ip]
     lib.bm3d_stage_noalloc.argtypes = [sp, ip, vp, vp, vp, ip, ip, ctypes.c_size_t,
                                        ctypes.c_float, vp]
+    lib.bm3d_noalloc_check.argtypes = [vp]
     lib.bm3d_batch_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
                                       ctypes.POINTER(vp)]
     lib.bm3d_batch3_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,

@@ -43,6 +43,20 @@ int bm3d::ensure(bm3d_ctx *ctx, DevBuf &b, size_t bytes)
     return BM3D_OK;
 }
 
+cudaError_t bm3d::raise_smem_limit(const void *kern, size_t bytes)
+{
+    static std::mutex mu;  // read-compare-set must not interleave across threads
+    std::lock_guard<std::mutex> lock(mu);
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) return e;
+    if (fa.maxDynamicSharedSizeBytes >= 0 &&
+        static_cast<size_t>(fa.maxDynamicSharedSizeBytes) >= bytes)
+        return cudaSuccess;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(bytes));
+}
+
 #define BM3D_DECLARE_UNIT(name) cudaError_t bm3d_upload_dct_tables_##name(const bm3d::DctTableData &);
 BM3D_KERNEL_UNITS(BM3D_DECLARE_UNIT)
 #undef BM3D_DECLARE_UNIT
@@ -401,8 +415,7 @@ static int launch_one(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int warps)
     const SmemPlan sp =
         plan_smem<T>(NPL, W, a.ref_alias_src, a.region_h, a.region_pitch, a.key_slots, warps,
                      false, kBS, kGSMax, a.tile_x * a.tile_y);
-    CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sp.total)));
+    CK(ctx, raise_smem_limit(kern, sp.total));
     const int grid = a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ctx->timing && !a.bm_only) {
@@ -433,8 +446,7 @@ static int launch_generic(bm3d_ctx *ctx, StageArgs<T> &a, cudaStream_t s, int wa
     const SmemPlan sp = plan_smem<T>(NPL, W, a.ref_alias_src, a.region_h, a.region_pitch,
                                      a.key_slots, warps, true, a.block_size, a.group_size,
                                      a.tile_x * a.tile_y);
-    CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sp.total)));
+    CK(ctx, raise_smem_limit(kern, sp.total));
     const int grid = a.tiles_x * ((a.ny + a.tile_y - 1) / a.tile_y);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (ctx->timing && !a.bm_only) {
@@ -982,10 +994,18 @@ NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
 std::mutex g_noalloc_mu;
 
 // Status for a failed step: CUDA errors map to BM3D_ERR_CUDA, everything else
-// to the given code. (The message names the step for readers of this file.)
-int noalloc_error(const char *, cudaError_t e = cudaSuccess, int code = BM3D_ERR_INVALID)
+// to the given code. The message (with the CUDA error text, if any) becomes
+// this thread's context-free error, which bm3d_last_error(NULL) returns.
+int noalloc_error(const char *what, cudaError_t e = cudaSuccess, int code = BM3D_ERR_INVALID)
 {
-    return e == cudaSuccess ? code : BM3D_ERR_CUDA;
+    if (e != cudaSuccess) {
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s: %s", what, cudaGetErrorString(e));
+        g_create_error = buf;
+        return BM3D_ERR_CUDA;
+    }
+    g_create_error = what;
+    return code;
 }
 
 // Set-up once per device, with that device current: the device address of the
@@ -999,13 +1019,18 @@ int noalloc_setup(int dev, NoAllocDevice **out)
         *out = &d;
         return BM3D_OK;
     }
+    int major = 0, sm = 0, optin = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (e != cudaSuccess) return noalloc_error("cudaDeviceGetAttribute", e);
+    if (major < 10)
+        return noalloc_error("bm3d_stage_noalloc: this build targets sm_100a (B200)",
+                             cudaSuccess, BM3D_ERR_CUDA);
     void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess) return noalloc_error("cudaGetSymbolAddress(g_noalloc_scratch)", e);
     // the cosine tables live in fixed-size host arrays (no heap), uploaded per device
     if ((e = upload_dct_tables()) != cudaSuccess)
         return noalloc_error("cudaMemcpyToSymbol(cosine tables)", e);
-    int sm = 0, optin = 0;
     if ((e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess ||
         (e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) !=
             cudaSuccess)
@@ -1018,6 +1043,15 @@ int noalloc_setup(int dev, NoAllocDevice **out)
     return BM3D_OK;
 }
 
+// Offsets inside the scratch array after the two accumulator planes: the
+// per-call |src| maximum (256 bytes, cleared by every call), then the counters:
+// four statistics (cleared by every call) and the consistency counter, which
+// starts at zero when the library loads and is cleared only by
+// bm3d_noalloc_check, so it covers every call since the last check.
+constexpr size_t kNoAllocAbsmaxOff = 2 * kNoAllocAccBytes;
+constexpr size_t kNoAllocStatsOff = kNoAllocAbsmaxOff + 256;
+constexpr size_t kNoAllocClearBytes = 256 + 4 * sizeof(unsigned long long);
+
 }  // namespace
 
 extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, float *dst,
@@ -1029,12 +1063,15 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     const Guard g = check_params(params, 1);
     if (g == Guard::Invalid) return noalloc_error("bm3d_stage_noalloc: invalid parameters");
     // the register-resident kernel only: BlockSize 8, GroupSize <= 16
-    if (g == Guard::Unsupported || !fast_path(params)) return BM3D_ERR_UNSUPPORTED;
+    if (g == Guard::Unsupported || !fast_path(params))
+        return noalloc_error("bm3d_stage_noalloc: only BlockSize 8 with GroupSize <= 16",
+                             cudaSuccess, BM3D_ERR_UNSUPPORTED);
     if (width < params->block_size || height < params->block_size ||
         stride < static_cast<size_t>(width))
         return noalloc_error("bm3d_stage_noalloc: width/height below BlockSize or stride < width");
     if (static_cast<size_t>(width) * static_cast<size_t>(height) > kNoAllocMaxPixels)
-        return BM3D_ERR_TOO_LARGE;  // larger than the 2,097,152-pixel static scratch
+        return noalloc_error("bm3d_stage_noalloc: plane larger than the 2,097,152-pixel static "
+                             "scratch", cudaSuccess, BM3D_ERR_TOO_LARGE);
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return noalloc_error("cudaGetDevice", e);
@@ -1055,9 +1092,8 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     // The shared scratch: this call's accumulators start from zero below.
     long long *num = reinterpret_cast<long long *>(d->scratch);
     long long *den = reinterpret_cast<long long *>(d->scratch + kNoAllocAccBytes);
-    float *absmax = reinterpret_cast<float *>(d->scratch + 2 * kNoAllocAccBytes);
-    unsigned long long *stats =
-        reinterpret_cast<unsigned long long *>(d->scratch + 2 * kNoAllocAccBytes + 256);
+    float *absmax = reinterpret_cast<float *>(d->scratch + kNoAllocAbsmaxOff);
+    unsigned long long *stats = reinterpret_cast<unsigned long long *>(d->scratch + kNoAllocStatsOff);
 
     StageArgs<float> a;
     std::memset(&a, 0, sizeof(a));
@@ -1072,7 +1108,7 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     info.smem_optin = d->smem_optin;
     int warps;
     rc = plan_geometry(&info, a, params, wiener != 0, 1, width, height, warps);
-    if (rc != BM3D_OK) return rc;
+    if (rc != BM3D_OK) return noalloc_error(info.err.c_str(), cudaSuccess, rc);
     const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, params->group_size);
     a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
     a.absmax = absmax;
@@ -1085,16 +1121,45 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     const int threads = 256;
     const int blocks = static_cast<int>(
         std::min<long long>((npx + threads - 1) / threads, static_cast<long long>(d->sm_count) * 8));
-    if ((e = cudaMemsetAsync(absmax, 0, 256 + 256, s)) != cudaSuccess)
+    // |src| maximum and statistics start at zero; the consistency counter
+    // (stats[4]) is left alone so bm3d_noalloc_check sees every call
+    if ((e = cudaMemsetAsync(absmax, 0, kNoAllocClearBytes, s)) != cudaSuccess)
         return noalloc_error("cudaMemsetAsync(scratch header)", e);
     prep_kernel<float><<<blocks, threads, 0, s>>>(num, den, src, a.stride, width, height, absmax);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("prep_kernel", e);
     rc = launch_stage(&info, a, wiener != 0, 1, s, warps);
-    if (rc != BM3D_OK) return rc;
+    if (rc != BM3D_OK) return noalloc_error(info.err.c_str(), cudaSuccess, rc);
     const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
     normalize_kernel<float><<<ngrid, 256, 0, s>>>(dst, a.stride, num, den, width, height,
                                                   a.block_size);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("normalize_kernel", e);
     return BM3D_OK;
+}
+
+extern "C" int bm3d_noalloc_check(void *stream)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return noalloc_error("cudaGetDevice", e);
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return noalloc_error("bm3d_noalloc_check: device id");
+    NoAllocDevice *d = nullptr;
+    int rc = noalloc_setup(dev, &d);
+    if (rc != BM3D_OK) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess)
+        return noalloc_error("cudaStreamSynchronize", e);
+    unsigned long long *bad =
+        reinterpret_cast<unsigned long long *>(d->scratch + kNoAllocStatsOff) + 4;
+    unsigned long long v = 0;
+    if ((e = cudaMemcpy(&v, bad, sizeof(v), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return noalloc_error("cudaMemcpy(consistency counter)", e);
+    if (v == 0) return BM3D_OK;
+    if ((e = cudaMemset(bad, 0, sizeof(v))) != cudaSuccess)
+        return noalloc_error("cudaMemset(consistency counter)", e);
+    const std::string msg = "internal error: " + std::to_string(v & 0xffffffffull) +
+                            " group blocks outside the staged window, " +
+                            std::to_string(v >> 32) +
+                            " tiles launched with too little shared memory";
+    return noalloc_error(msg.c_str(), cudaSuccess, BM3D_ERR_CUDA);
 }
 

@@ -228,8 +228,7 @@ int launch_batch_stage(bm3d_batch *B, StageBuild &sbd, int *counter, cudaStream_
     const int *base = static_cast<const int *>(sbd.base.ptr);
     int nimg = sbd.nact;
     auto go = [&](const void *kern) -> int {
-        CK(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(sbd.smem)));
+        CK(ctx, raise_smem_limit(kern, sbd.smem));
         int per_sm = 0;
         CK(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sbd.warps * kWarp,
                                                               sbd.smem));

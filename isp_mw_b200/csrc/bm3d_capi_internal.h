@@ -79,6 +79,15 @@ int cuda_fail(bm3d_ctx *ctx, cudaError_t e, const char *what);
 // Grow a context buffer to at least `bytes`.
 int ensure(bm3d_ctx *ctx, DevBuf &b, size_t bytes);
 
+// Raise a kernel's dynamic shared memory limit to at least `bytes`; never
+// lower it. The limit belongs to the kernel function and is shared by every
+// context, batch and captured graph in the process: a graph node captured at
+// a larger size must stay launchable after a later call (another batch's
+// autotuning, a smaller tile) asks for less. A profiler that re-launches a
+// graph node on its own checks the node's size against the function's
+// current limit.
+cudaError_t raise_smem_limit(const void *kern, size_t bytes);
+
 template <typename T>
 inline int copy_plane(bm3d_ctx *ctx, T *dst, size_t dpitch, const T *src, size_t spitch, int w,
                       int h, cudaMemcpyKind kind, cudaStream_t s)

@@ -25,7 +25,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 BUILD_DIR = os.path.join(HERE, "_build")
-REFERENCE_TREE = "/root/reference"
+# where the reference checkout lives (read-only; only oracle/Makefile compiles from it)
+REFERENCE_TREE = os.environ.get("ISP_MW_REFERENCE", "/root/reference")
 
 
 class StageParams(ctypes.Structure):
@@ -74,7 +75,7 @@ def build(reference: bool = True) -> None:
     targets = ["port"]
     if reference and os.path.isdir(REFERENCE_TREE):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_TREE}"] + targets, check=True)
 
 
 _libs: dict = {}
@@ -266,6 +267,20 @@ def plane_quant(bits: int, pc: bool = True, chroma: bool = False):
 
 def backend(kind: str = "port", dtype=np.float32) -> _Backend:
     return _Backend(kind, dtype)
+
+
+def set_f32_transform_mode(kind: str, mode: int) -> int:
+    """Select how the FP32 oracle evaluates its 3-D DCT (see
+    ``oracle_dct_set_f32_mode`` in oracle/dct_ref.h): 0 = double accumulation
+    (the default the fixtures were made with), 1 / 2 / 3 = float arithmetic
+    per axis, terms summed forward / backward / pairwise. Returns the previous
+    mode."""
+    path = (os.path.join(REF_DIR, "libbm3d_ref_f32.so") if kind == "reference"
+            else os.path.join(BUILD_DIR, "libbm3d_oracle.so"))
+    lib = _load(path)
+    old = int(lib.oracle_dct_get_f32_mode())
+    lib.oracle_dct_set_f32_mode(int(mode))
+    return old
 
 
 def reference_stage_default(profile: str, wiener: bool, sigma: Sequence[float]) -> dict:

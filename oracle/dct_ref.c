@@ -76,6 +76,60 @@ void oracle_dct_plan_destroy(oracle_dct_plan *p)
 DEFINE_AXIS(axis_f64acc, double)
 DEFINE_AXIS(axis_f80acc, long double)
 
+/* FP32 variants for the self-divergence envelope: the same definitions
+ * evaluated in float, each axis rounded to float before the next, with the
+ * cosines rounded to float -- as an FP32 FFT library's codelets compute.
+ * order 0 sums the terms of each output from the first input up, order 1
+ * from the last input down, order 2 pairwise (a balanced tree, the way
+ * butterfly stages combine partial sums). */
+static float pairwise_f32(const float *t, int n)
+{
+    if (n == 1) return t[0];
+    const int h = n / 2;
+    return pairwise_f32(t, h) + pairwise_f32(t + h, n - h);
+}
+
+static void axis_f32acc(float *buf, const long double *tab, int n, int stride, int inner,
+                        int outer, int order)
+{
+    float line[64];
+    float *tmp = n <= 64 ? line : (float *)malloc(sizeof(float) * (size_t)n);
+    for (int o = 0; o < outer; ++o) {
+        for (int in = 0; in < inner; ++in) {
+            float *base = buf + (size_t)o * (size_t)n * (size_t)stride + in;
+            for (int k = 0; k < n; ++k) {
+                float s = 0.0f;
+                const long double *row = tab + (size_t)k * (size_t)n;
+                if (order == 2) {
+                    float terms[64];
+                    for (int j = 0; j < n && j < 64; ++j) terms[j] = (float)row[j] * base[(size_t)j * stride];
+                    s = pairwise_f32(terms, n < 64 ? n : 64);
+                } else if (order == 1) {
+                    for (int j = n - 1; j >= 0; --j) s += (float)row[j] * base[(size_t)j * stride];
+                } else {
+                    for (int j = 0; j < n; ++j) s += (float)row[j] * base[(size_t)j * stride];
+                }
+                tmp[k] = s;
+            }
+            for (int k = 0; k < n; ++k) base[(size_t)k * stride] = tmp[k];
+        }
+    }
+    if (tmp != line) free(tmp);
+}
+
+static int g_f32_mode = 0;
+
+void oracle_dct_set_f32_mode(int mode) { g_f32_mode = (mode >= 0 && mode <= 3) ? mode : 0; }
+int oracle_dct_get_f32_mode(void) { return g_f32_mode; }
+
+static void exec_f32_float(const oracle_dct_plan *p, float *data, int order)
+{
+    const int n0 = p->n[0], n1 = p->n[1], n2 = p->n[2];
+    axis_f32acc(data, p->tab[2], n2, 1, 1, n0 * n1, order);
+    axis_f32acc(data, p->tab[1], n1, n2, n2, n0, order);
+    axis_f32acc(data, p->tab[0], n0, n1 * n2, n1 * n2, 1, order);
+}
+
 #define DEFINE_EXEC(NAME, T, ACC, AXIS)                                         \
     void NAME(const oracle_dct_plan *p, T *data)                                \
     {                                                                           \
@@ -91,6 +145,12 @@ DEFINE_AXIS(axis_f80acc, long double)
         if (buf != stackbuf) free(buf);                                         \
     }
 
-DEFINE_EXEC(oracle_dct_exec_f32, float, double, axis_f64acc)
+DEFINE_EXEC(exec_f32_double, float, double, axis_f64acc)
+
+void oracle_dct_exec_f32(const oracle_dct_plan *p, float *data)
+{
+    if (g_f32_mode == 0) exec_f32_double(p, data);
+    else exec_f32_float(p, data, g_f32_mode - 1);
+}
 DEFINE_EXEC(oracle_dct_exec_f64, double, long double, axis_f80acc)
 DEFINE_EXEC(oracle_dct_exec_f80, long double, long double, axis_f80acc)

@@ -29,6 +29,18 @@ void oracle_dct_exec_f32(const oracle_dct_plan *p, float *data);
 void oracle_dct_exec_f64(const oracle_dct_plan *p, double *data);
 void oracle_dct_exec_f80(const oracle_dct_plan *p, long double *data);
 
+/* How oracle_dct_exec_f32 evaluates the transform (process-wide):
+ *   0 (default): accumulate all three axes in double, round once;
+ *   1: in float, each axis rounded to float, terms summed in index order;
+ *   2: as 1 with the terms summed in reverse index order;
+ *   3: as 1 with the terms summed pairwise (balanced tree).
+ * Modes 1-3 are three more valid FP32 evaluations of the same transform;
+ * the parity tests run the reference's chain under them to measure how far
+ * the reference diverges from itself when only its transform rounding
+ * changes. */
+void oracle_dct_set_f32_mode(int mode);
+int oracle_dct_get_f32_mode(void);
+
 #ifdef __cplusplus
 }
 #endif

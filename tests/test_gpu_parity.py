@@ -134,19 +134,55 @@ def _oracle(oracle_mod, dtype=np.float32):
     return oracle_mod.backend(kind, dtype)
 
 
+# The chained pipeline's bar. Its final stage matches blocks on the basic
+# estimate, so a basic estimate that differs from the reference's in the 7th
+# digit flips matches between nearly equal keys, and each flip moves a few
+# pixels by up to ~1e-2. The reference does the same to itself: run with its
+# transform evaluated in FP32 (three summation orders, oracle/dct_ref.h modes
+# 1-3) instead of the double-accumulating default, its own chained output moves
+# by up to 1.1e-2 at 1080p. Where the chained max-abs is above 1e-3 the GPU
+# chain must stay inside that self-divergence envelope: max-abs and the count
+# of pixels over 1e-3 within ENV_FACTOR x the largest of the three, and MSE
+# within ENV_FACTOR x the largest (PSNR within 3 dB). ENV_FACTOR allows for the
+# envelope being estimated from three samples of a chaotic quantity.
+ENV_FACTOR = 2.0
+ENV_MODES = (1, 2, 3)
+
+
+def chain_envelope(oracle_mod, orc, b, f, noisy, rf0):
+    """Divergence of the reference's chain from itself (mode 0) when only its
+    FP32 transform rounding changes: max over modes 1-3 of max-abs and pixel
+    count over 1e-3, and the largest MSE."""
+    env = {"max_abs": 0.0, "n_over": 0, "mse": 0.0}
+    if orc.kind != "reference":
+        pytest.skip("the self-divergence envelope needs the compiled reference")
+    try:
+        for mode in ENV_MODES:
+            oracle_mod.set_f32_transform_mode("reference", mode)
+            rb = orc.stage(False, b, noisy)
+            rf = orc.stage(True, f, noisy, rb)
+            d = np.abs(rf.astype(np.float64) - rf0.astype(np.float64))
+            env["max_abs"] = max(env["max_abs"], float(d.max()))
+            env["n_over"] = max(env["n_over"], int((d > MAX_ABS).sum()))
+            env["mse"] = max(env["mse"], float(np.mean(d * d)))
+    finally:
+        oracle_mod.set_f32_transform_mode("reference", 0)
+    return env
+
+
 @pytest.mark.parametrize("shape,s255,seed", [((512, 512), 25.0, 0), ((1080, 1920), 25.0, 1),
                                              ((1080, 1920), 5.0, 2), ((1080, 1920), 50.0, 3),
-                                             ((301, 257), 10.0, 4), ((512, 512), 50.0, 6)])
+                                             ((1080, 1920), 10.0, 7), ((301, 257), 10.0, 4),
+                                             ((512, 512), 50.0, 6)])
 def test_against_oracle(ctx, oracle_mod, shape, s255, seed):
     """Seeded workloads of the benchmark's shapes.
 
     Each stage is held to the strict bar on identical inputs: group lists
     (>= 99.9 %, exact in practice) and max-abs <= 1e-3 / >= 60 dB. The chained
-    pipeline (final stage fed by our own basic estimate) is held to >= 60 dB:
-    its basic estimate differs from the reference's in the 7th digit, which
-    legitimately flips a few final-stage block-matching decisions on near-equal
-    keys (the same happens to the reference's own code with an FP32-reordered
-    transform), so its max-abs is reported, not bounded. The error of the FP32
+    pipeline (final stage fed by our own basic estimate) against the
+    reference's own chain: max-abs <= 1e-3, or, where that is exceeded, inside
+    the reference's self-divergence envelope (ENV_FACTOR above), and always
+    >= 60 dB with >= 99.9 % of final groups matched. The error of the FP32
     result against an FP64 run of the same kernels is reported too."""
     from isp_mw_b200 import synth
     import isp_mw_b200
@@ -177,10 +213,20 @@ def test_against_oracle(ctx, oracle_mod, shape, s255, seed):
     frac = group_match(name + ":final_groups_chained", gf, orc.groups(True, f.as_dict(), rb),
                        keys=False)
     d = np.abs(full.astype(np.float64) - rf)
+    max_abs, n_over, mse = float(d.max()), int((d > MAX_ABS).sum()), float(np.mean(d * d))
     p_ref = psnr_to(full, rf)
-    report(test=name + ":full_chained", max_abs=float(d.max()), psnr=p_ref,
-           n_over=int((d > MAX_ABS).sum()), frac_over=float((d > MAX_ABS).mean()))
-    assert p_ref >= MIN_PSNR and frac >= 0.999
+    rec = dict(test=name + ":full_chained", max_abs=max_abs, psnr=p_ref, n_over=n_over,
+               frac_over=float((d > MAX_ABS).mean()))
+    if max_abs > MAX_ABS:
+        env = chain_envelope(oracle_mod, orc, b.as_dict(), f.as_dict(), noisy, rf)
+        rec.update(env_max_abs=env["max_abs"], env_n_over=env["n_over"], env_mse=env["mse"])
+        report(**rec)
+        assert max_abs <= ENV_FACTOR * env["max_abs"], (name, max_abs, env)
+        assert n_over <= ENV_FACTOR * max(1, env["n_over"]), (name, n_over, env)
+        assert mse <= ENV_FACTOR * env["mse"], (name, mse, env)
+    else:
+        report(**rec)
+    assert p_ref >= MIN_PSNR and frac >= 0.999, (name, p_ref, frac)
     assert np.array_equal(full, final)  # bm3d_full == stage + stage, bit for bit
     # FP64 run of the same kernels: error of the FP32 result against it
     n64 = noisy.astype(np.float64)
