@@ -357,6 +357,13 @@ int bm3d_set_kernel_timing(bm3d_ctx *ctx, int on);
  * recorded launches to finish. */
 int bm3d_kernel_time(bm3d_ctx *ctx, int wiener, double *ms, long long *launches);
 
+/* Fault injection for callers' error paths: the next `count` device buffer
+ * allocations of contexts and batches fail as if cudaMalloc had run out of
+ * memory (the call returns BM3D_ERR_NOMEM, nothing is left half-built, and
+ * later calls allocate normally); 0 turns it off. Process-wide. No
+ * counterpart in the reference, which exits on allocation failure. */
+int bm3d_inject_alloc_failures(int count);
+
 /* Tile shape used by the stage kernels: reference blocks per CTA tile
  * (tile_x x tile_y) and warps per CTA. 0 keeps the current value. */
 int bm3d_set_tiling(bm3d_ctx *ctx, int tile_x, int tile_y, int warps);

@@ -42,6 +42,7 @@ EXPORTS = [
     "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
     "bm3d_full_many", "bm3d_batch3_create", "bm3d_host_batch_create", "bm3d_host_batch3_create",
     "bm3d_host_batch_run", "bm3d_host_batch_join", "bm3d_host_batch_destroy",
+    "bm3d_inject_alloc_failures",
 ]
 
 
@@ -123,6 +124,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_stage_noalloc.argtypes = [sp, ip, vp, vp, vp, ip, ip, ctypes.c_size_t,
                                        ctypes.c_float, vp]
     lib.bm3d_noalloc_check.argtypes = [vp]
+    lib.bm3d_inject_alloc_failures.argtypes = [ip]
     lib.bm3d_batch_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
                                       ctypes.POINTER(vp)]
     lib.bm3d_batch3_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,

@@ -47,35 +47,27 @@ __global__ void __launch_bounds__(GENERIC ? 256 : 512, 1)
 template <typename T> struct BatchPlane {
     typename AccOf<T>::type *num, *den;
     const T *src;
+    const T *ref;              // counted for non-finite pixels too when not null
     T *dst;
     long long src_stride, dst_stride;
     int width, height;
     int block_size;
     float *absmax;
+    int log2_bound, log2_corner;  // fixed-point bounds of the stage (StageArgs)
+    unsigned *nonfinite;       // non-finite src / ref pixels (may be null)
+    unsigned char *poison;     // pixels a non-finite term reached (may be null)
 };
 
-// Zero each plane's sums and fold its max |src| (grid.y = plane).
+// Zero each plane's sums, fold its max finite |src| and count its non-finite
+// pixels (grid.y = plane).
 template <typename T>
 __global__ void prep_batch_kernel(const BatchPlane<T> *planes)
 {
     const BatchPlane<T> q = planes[blockIdx.y];
-    const long long n = static_cast<long long>(q.width) * q.height;
-    float m = 0.0f;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        q.num[i] = 0;
-        q.den[i] = 0;
-        const long long y = i / q.width, x = i - y * q.width;
-        const float v = fabsf(static_cast<float>(q.src[y * q.src_stride + x]));
-        m = v > m ? v : m;
-    }
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) {
-        const float w = __shfl_xor_sync(0xffffffffu, m, o);
-        m = w > m ? w : m;
-    }
-    if ((threadIdx.x & 31) == 0 && m > 0.0f)
-        atomicMax(reinterpret_cast<int *>(q.absmax), __float_as_int(fminf(m, 3.0e38f)));
+    prep_plane<T>(q.num, q.den, q.src, q.ref, q.src_stride, q.width, q.height, q.absmax,
+                  q.nonfinite, q.poison,
+                  blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x,
+                  static_cast<long long>(gridDim.x) * blockDim.x);
 }
 
 // dst = num / den for every plane (grid.y = plane); each CTA walks the
@@ -89,7 +81,8 @@ __global__ void __launch_bounds__(256) normalize_batch_kernel(const BatchPlane<T
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int ty = tile / tx, txi = tile - ty * tx;
         normalize_tile<T>(q.dst, q.dst_stride, q.num, q.den, q.width, q.height, q.block_size,
-                          ty * kNormTile, txi * kNormTile);
+                          ty * kNormTile, txi * kNormTile, q.poison, q.absmax, q.log2_bound,
+                          q.log2_corner);
     }
 }
 

@@ -4,6 +4,9 @@
 // in bm3d_capi_batch.cu.
 #include "bm3d_capi_internal.h"
 
+#include <atomic>
+#include <type_traits>
+
 static thread_local std::string g_create_error;
 
 static void drain_timing(bm3d_ctx *ctx)
@@ -32,12 +35,25 @@ int bm3d::cuda_fail(bm3d_ctx *ctx, cudaError_t e, const char *what)
     return e == cudaErrorMemoryAllocation ? BM3D_ERR_NOMEM : BM3D_ERR_CUDA;
 }
 
+// Allocations still to fail on purpose (bm3d_inject_alloc_failures).
+static std::atomic<int> g_fail_allocs{0};
+
+extern "C" int bm3d_inject_alloc_failures(int count)
+{
+    if (count < 0) return BM3D_ERR_INVALID;
+    g_fail_allocs.store(count);
+    return BM3D_OK;
+}
+
 int bm3d::ensure(bm3d_ctx *ctx, DevBuf &b, size_t bytes)
 {
     if (b.bytes >= bytes) return BM3D_OK;
     if (b.ptr) cudaFree(b.ptr);
     b.ptr = nullptr;
     b.bytes = 0;
+    for (int left = g_fail_allocs.load(); left > 0; left = g_fail_allocs.load())
+        if (g_fail_allocs.compare_exchange_weak(left, left - 1))
+            return cuda_fail(ctx, cudaErrorMemoryAllocation, "cudaMalloc (injected failure)");
     CK(ctx, cudaMalloc(&b.ptr, bytes));
     b.bytes = bytes;
     return BM3D_OK;
@@ -174,8 +190,10 @@ extern "C" int bm3d_ctx_create(bm3d_ctx **out, int device)
     }
     cudaMemset(ctx->stats, 0, kStats * sizeof(unsigned long long));
     e = cudaMalloc(&ctx->absmax, kMaxPlanes * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->nonfinite, kMaxPlanes * sizeof(unsigned));
     if (e != cudaSuccess) {
         cudaFree(ctx->stats);
+        if (ctx->absmax) cudaFree(ctx->absmax);
         delete ctx;
         return cuda_fail(nullptr, e, "cudaMalloc(absmax)");
     }
@@ -205,6 +223,7 @@ extern "C" int bm3d_ctx_create(bm3d_ctx **out, int device)
         if (e != cudaSuccess) {
             cudaFree(ctx->stats);
             cudaFree(ctx->absmax);
+            cudaFree(ctx->nonfinite);
             cudaFree(ctx->gtab_f);
             cudaFree(ctx->gtab_d);
             delete ctx;
@@ -231,6 +250,7 @@ extern "C" void bm3d_ctx_destroy(bm3d_ctx *ctx)
     for (auto &b : ctx->groups) fr(b);
     for (auto &b : ctx->conv) fr(b);
     for (auto &b : ctx->ints) fr(b);
+    for (auto &b : ctx->poison) fr(b);
     for (auto &sl : ctx->pipe) {
         fr(sl.in);
         fr(sl.out);
@@ -241,6 +261,7 @@ extern "C" void bm3d_ctx_destroy(bm3d_ctx *ctx)
     if (ctx->down) cudaStreamDestroy(ctx->down);
     if (ctx->stats) cudaFree(ctx->stats);
     if (ctx->absmax) cudaFree(ctx->absmax);
+    if (ctx->nonfinite) cudaFree(ctx->nonfinite);
     if (ctx->gtab_f) cudaFree(ctx->gtab_f);
     if (ctx->gtab_d) cudaFree(ctx->gtab_d);
     drain_timing(ctx);
@@ -572,22 +593,31 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
     const int threads = 256;
     const int blocks = static_cast<int>(std::min<long long>((npx + threads - 1) / threads,
                                                             static_cast<long long>(ctx->sm_count) * 8));
-    // At most 2 * (reference blocks) * GroupSize terms reach one pixel (block
-    // (0, 0) can sit in every group, twice).
-    const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, p->group_size);
-    a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
+    fixed_point_bounds(p, width, height, a.log2_bound, a.log2_corner);
     a.absmax = ctx->absmax;
-    if (!bm_only) CK(ctx, cudaMemsetAsync(ctx->absmax, 0, kMaxPlanes * sizeof(float), s));
+    // FP32 sums are fixed point: planes with NaN / Inf pixels take the checking
+    // aggregation (FP64 sums are doubles and carry them like the reference's)
+    constexpr bool kFixed = std::is_same<Acc, long long>::value;
+    a.nonfinite = kFixed ? ctx->nonfinite : nullptr;
+    if (!bm_only) {
+        CK(ctx, cudaMemsetAsync(ctx->absmax, 0, kMaxPlanes * sizeof(float), s));
+        CK(ctx, cudaMemsetAsync(ctx->nonfinite, 0, kMaxPlanes * sizeof(unsigned), s));
+    }
     for (int c = 0; c < nplanes; ++c) {
         if (!(a.active & (1 << c)) && !bm_only) continue;
         if ((rc = ensure(ctx, ctx->acc[2 * c], acc_bytes)) != BM3D_OK) return rc;
         if ((rc = ensure(ctx, ctx->acc[2 * c + 1], acc_bytes)) != BM3D_OK) return rc;
         a.num[c] = static_cast<Acc *>(ctx->acc[2 * c].ptr);
         a.den[c] = static_cast<Acc *>(ctx->acc[2 * c + 1].ptr);
+        if (kFixed) {
+            if ((rc = ensure(ctx, ctx->poison[c], static_cast<size_t>(npx))) != BM3D_OK) return rc;
+            a.poison[c] = static_cast<unsigned char *>(ctx->poison[c].ptr);
+        }
         if (!bm_only) {
-            prep_kernel<T><<<blocks, threads, 0, s>>>(a.num[c], a.den[c], src[c],
-                                                      static_cast<long long>(stride), width,
-                                                      height, ctx->absmax + c);
+            prep_kernel<T><<<blocks, threads, 0, s>>>(
+                a.num[c], a.den[c], src[c], static_cast<long long>(stride), width, height,
+                ctx->absmax + c, ref[c] != src[c] ? ref[c] : nullptr,
+                kFixed ? ctx->nonfinite + c : nullptr, a.poison[c]);
             CK(ctx, cudaGetLastError());
         }
     }
@@ -606,7 +636,9 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
         if (!(a.active & (1 << c))) continue;
         const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
         normalize_kernel<T><<<ngrid, 256, 0, s>>>(dst[c], static_cast<long long>(stride), a.num[c],
-                                                  a.den[c], width, height, a.block_size);
+                                                  a.den[c], width, height, a.block_size,
+                                                  a.poison[c], ctx->absmax + c, a.log2_bound,
+                                                  a.log2_corner);
         CK(ctx, cudaGetLastError());
     }
     return BM3D_OK;
@@ -977,8 +1009,9 @@ namespace {
 
 constexpr size_t kNoAllocMaxPixels = size_t(1) << 21;  // 2,097,152 pixels (1920x1080 fits)
 constexpr size_t kNoAllocAccBytes = kNoAllocMaxPixels * sizeof(long long);
-// num (int64 per pixel) | den (int64 per pixel) | absmax (4 floats) | counters (8 x u64)
-constexpr size_t kNoAllocBytes = 2 * kNoAllocAccBytes + 256 + 256;
+// num (int64 per pixel) | den (int64 per pixel) | header: absmax (4 floats) at 0,
+// non-finite pixel count at 128 | counters (8 x u64) | poison map (1 byte per pixel)
+constexpr size_t kNoAllocBytes = 2 * kNoAllocAccBytes + 256 + 256 + kNoAllocMaxPixels;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -1049,7 +1082,9 @@ int noalloc_setup(int dev, NoAllocDevice **out)
 // starts at zero when the library loads and is cleared only by
 // bm3d_noalloc_check, so it covers every call since the last check.
 constexpr size_t kNoAllocAbsmaxOff = 2 * kNoAllocAccBytes;
+constexpr size_t kNoAllocNonfiniteOff = kNoAllocAbsmaxOff + 128;
 constexpr size_t kNoAllocStatsOff = kNoAllocAbsmaxOff + 256;
+constexpr size_t kNoAllocPoisonOff = kNoAllocStatsOff + 256;
 constexpr size_t kNoAllocClearBytes = 256 + 4 * sizeof(unsigned long long);
 
 }  // namespace
@@ -1093,6 +1128,8 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     long long *num = reinterpret_cast<long long *>(d->scratch);
     long long *den = reinterpret_cast<long long *>(d->scratch + kNoAllocAccBytes);
     float *absmax = reinterpret_cast<float *>(d->scratch + kNoAllocAbsmaxOff);
+    unsigned *nonfinite = reinterpret_cast<unsigned *>(d->scratch + kNoAllocNonfiniteOff);
+    unsigned char *poison = d->scratch + kNoAllocPoisonOff;
     unsigned long long *stats = reinterpret_cast<unsigned long long *>(d->scratch + kNoAllocStatsOff);
 
     StageArgs<float> a;
@@ -1109,9 +1146,10 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     int warps;
     rc = plan_geometry(&info, a, params, wiener != 0, 1, width, height, warps);
     if (rc != BM3D_OK) return noalloc_error(info.err.c_str(), cudaSuccess, rc);
-    const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, params->group_size);
-    a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
+    fixed_point_bounds(params, width, height, a.log2_bound, a.log2_corner);
     a.absmax = absmax;
+    a.nonfinite = nonfinite;
+    a.poison[0] = poison;
     a.num[0] = num;
     a.den[0] = den;
     a.stats = stats;
@@ -1125,13 +1163,15 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     // (stats[4]) is left alone so bm3d_noalloc_check sees every call
     if ((e = cudaMemsetAsync(absmax, 0, kNoAllocClearBytes, s)) != cudaSuccess)
         return noalloc_error("cudaMemsetAsync(scratch header)", e);
-    prep_kernel<float><<<blocks, threads, 0, s>>>(num, den, src, a.stride, width, height, absmax);
+    prep_kernel<float><<<blocks, threads, 0, s>>>(num, den, src, a.stride, width, height, absmax,
+                                                  ref != src ? ref : nullptr, nonfinite, poison);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("prep_kernel", e);
     rc = launch_stage(&info, a, wiener != 0, 1, s, warps);
     if (rc != BM3D_OK) return noalloc_error(info.err.c_str(), cudaSuccess, rc);
     const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
     normalize_kernel<float><<<ngrid, 256, 0, s>>>(dst, a.stride, num, den, width, height,
-                                                  a.block_size);
+                                                  a.block_size, poison, absmax, a.log2_bound,
+                                                  a.log2_corner);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("normalize_kernel", e);
     return BM3D_OK;
 }

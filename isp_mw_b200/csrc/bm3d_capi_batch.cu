@@ -122,6 +122,8 @@ struct bm3d_batch {
     std::vector<Guard> gb, gf;
     std::vector<size_t> acc_off, basic_off;  // per plane: offsets into acc (int64) and basic (float)
     DevBuf acc, basic, absmax, counters, planes_b, planes_f;
+    DevBuf nonfinite, poison;  // per plane: non-finite input pixels; pixels they reached
+    std::vector<size_t> poison_off;  // per plane: offset into poison (bytes)
     DevBuf bad;  // the kernels' consistency counter (bm3d_batch_check)
     int nq_b = 0, nq_f = 0;  // entries of planes_b / planes_f (planes each stage filters)
     StageBuild sb, sf;
@@ -187,8 +189,10 @@ int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuil
             a.den[c] = a.num[c] + static_cast<size_t>(a.width) * a.height;
         }
         a.absmax = static_cast<float *>(B->absmax.ptr) + i * npl;
-        const double terms = 2.0 * static_cast<double>(a.nx) * a.ny * std::max(1, p->group_size);
-        a.log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, terms))));
+        a.nonfinite = static_cast<const unsigned *>(B->nonfinite.ptr) + i * npl;
+        for (int c = 0; c < npl; ++c)
+            a.poison[c] = static_cast<unsigned char *>(B->poison.ptr) + B->poison_off[i * npl + c];
+        fixed_point_bounds(p, a.width, a.height, a.log2_bound, a.log2_corner);
         a.dct_fwd = ctx->gtab_f;
         a.dct_inv = ctx->gtab_f ? ctx->gtab_f + kDctTableSize : nullptr;
         const SmemPlan sp = plan_smem<float>(npl, wiener, a.ref_alias_src, a.region_h,
@@ -285,6 +289,7 @@ int enqueue_batch(bm3d_batch *B, cudaStream_t s)
         }
     }
     CK(ctx, cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * B->n * B->npl, s));
+    CK(ctx, cudaMemsetAsync(B->nonfinite.ptr, 0, sizeof(unsigned) * B->n * B->npl, s));
     if ((rc = launch_planes(B, B->planes_b, true, s)) != BM3D_OK) return rc;
     if ((rc = launch_batch_stage<false>(B, B->sb, counters, s)) != BM3D_OK) return rc;
     if ((rc = launch_planes(B, B->planes_b, false, s)) != BM3D_OK) return rc;
@@ -420,6 +425,7 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
             B->dst.push_back(dst[k]);
             B->acc_off.push_back(acc_total);
             B->basic_off.push_back(basic_total);
+            B->poison_off.push_back(acc_total / 2);
             acc_total += 2 * static_cast<size_t>(width[i]) * height[i];
             basic_total += stride[i] * height[i];
         }
@@ -428,6 +434,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
     if ((rc = ensure(ctx, B->acc, sizeof(long long) * acc_total)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->basic, sizeof(float) * basic_total)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->absmax, sizeof(float) * count * npl)) != BM3D_OK) return fail(rc);
+    if ((rc = ensure(ctx, B->nonfinite, sizeof(unsigned) * count * npl)) != BM3D_OK) return fail(rc);
+    if ((rc = ensure(ctx, B->poison, acc_total / 2)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->counters, 2 * sizeof(int))) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->bad, sizeof(unsigned long long))) != BM3D_OK) return fail(rc);
     CK(ctx, cudaMemset(B->bad.ptr, 0, sizeof(unsigned long long)));
@@ -444,6 +452,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
                 bp.num = static_cast<long long *>(B->acc.ptr) + B->acc_off[k];
                 bp.den = bp.num + static_cast<size_t>(width[i]) * height[i];
                 bp.src = src[k];
+                // the final stage's Wiener weights come from the basic estimate
+                bp.ref = st ? static_cast<const float *>(B->basic.ptr) + B->basic_off[k] : nullptr;
                 bp.dst = st ? dst[k] : static_cast<float *>(B->basic.ptr) + B->basic_off[k];
                 bp.src_stride = static_cast<long long>(stride[i]);
                 bp.dst_stride = static_cast<long long>(stride[i]);
@@ -451,6 +461,9 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
                 bp.height = height[i];
                 bp.block_size = pp.block_size;
                 bp.absmax = static_cast<float *>(B->absmax.ptr) + k;
+                fixed_point_bounds(&pp, width[i], height[i], bp.log2_bound, bp.log2_corner);
+                bp.nonfinite = static_cast<unsigned *>(B->nonfinite.ptr) + k;
+                bp.poison = static_cast<unsigned char *>(B->poison.ptr) + B->poison_off[k];
                 q.push_back(bp);
             }
         }
@@ -475,6 +488,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
             if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemcpy2DAsync"));
         }
     e = cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * count * npl, B->cap);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(B->nonfinite.ptr, 0, sizeof(unsigned) * count * npl, B->cap);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemsetAsync"));
     if ((rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap,
                                 force_tiling)) != BM3D_OK)
@@ -566,7 +581,8 @@ extern "C" void bm3d_batch_destroy(bm3d_batch *B)
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     if (B->cap) cudaStreamDestroy(B->cap);
-    for (DevBuf *b : {&B->acc, &B->basic, &B->absmax, &B->counters, &B->bad, &B->planes_b, &B->planes_f,
+    for (DevBuf *b : {&B->acc, &B->basic, &B->absmax, &B->nonfinite, &B->poison, &B->counters,
+                      &B->bad, &B->planes_b, &B->planes_f,
                       &B->sb.args, &B->sb.base, &B->sf.args, &B->sf.base})
         if (b->ptr) cudaFree(b->ptr);
     delete B;

@@ -8,6 +8,7 @@
 #include "bm3d_batch.cuh"
 #include "bm3d_kernels.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -39,8 +40,10 @@ struct bm3d_ctx {
     DevBuf groups[3];                 // debug group dump
     DevBuf conv[3 * kMaxPlanes];      // float working planes of the integer paths: src, ref, dst
     DevBuf ints[3 * kMaxPlanes];      // host-mode staging of integer planes: src, ref, dst
+    DevBuf poison[kMaxPlanes];        // per plane: pixels a non-finite term reached (1 B / pixel)
     unsigned long long *stats = nullptr;
-    float *absmax = nullptr;          // per plane max |src| of the running stage
+    float *absmax = nullptr;          // per plane max finite |src| of the running stage
+    unsigned *nonfinite = nullptr;    // per plane non-finite src / ref pixels of the running stage
     float *gtab_f = nullptr;          // generic path cosine matrices: fwd | inv (float)
     double *gtab_d = nullptr;         // same in double
     cudaStream_t last_stream = nullptr;
@@ -109,6 +112,25 @@ bool fast_args(int block_size, int group_size);
 template <typename T>
 void fill_tables(StageArgs<T> &a, const bm3d_stage_params *p, bool wiener, int nplanes,
                  double value_range);
+
+// Fixed-point bounds of one stage on a width x height plane (fixed_scale):
+// ceil(log2) of the most terms that reach one pixel outside block (0, 0) --
+// group members lie within BMrange of their reference block, so only the
+// reference positions within BlockSize + 2 BMrange of the pixel, per axis,
+// reach it, GroupSize terms each -- and of those that reach block (0, 0)'s
+// pixels and its weight origin, which every group may also hold twice (the
+// reference's trailing (0, 0) candidate, include/Block.h:668-687).
+inline void fixed_point_bounds(const bm3d_stage_params *p, int width, int height, int &log2_bound,
+                               int &log2_corner)
+{
+    const int bs = p->block_size, step = std::max(1, p->block_step);
+    const int range = p->bm_step > 0 ? p->bm_range / p->bm_step * p->bm_step : p->bm_range;
+    const int per_axis = (bs + 2 * std::max(0, range) + step - 1) / step + 1;
+    const double local = static_cast<double>(per_axis) * per_axis * std::max(1, p->group_size);
+    const double refs = static_cast<double>(ref_count(width - bs, step)) * ref_count(height - bs, step);
+    log2_bound = static_cast<int>(std::ceil(std::log2(std::max(2.0, local))));
+    log2_corner = static_cast<int>(std::ceil(std::log2(std::max(2.0, 2.0 * refs + local))));
+}
 
 // Host-mode calls end synchronised; fails if the kernels' invariant counter
 // is nonzero.

@@ -236,12 +236,22 @@ template <> struct AccOf<double> { using type = double; };
 // 64 * absmax (a filtered block value is bounded by the group's L2 norm,
 // <= 32 * absmax for a 1024-pixel group, times a weight <= 1), so a pixel's
 // sum stays below 2^62.
+//
+// Two bounds are used per plane. A pixel outside block (0, 0) is reached only
+// by group members within BMrange of their reference block, so by at most
+// (ceil((BS + 2 BMrange) / step) + 1)^2 * GroupSize terms (the reference
+// positions whose search window can hold a block covering it, the clamped
+// last row / column included). Block (0, 0) is also the trailing candidate of
+// every reference block's list (include/Block.h:668-687), so its pixels -- and
+// its block weight, summed at origin (0, 0) -- may get up to two terms from
+// every group. Each pixel and each weight origin keeps the scale of its class;
+// the normalisation converts between them.
 __device__ __forceinline__ float fixed_scale(float absmax, int log2_bound)
 {
-    if (!(absmax > 0.0f) || !(absmax < 3.0e38f)) absmax = 1.0f;
+    if (!(absmax > 0.0f) || !(absmax <= 3.4028235e38f)) absmax = 1.0f;
     int e = 0;
-    frexpf(absmax * 64.0f, &e);  // absmax * 64 < 2^e
-    int s = 62 - e - log2_bound;
+    frexpf(absmax, &e);  // absmax < 2^e, so 64 * absmax < 2^(e + 6)
+    int s = 62 - (e + 6) - log2_bound;
     s = s < -60 ? -60 : (s > 60 ? 60 : s);
     return ldexpf(1.0f, s);
 }
@@ -255,8 +265,16 @@ template <typename T> struct StageArgs {
     const T *ref[kMaxPlanes];   // basic: plane 0 drives matching; final: basic estimate
     typename AccOf<T>::type *num[kMaxPlanes];  // numerator sums, width x height, pitch = width
     typename AccOf<T>::type *den[kMaxPlanes];  // weight sums, same layout
-    const float *absmax;        // per plane max |src| (device), sets the fixed-point scale
-    int log2_bound;             // ceil(log2(max contributions to one pixel))
+    const float *absmax;        // per plane max finite |src| (device), sets the fixed-point scale
+    int log2_bound;             // ceil(log2(max contributions to one pixel outside block (0, 0)))
+    int log2_corner;            // the same for block (0, 0)'s pixels, which every group may reach
+    // FP32 only (null for FP64, whose double sums carry NaN / Inf themselves):
+    // per plane, the count of non-finite src / ref pixels found by the prep
+    // kernel, and a byte per pixel (pitch = width) that marks pixels a
+    // non-finite term reached. The kernels look at the count once per tile and
+    // take the checking aggregation only when it is nonzero.
+    const unsigned *nonfinite;
+    unsigned char *poison[kMaxPlanes];
     int active;                 // bit p set: plane p is filtered (sigma[p] > 0)
     int width, height;
     long long stride;           // row pitch of src / ref, in elements

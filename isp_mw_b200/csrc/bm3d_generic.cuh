@@ -224,7 +224,7 @@ __device__ __forceinline__ void group_index(int e, int bs, int bsq, int &z, int 
 template <typename T, bool WIENER>
 __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
                                int n, int lane, T *Gs, T *Gr, float scale,
-                               unsigned &n_bad, int pt = -1)
+                               unsigned &n_bad, int pt = -1, bool check = false)
 {
     // p indexes the tile's windows; pt (default p) the plane's threshold /
     // Wiener tables, which differ when planes share one set of windows
@@ -290,8 +290,30 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         if (!block_in_tile(t, q.y, q.x)) continue;
         int pitch;
         auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
-        acc_add(dn + y * pitch + x, Gs[z * zs + y * rs + x] * numW, scale);
-        if (y == 0 && x == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
+        if (!check && (q.y >= bs || q.x >= bs)) {
+            acc_add(dn + y * pitch + x, Gs[z * zs + y * rs + x] * numW, scale);
+            if (y == 0 && x == 0)
+                acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
+        } else {
+            // a member reaching block (0, 0)'s pixels (their own scale), or a plane
+            // with non-finite pixels (per-term check, marks into the poison map)
+            const float scale_c = fixed_scale(a.absmax[pt], a.log2_corner);
+            unsigned char *const poison = poison_map(a, pt);
+            const bool corner = q.y + y < bs && q.x + x < bs;
+            unsigned char *mk =
+                poison ? poison + static_cast<long long>(q.y) * a.width + q.x : nullptr;
+            acc_add_checked(dn + y * pitch + x, Gs[z * zs + y * rs + x] * numW,
+                            corner ? scale_c : scale,
+                            mk ? mk + static_cast<long long>(y) * a.width + x : nullptr);
+            if (y == 0 && x == 0) {
+                const float sd = (q.y == 0 && q.x == 0) ? scale_c : scale;
+                if (mk == nullptr || fabsf(static_cast<float>(denW) * sd) < kFixedLimit)
+                    acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, sd);
+                else  // the block's weight reaches all of its pixels
+                    for (int i = 0; i < bsq; ++i)
+                        mk[static_cast<long long>(i / bs) * a.width + i % bs] = 1;
+            }
+        }
     }
     __syncwarp();
 }
@@ -332,8 +354,12 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
     // per-tile counters (small: 32 bits suffice), flushed once per tile
     unsigned n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
     float scale[NPL];
+    bool check[NPL];
 #pragma unroll
-    for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
+    for (int p = 0; p < NPL; ++p) {
+        scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
+        check[p] = poison_map(a, p) != nullptr;
+    }
     const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
     for (int r = warp; r < nrefs; r += nwarps) {
         const int ky = ky0 + r / tw, kx = kx0 + r % tw;
@@ -352,7 +378,8 @@ __device__ __forceinline__ void generic_tile_body(const StageArgs<T> &a, int til
 #pragma unroll
             for (int p = 0; p < NPL; ++p)
                 if (a.active & (1 << p))
-                    filter_generic<T, WIENER>(a, t, p, list, n, lane, Gs, Gr, scale[p], n_bad);
+                    filter_generic<T, WIENER>(a, t, p, list, n, lane, Gs, Gr, scale[p], n_bad,
+                                              -1, check[p]);
         }
         __syncwarp();
     }
@@ -409,6 +436,7 @@ __device__ __forceinline__ void generic_tile_body_seq3(const StageArgs<T> &a, in
         if (c > 0 && !filt) continue;
         stage_plane<T, WIENER>(a, t, c);
         const float scale = fixed_scale(a.absmax[c], a.log2_bound);
+        const bool check = poison_map(a, c) != nullptr;
         for (int r = warp; r < nrefs; r += nwarps) {
             int n;
             if (c == 0) {
@@ -440,7 +468,8 @@ __device__ __forceinline__ void generic_tile_body_seq3(const StageArgs<T> &a, in
                 }
             }
             __syncwarp();
-            if (filt) filter_generic<T, WIENER>(a, t, 0, list, n, lane, Gs, Gr, scale, n_bad, c);
+            if (filt)
+                filter_generic<T, WIENER>(a, t, 0, list, n, lane, Gs, Gr, scale, n_bad, c, check);
             __syncwarp();
         }
         __syncthreads();

@@ -9,6 +9,8 @@
 // BM3D_Final::CollaborativeFilter (source/BM3D.cpp:411-457).
 #pragma once
 
+#include <type_traits>
+
 #include "bm3d_device.cuh"
 #include "dct.cuh"
 
@@ -139,6 +141,28 @@ __device__ __forceinline__ void acc_add(long long *p, float v, float scale)
               static_cast<unsigned long long>(__float2ll_rn(v * scale)));
 }
 __device__ __forceinline__ void acc_add(double *p, double v, float) { atomicAdd(p, v); }
+
+// The same for planes with non-finite pixels: a term that has no fixed-point
+// value (NaN, +-Inf, or beyond the 2^62 range) marks its pixel instead, and
+// the normalisation writes NaN there -- what the reference's float sums give
+// once a NaN or an Inf of either sign reaches them (source/BM3D.cpp:130-135).
+// Finite terms are converted exactly as acc_add does; with no mark they are
+// always converted.
+constexpr float kFixedLimit = 4.0e18f;
+__device__ __forceinline__ void acc_add_checked(long long *p, float v, float scale,
+                                                unsigned char *mark)
+{
+    const float x = v * scale;
+    if (mark == nullptr || fabsf(x) < kFixedLimit)
+        atomicAdd(reinterpret_cast<unsigned long long *>(p),
+                  static_cast<unsigned long long>(__float2ll_rn(x)));
+    else
+        *mark = 1;
+}
+__device__ __forceinline__ void acc_add_checked(double *p, double v, float, unsigned char *)
+{
+    atomicAdd(p, v);
+}
 __device__ __forceinline__ void acc_flush(long long *p, long long v)
 {
     atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
@@ -699,11 +723,63 @@ __device__ __forceinline__ void group_inv(T *G, int n, int lane, T (&a)[kGSMax],
 __device__ __forceinline__ float wiener_weight(float y2, float s2) { return __fdividef(y2, y2 + s2); }
 __device__ __forceinline__ double wiener_weight(double y2, double s2) { return y2 / (y2 + s2); }
 
+// The poison map of plane p when its inputs hold non-finite pixels, else null
+// (the normal, unchecked aggregation).
+template <typename T>
+__device__ __forceinline__ unsigned char *poison_map(const StageArgs<T> &a, int p)
+{
+    if (a.nonfinite == nullptr || a.poison[p] == nullptr) return nullptr;
+    return a.nonfinite[p] != 0 ? a.poison[p] : nullptr;
+}
+
+// One 8 x 8 group member whose footprint reaches block (0, 0)'s pixels, or any
+// member on a plane with non-finite pixels: per pixel, the scale of its class
+// (block (0, 0) or not) and, with a poison map, the check of acc_add_checked.
+// gz is the member's transformed block in the group buffer; lane half h
+// aggregates rows 4h .. 4h + 3 and h == 0 adds the block weight at the
+// member's origin. `plane` indexes the plane's scale and poison map.
+template <typename T>
+__device__ __forceinline__ void aggregate_member_slow(const StageArgs<T> &a, const Tile<T> &t, int p,
+                                                      int plane, BlockPos q, const T *gz, int h,
+                                                      T numW, T denW, float scale)
+{
+    const float scale_c = fixed_scale(a.absmax[plane], a.log2_corner);
+    unsigned char *const poison = poison_map(a, plane);
+    int pitch;
+    auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
+#pragma unroll 1
+    for (int r = 0; r < 4; ++r) {
+        const int y = 4 * h + r;
+        T v[8];
+        Vec4<T>::load(gz + gidx(y, 0), v[0], v[1], v[2], v[3]);
+        Vec4<T>::load(gz + gidx(y, 4), v[4], v[5], v[6], v[7]);
+        redft01_8(v);
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+            const bool corner = q.y + y < kBS && q.x + x < kBS;
+            unsigned char *mk =
+                poison ? poison + static_cast<long long>(q.y + y) * a.width + q.x + x : nullptr;
+            acc_add_checked(dn + y * pitch + x, v[x] * numW, corner ? scale_c : scale, mk);
+        }
+    }
+    if (h == 0) {
+        const float sd = (q.y == 0 && q.x == 0) ? scale_c : scale;
+        if (poison == nullptr || fabsf(static_cast<float>(denW) * sd) < kFixedLimit)
+            acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, sd);
+        else  // the block's weight reaches all of its pixels
+            for (int i = 0; i < kBS * kBS; ++i)
+                poison[static_cast<long long>(q.y + (i >> 3)) * a.width + q.x + (i & 7)] = 1;
+    }
+}
+
 // Collaborative filtering of one group on plane p, aggregated into the CTA's
 // accumulator windows.
+// `check`: the plane holds non-finite pixels (poison_map is not null), so
+// every member goes through the checking aggregation.
 template <typename T, bool WIENER>
 __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
-                             int n, int lane, T *G, float scale, unsigned &n_bad, int pt = -1)
+                             int n, int lane, T *G, float scale, unsigned &n_bad, int pt = -1,
+                             bool check = false)
 {
     // p indexes the tile's windows; pt (default p) the plane's threshold /
     // Wiener tables, which differ when planes share one set of windows
@@ -770,20 +846,24 @@ __device__ void filter_group(const StageArgs<T> &a, const Tile<T> &t, int p, con
     const int z = lane >> 1, h = lane & 1;
     if (z < n && block_in_tile(t, list[z].y, list[z].x)) {
         const BlockPos q = list[z];
-        int pitch;
-        auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
         const T *gz = G + z * kGroupStride;
+        if (!check && (q.y >= kBS || q.x >= kBS)) {
+            int pitch;
+            auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
 #pragma unroll 1
-        for (int r = 0; r < 4; ++r) {
-            const int y = 4 * h + r;
-            T v[8];
-            Vec4<T>::load(gz + gidx(y, 0), v[0], v[1], v[2], v[3]);
-            Vec4<T>::load(gz + gidx(y, 4), v[4], v[5], v[6], v[7]);
-            redft01_8(v);
+            for (int r = 0; r < 4; ++r) {
+                const int y = 4 * h + r;
+                T v[8];
+                Vec4<T>::load(gz + gidx(y, 0), v[0], v[1], v[2], v[3]);
+                Vec4<T>::load(gz + gidx(y, 4), v[4], v[5], v[6], v[7]);
+                redft01_8(v);
 #pragma unroll
-            for (int x = 0; x < 8; ++x) acc_add(dn + y * pitch + x, v[x] * numW, scale);
+                for (int x = 0; x < 8; ++x) acc_add(dn + y * pitch + x, v[x] * numW, scale);
+            }
+            if (h == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
+        } else {
+            aggregate_member_slow<T>(a, t, p, pt, q, gz, h, numW, denW, scale);
         }
-        if (h == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
     }
     __syncwarp();
 }
@@ -1018,8 +1098,12 @@ __device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile,
     // per-tile counters (small: 32 bits suffice), flushed once per tile
     unsigned n_sum = 0, n_sq = 0, n_cand = 0, n_fix = 0, n_bad = 0;
     float scale[NPL];
+    bool check[NPL];
 #pragma unroll
-    for (int p = 0; p < NPL; ++p) scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
+    for (int p = 0; p < NPL; ++p) {
+        scale[p] = fixed_scale(a.absmax[p], a.log2_bound);
+        check[p] = poison_map(a, p) != nullptr;
+    }
     const int tw = kx1 - kx0, nrefs = tw * (ky1 - ky0);
     for (int r = warp; r < nrefs; r += nwarps) {
         const int ky = ky0 + r / tw, kx = kx0 + r % tw;
@@ -1032,7 +1116,8 @@ __device__ __forceinline__ void stage_tile_body(const StageArgs<T> &a, int tile,
 #pragma unroll
             for (int p = 0; p < NPL; ++p)
                 if (a.active & (1 << p))
-                    filter_group<T, WIENER>(a, t, p, list, n, lane, G, scale[p], n_bad);
+                    filter_group<T, WIENER>(a, t, p, list, n, lane, G, scale[p], n_bad, -1,
+                                            check[p]);
         }
         __syncwarp();
     }
@@ -1153,6 +1238,7 @@ __device__ __forceinline__ void stage_tile_body_seq3(const StageArgs<T> &a, int 
         if (c > 0 && !filt) continue;
         stage_plane<T, WIENER>(a, t, c);
         const float scale = fixed_scale(a.absmax[c], a.log2_bound);
+        const bool check = poison_map(a, c) != nullptr;
         for (int r = warp; r < nrefs; r += nwarps) {
             int n;
             if (c == 0) {
@@ -1180,7 +1266,7 @@ __device__ __forceinline__ void stage_tile_body_seq3(const StageArgs<T> &a, int 
                 }
             }
             __syncwarp();
-            if (filt) filter_group<T, WIENER>(a, t, 0, list, n, lane, G, scale, n_bad, c);
+            if (filt) filter_group<T, WIENER>(a, t, 0, list, n, lane, G, scale, n_bad, c, check);
             __syncwarp();
         }
         __syncthreads();
@@ -1200,7 +1286,8 @@ __global__ void __launch_bounds__(512, 1) stage_kernel(const StageArgs<T> a)
 }
 
 // dst = num / den (source/BM3D.cpp:130-135, include/Image_Type.hpp:319-332).
-// Both sums carry the same fixed-point scale, which cancels.
+// Outside block (0, 0) both sums carry the same fixed-point scale, which
+// cancels.
 __device__ __forceinline__ float ratio(long long n, long long d)
 {
     return static_cast<float>(static_cast<double>(n) / static_cast<double>(d));
@@ -1214,21 +1301,35 @@ constexpr int kNormTile = 32;
 // sum of the block weights W at the bs x bs origins whose block covers
 // (y, x): y - bs < oy <= y, x - bs < ox <= x. Separable sums over a
 // shared-memory copy of W; exact for integer sums.
+//
+// FP32 (fixed point): block (0, 0)'s pixels and the weight at origin (0, 0)
+// carry the scale of log2_corner, everything else that of log2_bound
+// (fixed_scale); for those pixels den = (sum of the other weights) * ratio +
+// W(0, 0), ratio = corner scale / general scale (a power of two, exact).
+// Pixels marked in `poison` (may be null) get NaN: a non-finite term reached
+// them (acc_add_checked).
 template <typename T>
 __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
                                                const typename AccOf<T>::type *num,
                                                const typename AccOf<T>::type *wsum, int width,
-                                               int height, int bs, int y0, int x0)
+                                               int height, int bs, int y0, int x0,
+                                               const unsigned char *poison = nullptr,
+                                               const float *absmax = nullptr, int log2_bound = 0,
+                                               int log2_corner = 0)
 {
     using Acc = typename AccOf<T>::type;
+    constexpr bool kFixed = std::is_same<Acc, long long>::value;
     constexpr int N = kNormTile, E = N + kBSMax - 1;
     __shared__ Acc w[E][E];
     __shared__ Acc hs[E][N];
     const int ext = N + bs - 1;
+    // origin (0, 0) is summed apart in fixed point (its own scale)
+    const bool split = kFixed && y0 < bs && x0 < bs;
     for (int i = threadIdx.x; i < ext * ext; i += blockDim.x) {
         const int ly = i / ext, lx = i - ly * ext;
         const int gy = y0 - bs + 1 + ly, gx = x0 - bs + 1 + lx;
-        w[ly][lx] = (gy >= 0 && gx >= 0 && gy < height && gx < width)
+        w[ly][lx] = (gy >= 0 && gx >= 0 && gy < height && gx < width &&
+                     !(split && gy == 0 && gx == 0))
                         ? wsum[static_cast<long long>(gy) * width + gx]
                         : Acc(0);
     }
@@ -1240,13 +1341,26 @@ __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
         hs[ly][lx] = v;
     }
     __syncthreads();
+    double cratio = 1.0;
+    if (split) {
+        const float am = absmax != nullptr ? *absmax : 1.0f;
+        cratio = static_cast<double>(fixed_scale(am, log2_corner)) /
+                 static_cast<double>(fixed_scale(am, log2_bound));
+    }
     for (int i = threadIdx.x; i < N * N; i += blockDim.x) {
         const int ly = i / N, lx = i - ly * N;
         const int gy = y0 + ly, gx = x0 + lx;
         if (gy >= height || gx >= width) continue;
         Acc d = 0;
         for (int k = 0; k < bs; ++k) d += hs[ly + k][lx];
-        dst[gy * dst_stride + gx] = ratio(num[static_cast<long long>(gy) * width + gx], d);
+        const long long g = static_cast<long long>(gy) * width + gx;
+        T out;
+        if (split && gy < bs && gx < bs)  // block (0, 0): covered by origin (0, 0)
+            out = static_cast<T>(static_cast<double>(num[g]) /
+                                 (static_cast<double>(d) * cratio + static_cast<double>(wsum[0])));
+        else
+            out = ratio(num[g], d);
+        dst[gy * dst_stride + gx] = (poison != nullptr && poison[g]) ? static_cast<T>(NAN) : out;
     }
     __syncthreads();  // before the next tile overwrites w / hs
 }
@@ -1255,35 +1369,62 @@ __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
 template <typename T>
 __global__ void __launch_bounds__(256)
     normalize_kernel(T *dst, long long dst_stride, const typename AccOf<T>::type *num,
-                     const typename AccOf<T>::type *wsum, int width, int height, int bs)
+                     const typename AccOf<T>::type *wsum, int width, int height, int bs,
+                     const unsigned char *poison = nullptr, const float *absmax = nullptr,
+                     int log2_bound = 0, int log2_corner = 0)
 {
     normalize_tile<T>(dst, dst_stride, num, wsum, width, height, bs, blockIdx.y * kNormTile,
-                      blockIdx.x * kNormTile);
+                      blockIdx.x * kNormTile, poison, absmax, log2_bound, log2_corner);
 }
 
-// Zero one plane's accumulators and fold max |src| into *absmax (which the
-// caller zeroes first). Non-negative floats order like their bit patterns.
+// Zero one plane's accumulators and fold the largest finite |src| into
+// *absmax (which the caller zeroes first; non-negative floats order like their
+// bit patterns). With `nonfinite` (FP32 only) it also counts the NaN / Inf
+// pixels of src and of ref (when given) into *nonfinite and clears the poison
+// map, so that the stage kernel checks its terms only on such planes.
 template <typename T>
-__global__ void prep_kernel(typename AccOf<T>::type *num, typename AccOf<T>::type *den,
-                            const T *src, long long stride, int width, int height, float *absmax)
+__device__ __forceinline__ void prep_plane(typename AccOf<T>::type *num,
+                                           typename AccOf<T>::type *den, const T *src,
+                                           const T *ref, long long stride, int width, int height,
+                                           float *absmax, unsigned *nonfinite,
+                                           unsigned char *poison, long long start,
+                                           long long step)
 {
     const long long n = static_cast<long long>(width) * height;
     float m = 0.0f;
-    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    unsigned bad = 0;
+    for (long long i = start; i < n; i += step) {
         num[i] = 0;
         den[i] = 0;
         const long long y = i / width, x = i - y * width;
         const float v = fabsf(static_cast<float>(src[y * stride + x]));
-        m = v > m ? v : m;  // NaN is skipped
+        if (v <= 3.4028235e38f) m = v > m ? v : m;  // NaN and Inf are skipped
+        else ++bad;
+        if (ref != nullptr && !(fabsf(static_cast<float>(ref[y * stride + x])) <= 3.4028235e38f))
+            ++bad;
+        if (poison != nullptr) poison[i] = 0;
     }
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
         const float q = __shfl_xor_sync(0xffffffffu, m, o);
         m = q > m ? q : m;
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
     }
-    if ((threadIdx.x & 31) == 0 && m > 0.0f)
-        atomicMax(reinterpret_cast<int *>(absmax), __float_as_int(fminf(m, 3.0e38f)));
+    if ((threadIdx.x & 31) == 0) {
+        if (m > 0.0f) atomicMax(reinterpret_cast<int *>(absmax), __float_as_int(m));
+        if (nonfinite != nullptr && bad) atomicAdd(nonfinite, bad);
+    }
+}
+
+template <typename T>
+__global__ void prep_kernel(typename AccOf<T>::type *num, typename AccOf<T>::type *den,
+                            const T *src, long long stride, int width, int height, float *absmax,
+                            const T *ref = nullptr, unsigned *nonfinite = nullptr,
+                            unsigned char *poison = nullptr)
+{
+    prep_plane<T>(num, den, src, ref, stride, width, height, absmax, nonfinite, poison,
+                  blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x,
+                  static_cast<long long>(gridDim.x) * blockDim.x);
 }
 
 }  // namespace bm3d
