@@ -303,6 +303,22 @@ int bm3d_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *basic,
                        const bm3d_stage_params *final_, float *const dst[],
                        const float *const src[], const int width[], const int height[],
                        const size_t stride[], int autotune, bm3d_batch **out);
+/* Final (Wiener) stage only, over `count` device planes (or, for the "3" form,
+ * images of three planes sharing the groups matched on ref[3 * i]) with the
+ * caller's reference planes ref[] in place of the basic estimates -- e.g. the
+ * learned pilot's estimates (bm3d_pilot_estimate). ref planes have the same
+ * size and row pitch as src. Otherwise as bm3d_batch_create /
+ * bm3d_batch3_create; results equal per-plane bm3d_stage (wiener = 1) /
+ * bm3d_stage3 with the same ref, bit for bit. Replaces looping the reference's
+ * BM3D_Final over images (source/BM3D.cpp:411-457). */
+int bm3d_batch_final_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *final_,
+                            float *const dst[], const float *const src[],
+                            const float *const ref[], const int width[], const int height[],
+                            const size_t stride[], int autotune, bm3d_batch **out);
+int bm3d_batch3_final_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *final_,
+                             float *const dst[], const float *const src[],
+                             const float *const ref[], const int width[], const int height[],
+                             const size_t stride[], int autotune, bm3d_batch **out);
 int bm3d_batch_run(bm3d_batch *batch, void *stream);
 /* Waits for `stream` and returns BM3D_ERR_CUDA (counts in bm3d_last_error of
  * the batch's context) if the batch kernels' consistency counter has moved
@@ -341,6 +357,13 @@ int bm3d_host_batch_run(bm3d_host_batch *batch, float *const dst[], const float 
                         const size_t stride[], int async, void *stream);
 int bm3d_host_batch_join(bm3d_host_batch *batch, void *stream);
 void bm3d_host_batch_destroy(bm3d_host_batch *batch);
+
+/* Runs the batch's pipeline once outside its graph, on `stream`, with CUDA
+ * events around the two persistent stage launches, and returns their device
+ * times in ms[0] (basic; 0 for a final-stage-only batch) and ms[1] (final);
+ * results as bm3d_batch_run. For measuring the kernels the graph replays. No
+ * counterpart in the reference. */
+int bm3d_batch_stage_times(bm3d_batch *batch, void *stream, float ms[2]);
 
 /* tile_x, tile_y, warps of the basic stage, then of the final stage. */
 int bm3d_batch_tuning(const bm3d_batch *batch, int out[6]);

@@ -42,7 +42,8 @@ EXPORTS = [
     "bm3d_batch_destroy", "bm3d_plane_int", "bm3d_stage_int", "bm3d_frame", "bm3d_stage_frame",
     "bm3d_full_many", "bm3d_batch3_create", "bm3d_host_batch_create", "bm3d_host_batch3_create",
     "bm3d_host_batch_run", "bm3d_host_batch_join", "bm3d_host_batch_destroy",
-    "bm3d_inject_alloc_failures",
+    "bm3d_inject_alloc_failures", "bm3d_batch_stage_times", "bm3d_batch_final_create",
+    "bm3d_batch3_final_create",
 ]
 
 
@@ -137,6 +138,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_host_batch_destroy.restype = None
     lib.bm3d_batch_run.argtypes = [vp, vp]
     lib.bm3d_batch_tuning.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    lib.bm3d_batch_stage_times.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_float)]
+    lib.bm3d_batch_final_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
+                                            ctypes.POINTER(vp)]
+    lib.bm3d_batch3_final_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
+                                             ctypes.POINTER(vp)]
     lib.bm3d_batch_destroy.argtypes = [vp]
     lib.bm3d_batch_destroy.restype = None
     quant = [ip, ip, ctypes.c_size_t, ip, ip, ip, ip, vp]   # w, h, stride, floor, neutral, ceil, mem, stream
@@ -413,7 +419,10 @@ class Batch:
     are filtered as three planes sharing luma groups (``bm3d_batch3_create``)."""
 
     def __init__(self, ctx: "Context", basic: Sequence[StageParams], final: Sequence[StageParams],
-                 dst: Sequence, src: Sequence, autotune: bool = True):
+                 dst: Sequence, src: Sequence, autotune: bool = True, ref: Optional[Sequence] = None):
+        """With `ref` (planes shaped like src), the batch runs the final stage
+        only, with those planes in place of the basic estimates
+        (``bm3d_batch_final_create``); `basic` is then ignored."""
         n = len(src)
         if not (len(basic) == len(final) == len(dst) == n) or n == 0:
             raise ValueError("one basic/final parameter set and dst per src image")
@@ -429,7 +438,9 @@ class Batch:
                 if len(shapes) != 1:
                     raise ValueError("the planes of an image must have one size")
         npl = 3 if three else 1
-        self._keep = (list(dst), list(src))
+        if ref is not None and three:
+            ref = [p for x in ref for p in x]
+        self._keep = (list(dst), list(src), None if ref is None else list(ref))
         infos_d = [_plane_info(d) for d in dst]
         infos_s = [_plane_info(x) for x in src]
         if any(i[1] != MEM_DEVICE for i in infos_d + infos_s):
@@ -448,9 +459,20 @@ class Batch:
         h = (ctypes.c_int * n)(*[i[3] for i in first])
         st = (ctypes.c_size_t * n)(*[i[4] for i in first])
         self.h = ctypes.c_void_p()
-        create = ctx.lib.bm3d_batch3_create if npl == 3 else ctx.lib.bm3d_batch_create
-        rc = create(ctx.h, n, pb, pf, vp(*[i[0] for i in infos_d]), vp(*[i[0] for i in infos_s]),
-                    w, h, st, int(autotune), ctypes.byref(self.h))
+        if ref is None:
+            create = ctx.lib.bm3d_batch3_create if npl == 3 else ctx.lib.bm3d_batch_create
+            rc = create(ctx.h, n, pb, pf, vp(*[i[0] for i in infos_d]),
+                        vp(*[i[0] for i in infos_s]), w, h, st, int(autotune),
+                        ctypes.byref(self.h))
+        else:
+            infos_r = [_plane_info(x) for x in ref]
+            if any(a[1:5] != b[1:5] for a, b in zip(infos_r, infos_s)):
+                raise ValueError("ref planes must match src in memory, size and pitch")
+            create = (ctx.lib.bm3d_batch3_final_create if npl == 3
+                      else ctx.lib.bm3d_batch_final_create)
+            rc = create(ctx.h, n, pf, vp(*[i[0] for i in infos_d]), vp(*[i[0] for i in infos_s]),
+                        vp(*[i[0] for i in infos_r]), w, h, st, int(autotune),
+                        ctypes.byref(self.h))
         ctx._check(rc, allow_copied=False)
         self.pixels = sum(i[2] * i[3] for i in first)  # image pixels (per plane for 3-plane images)
 
@@ -467,6 +489,16 @@ class Batch:
             import torch
             stream = torch.cuda.current_stream().cuda_stream
         self.ctx._check(self.ctx.lib.bm3d_batch_check(self.h, stream), allow_copied=False)
+
+    def stage_times(self, stream: Optional[int] = None):
+        """Device ms of the basic and final persistent stage launches, from one
+        eager run of the pipeline (``bm3d_batch_stage_times``)."""
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream
+        out = (ctypes.c_float * 2)()
+        self.ctx._check(self.ctx.lib.bm3d_batch_stage_times(self.h, stream, out))
+        return float(out[0]), float(out[1])
 
     def tuning(self):
         out = (ctypes.c_int * 6)()

@@ -124,6 +124,9 @@ struct bm3d_batch {
     DevBuf acc, basic, absmax, counters, planes_b, planes_f;
     DevBuf nonfinite, poison;  // per plane: non-finite input pixels; pixels they reached
     std::vector<size_t> poison_off;  // per plane: offset into poison (bytes)
+    // final-stage-only batches: the caller's reference planes (e.g. the learned
+    // pilot's estimates) stand in for the basic estimates; empty otherwise
+    std::vector<const float *> ext_ref;
     DevBuf bad;  // the kernels' consistency counter (bm3d_batch_check)
     int nq_b = 0, nq_f = 0;  // entries of planes_b / planes_f (planes each stage filters)
     StageBuild sb, sf;
@@ -153,6 +156,7 @@ int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuil
     for (int i = 0; i < B->n; ++i) {
         const bm3d_stage_params *p = wiener ? &B->pf[i] : &B->pb[i];
         if ((wiener ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
+        if (!wiener && !B->ext_ref.empty()) continue;  // no basic stage: references supplied
         StageArgs<float> a;
         std::memset(&a, 0, sizeof(a));
         a.bad = static_cast<unsigned long long *>(B->bad.ptr);
@@ -183,8 +187,10 @@ int build_stage(bm3d_batch *B, bool wiener, int tx, int ty, int warps, StageBuil
         for (int c = 0; c < npl; ++c) {
             const int k = i * npl + c;
             a.src[c] = B->src[k];
-            a.ref[c] = wiener ? static_cast<const float *>(B->basic.ptr) + B->basic_off[k]
-                              : B->src[k];
+            a.ref[c] = !wiener ? B->src[k]
+                       : !B->ext_ref.empty()
+                           ? B->ext_ref[k]
+                           : static_cast<const float *>(B->basic.ptr) + B->basic_off[k];
             a.num[c] = static_cast<long long *>(B->acc.ptr) + B->acc_off[k];
             a.den[c] = a.num[c] + static_cast<size_t>(a.width) * a.height;
         }
@@ -268,8 +274,10 @@ int launch_planes(bm3d_batch *B, const DevBuf &planes, bool prep, cudaStream_t s
     return BM3D_OK;
 }
 
-// The whole pipeline, enqueued on s (captured into the graph).
-int enqueue_batch(bm3d_batch *B, cudaStream_t s)
+// The whole pipeline, enqueued on s (captured into the graph). With `ev`,
+// events ev[0] / ev[1] bracket the basic stage's persistent launch and ev[2] /
+// ev[3] the final stage's (an eager run for timing; not used in the graph).
+int enqueue_batch(bm3d_batch *B, cudaStream_t s, cudaEvent_t *ev = nullptr)
 {
     bm3d_ctx *ctx = B->ctx;
     int rc;
@@ -278,7 +286,8 @@ int enqueue_batch(bm3d_batch *B, cudaStream_t s)
         for (int c = 0; c < B->npl; ++c) {
             const int k = i * B->npl + c;
             float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[k];
-            const bool b_off = B->gb[i] != Guard::Run || !(B->pb[i].sigma[c] > 0 || B->npl == 1);
+            const bool b_off = B->ext_ref.empty() &&
+                               (B->gb[i] != Guard::Run || !(B->pb[i].sigma[c] > 0 || B->npl == 1));
             const bool f_off = B->gf[i] != Guard::Run || !(B->pf[i].sigma[c] > 0 || B->npl == 1);
             if (b_off)
                 CK(ctx, cudaMemcpy2DAsync(bi, B->stride[i] * 4, B->src[k], B->stride[i] * 4,
@@ -291,10 +300,14 @@ int enqueue_batch(bm3d_batch *B, cudaStream_t s)
     CK(ctx, cudaMemsetAsync(B->absmax.ptr, 0, sizeof(float) * B->n * B->npl, s));
     CK(ctx, cudaMemsetAsync(B->nonfinite.ptr, 0, sizeof(unsigned) * B->n * B->npl, s));
     if ((rc = launch_planes(B, B->planes_b, true, s)) != BM3D_OK) return rc;
+    if (ev) CK(ctx, cudaEventRecord(ev[0], s));
     if ((rc = launch_batch_stage<false>(B, B->sb, counters, s)) != BM3D_OK) return rc;
+    if (ev) CK(ctx, cudaEventRecord(ev[1], s));
     if ((rc = launch_planes(B, B->planes_b, false, s)) != BM3D_OK) return rc;
     if ((rc = launch_planes(B, B->planes_f, true, s)) != BM3D_OK) return rc;
+    if (ev) CK(ctx, cudaEventRecord(ev[2], s));
     if ((rc = launch_batch_stage<true>(B, B->sf, counters + 1, s)) != BM3D_OK) return rc;
+    if (ev) CK(ctx, cudaEventRecord(ev[3], s));
     if ((rc = launch_planes(B, B->planes_f, false, s)) != BM3D_OK) return rc;
     return BM3D_OK;
 }
@@ -378,7 +391,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
                             const bm3d_stage_params *final_, float *const dst[],
                             const float *const src[], const int width[], const int height[],
                             const size_t stride[], int autotune, bm3d_batch **out,
-                            const int *force_tiling = nullptr)
+                            const int *force_tiling = nullptr,
+                            const float *const ext_ref[] = nullptr)
 {
     if (!ctx || !out || count < 1 || !basic || !final_ || !dst || !src || !width || !height ||
         !stride)
@@ -421,13 +435,15 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
         for (int c = 0; c < npl; ++c) {
             const int k = i * npl + c;
             if (!src[k] || !dst[k]) return fail(batch_fail(ctx, "bad plane"));
+            if (ext_ref && !ext_ref[k]) return fail(batch_fail(ctx, "bad reference plane"));
             B->src.push_back(src[k]);
             B->dst.push_back(dst[k]);
+            if (ext_ref) B->ext_ref.push_back(ext_ref[k]);
             B->acc_off.push_back(acc_total);
             B->basic_off.push_back(basic_total);
             B->poison_off.push_back(acc_total / 2);
             acc_total += 2 * static_cast<size_t>(width[i]) * height[i];
-            basic_total += stride[i] * height[i];
+            if (!ext_ref) basic_total += stride[i] * height[i];
         }
     }
     int rc;
@@ -444,6 +460,7 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
         std::vector<BatchPlane<float>> q;
         for (int i = 0; i < count; ++i) {
             if ((st ? B->gf[i] : B->gb[i]) != Guard::Run) continue;
+            if (!st && ext_ref) continue;  // no basic stage
             const bm3d_stage_params &pp = st ? final_[i] : basic[i];
             for (int c = 0; c < npl; ++c) {
                 if (npl > 1 && !(pp.sigma[c] > 0)) continue;  // plane left alone by the stage
@@ -453,7 +470,9 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
                 bp.den = bp.num + static_cast<size_t>(width[i]) * height[i];
                 bp.src = src[k];
                 // the final stage's Wiener weights come from the basic estimate
-                bp.ref = st ? static_cast<const float *>(B->basic.ptr) + B->basic_off[k] : nullptr;
+                bp.ref = !st ? nullptr
+                         : ext_ref ? ext_ref[k]
+                                   : static_cast<const float *>(B->basic.ptr) + B->basic_off[k];
                 bp.dst = st ? dst[k] : static_cast<float *>(B->basic.ptr) + B->basic_off[k];
                 bp.src_stride = static_cast<long long>(stride[i]);
                 bp.dst_stride = static_cast<long long>(stride[i]);
@@ -480,7 +499,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
     // planes whose basic stage is a copy must hold src before the final stage tunes
     for (int i = 0; i < count; ++i)
         for (int c = 0; c < npl; ++c) {
-            if (B->gb[i] == Guard::Run && (npl == 1 || basic[i].sigma[c] > 0)) continue;
+            if (ext_ref || (B->gb[i] == Guard::Run && (npl == 1 || basic[i].sigma[c] > 0)))
+                continue;
             const int k = i * npl + c;
             float *bi = static_cast<float *>(B->basic.ptr) + B->basic_off[k];
             e = cudaMemcpy2DAsync(bi, stride[i] * 4, src[k], stride[i] * 4, width[i] * 4, height[i],
@@ -491,8 +511,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
     if (e == cudaSuccess)
         e = cudaMemsetAsync(B->nonfinite.ptr, 0, sizeof(unsigned) * count * npl, B->cap);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemsetAsync"));
-    if ((rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap,
-                                force_tiling)) != BM3D_OK)
+    if (!ext_ref && (rc = tune_stage<false>(B, B->sb, B->planes_b, autotune != 0, B->cap,
+                                            force_tiling)) != BM3D_OK)
         return fail(rc);
     if ((rc = tune_stage<true>(B, B->sf, B->planes_f, autotune != 0, B->cap,
                                force_tiling ? force_tiling + 3 : nullptr)) != BM3D_OK)
@@ -533,6 +553,49 @@ extern "C" int bm3d_batch3_create(bm3d_ctx *ctx, int count, const bm3d_stage_par
 {
     return batch_create_any(ctx, 3, count, basic, final_, dst, src, width, height, stride,
                             autotune, out);
+}
+
+extern "C" int bm3d_batch_final_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *final_,
+                                       float *const dst[], const float *const src[],
+                                       const float *const ref[], const int width[],
+                                       const int height[], const size_t stride[], int autotune,
+                                       bm3d_batch **out)
+{
+    if (!ref) return BM3D_ERR_INVALID;
+    return batch_create_any(ctx, 1, count, final_, final_, dst, src, width, height, stride,
+                            autotune, out, nullptr, ref);
+}
+
+extern "C" int bm3d_batch3_final_create(bm3d_ctx *ctx, int count, const bm3d_stage_params *final_,
+                                        float *const dst[], const float *const src[],
+                                        const float *const ref[], const int width[],
+                                        const int height[], const size_t stride[], int autotune,
+                                        bm3d_batch **out)
+{
+    if (!ref) return BM3D_ERR_INVALID;
+    return batch_create_any(ctx, 3, count, final_, final_, dst, src, width, height, stride,
+                            autotune, out, nullptr, ref);
+}
+
+extern "C" int bm3d_batch_stage_times(bm3d_batch *B, void *stream, float ms[2])
+{
+    if (!B || !ms) return BM3D_ERR_INVALID;
+    bm3d_ctx *ctx = B->ctx;
+    CK(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int rc = BM3D_OK;
+    for (auto &e : ev)
+        if (rc == BM3D_OK && cudaEventCreate(&e) != cudaSuccess) rc = BM3D_ERR_CUDA;
+    if (rc == BM3D_OK) rc = enqueue_batch(B, s, ev);
+    if (rc == BM3D_OK && cudaEventSynchronize(ev[3]) != cudaSuccess) rc = BM3D_ERR_CUDA;
+    if (rc == BM3D_OK && (cudaEventElapsedTime(&ms[0], ev[0], ev[1]) != cudaSuccess ||
+                          cudaEventElapsedTime(&ms[1], ev[2], ev[3]) != cudaSuccess))
+        rc = BM3D_ERR_CUDA;
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    if (rc == BM3D_ERR_CUDA && ctx->err.empty()) ctx->err = "bm3d_batch_stage_times: event failure";
+    return rc;
 }
 
 extern "C" int bm3d_batch_run(bm3d_batch *B, void *stream)

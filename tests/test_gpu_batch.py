@@ -170,3 +170,56 @@ def test_batch_rejects_bad_planes(bm3d_lib):
         isp_mw_b200.Batch(ctx, [pb, other], [pf, pf], [torch.empty_like(ok)] * 2, [ok, ok])
     assert e.value.code == isp_mw_b200.BM3D_ERR_INVALID
     ctx.close()
+
+
+@pytest.mark.parametrize("planes", [1, 3])
+def test_final_only_batch_equals_per_plane_final(bm3d_lib, planes):
+    """A batch given reference planes (bm3d_batch_final_create /
+    bm3d_batch3_final_create: the pilot's estimates in the learned-pilot
+    pipeline) runs the final stage only and equals per-plane bm3d_stage
+    (wiener = 1) / bm3d_stage3 on the same reference, bit for bit; its stage
+    timing reports no basic stage."""
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    ctx = isp_mw_b200.Context(0)
+    shapes = [(130, 97), (64, 200), (181, 150)]
+    srcs, refs, dsts, pfs, want = [], [], [], [], []
+    for k, (h, w) in enumerate(shapes):
+        s255 = 12.0 + 9.0 * k
+        sp = [synth.sigma_param(s255)] * 3
+        pb = isp_mw_b200.stage_params_default("fast", False, sp)
+        pf = isp_mw_b200.stage_params_default("fast", True, sp)
+        src = [torch.from_numpy(synth.pair(h, w, s255, 500 + 3 * k + c)[1]).cuda()
+               for c in range(planes)]
+        # any reference plane will do; a smoothed copy of the basic estimate
+        basic = [torch.empty_like(x) for x in src]
+        if planes == 1:
+            ctx.stage(pb, False, basic[0], src[0])
+        else:
+            ctx.stage3(pb, False, basic, src)
+        ref = [(0.9 * b + 0.1 * x).contiguous() for b, x in zip(basic, src)]
+        out = [torch.empty_like(x) for x in src]
+        if planes == 1:
+            ctx.stage(pf, True, out[0], src[0], ref[0])
+        else:
+            ctx.stage3(pf, True, out, src, ref)
+        srcs.append(src if planes == 3 else src[0])
+        refs.append(ref if planes == 3 else ref[0])
+        dsts.append([torch.full_like(x, -1.0) for x in src] if planes == 3
+                    else torch.full_like(src[0], -1.0))
+        pfs.append(pf)
+        want.append(out)
+    batch = isp_mw_b200.Batch(ctx, pfs, pfs, dsts, srcs, autotune=False, ref=refs)
+    for _ in range(2):
+        batch.run()
+        torch.cuda.synchronize()
+        for k in range(len(shapes)):
+            got = dsts[k] if planes == 3 else [dsts[k]]
+            for c in range(planes):
+                assert torch.equal(got[c], want[k][c]), (k, c)
+    tb, tf = batch.stage_times()
+    assert tb < 0.05 and tf > 0.0
+    batch.check()
+    batch.close()
+    ctx.close()
