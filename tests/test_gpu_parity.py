@@ -140,12 +140,16 @@ def _oracle(oracle_mod, dtype=np.float32):
 # pixels by up to ~1e-2. The reference does the same to itself: run with its
 # transform evaluated in FP32 (three summation orders, oracle/dct_ref.h modes
 # 1-3) instead of the double-accumulating default, its own chained output moves
-# by up to 1.1e-2 at 1080p. Where the chained max-abs is above 1e-3 the GPU
-# chain must stay inside that self-divergence envelope: max-abs and the count
-# of pixels over 1e-3 within ENV_FACTOR x the largest of the three, and MSE
-# within ENV_FACTOR x the largest (PSNR within 3 dB). ENV_FACTOR allows for the
-# envelope being estimated from three samples of a chaotic quantity.
-ENV_FACTOR = 2.0
+# by up to 1.1e-2 at 1080p (CPU test in test_oracle.py; the envelope is also
+# measured here and reported). Such flips are rare events, so an envelope of a
+# few samples is no bound: where the chained max-abs is above 1e-3 the test
+# instead explains every excess pixel. Each pixel over 1e-3 must lie in the
+# footprint of a final-stage group that differs between the two chains, and
+# each such difference must be a near-tie: at every rank the two groups' keys
+# agree within NEAR_TIE relative, and a member only one chain keeps sits within
+# NEAR_TIE of the matching threshold.
+from chain_parity import NEAR_TIE, explain_chain_divergence  # noqa: E402
+
 ENV_MODES = (1, 2, 3)
 
 
@@ -154,8 +158,6 @@ def chain_envelope(oracle_mod, orc, b, f, noisy, rf0):
     FP32 transform rounding changes: max over modes 1-3 of max-abs and pixel
     count over 1e-3, and the largest MSE."""
     env = {"max_abs": 0.0, "n_over": 0, "mse": 0.0}
-    if orc.kind != "reference":
-        pytest.skip("the self-divergence envelope needs the compiled reference")
     try:
         for mode in ENV_MODES:
             oracle_mod.set_f32_transform_mode("reference", mode)
@@ -180,9 +182,9 @@ def test_against_oracle(ctx, oracle_mod, shape, s255, seed):
     Each stage is held to the strict bar on identical inputs: group lists
     (>= 99.9 %, exact in practice) and max-abs <= 1e-3 / >= 60 dB. The chained
     pipeline (final stage fed by our own basic estimate) against the
-    reference's own chain: max-abs <= 1e-3, or, where that is exceeded, inside
-    the reference's self-divergence envelope (ENV_FACTOR above), and always
-    >= 60 dB with >= 99.9 % of final groups matched. The error of the FP32
+    reference's own chain: max-abs <= 1e-3, or, where that is exceeded, every
+    excess pixel explained by a near-tie final-stage match flip (NEAR_TIE
+    above), and always >= 60 dB with >= 99.9 % of final groups matched. The error of the FP32
     result against an FP64 run of the same kernels is reported too."""
     from isp_mw_b200 import synth
     import isp_mw_b200
@@ -210,20 +212,22 @@ def test_against_oracle(ctx, oracle_mod, shape, s255, seed):
     rf = orc.stage(True, f.as_dict(), noisy, rb)
     full = np.empty_like(noisy)
     ctx.full(b, f, full, noisy)
-    frac = group_match(name + ":final_groups_chained", gf, orc.groups(True, f.as_dict(), rb),
-                       keys=False)
+    rgf = orc.groups(True, f.as_dict(), rb)
+    frac = group_match(name + ":final_groups_chained", gf, rgf, keys=False)
     d = np.abs(full.astype(np.float64) - rf)
     max_abs, n_over, mse = float(d.max()), int((d > MAX_ABS).sum()), float(np.mean(d * d))
     p_ref = psnr_to(full, rf)
     rec = dict(test=name + ":full_chained", max_abs=max_abs, psnr=p_ref, n_over=n_over,
                frac_over=float((d > MAX_ABS).mean()))
     if max_abs > MAX_ABS:
-        env = chain_envelope(oracle_mod, orc, b.as_dict(), f.as_dict(), noisy, rf)
-        rec.update(env_max_abs=env["max_abs"], env_n_over=env["n_over"], env_mse=env["mse"])
+        unexplained, worst, flips = explain_chain_divergence(d, gf, rgf, f)
+        rec.update(flipped_groups=flips, worst_key_gap=worst, unexplained=unexplained)
+        if orc.kind == "reference":
+            env = chain_envelope(oracle_mod, orc, b.as_dict(), f.as_dict(), noisy, rf)
+            rec.update(env_max_abs=env["max_abs"], env_n_over=env["n_over"], env_mse=env["mse"])
         report(**rec)
-        assert max_abs <= ENV_FACTOR * env["max_abs"], (name, max_abs, env)
-        assert n_over <= ENV_FACTOR * max(1, env["n_over"]), (name, n_over, env)
-        assert mse <= ENV_FACTOR * env["mse"], (name, mse, env)
+        assert unexplained == 0, (name, rec)
+        assert worst <= NEAR_TIE, (name, rec)
     else:
         report(**rec)
     assert p_ref >= MIN_PSNR and frac >= 0.999, (name, p_ref, frac)

@@ -183,3 +183,31 @@ def test_chain_self_divergence_under_fp32_transform(oracle_mod):
     finally:
         oracle_mod.set_f32_transform_mode("port", 0)
     assert worst > 1e-3, worst
+
+
+def test_chain_self_divergence_is_near_tie_match_flips(oracle_mod):
+    """The reference's own chain, run with its FP32 transform summed in
+    another order, exceeds 1e-3 only at pixels of final-stage groups that
+    changed between the two runs, and every change is a near-tie (keys within
+    1e-3 relative, in practice ~1e-6): the property the GPU chain is held to
+    where it exceeds the strict bar (tests/test_gpu_parity.py)."""
+    from chain_parity import NEAR_TIE, explain_chain_divergence
+    from isp_mw_b200 import synth
+    import isp_mw_b200
+    _, noisy = synth.pair(512, 512, 50.0, 6)
+    sp = [synth.sigma_param(50.0)] * 3
+    b = isp_mw_b200.stage_params_default("fast", False, sp)
+    f = isp_mw_b200.stage_params_default("fast", True, sp)
+    port = oracle_mod.backend("port", np.float32)
+    rb0, rf0 = port.full(b.as_dict(), f.as_dict(), noisy)
+    g0 = port.groups(True, f.as_dict(), rb0)
+    try:
+        oracle_mod.set_f32_transform_mode("port", 1)
+        rb, rf = port.full(b.as_dict(), f.as_dict(), noisy)
+        g1 = port.groups(True, f.as_dict(), rb)
+    finally:
+        oracle_mod.set_f32_transform_mode("port", 0)
+    d = np.abs(rf.astype(np.float64) - rf0)
+    assert (d > 1e-3).sum() > 0
+    unexplained, worst, flips = explain_chain_divergence(d, g1, g0, f)
+    assert unexplained == 0 and worst <= NEAR_TIE and 0 < flips <= 20, (unexplained, worst, flips)
