@@ -11,10 +11,14 @@ size exceeds the 126 MB L2.
 Our arm times K steps with CUDA events (barrier + synchronize on both sides,
 max over ranks) on device-resident planes -> ``value``; then the same steps
 through the C ABI with pinned host planes (host->device copy, filter,
-device->host copy inside the timed region) -> ``e2e``. The reference arm
+device->host copy inside the timed region) -> ``e2e``. The roofline is taken
+on the kernel the steps replay (the batch's persistent final-stage launch).
+After the headline, the default run adds the 64-plane mixed batch (batch64)
+and the 16-frame 4K YUV batch (yuv4k16) as extra keys. The reference arm
 (--impl reference) runs the reference's own CPU BM3D (oracle/_ref, compiled
 from the reference sources; the C restatement when that build is absent) on
-the host cores, one bounded sample of the workload per step.
+the host cores: each step is one wave of whole 1920x1080 planes of the sweep,
+one per thread (the reference is single-threaded per plane).
 Multi-GPU: every rank filters its own planes (independent images, no
 collective on the data path): weak scaling.
 """
@@ -40,6 +44,17 @@ W, H = 1920, 1080
 SIGMAS = (5.0, 10.0, 25.0, 50.0)
 RING = 4
 METRIC = "BM3D MP/s (basic+final, 1920x1080 luma, sigma sweep 5/10/25/50)"
+
+
+def sweep_config(world: int) -> dict:
+    """The headline workload's config, printed identically by both arms."""
+    return {"workload": "BM3D basic+final, fast profile, 4 x 1920x1080 f32 luma planes "
+                        "(sigma 5/10/25/50 per 255) per step",
+            "width": W, "height": H, "planes_per_step": len(SIGMAS), "profile": "fast",
+            "sigma_255": list(SIGMAS),
+            "l2": f"inputs rotate over {RING} sets ({RING * len(SIGMAS) * W * H * 4 / 1e6:.0f} MB) "
+                  "> 126 MB L2",
+            "parallelism": f"replicas x{world} (independent planes per GPU)"}
 
 
 def dist_env():
@@ -175,6 +190,72 @@ def batch_inputs(rank: int):
         _, noisy = synth.pair(h, w, float(sigmas[k]), 10_000 * (rank + 1) + k)
         planes.append(noisy)
     return planes, sigmas
+
+
+def _timed_batch_runs(batch, dev, steps, warmup):
+    import torch
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warmup):
+        batch.run(stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        batch.run(stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    return ev0.elapsed_time(ev1) / steps
+
+
+def measure_batch64(ctx, dev, rank, steps=10, warmup=3):
+    """configs[2] on this GPU: the 64 mixed-size planes in one batch (device
+    planes, CUDA-event timed steps)."""
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    planes, sigmas = batch_inputs(rank)
+    pbs, pfs = [], []
+    for s255 in sigmas:
+        sp = [synth.sigma_param(float(s255))] * 3
+        pbs.append(isp_mw_b200.stage_params_default("fast", False, sp))
+        pfs.append(isp_mw_b200.stage_params_default("fast", True, sp))
+    srcs = [torch.from_numpy(p).to(dev) for p in planes]
+    dsts = [torch.empty_like(x) for x in srcs]
+    batch = isp_mw_b200.Batch(ctx, pbs, pfs, dsts, srcs, autotune=True)
+    ms = _timed_batch_runs(batch, dev, steps, warmup)
+    mp = batch.pixels / 1e6
+    out = {"workload": "64 planes, W,H ~ U[256,2048], sigma ~ U[5,50]/255, basic+final in one "
+                       "persistent launch per stage from a CUDA graph (this GPU)",
+           "value": round(mp / (ms / 1e3), 3), "unit": "MP/s", "steps": steps,
+           "ms_per_step": round(ms, 4), "per_image_ms": round(ms / BATCH_N, 5),
+           "megapixels": round(mp, 3), "tiling": batch.tuning()}
+    batch.close()
+    return out
+
+
+def measure_yuv4k16(ctx, dev, rank, steps=3, warmup=2):
+    """configs[4] (plain batched form) on this GPU: 16 YUV 4:4:4 3840x2160
+    frames, luma groups reused for chroma, one batch."""
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    frames = yuv_inputs(rank)
+    sp = [synth.sigma_param(YUV_SIGMAS[c], c) for c in range(3)]
+    pb = isp_mw_b200.stage_params_default("fast", False, sp)
+    pf = isp_mw_b200.stage_params_default("fast", True, sp)
+    srcs = [[torch.from_numpy(p).to(dev) for p in f] for f in frames]
+    dsts = [[torch.empty_like(p) for p in f] for f in srcs]
+    batch = isp_mw_b200.Batch(ctx, [pb] * YUV_FRAMES, [pf] * YUV_FRAMES, dsts, srcs, autotune=True)
+    ms = _timed_batch_runs(batch, dev, steps, warmup)
+    mp = YUV_FRAMES * YUV_W * YUV_H / 1e6
+    out = {"workload": "16 frames of 3840x2160 YUV 4:4:4 (sigma 15/10/10), luma groups reused "
+                       "for chroma, basic+final in one persistent launch per stage from a CUDA "
+                       "graph (this GPU); MP counts frame pixels",
+           "value": round(mp / (ms / 1e3), 3), "unit": "MP/s", "steps": steps,
+           "ms_per_step": round(ms, 3), "per_frame_ms": round(ms / YUV_FRAMES, 4),
+           "tiling": batch.tuning()}
+    batch.close()
+    return out
 
 
 YUV_FRAMES, YUV_W, YUV_H = 16, 3840, 2160
@@ -401,11 +482,17 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
-# DRAM bytes per launch of the stage kernels on one 1920x1080 plane, from one
-# ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum); the command
-# and the full figures are in profiles/stage_kernel_{final,basic}_1080p_full.txt.
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per persistent
+# batch launch over the step's four 1920x1080 planes. Until a capture of the
+# batch kernel itself is committed these are four times the per-plane
+# stage_kernel captures (profiles/stage_kernel_{final,basic}_1080p_full.txt):
+# the batch kernel runs the same per-tile body over the same tiles.
 TRAFFIC_FINAL_1080P = 46.487e6 + 0.0e6
 TRAFFIC_BASIC_1080P = 37.286e6 + 0.004e6
+TRAFFIC_BATCH_FINAL_4X1080P = 4 * TRAFFIC_FINAL_1080P
+TRAFFIC_BATCH_BASIC_4X1080P = 4 * TRAFFIC_BASIC_1080P
+TRAFFIC_SOURCE = ("4 x the per-plane stage_kernel capture on one 1920x1080 plane, sigma 25 "
+                  "(profiles/stage_kernel_final_1080p_full.txt, stage_kernel_basic_1080p_full.txt)")
 
 
 def run_ours(args):
@@ -454,26 +541,38 @@ def run_ours(args):
     mp_step = len(SIGMAS) * W * H / 1e6
     value = world * mp_step * args.steps / (ms_max / 1e3)
 
-    # Kernel roofline: per-launch times of the final-stage kernel (the larger
-    # of the two) from events on its launch stream, over a separate pass.
+    # Kernel roofline, on the kernel the timed steps replay: the batch's
+    # persistent stage launches (four planes each), timed with CUDA events on
+    # their stream in eager runs of the same pipeline. Algorithmic FLOPs come
+    # from the kernels' own counters (group sizes, candidates) of per-plane
+    # runs on the same inputs, which produce the same groups.
     ctx.set_kernel_timing(True)
-    flops = {False: 0.0, True: 0.0}
-    for i in range(args.steps):
-        planes = dev_sets[i % RING]
+    flops_set = []
+    for r in range(RING):
+        fl = {False: 0.0, True: 0.0}
         for k in range(len(SIGMAS)):
             b = torch.empty_like(outs[k])
-            ctx.stage(params[k][0], False, b, planes[k])
-            flops[False] += algorithmic_flops(ctx.last_stats(), False)
-            ctx.stage(params[k][1], True, outs[k], planes[k], b)
-            flops[True] += algorithmic_flops(ctx.last_stats(), True)
-    t_basic, n_basic = ctx.kernel_time(False)
+            ctx.stage(params[k][0], False, b, dev_sets[r][k])
+            fl[False] += algorithmic_flops(ctx.last_stats(), False)
+            ctx.stage(params[k][1], True, outs[k], dev_sets[r][k], b)
+            fl[True] += algorithmic_flops(ctx.last_stats(), True)
+        flops_set.append(fl)
+    t_basic, n_basic = ctx.kernel_time(False)  # per-plane stage_kernel launches (reported beside)
     t_final, n_final = ctx.kernel_time(True)
     ctx.set_kernel_timing(False)
+    reps = max(RING, min(args.steps, 40))
+    bt = {False: 0.0, True: 0.0}
+    bfl = {False: 0.0, True: 0.0}
+    for i in range(reps):
+        tb, tf = batches[i % RING].stage_times(stream.cuda_stream)
+        bt[False] += tb
+        bt[True] += tf
+        bfl[False] += flops_set[i % RING][False]
+        bfl[True] += flops_set[i % RING][True]
     clk.__exit__(None, None, None)
-    dom = True if t_final >= t_basic else False
-    t_dom, n_dom = (t_final, n_final) if dom else (t_basic, n_basic)
-    per_launch_ms = t_dom / max(1, n_dom)
-    achieved = flops[dom] / max(1, n_dom) / (per_launch_ms / 1e3) / 1e12
+    dom = bt[True] >= bt[False]
+    per_launch_ms = bt[dom] / reps
+    achieved = bfl[dom] / reps / (per_launch_ms / 1e3) / 1e12
     clocks = clk.summary(m0, m1)
     sm_max = clocks.get("sm_max_mhz") or 1965.0
     peak_fp32 = 148 * 128 * 2 * sm_max * 1e6 / 1e12
@@ -507,6 +606,14 @@ def run_ours(args):
     e_ms = shard.max_over_ranks(max(ev0.elapsed_time(ev1), e_wall), dev)
     e2e_value = world * mp_step * args.steps / (e_ms / 1e3)
 
+    # configs[2] and configs[4] as extra keys, measured after the headline
+    # (outside its timed region): the 64-plane mixed batch and the 16-frame
+    # 4K YUV batch, device-resident, CUDA-event timed
+    extras = {}
+    if not args.no_extras:
+        extras["batch64"] = measure_batch64(ctx, dev, rank, steps=10, warmup=3)
+        extras["yuv4k16"] = measure_yuv4k16(ctx, dev, rank, steps=3, warmup=2)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(host_sets[0], budget_s=args.cpu_seconds)
@@ -517,7 +624,7 @@ def run_ours(args):
             hbm_peak, hbm_source = float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
         else:  # an earlier STREAM-style copy measurement on these B200s
             hbm_peak, hbm_source = 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
-        traffic = TRAFFIC_FINAL_1080P if dom else TRAFFIC_BASIC_1080P
+        traffic = (TRAFFIC_BATCH_FINAL_4X1080P if dom else TRAFFIC_BATCH_BASIC_4X1080P)
         line = {
             "metric": METRIC,
             "value": round(value, 3),
@@ -531,44 +638,43 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic (seeded piecewise-smooth planes + Gaussian noise)",
-            "config": {"workload": "BM3D basic+final, fast profile, 4 x 1920x1080 f32 luma "
-                                   "planes (sigma 5/10/25/50 per 255) per step, one batched "
-                                   "graph replay (persistent basic + final launches) per step",
-                       "width": W, "height": H, "planes_per_step": len(SIGMAS),
-                       "profile": "fast", "sigma_255": list(SIGMAS),
-                       "l2": f"inputs rotate over {RING} sets ({RING * len(SIGMAS) * W * H * 4 / 1e6:.0f} MB) "
-                             "> 126 MB L2",
-                       "tiling": batches[0].tuning(),
-                       "parallelism": f"replicas x{world} (independent planes per GPU)"},
+            "config": sweep_config(world),
+            "step": "one batched graph replay (persistent basic + final launches over the 4 "
+                    "planes) per step",
+            "tiling": batches[0].tuning(),
             "e2e": {"value": round(e2e_value, 3), "unit": "MP/s",
                     "h2d_bytes_per_step": len(SIGMAS) * W * H * 4,
                     "d2h_bytes_per_step": len(SIGMAS) * W * H * 4},
             "gpu_launches": args.steps * 6,
             "roofline": {
                 "bound": "fp32",
-                "kernel": "stage_kernel (final)" if dom else "stage_kernel (basic)",
+                "kernel": "batch_stage_kernel (final)" if dom else "batch_stage_kernel (basic)",
+                "launch": "one persistent launch over the 4 planes of a step, the kernel the "
+                          "timed steps replay; CUDA events on its stream in eager runs of the "
+                          "same pipeline",
                 "achieved": round(achieved, 3),
                 "peak": round(peak_fp32, 2),
                 "unit": "TFLOP/s",
                 "frac": round(achieved / peak_fp32, 4),
                 "traffic": traffic,
-                "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, one "
-                                  "ncu capture of the same kernel on one 1920x1080 plane, "
-                                  "sigma 25 (profiles/stage_kernel_"
-                                  + ("final" if dom else "basic") + "_1080p_full.txt)",
+                "traffic_source": TRAFFIC_SOURCE,
                 "peak_source": "nominal FP32 FMA rate 148 SM x 128 lanes x 2 flop x max SM clock "
                                "(MEASURED_PEAKS.json has no FP32 SIMT figure)",
                 "per_launch_ms": round(per_launch_ms, 4),
-                "algorithmic_gflop_per_launch": round(flops[dom] / max(1, n_dom) / 1e9, 3),
+                "algorithmic_gflop_per_launch": round(bfl[dom] / reps / 1e9, 3),
                 "hbm_peak_gbs": hbm_peak,
                 "hbm_peak_source": hbm_source,
                 "dram_gbs": round(traffic / (per_launch_ms / 1e3) / 1e9, 1),
                 "dram_frac": round(traffic / (per_launch_ms / 1e3) / 1e9 / hbm_peak, 4),
             },
+            "batch_stage_ms_per_launch": {"basic": round(bt[False] / reps, 4),
+                                          "final": round(bt[True] / reps, 4)},
             "stage_ms_per_plane": {"basic": round(t_basic / max(1, n_basic), 4),
-                                   "final": round(t_final / max(1, n_final), 4)},
+                                   "final": round(t_final / max(1, n_final), 4),
+                                   "kernel": "stage_kernel, one launch per plane"},
             "clocks": clocks,
         }
+        line.update(extras)
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
@@ -604,12 +710,17 @@ def _cpu_tasks(planes, rows: int, count: int = 0):
     return tasks
 
 
+def _plane_tasks(planes, count: int):
+    """`count` whole-plane tasks cycling over the step's planes."""
+    return [(k % len(planes), planes[k % len(planes)]) for k in range(count)]
+
+
 def _run_cpu(backend, tasks, cores):
     px = sum(t[1].size for t in tasks)
 
     def one(t):
-        k, strip = t
-        backend.full(_PARAMS[k][0], _PARAMS[k][1], strip)
+        k, plane = t
+        backend.full(_PARAMS[k][0], _PARAMS[k][1], plane)
 
     t0 = time.perf_counter()
     with cf.ThreadPoolExecutor(max_workers=cores) as ex:
@@ -635,23 +746,46 @@ def _init_params():
                             isp_mw_b200.stage_params_default("fast", True, sp).as_dict()))
 
 
+def _bm_only(backend, plane, k):
+    """Single-thread seconds of the reference's block matching alone over the
+    basic and final scans of one plane (BM3D_Base::BlockMatching,
+    source/BM3D.cpp:221-236, through the group dump), against the whole
+    basic + final on that plane."""
+    b, f = _PARAMS[k]
+    t0 = time.perf_counter()
+    basic = backend.stage(False, b, plane)
+    t1 = time.perf_counter()
+    backend.stage(True, f, plane, basic)
+    t2 = time.perf_counter()
+    backend.groups(False, b, plane)
+    t3 = time.perf_counter()
+    backend.groups(True, f, basic)
+    t4 = time.perf_counter()
+    return {"plane": f"1920x1080 sigma {SIGMAS[k]:g}", "threads": 1,
+            "basic_s": round(t1 - t0, 3), "final_s": round(t2 - t1, 3),
+            "bm_basic_s": round(t3 - t2, 3), "bm_final_s": round(t4 - t3, 3),
+            "bm_fraction": round((t4 - t2) / (t2 - t0), 3)}
+
+
 def cpu_baseline(planes, budget_s: float = 20.0):
-    """The reference's CPU BM3D on this host's cores, on a bounded sample:
-    horizontal strips of the step's planes, one strip per task."""
+    """The reference's CPU BM3D on this host's cores, on a bounded sample of
+    the workload: whole 1920x1080 planes of the step (basic + final each, the
+    reference being single-threaded per plane), one plane per core at a time,
+    waves until about `budget_s`; plus the block-matching share of one plane."""
     kind, backend = _ref_backend()
     _init_params()
     cores = len(os.sched_getaffinity(0))
-    # size the sample: strips of 120 rows; take as many as fit the budget
-    tasks = _cpu_tasks(planes, 120)
-    px1, t1 = _run_cpu(backend, tasks[:cores], cores)  # calibration
-    rate = px1 / t1
-    n = max(cores, int(budget_s * rate / tasks[0][1].size) // cores * cores)
-    tasks = _cpu_tasks(planes, 120, n)[:n]
-    px, t = _run_cpu(backend, tasks, cores)
+    px, t = _run_cpu(backend, _plane_tasks(planes, cores), cores)  # first wave calibrates
+    waves = max(1, int(round(budget_s / t)))
+    if waves > 1:
+        px2, t2 = _run_cpu(backend, _plane_tasks(planes, cores * (waves - 1)), cores)
+        px, t = px + px2, t + t2
+    n = cores * waves
     return {"value": round(px / t / 1e6, 4), "unit": "MP/s", "cores": cores, "kind": kind,
-            "sample": f"{n} strips of 1920x120 cycled over the step's 4 planes (sigma sweep), "
-                      f"basic+final fast profile, {px / 1e6:.2f} MP in {t:.1f} s on {cores} "
-                      f"threads, one strip per task"}
+            "sample": f"{n} whole 1920x1080 planes cycled over the step's 4 planes (sigma "
+                      f"sweep), basic+final fast profile, {px / 1e6:.1f} MP in {t:.1f} s, one "
+                      f"plane per thread at a time on {cores} threads",
+            "bm_only": _bm_only(backend, planes[2], 2)}
 
 
 def run_reference(args):
@@ -662,18 +796,28 @@ def run_reference(args):
     _init_params()
     cores = len(os.sched_getaffinity(0))
     planes = make_inputs(0)[0]
-    tasks = _cpu_tasks(planes, 120)
-    # calibrate: one wave of `cores` strips in parallel; a step is as many
-    # waves as fit so that warm-up + timed steps take about 150 s
-    _, t1 = _run_cpu(backend, tasks[:cores], cores)
-    budget = 150.0 / max(1, args.steps + args.warmup)
-    per_step = cores * max(1, min(32, int(budget / max(1e-6, t1))))
-    tasks = _cpu_tasks(planes, 120, per_step)
-    for i in range(args.warmup):
-        _run_cpu(backend, tasks[:per_step], cores)
+    # a step is one wave: `cores` whole planes of the sweep, one per thread.
+    # The first warm-up wave calibrates; when the run would not end within
+    # about five minutes, each step is a wave of strips instead (the ratio of
+    # whole-plane to strip rate measured on the same cores is reported).
+    tasks = _plane_tasks(planes, cores)
+    px0, t0 = _run_cpu(backend, tasks, cores)
+    sample = f"one wave per step: {cores} whole 1920x1080 planes of the sweep, one per thread"
+    strip_ratio = None
+    if (args.steps + max(0, args.warmup - 1)) * t0 > 300.0:
+        strips = _cpu_tasks(planes, 120)
+        _, ts = _run_cpu(backend, strips[:cores], cores)
+        per_step = cores * max(1, int(300.0 / max(1, args.steps + args.warmup) / max(1e-6, ts)))
+        tasks = _cpu_tasks(planes, 120, per_step)[:per_step]
+        spx, st = _run_cpu(backend, tasks, cores)
+        strip_ratio = round((px0 / t0) / (spx / st), 4)
+        sample = (f"{per_step} strips of 1920x120 per step (whole planes would exceed the time "
+                  f"budget), on {cores} threads")
+    for _ in range(max(0, args.warmup - 1)):
+        _run_cpu(backend, tasks, cores)
     tot_px, tot_t = 0, 0.0
-    for i in range(args.steps):
-        px, t = _run_cpu(backend, tasks[:per_step], cores)
+    for _ in range(args.steps):
+        px, t = _run_cpu(backend, tasks, cores)
         tot_px += px
         tot_t += t
     value = tot_px / tot_t / 1e6
@@ -691,15 +835,14 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded piecewise-smooth planes + Gaussian noise)",
-        "config": {"workload": "BM3D basic+final, fast profile, 1920x1080 f32 luma planes "
-                               "(sigma 5/10/25/50 per 255)", "width": W, "height": H,
-                   "profile": "fast", "sigma_255": list(SIGMAS)},
+        "config": sweep_config(world),
         "cpu_baseline": {"value": round(value, 4), "unit": "MP/s", "cores": cores, "kind": kind,
-                         "sample": f"{per_step} strips of 1920x120 per step cycled over the 4 "
-                                   f"planes of the sigma sweep, on {cores} threads"},
+                         "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "MP/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if strip_ratio is not None:
+        line["cpu_baseline"]["whole_over_strip_rate"] = strip_ratio
     print(json.dumps(line), flush=True)
 
 
@@ -710,6 +853,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batch64 / yuv4k16 figures the default run adds")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--workload", default="sweep1080", choices=["sweep1080", "batch64", "yuv4k16"],
                     help="sweep1080: 4 x 1920x1080 sigma sweep (headline); batch64: 64 uneven "
