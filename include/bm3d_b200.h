@@ -380,6 +380,77 @@ int bm3d_set_kernel_timing(bm3d_ctx *ctx, int on);
  * recorded launches to finish. */
 int bm3d_kernel_time(bm3d_ctx *ctx, int wiener, double *ms, long long *launches);
 
+/* ---- Learned pilot ------------------------------------------------------
+ * A small convolutional network that stands in for the basic estimate feeding
+ * the final (Wiener) stage: 8 layers of 3 x 3 convolutions, 48 channels, ReLU,
+ * BF16 weights and activations with FP32 accumulation (tensor cores for the
+ * 48 -> 48 layers), inputs the noisy plane and a constant noise-level plane
+ * (true noise std on the 0-1 scale), output noisy + predicted residual. It is
+ * trained (bm3d_pilot_train_step, Adam on FP32 master weights) to regress the
+ * basic estimate this library computes. No counterpart in the reference,
+ * whose final stage takes the basic estimate as `ref`
+ * (BM3D_Final::CollaborativeFilter, source/BM3D.cpp:411-457); the plain
+ * basic estimate stays available and is what the pilot is judged against. */
+typedef struct bm3d_pilot bm3d_pilot;
+
+/* Number of FP32 parameters (weights and biases of the eight layers). */
+int bm3d_pilot_param_count(void);
+
+/* A pilot on the context's device, He-initialised from `seed`. */
+int bm3d_pilot_create(bm3d_ctx *ctx, unsigned long long seed, bm3d_pilot **out);
+void bm3d_pilot_destroy(bm3d_pilot *p);
+
+/* Parameters as one host FP32 vector of bm3d_pilot_param_count() values:
+ * W1 [48][2][3][3], b1 [48], then for layers 2..7 W [48][48][3][3] and b
+ * [48], then W8 [1][48][3][3] and b8 (PyTorch Conv2d weight order). Setting
+ * them resets the optimiser state. */
+int bm3d_pilot_set_params(bm3d_pilot *p, const float *host, int count);
+int bm3d_pilot_get_params(bm3d_pilot *p, float *host, int count);
+/* The loss gradient of the last bm3d_pilot_train_step, same order. */
+int bm3d_pilot_get_grad(bm3d_pilot *p, float *host, int count);
+
+/* Checkpoint file: parameters, optimiser moments and step count. */
+int bm3d_pilot_save(bm3d_pilot *p, const char *path);
+int bm3d_pilot_load(bm3d_pilot *p, const char *path);
+
+/* dst = pilot(src) for `count` planes of width x height, row pitch `stride`,
+ * planes `img_stride` elements apart; sigma[i] = true noise std (0-1 scale)
+ * of plane i (host memory for BM3D_MEM_HOST, device otherwise). */
+int bm3d_pilot_estimate(bm3d_pilot *p, float *dst, const float *src, int count, int width,
+                        int height, size_t stride, size_t img_stride, const float *sigma, int mem,
+                        void *stream);
+
+/* One Adam step on `count` crops of height x width in DEVICE memory, stored
+ * back to back (pitch = width): noisy inputs, targets (the basic estimates)
+ * and per-crop noise std `sigma` (device). Loss = mean squared error of the
+ * output against the target; written to *loss (after a synchronisation) when
+ * loss is not NULL. */
+int bm3d_pilot_train_step(bm3d_pilot *p, int count, int height, int width, const float *noisy,
+                          const float *target, const float *sigma, float lr, double *loss,
+                          void *stream);
+
+/* Pilot then final stage on one plane: the final (Wiener) stage takes the
+ * pilot's estimate as its reference in place of the basic estimate. The
+ * pilot's noise-level input is final_->sigma[0] with the reference's OPP
+ * luma scaling applied (include/BM3D.h:246-253). Replaces, for this
+ * pipeline, the basic -> final sequence of BM3D::process_Plane_FL
+ * (source/BM3D.cpp:464-472). */
+int bm3d_pilot_full(bm3d_ctx *ctx, bm3d_pilot *p, const bm3d_stage_params *final_, float *dst,
+                    const float *src, int width, int height, size_t stride, float value_range,
+                    int mem, void *stream);
+
+/* Layer-level entry points of the pilot's tensor-core kernels, on DEVICE
+ * memory (BF16 activations [n][h][w][48]): one 48 -> 48 3 x 3 convolution with
+ * padding 1 and FP32 weights [48][48][3][3] (mode 0: + bias, ReLU; mode 1:
+ * + bias; mode 2: the data gradient -- the transposed, flipped convolution --
+ * kept where aux > 0), and the weight / bias gradients of such a layer from
+ * its input x and the gradient g at its output. Both synchronise `stream`.
+ * For tests and tools; no counterpart in the reference. */
+int bm3d_pilot_conv48(bm3d_ctx *ctx, int n, int h, int w, const void *x, const float *weight,
+                      const float *bias, const void *aux, int mode, void *y, void *stream);
+int bm3d_pilot_wgrad48(bm3d_ctx *ctx, int n, int h, int w, const void *x, const void *g, float *dw,
+                       float *db, void *stream);
+
 /* Fault injection for callers' error paths: the next `count` device buffer
  * allocations of contexts and batches fail as if cudaMalloc had run out of
  * memory (the call returns BM3D_ERR_NOMEM, nothing is left half-built, and

@@ -44,6 +44,10 @@ EXPORTS = [
     "bm3d_host_batch_run", "bm3d_host_batch_join", "bm3d_host_batch_destroy",
     "bm3d_inject_alloc_failures", "bm3d_batch_stage_times", "bm3d_batch_final_create",
     "bm3d_batch3_final_create",
+    "bm3d_pilot_param_count", "bm3d_pilot_create", "bm3d_pilot_destroy", "bm3d_pilot_set_params",
+    "bm3d_pilot_get_params", "bm3d_pilot_get_grad", "bm3d_pilot_save", "bm3d_pilot_load",
+    "bm3d_pilot_estimate", "bm3d_pilot_train_step", "bm3d_pilot_full", "bm3d_pilot_conv48",
+    "bm3d_pilot_wgrad48",
 ]
 
 
@@ -126,6 +130,23 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                        ctypes.c_float, vp]
     lib.bm3d_noalloc_check.argtypes = [vp]
     lib.bm3d_inject_alloc_failures.argtypes = [ip]
+    lib.bm3d_pilot_param_count.argtypes = []
+    lib.bm3d_pilot_create.argtypes = [vp, ctypes.c_ulonglong, ctypes.POINTER(vp)]
+    lib.bm3d_pilot_destroy.argtypes = [vp]
+    lib.bm3d_pilot_destroy.restype = None
+    lib.bm3d_pilot_set_params.argtypes = [vp, vp, ip]
+    lib.bm3d_pilot_get_params.argtypes = [vp, vp, ip]
+    lib.bm3d_pilot_get_grad.argtypes = [vp, vp, ip]
+    lib.bm3d_pilot_save.argtypes = [vp, cp]
+    lib.bm3d_pilot_load.argtypes = [vp, cp]
+    lib.bm3d_pilot_estimate.argtypes = [vp, vp, vp, ip, ip, ip, ctypes.c_size_t, ctypes.c_size_t,
+                                        vp, ip, vp]
+    lib.bm3d_pilot_train_step.argtypes = [vp, ip, ip, ip, vp, vp, vp, ctypes.c_float,
+                                          ctypes.POINTER(ctypes.c_double), vp]
+    lib.bm3d_pilot_full.argtypes = [vp, vp, sp, vp, vp, ip, ip, ctypes.c_size_t, ctypes.c_float,
+                                    ip, vp]
+    lib.bm3d_pilot_conv48.argtypes = [vp, ip, ip, ip, vp, vp, vp, vp, ip, vp, vp]
+    lib.bm3d_pilot_wgrad48.argtypes = [vp, ip, ip, ip, vp, vp, vp, vp, vp]
     lib.bm3d_batch_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
                                       ctypes.POINTER(vp)]
     lib.bm3d_batch3_create.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, vp, ip,
@@ -731,3 +752,104 @@ class BM3D:
         else:
             dst = _empty_like(src)
         return self.process(dst, src, ref, value_range)
+
+
+class Pilot:
+    """``bm3d_pilot``: the learned pilot (8 layers of 3 x 3 convolutions, 48
+    channels, BF16 with FP32 accumulation on the tensor cores) that stands in
+    for the basic estimate feeding the final (Wiener) stage. Training data and
+    the loop live in ``isp_mw_b200.pilot``."""
+
+    def __init__(self, ctx: "Context", seed: int = 0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.h = ctypes.c_void_p()
+        ctx._check(self.lib.bm3d_pilot_create(ctx.h, int(seed), ctypes.byref(self.h)),
+                   allow_copied=False)
+        self.count = int(self.lib.bm3d_pilot_param_count())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bm3d_pilot_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.count, np.float32)
+        self.ctx._check(self.lib.bm3d_pilot_get_params(self.h, out.ctypes.data, self.count))
+        return out
+
+    def grad(self) -> np.ndarray:
+        out = np.empty(self.count, np.float32)
+        self.ctx._check(self.lib.bm3d_pilot_get_grad(self.h, out.ctypes.data, self.count))
+        return out
+
+    def set_params(self, values: np.ndarray):
+        v = np.ascontiguousarray(values, dtype=np.float32)
+        if v.size != self.count:
+            raise ValueError(f"expected {self.count} parameters")
+        self.ctx._check(self.lib.bm3d_pilot_set_params(self.h, v.ctypes.data, self.count))
+
+    def save(self, path: str):
+        self.ctx._check(self.lib.bm3d_pilot_save(self.h, path.encode()))
+
+    def load(self, path: str):
+        self.ctx._check(self.lib.bm3d_pilot_load(self.h, path.encode()))
+
+    def estimate(self, dst, src, sigma):
+        """dst = pilot(src): one plane (2-D) or a stack of planes (3-D, numpy
+        host arrays or contiguous CUDA tensors); sigma = true noise std (0-1
+        scale), one per plane."""
+        if _is_torch(src):
+            import torch
+            if src.dim() == 2:
+                src, dst = src.unsqueeze(0), dst.unsqueeze(0)
+            n, h, w = src.shape
+            if not (src.is_contiguous() and dst.is_contiguous()):
+                raise ValueError("pilot planes must be contiguous")
+            sig = torch.as_tensor(np.broadcast_to(np.asarray(sigma, np.float32), (n,)).copy(),
+                                  device=src.device)
+            stream = torch.cuda.current_stream(src.device)
+            rc = self.lib.bm3d_pilot_estimate(self.h, dst.data_ptr(), src.data_ptr(), n, w, h, w,
+                                              h * w, sig.data_ptr(), MEM_DEVICE, stream.cuda_stream)
+            self.ctx._check(rc)
+            stream.synchronize()
+            return dst
+        s3 = np.ascontiguousarray(src, np.float32)
+        if s3.ndim == 2:
+            s3 = s3[None]
+        n, h, w = s3.shape
+        out = np.empty_like(s3)
+        sig = np.ascontiguousarray(np.broadcast_to(np.asarray(sigma, np.float32), (n,)))
+        rc = self.lib.bm3d_pilot_estimate(self.h, out.ctypes.data, s3.ctypes.data, n, w, h, w,
+                                          h * w, sig.ctypes.data, MEM_HOST, None)
+        self.ctx._check(rc)
+        dst[...] = out.reshape(dst.shape)
+        return dst
+
+    def train_step(self, noisy, target, sigma, lr: float, want_loss: bool = True):
+        """One Adam step on CUDA tensors noisy / target [n, h, w] and sigma [n];
+        returns the mean squared error (before the step) when want_loss."""
+        import torch
+        n, h, w = noisy.shape
+        loss = ctypes.c_double(0.0)
+        rc = self.lib.bm3d_pilot_train_step(
+            self.h, n, h, w, noisy.data_ptr(), target.data_ptr(), sigma.data_ptr(),
+            ctypes.c_float(lr), ctypes.byref(loss) if want_loss else None,
+            torch.cuda.current_stream(noisy.device).cuda_stream)
+        self.ctx._check(rc)
+        return loss.value if want_loss else None
+
+    def full(self, final: StageParams, dst, src, value_range: float = 1.0) -> int:
+        """Pilot, then the final stage with the pilot's estimate as reference
+        (``bm3d_pilot_full``)."""
+        dp, mem, w, h, stride, _ = _plane_info(dst)
+        spp, *_ = _plane_info(src)
+        rc = self.lib.bm3d_pilot_full(self.ctx.h, self.h, ctypes.byref(final), dp, spp, w, h,
+                                      stride, value_range, mem, _stream_of(dst))
+        return self.ctx._check(rc)

@@ -1,0 +1,746 @@
+// Kernels of the learned pilot: an 8-layer 3 x 3 convolutional network with
+// 48 hidden channels, ReLU, BF16 weights and activations and FP32
+// accumulation, whose output (noisy + predicted residual) stands in for the
+// BM3D basic estimate that feeds the final (Wiener) stage.
+//
+// Layer 1 (2 -> 48: the noisy plane and a noise-level plane) and layer 8
+// (48 -> 1) are small and run on the FP32 pipes. Layers 2-7 (48 -> 48, 98 %
+// of the arithmetic) and their backward passes run on the tensor cores
+// (tcgen05, accumulators in tensor memory).
+//
+// Activations are BF16, NHWC with 48 channels (96 bytes per pixel), images
+// stored back to back. A 48 -> 48 layer works on tiles of 16 x 8 output pixels
+// (the MMA's M = 128). The tile's input, with a one-pixel halo, sits in shared
+// memory as three row-shifted copies (dy = -1, 0, +1), each 18 columns of
+// [channel / 8][row (8)][channel % 8] BF16 -- 768 bytes per column. In that
+// layout the 128 x 48 operand of tap (dy, dx) starts dx columns into copy dy
+// (K-major, no swizzle: LBO = 128 bytes between 8-channel groups, SBO = 768
+// bytes between 8-pixel columns), so each tap is three MMAs of K = 16 with no
+// data movement. The same buffers, read as MN-major operands (LBO = 768,
+// SBO = 128), give the weight gradient's pixel-reduction MMAs.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "pilot_tc.cuh"
+
+namespace pilot {
+
+constexpr int kC = 48;                          // hidden channels
+constexpr int kTX = 16, kTY = 8;                // output tile (128 pixels)
+constexpr int kColBytes = kTY * kC * 2;         // 768: one tile column
+constexpr int kCols = kTX + 2;                  // 18 input columns per row-shifted copy
+constexpr int kCopyBytes = kCols * kColBytes;   // 13824
+constexpr int kTileBytes = 3 * kCopyBytes;      // 41472: the three copies
+constexpr int kTileChunks = kTileBytes / 16;    // 2592 16-byte chunks
+constexpr int kTapBytes = kC * kC * 2;          // 4608: one tap, [co / 8][ci / 8][co % 8][ci % 8]
+constexpr int kWeightBytes = 9 * kTapBytes;     // 41472
+constexpr int kConvThreads = 128;               // four warps: one per 32 TMEM lanes
+constexpr int kAccCols = 64;                    // TMEM columns per accumulator (48 used)
+constexpr uint32_t kWaitLimit = 1u << 24;       // polls before a wait gives up
+constexpr uint32_t kIdescFwd = instr_desc_bf16(128, kC, false, false);
+
+// Parameters: W1 48x2x3x3 + b1, six 48x48x3x3 + biases, W8 1x48x3x3 + b8.
+constexpr int kW1 = kC * 2 * 9, kWmid = kC * kC * 9, kW8 = kC * 9;
+constexpr int kOffB1 = kW1;
+constexpr int kOffMid = kOffB1 + kC;  // layer l (2..7): W at kOffMid + (l - 2) (kWmid + kC)
+constexpr int kOffW8 = kOffMid + 6 * (kWmid + kC);
+constexpr int kOffB8 = kOffW8 + kW8;
+constexpr int kParams = kOffB8 + 1;
+__host__ __device__ constexpr int off_w(int layer) { return kOffMid + (layer - 2) * (kWmid + kC); }
+__host__ __device__ constexpr int off_b(int layer) { return off_w(layer) + kWmid; }
+
+enum ConvMode { kBiasRelu = 0, kBias = 1, kMaskPrev = 2 };
+
+struct ConvArgs {
+    const __nv_bfloat16 *x;    // input activations [n][h][w][48]
+    __nv_bfloat16 *y;          // output [n][h][w][48]
+    const uint4 *wt;           // packed weights (kWeightBytes)
+    const float *bias;         // [48]: kBiasRelu, kBias
+    const __nv_bfloat16 *aux;  // kMaskPrev: y = acc where aux > 0, else 0
+    int n, h, w;
+    int tiles_x, tiles_y, tiles;
+    int mode;
+    unsigned *err;             // set when a wait gave up
+};
+
+__device__ __forceinline__ void tile_origin(int tile, int tiles_x, int tiles_y, int &img, int &y0,
+                                            int &x0)
+{
+    const int per = tiles_x * tiles_y;
+    img = tile / per;
+    const int r = tile - img * per;
+    const int ty = r / tiles_x;
+    y0 = ty * kTY;
+    x0 = (r - ty * tiles_x) * kTX;
+}
+
+// The three row-shifted copies of a tile's input (zero outside the image),
+// chunk i = ((dy * 18 + column) * 6 + channel / 8) * 8 + row at byte 16 i.
+__device__ __forceinline__ void load_conv_tile(const __nv_bfloat16 *x, int h, int w, int img, int y0,
+                                               int x0, unsigned char *buf)
+{
+    for (int i = threadIdx.x; i < kTileChunks; i += blockDim.x) {
+        const int yy = i & 7;
+        int r = i >> 3;
+        const int ch = r % 6;
+        r /= 6;
+        const int col = r % kCols;
+        const int dy = r / kCols;
+        const int gy = y0 + yy + dy - 1, gx = x0 + col - 1;
+        const bool ok = gy >= 0 && gy < h && gx >= 0 && gx < w;
+        const __nv_bfloat16 *src =
+            ok ? x + ((static_cast<long long>(img) * h + gy) * w + gx) * kC + ch * 8 : x;
+        cp_async16(buf + i * 16, src, ok);
+    }
+    cp_async_commit();
+}
+
+// 27 MMAs: 9 taps x 3 steps of 16 input channels, into accumulator d_tmem.
+__device__ __forceinline__ void issue_conv_mmas(uint32_t a_base, uint32_t w_base, uint32_t d_tmem)
+{
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const uint64_t ad = smem_desc(a_base + dy * kCopyBytes + dx * kColBytes + s * 256, 128, 768);
+            const uint64_t bd = smem_desc(w_base + tap * kTapBytes + s * 256, 128, 768);
+            mma_bf16(d_tmem, ad, bd, kIdescFwd, tap > 0 || s > 0);
+        }
+    }
+}
+
+// Epilogue of one tile: this thread's pixel (TMEM lane) x 48 channels.
+__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, int tile, uint32_t acc_taddr)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float v[48];
+    {
+        float t0[16], t1[16], t2[16];
+        const uint32_t ta = acc_taddr + (static_cast<uint32_t>(32 * warp) << 16);
+        tmem_ld16(ta, t0);
+        tmem_ld16(ta + 16, t1);
+        tmem_ld16(ta + 32, t2);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            v[i] = t0[i];
+            v[16 + i] = t1[i];
+            v[32 + i] = t2[i];
+        }
+    }
+    int img, y0, x0;
+    tile_origin(tile, a.tiles_x, a.tiles_y, img, y0, x0);
+    const int m = 32 * warp + lane;
+    const int gy = y0 + (m & 7), gx = x0 + (m >> 3);
+    if (gy >= a.h || gx >= a.w) return;
+    const long long px = (static_cast<long long>(img) * a.h + gy) * a.w + gx;
+    if (a.mode == kMaskPrev) {
+        const uint4 *mp = reinterpret_cast<const uint4 *>(a.aux + px * kC);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const uint4 u = mp[q];
+            const unsigned wd[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                // bf16 > 0: sign bit clear and nonzero
+                if ((wd[k] & 0x8000u) || (wd[k] & 0xffffu) == 0) v[q * 8 + 2 * k] = 0.0f;
+                if ((wd[k] >> 31) || (wd[k] >> 16) == 0) v[q * 8 + 2 * k + 1] = 0.0f;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < kC; ++c) {
+            v[c] += __ldg(a.bias + c);
+            if (a.mode == kBiasRelu) v[c] = fmaxf(v[c], 0.0f);
+        }
+    }
+    uint4 *dst = reinterpret_cast<uint4 *>(a.y + px * kC);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        uint32_t p[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[q * 8 + 2 * k], v[q * 8 + 2 * k + 1]);
+            p[k] = *reinterpret_cast<const uint32_t *>(&b2);
+        }
+        dst[q] = make_uint4(p[0], p[1], p[2], p[3]);
+    }
+}
+
+// One 48 -> 48 3 x 3 convolution (padding 1) over every tile: persistent CTAs
+// of 128 threads, one per SM. Shared memory: weights | operand tile x 2 |
+// 2 mbarriers | TMEM slot. The MMAs of one tile run while the previous tile's
+// accumulator is read out and the next tile's operands load.
+constexpr int kConvSmem = kWeightBytes + 2 * kTileBytes + 64;
+
+__global__ void __launch_bounds__(kConvThreads, 1) conv48_kernel(const ConvArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    unsigned char *wsm = smem;
+    unsigned char *const abuf0 = smem + kWeightBytes;  // operand tile b at abuf0 + b * kTileBytes
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kWeightBytes + 2 * kTileBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    __shared__ int abort_flag;
+
+    const int tid = threadIdx.x;
+    if (blockIdx.x >= a.tiles) return;
+    for (int i = tid; i < kWeightBytes / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(wsm)[i] = __ldg(a.wt + i);
+    if (tid == 0) {
+        abort_flag = 0;
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        fence_mbar_init();
+    }
+    if ((tid >> 5) == 0) tmem_alloc(tslot, 2 * kAccCols);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+    const uint32_t w_base = smem_u32(wsm);
+
+    int img, y0, x0;
+    tile_origin(blockIdx.x, a.tiles_x, a.tiles_y, img, y0, x0);
+    load_conv_tile(a.x, a.h, a.w, img, y0, x0, abuf0);
+    int it = 0, prev = -1;
+    for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+        const int b = it & 1;
+        cp_async_wait_all();
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (abort_flag) break;
+        if (tid == 0) {
+            tc_fence_after();
+            issue_conv_mmas(smem_u32(abuf0 + b * kTileBytes), w_base, tbase + b * kAccCols);
+            mma_commit(&mbar[b]);
+        }
+        if (prev >= 0) {  // epilogue of the previous tile while these MMAs run
+            const int pb = b ^ 1;
+            if (!mbar_wait(&mbar[pb], ((it - 1) >> 1) & 1, kWaitLimit)) {
+                abort_flag = 1;
+                if (a.err) atomicOr(a.err, 1u);
+            } else {
+                tc_fence_after();
+                conv_epilogue(a, prev, tbase + pb * kAccCols);
+            }
+        }
+        tc_fence_before();
+        // the other operand buffer is free: its MMAs (previous tile) completed
+        const int next = tile + gridDim.x;
+        if (next < a.tiles) {
+            tile_origin(next, a.tiles_x, a.tiles_y, img, y0, x0);
+            load_conv_tile(a.x, a.h, a.w, img, y0, x0, abuf0 + (b ^ 1) * kTileBytes);
+        }
+        prev = tile;
+    }
+    __syncthreads();
+    if (!abort_flag && prev >= 0) {
+        const int pb = (it - 1) & 1;
+        if (!mbar_wait(&mbar[pb], ((it - 1) >> 1) & 1, kWaitLimit)) {
+            if (a.err) atomicOr(a.err, 1u);
+        } else {
+            tc_fence_after();
+            conv_epilogue(a, prev, tbase + pb * kAccCols);
+        }
+    }
+    cp_async_wait_all();
+    tc_fence_before();
+    __syncthreads();
+    if ((tid >> 5) == 0) {
+        tc_fence_after();
+        tmem_dealloc(tbase, 2 * kAccCols);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradient of a 48 -> 48 layer on the tensor cores:
+//   dW[co][ci][ky][kx] = sum over pixels p of G[p][co] * X[p + (ky - 1, kx - 1)][ci]
+// One MMA per K-step of 16 pixels (two tile columns) and input-row shift dy:
+// A = G (MN-major, M = 128 rows of which co 0..47 are real; the rest read the
+// next columns and are discarded), B = the dy copy of X read as N = 144 =
+// (dx, ci) (MN-major: the three dx shifts of 48 channels are contiguous
+// 128-byte groups), D[dy] = 128 x 144 FP32 in TMEM. Each CTA accumulates over
+// its tiles and writes a partial dW (and the bias gradient from G) that
+// reduce_partials_kernel sums.
+constexpr int kGTileBytes = kCopyBytes;  // 16 columns of G plus two columns of slack
+constexpr int kWgBuf = kGTileBytes + kTileBytes;
+constexpr int kWgSmem = 2 * kWgBuf + 64;
+constexpr uint32_t kIdescWg = instr_desc_bf16(128, 3 * kC, true, true);
+constexpr int kWgPartial = kWmid + kC;  // per CTA: dW (PyTorch layout) then db
+
+struct WgradArgs {
+    const __nv_bfloat16 *x;  // layer input [n][h][w][48]
+    const __nv_bfloat16 *g;  // gradient at the layer's pre-activation output [n][h][w][48]
+    float *partial;          // [gridDim.x][kWgPartial]
+    int n, h, w;
+    int tiles_x, tiles_y, tiles;
+    unsigned *err;
+};
+
+__device__ __forceinline__ void load_g_tile(const __nv_bfloat16 *g, int h, int w, int img, int y0,
+                                            int x0, unsigned char *buf)
+{
+    // 16 columns x 6 channel groups x 8 rows; the two slack columns stay zero
+    for (int i = threadIdx.x; i < kTX * 48; i += blockDim.x) {
+        const int yy = i & 7;
+        int r = i >> 3;
+        const int ch = r % 6;
+        const int col = r / 6;
+        const int gy = y0 + yy, gx = x0 + col;
+        const bool ok = gy < h && gx < w;
+        const __nv_bfloat16 *src =
+            ok ? g + ((static_cast<long long>(img) * h + gy) * w + gx) * kC + ch * 8 : g;
+        cp_async16(buf + i * 16, src, ok);
+    }
+}
+
+__global__ void __launch_bounds__(kConvThreads, 1) wgrad48_kernel(const WgradArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    // operand buffer b (G tile, then the three X copies) at smem + b * kWgBuf
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + 2 * kWgBuf);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
+    __shared__ int abort_flag;
+
+    const int tid = threadIdx.x;
+    // zero both buffers once: the G tiles' slack columns are read as discarded rows
+    for (int i = tid; i < 2 * kWgBuf / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(smem)[i] = make_uint4(0, 0, 0, 0);
+    if (tid == 0) {
+        abort_flag = 0;
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        fence_mbar_init();
+    }
+    if ((tid >> 5) == 0) tmem_alloc(tslot, 512);
+    __syncthreads();
+    const uint32_t tbase = *tslot;
+
+    int img, y0, x0;
+    float bsum = 0.0f;  // thread tid < 48: bias gradient of channel tid
+    int it = 0;
+    if (blockIdx.x < a.tiles) {
+        tile_origin(blockIdx.x, a.tiles_x, a.tiles_y, img, y0, x0);
+        load_g_tile(a.g, a.h, a.w, img, y0, x0, smem);
+        load_conv_tile(a.x, a.h, a.w, img, y0, x0, smem + kGTileBytes);
+    }
+    for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+        const int b = it & 1;
+        cp_async_wait_all();
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (abort_flag) break;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t gb = smem_u32(smem + b * kWgBuf), xb = gb + kGTileBytes;
+#pragma unroll 1
+            for (int s = 0; s < kTX / 2; ++s) {
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy) {
+                    const uint64_t ad = smem_desc(gb + s * 2 * kColBytes, 768, 128);
+                    const uint64_t bd = smem_desc(xb + dy * kCopyBytes + s * 2 * kColBytes, 768, 128);
+                    mma_bf16(tbase + dy * 3 * kC, ad, bd, kIdescWg, it > 0 || s > 0);
+                }
+            }
+            mma_commit(&mbar[b]);
+        }
+        if (tid < kC) {  // bias gradient from the staged G tile
+            const __nv_bfloat16 *gs = reinterpret_cast<const __nv_bfloat16 *>(smem + b * kWgBuf);
+            const int ch = tid >> 3, c8 = tid & 7;
+            for (int col = 0; col < kTX; ++col)
+#pragma unroll
+                for (int yy = 0; yy < 8; ++yy)
+                    bsum += __bfloat162float(gs[((col * 6 + ch) * 8 + yy) * 8 + c8]);
+        }
+        // the other buffer is free once the previous tile's MMAs completed
+        const int next = tile + gridDim.x;
+        if (it > 0) {
+            if (!mbar_wait(&mbar[b ^ 1], ((it - 1) >> 1) & 1, kWaitLimit)) {
+                abort_flag = 1;
+                if (a.err) atomicOr(a.err, 1u);
+            }
+        }
+        __syncthreads();  // bias reads of this buffer done; wait results published
+        if (abort_flag) break;
+        if (next < a.tiles) {
+            tile_origin(next, a.tiles_x, a.tiles_y, img, y0, x0);
+            load_g_tile(a.g, a.h, a.w, img, y0, x0, smem + (b ^ 1) * kWgBuf);
+            load_conv_tile(a.x, a.h, a.w, img, y0, x0, smem + (b ^ 1) * kWgBuf + kGTileBytes);
+        }
+    }
+    __syncthreads();
+    float *out = a.partial + static_cast<long long>(blockIdx.x) * kWgPartial;
+    const bool ok = !abort_flag && it > 0 &&
+                    mbar_wait(&mbar[(it - 1) & 1], ((it - 1) >> 1) & 1, kWaitLimit);
+    if (!ok && !abort_flag && it > 0 && a.err) atomicOr(a.err, 1u);
+    tc_fence_after();
+    const int warp = tid >> 5, lane = tid & 31;
+    if (ok && warp < 2) {  // TMEM lanes 0..63 hold co = lane (rows >= 48 discarded)
+        const int co = 32 * warp + lane;
+        const uint32_t ta = tbase + (static_cast<uint32_t>(32 * warp) << 16);
+#pragma unroll 1
+        for (int c16 = 0; c16 < 27; ++c16) {  // 432 columns: (dy, dx, ci)
+            float v[16];
+            tmem_ld16(ta + c16 * 16, v);
+            tmem_wait_ld();
+            if (co < kC) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int col = c16 * 16 + i;
+                    const int dy = col / 144, rem = col - 144 * dy;
+                    const int dx = rem / kC, ci = rem - kC * dx;
+                    out[((co * kC + ci) * 3 + dy) * 3 + dx] = v[i];
+                }
+            }
+        }
+    } else if (!ok && tid < kC) {
+        for (int i = tid; i < kWmid; i += kC) out[i] = 0.0f;
+    }
+    if (tid < kC) out[kWmid + tid] = (ok || it == 0) ? bsum : 0.0f;
+    cp_async_wait_all();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tbase, 512);
+    }
+}
+
+// out[i] = sum over the `parts` partial vectors (`stride` floats apart) of element i < len;
+// a fixed order, so the sums are reproducible
+__global__ void reduce_partials_kernel(const float *partial, int parts, int len, int stride,
+                                       float *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int p = 0; p < parts; ++p) s += partial[static_cast<long long>(p) * stride + i];
+        out[i] = static_cast<float>(s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP32-pipe layers.
+
+// Layer 1: [noisy, sigma map] -> 48 channels, ReLU. in = plane with row pitch
+// `stride` per image (images `img_stride` elements apart); sigma[img] is the
+// noise level (0-1 scale) of the constant second input channel, which is zero
+// outside the image like the first.
+struct InArgs {
+    const float *in;
+    long long stride, img_stride;
+    const float *sigma;
+    const float *wb;  // W1 [48][2][3][3] then b1 [48] (FP32 master copy)
+    __nv_bfloat16 *y;
+    int n, h, w;
+};
+
+__global__ void __launch_bounds__(256) conv_in_kernel(const InArgs a)
+{
+    __shared__ float ws[kW1 + kC];
+    for (int i = threadIdx.x; i < kW1 + kC; i += blockDim.x) ws[i] = a.wb[i];
+    __syncthreads();
+    const long long total = static_cast<long long>(a.n) * a.h * a.w;
+    for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < total;
+         p += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int img = static_cast<int>(p / (static_cast<long long>(a.h) * a.w));
+        const int r = static_cast<int>(p - static_cast<long long>(img) * a.h * a.w);
+        const int y = r / a.w, x = r - y * a.w;
+        const float s = a.sigma[img];
+        float nb[9], sb[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
+            const bool ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+            nb[t] = ok ? __ldg(a.in + img * a.img_stride + yy * a.stride + xx) : 0.0f;
+            sb[t] = ok ? s : 0.0f;
+        }
+        uint32_t packed[24];
+#pragma unroll
+        for (int c = 0; c < kC; c += 2) {
+            float v0 = ws[kW1 + c], v1 = ws[kW1 + c + 1];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                v0 += ws[(c * 2 + 0) * 9 + t] * nb[t] + ws[(c * 2 + 1) * 9 + t] * sb[t];
+                v1 += ws[((c + 1) * 2 + 0) * 9 + t] * nb[t] + ws[((c + 1) * 2 + 1) * 9 + t] * sb[t];
+            }
+            const __nv_bfloat162 b2 = __floats2bfloat162_rn(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
+            packed[c >> 1] = *reinterpret_cast<const uint32_t *>(&b2);
+        }
+        uint4 *dst = reinterpret_cast<uint4 *>(a.y + p * kC);
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            dst[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
+    }
+}
+
+// Layer 8: 48 -> 1 plus the residual: out = noisy + b8 + conv(X7, W8). With a
+// target it also writes dOut = 2 (out - target) / count and adds the squared
+// error to *loss.
+struct OutArgs {
+    const __nv_bfloat16 *x;  // X7 [n][h][w][48]
+    const float *noisy;
+    long long stride, img_stride;  // of noisy, out, target
+    const float *wb;               // W8 [48][3][3] then b8
+    float *out;
+    const float *target;  // may be null (inference)
+    float *dout;          // [n][h][w] (training)
+    double *loss;         // (training)
+    float inv_count;
+    int n, h, w;
+};
+
+__global__ void __launch_bounds__(256) conv_out_kernel(const OutArgs a)
+{
+    __shared__ float ws[kW8 + 1];
+    __shared__ double red[8];
+    for (int i = threadIdx.x; i < kW8 + 1; i += blockDim.x) ws[i] = a.wb[i];
+    __syncthreads();
+    const long long total = static_cast<long long>(a.n) * a.h * a.w;
+    double err2 = 0.0;
+    for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < total;
+         p += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int img = static_cast<int>(p / (static_cast<long long>(a.h) * a.w));
+        const int r = static_cast<int>(p - static_cast<long long>(img) * a.h * a.w);
+        const int y = r / a.w, x = r - y * a.w;
+        float acc = ws[kW8];
+#pragma unroll 1
+        for (int t = 0; t < 9; ++t) {
+            const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
+            if (yy < 0 || yy >= a.h || xx < 0 || xx >= a.w) continue;
+            const uint4 *src = reinterpret_cast<const uint4 *>(
+                a.x + ((static_cast<long long>(img) * a.h + yy) * a.w + xx) * kC);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const uint4 u = __ldg(src + q);
+                const unsigned wd[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int c = q * 8 + 2 * k;
+                    acc += ws[c * 9 + t] * __uint_as_float(wd[k] << 16) +
+                           ws[(c + 1) * 9 + t] * __uint_as_float(wd[k] & 0xffff0000u);
+                }
+            }
+        }
+        const long long o = img * a.img_stride + static_cast<long long>(y) * a.stride + x;
+        const float v = a.noisy[o] + acc;
+        a.out[o] = v;
+        if (a.target != nullptr) {
+            const float e = v - a.target[o];
+            a.dout[p] = 2.0f * e * a.inv_count;
+            err2 += static_cast<double>(e) * e;
+        }
+    }
+    if (a.target == nullptr) return;
+    for (int o = 16; o >= 1; o >>= 1) err2 += __shfl_xor_sync(0xffffffffu, err2, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = err2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) s += red[i];
+        atomicAdd(a.loss, s);
+    }
+}
+
+// Backward of layer 8 into layer 7's pre-activation gradient:
+// G7[p][ci] = (X7[p][ci] > 0) * sum_t W8[ci][t] dOut[p - (t - center)].
+struct OutBackArgs {
+    const __nv_bfloat16 *x7;
+    const float *dout;
+    const float *wb;
+    __nv_bfloat16 *g;
+    int n, h, w;
+};
+
+__global__ void __launch_bounds__(256) out_backward_kernel(const OutBackArgs a)
+{
+    __shared__ float ws[kW8];
+    for (int i = threadIdx.x; i < kW8; i += blockDim.x) ws[i] = a.wb[i];
+    __syncthreads();
+    const long long total = static_cast<long long>(a.n) * a.h * a.w;
+    for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < total;
+         p += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int img = static_cast<int>(p / (static_cast<long long>(a.h) * a.w));
+        const int r = static_cast<int>(p - static_cast<long long>(img) * a.h * a.w);
+        const int y = r / a.w, x = r - y * a.w;
+        float d[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            // out(q) uses x(q + t - 1): x(p) reaches out(p - (t - 1))
+            const int yy = y - (t / 3 - 1), xx = x - (t % 3 - 1);
+            const bool ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+            d[t] = ok ? a.dout[(static_cast<long long>(img) * a.h + yy) * a.w + xx] : 0.0f;
+        }
+        const uint4 *xs = reinterpret_cast<const uint4 *>(a.x7 + p * kC);
+        uint4 *gd = reinterpret_cast<uint4 *>(a.g + p * kC);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const uint4 u = xs[q];
+            const unsigned wd[4] = {u.x, u.y, u.z, u.w};
+            uint32_t o[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int c = q * 8 + 2 * k;
+                float g0 = 0.0f, g1 = 0.0f;
+#pragma unroll
+                for (int t = 0; t < 9; ++t) {
+                    g0 += ws[c * 9 + t] * d[t];
+                    g1 += ws[(c + 1) * 9 + t] * d[t];
+                }
+                if (!(__uint_as_float(wd[k] << 16) > 0.0f)) g0 = 0.0f;
+                if (!(__uint_as_float(wd[k] & 0xffff0000u) > 0.0f)) g1 = 0.0f;
+                const __nv_bfloat162 b2 = __floats2bfloat162_rn(g0, g1);
+                o[k] = *reinterpret_cast<const uint32_t *>(&b2);
+            }
+            gd[q] = make_uint4(o[0], o[1], o[2], o[3]);
+        }
+    }
+}
+
+// Weight and bias gradients of layer 8: dW8[ci][t] = sum_p dOut[p] X7[p + t - 1][ci],
+// db8 = sum_p dOut[p]. One thread per (pixel, 8-channel group); per-CTA partials.
+constexpr int kW8Partial = kW8 + 1;
+
+__global__ void __launch_bounds__(256) wgrad_out_kernel(const __nv_bfloat16 *x7, const float *dout,
+                                                         int n, int h, int w, float *partial)
+{
+    __shared__ float red[kW8Partial];
+    for (int i = threadIdx.x; i < kW8Partial; i += blockDim.x) red[i] = 0.0f;
+    __syncthreads();
+    const long long total = static_cast<long long>(n) * h * w;
+    const int grp = threadIdx.x % 6;  // 8-channel group
+    float acc[72];
+#pragma unroll
+    for (int i = 0; i < 72; ++i) acc[i] = 0.0f;
+    float bacc = 0.0f;
+    const int per_block = blockDim.x / 6;
+    if (static_cast<int>(threadIdx.x) < per_block * 6) {
+        for (long long q = blockIdx.x * static_cast<long long>(per_block) + threadIdx.x / 6; q < total;
+             q += static_cast<long long>(gridDim.x) * per_block) {
+            // X7[q] reaches dOut[q - (t - 1)] through tap t
+            const int img = static_cast<int>(q / (static_cast<long long>(h) * w));
+            const int r = static_cast<int>(q - static_cast<long long>(img) * h * w);
+            const int y = r / w, x = r - y * w;
+            const uint4 u = reinterpret_cast<const uint4 *>(x7 + q * kC)[grp];
+            float xv[8];
+            const unsigned wd[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                xv[2 * k] = __uint_as_float(wd[k] << 16);
+                xv[2 * k + 1] = __uint_as_float(wd[k] & 0xffff0000u);
+            }
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                const int yy = y - (t / 3 - 1), xx = x - (t % 3 - 1);
+                const bool ok = yy >= 0 && yy < h && xx >= 0 && xx < w;
+                const float d = ok ? dout[(static_cast<long long>(img) * h + yy) * w + xx] : 0.0f;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) acc[t * 8 + k] += d * xv[k];
+            }
+            if (grp == 0) bacc += dout[q];
+        }
+#pragma unroll
+        for (int t = 0; t < 9; ++t)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) atomicAdd(&red[(grp * 8 + k) * 9 + t], acc[t * 8 + k]);
+        if (grp == 0) atomicAdd(&red[kW8], bacc);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kW8Partial; i += blockDim.x)
+        partial[static_cast<long long>(blockIdx.x) * kW8Partial + i] = red[i];
+}
+
+// Weight and bias gradients of layer 1: dW1[co][cin][t] = sum_p G1[p][co] In_cin[p + t - 1],
+// db1[co] = sum_p G1[p][co]; one thread per (pixel, 4-channel group).
+constexpr int kW1Partial = kW1 + kC;
+
+__global__ void __launch_bounds__(240) wgrad_in_kernel(const InArgs a, const __nv_bfloat16 *g1,
+                                                        float *partial)
+{
+    __shared__ float red[kW1Partial];
+    for (int i = threadIdx.x; i < kW1Partial; i += blockDim.x) red[i] = 0.0f;
+    __syncthreads();
+    const long long total = static_cast<long long>(a.n) * a.h * a.w;
+    const int grp = threadIdx.x % 12;  // 4-channel group
+    float acc[72], bacc[4];
+#pragma unroll
+    for (int i = 0; i < 72; ++i) acc[i] = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) bacc[i] = 0.0f;
+    const int per_block = blockDim.x / 12;
+    for (long long p = blockIdx.x * static_cast<long long>(per_block) + threadIdx.x / 12; p < total;
+         p += static_cast<long long>(gridDim.x) * per_block) {
+        const int img = static_cast<int>(p / (static_cast<long long>(a.h) * a.w));
+        const int r = static_cast<int>(p - static_cast<long long>(img) * a.h * a.w);
+        const int y = r / a.w, x = r - y * a.w;
+        const uint2 u = reinterpret_cast<const uint2 *>(g1 + p * kC)[grp];
+        const float gv[4] = {__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u),
+                             __uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u)};
+        const float s = a.sigma[img];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+            const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
+            const bool ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
+            const float nv = ok ? __ldg(a.in + img * a.img_stride + yy * a.stride + xx) : 0.0f;
+            const float sv = ok ? s : 0.0f;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                acc[(k * 2 + 0) * 9 + t] += gv[k] * nv;
+                acc[(k * 2 + 1) * 9 + t] += gv[k] * sv;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) bacc[k] += gv[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+        for (int i = 0; i < 18; ++i) atomicAdd(&red[(grp * 4 + k) * 18 + i], acc[k * 18 + i]);
+        atomicAdd(&red[kW1 + grp * 4 + k], bacc[k]);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kW1Partial; i += blockDim.x)
+        partial[static_cast<long long>(blockIdx.x) * kW1Partial + i] = red[i];
+}
+
+// Adam on the FP32 master parameters (bias-corrected step size precomputed).
+__global__ void adam_kernel(float *param, const float *grad, float *m, float *v, int count,
+                            float lr_t, float beta1, float beta2, float eps)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float g = grad[i];
+        const float mi = beta1 * m[i] + (1.0f - beta1) * g;
+        const float vi = beta2 * v[i] + (1.0f - beta2) * g * g;
+        m[i] = mi;
+        v[i] = vi;
+        param[i] -= lr_t * mi / (sqrtf(vi) + eps);
+    }
+}
+
+// Packs the six 48 -> 48 layers' FP32 weights [co][ci][ky][kx] into the
+// shared-memory operand layout, BF16: forward taps (dy, dx) = (ky, kx) with
+// N = co, K = ci; and the data-gradient form, taps flipped (2 - ky, 2 - kx)
+// with N = ci, K = co.
+__global__ void pack_weights_kernel(const float *params, __nv_bfloat16 *fwd, __nv_bfloat16 *bwd)
+{
+    const int per = 9 * kC * kC;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * per; i += gridDim.x * blockDim.x) {
+        const int layer = i / per;
+        int r = i - layer * per;
+        const int tap = r / (kC * kC);
+        r -= tap * kC * kC;
+        // r = element of the packed tap: [n / 8][k / 8][n % 8][k % 8]
+        const int ng = r / (6 * 64), kg = (r / 64) % 6, n8 = (r / 8) % 8, k8 = r % 8;
+        const int n = ng * 8 + n8, k = kg * 8 + k8;
+        const float *w = params + off_w(layer + 2);
+        const int ky = tap / 3, kx = tap % 3;
+        fwd[i] = __float2bfloat16_rn(w[((n * kC + k) * 3 + ky) * 3 + kx]);
+        bwd[i] = __float2bfloat16_rn(w[((k * kC + n) * 3 + (2 - ky)) * 3 + (2 - kx)]);
+    }
+}
+
+}  // namespace pilot

@@ -5,6 +5,11 @@ launches of one BM3D stage on one seeded synthetic plane (device memory).
 
 With `--time`, the launches are timed with CUDA events instead (for the
 profile tables): `--profile np --time` prints ms per launch of each stage.
+With `--batch N`, N planes of the sigma sweep (5/10/25/50, cycled) go through
+one batch (default tiling, no autotuning) and each launch is one eager run of
+its pipeline (the persistent batch_stage_kernel launches the benchmark's graph
+replays). With `--pilot`, each launch is the learned pilot on the plane
+(conv_in, six tensor-core conv48 layers, conv_out).
 """
 from __future__ import annotations
 
@@ -26,7 +31,14 @@ def main():
     ap.add_argument("--profile", default="fast", choices=["fast", "lc", "np", "high", "vn"])
     ap.add_argument("--time", action="store_true",
                     help="time both stages (CUDA events, --launches each) and print ms and MP/s")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="N > 0: one batch of N sweep planes, launches = eager pipeline runs")
+    ap.add_argument("--pilot", action="store_true", help="launches = pilot estimates of the plane")
     args = ap.parse_args()
+    if args.batch > 0:
+        return batch_case(args)
+    if args.pilot:
+        return pilot_case(args)
     if args.time:
         return time_stages(args)
     if args.planes == 3:
@@ -138,3 +150,50 @@ def three_planes(args):
 
 if __name__ == "__main__":
     main()
+
+
+def batch_case(args):
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    sig = [(5.0, 10.0, 25.0, 50.0)[k % 4] for k in range(args.batch)]
+    ctx = isp_mw_b200.Context(0)
+    srcs, pbs, pfs = [], [], []
+    for k, s in enumerate(sig):
+        srcs.append(torch.from_numpy(synth.pair(args.height, args.width, s, 3000 + k)[1]).cuda())
+        sp = [synth.sigma_param(s)] * 3
+        pbs.append(isp_mw_b200.stage_params_default(args.profile, False, sp))
+        pfs.append(isp_mw_b200.stage_params_default(args.profile, True, sp))
+    dsts = [torch.empty_like(x) for x in srcs]
+    batch = isp_mw_b200.Batch(ctx, pbs, pfs, dsts, srcs, autotune=False)
+    times = [batch.stage_times() for _ in range(args.warmup + args.launches)]
+    t = times[args.warmup:]
+    print(f"batch of {args.batch} {args.width}x{args.height}: basic "
+          f"{sum(x[0] for x in t) / len(t):.4f} ms, final {sum(x[1] for x in t) / len(t):.4f} ms "
+          f"per persistent launch")
+    batch.close()
+    ctx.close()
+
+
+def pilot_case(args):
+    import torch
+    import isp_mw_b200
+    from isp_mw_b200 import synth
+    _, noisy = synth.pair(args.height, args.width, args.sigma, 2024)
+    ctx = isp_mw_b200.Context(0)
+    p = isp_mw_b200.Pilot(ctx, seed=1)
+    src = torch.from_numpy(noisy).cuda()
+    out = torch.empty_like(src)
+    for _ in range(args.warmup):
+        p.estimate(out, src, args.sigma / 255.0)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.launches):
+        p.estimate(out, src, args.sigma / 255.0)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / max(1, args.launches)
+    print(f"pilot {args.width}x{args.height}: {ms:.3f} ms per estimate (CUDA events)")
+    p.close()
+    ctx.close()
