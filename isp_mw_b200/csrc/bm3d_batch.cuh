@@ -55,7 +55,8 @@ template <typename T> struct BatchPlane {
     float *absmax;
     int log2_bound, log2_corner;  // fixed-point bounds of the stage (StageArgs)
     unsigned *nonfinite;       // non-finite src / ref pixels (may be null)
-    unsigned char *poison;     // pixels a non-finite term reached (may be null)
+    unsigned char *poison;     // pixels a non-finite term reached (may be null; all zero
+                               // between stages: normalize_tile clears what it reads)
 };
 
 // Zero each plane's sums, fold its max finite |src| and count its non-finite
@@ -65,9 +66,7 @@ __global__ void prep_batch_kernel(const BatchPlane<T> *planes)
 {
     const BatchPlane<T> q = planes[blockIdx.y];
     prep_plane<T>(q.num, q.den, q.src, q.ref, q.src_stride, q.width, q.height, q.absmax,
-                  q.nonfinite, q.poison,
-                  blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x,
-                  static_cast<long long>(gridDim.x) * blockDim.x);
+                  q.nonfinite, blockIdx.x, gridDim.x);
 }
 
 // dst = num / den for every plane (grid.y = plane); each CTA walks the
@@ -81,8 +80,8 @@ __global__ void __launch_bounds__(256) normalize_batch_kernel(const BatchPlane<T
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int ty = tile / tx, txi = tile - ty * tx;
         normalize_tile<T>(q.dst, q.dst_stride, q.num, q.den, q.width, q.height, q.block_size,
-                          ty * kNormTile, txi * kNormTile, q.poison, q.absmax, q.log2_bound,
-                          q.log2_corner);
+                          ty * kNormTile, txi * kNormTile, q.poison, q.nonfinite, q.absmax,
+                          q.log2_bound, q.log2_corner);
     }
 }
 

@@ -609,15 +609,17 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
         if ((rc = ensure(ctx, ctx->acc[2 * c + 1], acc_bytes)) != BM3D_OK) return rc;
         a.num[c] = static_cast<Acc *>(ctx->acc[2 * c].ptr);
         a.den[c] = static_cast<Acc *>(ctx->acc[2 * c + 1].ptr);
-        if (kFixed) {
+        if (kFixed) {  // starts zeroed; normalisation leaves it zero
+            const bool grow = ctx->poison[c].bytes < static_cast<size_t>(npx);
             if ((rc = ensure(ctx, ctx->poison[c], static_cast<size_t>(npx))) != BM3D_OK) return rc;
+            if (grow) CK(ctx, cudaMemsetAsync(ctx->poison[c].ptr, 0, ctx->poison[c].bytes, s));
             a.poison[c] = static_cast<unsigned char *>(ctx->poison[c].ptr);
         }
         if (!bm_only) {
-            prep_kernel<T><<<blocks, threads, 0, s>>>(
+            prep_kernel<T><<<std::min(height, blocks), threads, 0, s>>>(
                 a.num[c], a.den[c], src[c], static_cast<long long>(stride), width, height,
                 ctx->absmax + c, ref[c] != src[c] ? ref[c] : nullptr,
-                kFixed ? ctx->nonfinite + c : nullptr, a.poison[c]);
+                kFixed ? ctx->nonfinite + c : nullptr);
             CK(ctx, cudaGetLastError());
         }
     }
@@ -637,8 +639,8 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
         const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
         normalize_kernel<T><<<ngrid, 256, 0, s>>>(dst[c], static_cast<long long>(stride), a.num[c],
                                                   a.den[c], width, height, a.block_size,
-                                                  a.poison[c], ctx->absmax + c, a.log2_bound,
-                                                  a.log2_corner);
+                                                  a.poison[c], a.nonfinite ? a.nonfinite + c : nullptr,
+                                                  ctx->absmax + c, a.log2_bound, a.log2_corner);
         CK(ctx, cudaGetLastError());
     }
     return BM3D_OK;
@@ -1163,15 +1165,15 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     // (stats[4]) is left alone so bm3d_noalloc_check sees every call
     if ((e = cudaMemsetAsync(absmax, 0, kNoAllocClearBytes, s)) != cudaSuccess)
         return noalloc_error("cudaMemsetAsync(scratch header)", e);
-    prep_kernel<float><<<blocks, threads, 0, s>>>(num, den, src, a.stride, width, height, absmax,
-                                                  ref != src ? ref : nullptr, nonfinite, poison);
+    prep_kernel<float><<<std::min(height, blocks), threads, 0, s>>>(
+        num, den, src, a.stride, width, height, absmax, ref != src ? ref : nullptr, nonfinite);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("prep_kernel", e);
     rc = launch_stage(&info, a, wiener != 0, 1, s, warps);
     if (rc != BM3D_OK) return noalloc_error(info.err.c_str(), cudaSuccess, rc);
     const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
     normalize_kernel<float><<<ngrid, 256, 0, s>>>(dst, a.stride, num, den, width, height,
-                                                  a.block_size, poison, absmax, a.log2_bound,
-                                                  a.log2_corner);
+                                                  a.block_size, poison, nonfinite, absmax,
+                                                  a.log2_bound, a.log2_corner);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("normalize_kernel", e);
     return BM3D_OK;
 }

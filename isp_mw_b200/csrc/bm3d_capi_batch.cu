@@ -452,6 +452,8 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
     if ((rc = ensure(ctx, B->absmax, sizeof(float) * count * npl)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->nonfinite, sizeof(unsigned) * count * npl)) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->poison, acc_total / 2)) != BM3D_OK) return fail(rc);
+    // all zero between stages: the normalisation clears what it reads
+    CK(ctx, cudaMemset(B->poison.ptr, 0, acc_total / 2));
     if ((rc = ensure(ctx, B->counters, 2 * sizeof(int))) != BM3D_OK) return fail(rc);
     if ((rc = ensure(ctx, B->bad, sizeof(unsigned long long))) != BM3D_OK) return fail(rc);
     CK(ctx, cudaMemset(B->bad.ptr, 0, sizeof(unsigned long long)));

@@ -54,7 +54,8 @@ int run_conv48(bm3d_ctx *ctx, const __nv_bfloat16 *x, __nv_bfloat16 *y, const __
     a.mode = mode;
     a.err = err;
     CK(ctx, raise_smem_limit(reinterpret_cast<const void *>(conv48_kernel), kConvSmem));
-    conv48_kernel<<<grid_for(ctx, a.tiles), kConvThreads, kConvSmem, s>>>(a);
+    conv48_kernel<<<std::max(1, std::min(a.tiles, kConvCtasPerSm * ctx->sm_count)), kConvThreads,
+                    kConvSmem, s>>>(a);
     CK(ctx, cudaGetLastError());
     return BM3D_OK;
 }

@@ -1306,14 +1306,17 @@ constexpr int kNormTile = 32;
 // carry the scale of log2_corner, everything else that of log2_bound
 // (fixed_scale); for those pixels den = (sum of the other weights) * ratio +
 // W(0, 0), ratio = corner scale / general scale (a power of two, exact).
-// Pixels marked in `poison` (may be null) get NaN: a non-finite term reached
-// them (acc_add_checked).
+// On planes whose prep found non-finite inputs (*nonfinite != 0) the pixels
+// marked in `poison` get NaN -- a non-finite term reached them
+// (acc_add_checked) -- and the map is cleared as it is read, so it is all
+// zero again for the next stage; other planes never touch it.
 template <typename T>
 __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
                                                const typename AccOf<T>::type *num,
                                                const typename AccOf<T>::type *wsum, int width,
                                                int height, int bs, int y0, int x0,
-                                               const unsigned char *poison = nullptr,
+                                               unsigned char *poison = nullptr,
+                                               const unsigned *nonfinite = nullptr,
                                                const float *absmax = nullptr, int log2_bound = 0,
                                                int log2_corner = 0)
 {
@@ -1341,6 +1344,7 @@ __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
         hs[ly][lx] = v;
     }
     __syncthreads();
+    const bool marked = poison != nullptr && nonfinite != nullptr && *nonfinite != 0;
     double cratio = 1.0;
     if (split) {
         const float am = absmax != nullptr ? *absmax : 1.0f;
@@ -1360,7 +1364,11 @@ __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
                                  (static_cast<double>(d) * cratio + static_cast<double>(wsum[0])));
         else
             out = ratio(num[g], d);
-        dst[gy * dst_stride + gx] = (poison != nullptr && poison[g]) ? static_cast<T>(NAN) : out;
+        if (marked && poison[g]) {
+            out = static_cast<T>(NAN);
+            poison[g] = 0;
+        }
+        dst[gy * dst_stride + gx] = out;
     }
     __syncthreads();  // before the next tile overwrites w / hs
 }
@@ -1370,39 +1378,40 @@ template <typename T>
 __global__ void __launch_bounds__(256)
     normalize_kernel(T *dst, long long dst_stride, const typename AccOf<T>::type *num,
                      const typename AccOf<T>::type *wsum, int width, int height, int bs,
-                     const unsigned char *poison = nullptr, const float *absmax = nullptr,
-                     int log2_bound = 0, int log2_corner = 0)
+                     unsigned char *poison = nullptr, const unsigned *nonfinite = nullptr,
+                     const float *absmax = nullptr, int log2_bound = 0, int log2_corner = 0)
 {
     normalize_tile<T>(dst, dst_stride, num, wsum, width, height, bs, blockIdx.y * kNormTile,
-                      blockIdx.x * kNormTile, poison, absmax, log2_bound, log2_corner);
+                      blockIdx.x * kNormTile, poison, nonfinite, absmax, log2_bound, log2_corner);
 }
 
 // Zero one plane's accumulators and fold the largest finite |src| into
 // *absmax (which the caller zeroes first; non-negative floats order like their
 // bit patterns). With `nonfinite` (FP32 only) it also counts the NaN / Inf
-// pixels of src and of ref (when given) into *nonfinite and clears the poison
-// map, so that the stage kernel checks its terms only on such planes.
+// pixels of src and of ref (when given) into *nonfinite, so that the stage
+// kernel checks its terms only on such planes. Rows row0, row0 + row_step, ...
+// of the plane, threads along each row.
 template <typename T>
 __device__ __forceinline__ void prep_plane(typename AccOf<T>::type *num,
                                            typename AccOf<T>::type *den, const T *src,
                                            const T *ref, long long stride, int width, int height,
-                                           float *absmax, unsigned *nonfinite,
-                                           unsigned char *poison, long long start,
-                                           long long step)
+                                           float *absmax, unsigned *nonfinite, int row0,
+                                           int row_step)
 {
-    const long long n = static_cast<long long>(width) * height;
     float m = 0.0f;
     unsigned bad = 0;
-    for (long long i = start; i < n; i += step) {
-        num[i] = 0;
-        den[i] = 0;
-        const long long y = i / width, x = i - y * width;
-        const float v = fabsf(static_cast<float>(src[y * stride + x]));
-        if (v <= 3.4028235e38f) m = v > m ? v : m;  // NaN and Inf are skipped
-        else ++bad;
-        if (ref != nullptr && !(fabsf(static_cast<float>(ref[y * stride + x])) <= 3.4028235e38f))
-            ++bad;
-        if (poison != nullptr) poison[i] = 0;
+    for (int y = row0; y < height; y += row_step) {
+        const long long o = static_cast<long long>(y) * width;
+        const T *s = src + static_cast<long long>(y) * stride;
+        const T *r = ref != nullptr ? ref + static_cast<long long>(y) * stride : nullptr;
+        for (int x = threadIdx.x; x < width; x += blockDim.x) {
+            num[o + x] = 0;
+            den[o + x] = 0;
+            const float v = fabsf(static_cast<float>(s[x]));
+            if (v <= 3.4028235e38f) m = v > m ? v : m;  // NaN and Inf are skipped
+            else ++bad;
+            if (r != nullptr && !(fabsf(static_cast<float>(r[x])) <= 3.4028235e38f)) ++bad;
+        }
     }
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
@@ -1416,15 +1425,14 @@ __device__ __forceinline__ void prep_plane(typename AccOf<T>::type *num,
     }
 }
 
+// One plane, one row per CTA at a time.
 template <typename T>
 __global__ void prep_kernel(typename AccOf<T>::type *num, typename AccOf<T>::type *den,
                             const T *src, long long stride, int width, int height, float *absmax,
-                            const T *ref = nullptr, unsigned *nonfinite = nullptr,
-                            unsigned char *poison = nullptr)
+                            const T *ref = nullptr, unsigned *nonfinite = nullptr)
 {
-    prep_plane<T>(num, den, src, ref, stride, width, height, absmax, nonfinite, poison,
-                  blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x,
-                  static_cast<long long>(gridDim.x) * blockDim.x);
+    prep_plane<T>(num, den, src, ref, stride, width, height, absmax, nonfinite, blockIdx.x,
+                  gridDim.x);
 }
 
 }  // namespace bm3d

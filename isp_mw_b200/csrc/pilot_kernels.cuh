@@ -11,13 +11,15 @@
 // Activations are BF16, NHWC with 48 channels (96 bytes per pixel), images
 // stored back to back. A 48 -> 48 layer works on tiles of 16 x 8 output pixels
 // (the MMA's M = 128). The tile's input, with a one-pixel halo, sits in shared
-// memory as three row-shifted copies (dy = -1, 0, +1), each 18 columns of
-// [channel / 8][row (8)][channel % 8] BF16 -- 768 bytes per column. In that
-// layout the 128 x 48 operand of tap (dy, dx) starts dx columns into copy dy
-// (K-major, no swizzle: LBO = 128 bytes between 8-channel groups, SBO = 768
-// bytes between 8-pixel columns), so each tap is three MMAs of K = 16 with no
-// data movement. The same buffers, read as MN-major operands (LBO = 768,
-// SBO = 128), give the weight gradient's pixel-reduction MMAs.
+// memory as 18 columns of [channel / 8][row (10)][channel % 8] BF16 -- 960
+// bytes per column. A core matrix (8 rows x 16 bytes) may start at any 16-byte
+// boundary, so the 128 x 48 operand of tap (dy, dx) starts dx columns and dy
+// rows into the tile (K-major, no swizzle: LBO = 160 bytes between 8-channel
+// groups, SBO = 960 bytes between 8-pixel columns), and each tap is three
+// MMAs of K = 16 with no data movement. Read as an MN-major operand the same
+// tile gives the weight gradient's pixel-reduction MMAs: the three dx shifts
+// of 48 channels are 18 channel groups 160 bytes apart (960 = 6 x 160),
+// columns LBO = 960 apart.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -28,11 +30,14 @@ namespace pilot {
 
 constexpr int kC = 48;                          // hidden channels
 constexpr int kTX = 16, kTY = 8;                // output tile (128 pixels)
-constexpr int kColBytes = kTY * kC * 2;         // 768: one tile column
-constexpr int kCols = kTX + 2;                  // 18 input columns per row-shifted copy
-constexpr int kCopyBytes = kCols * kColBytes;   // 13824
-constexpr int kTileBytes = 3 * kCopyBytes;      // 41472: the three copies
-constexpr int kTileChunks = kTileBytes / 16;    // 2592 16-byte chunks
+constexpr int kColBytes = kTY * kC * 2;         // 768: one column of 8 rows (gradient tile)
+constexpr int kHaloRows = kTY + 2;              // 10 input rows per column
+constexpr int kGroupBytes = kHaloRows * 16;     // 160: one 8-channel group of a halo column
+constexpr int kHaloColBytes = 6 * kGroupBytes;  // 960: one halo column
+constexpr int kCols = kTX + 2;                  // 18 input columns
+constexpr int kCopyBytes = kCols * kColBytes;   // 13824: gradient tile incl. two slack columns
+constexpr int kTileBytes = kCols * kHaloColBytes;  // 17280: the input tile with its halo
+constexpr int kTileChunks = kTileBytes / 16;    // 1080 16-byte chunks
 constexpr int kTapBytes = kC * kC * 2;          // 4608: one tap, [co / 8][ci / 8][co % 8][ci % 8]
 constexpr int kWeightBytes = 9 * kTapBytes;     // 41472
 constexpr int kConvThreads = 128;               // four warps: one per 32 TMEM lanes
@@ -75,19 +80,17 @@ __device__ __forceinline__ void tile_origin(int tile, int tiles_x, int tiles_y, 
     x0 = (r - ty * tiles_x) * kTX;
 }
 
-// The three row-shifted copies of a tile's input (zero outside the image),
-// chunk i = ((dy * 18 + column) * 6 + channel / 8) * 8 + row at byte 16 i.
+// A tile's input with its one-pixel halo (zero outside the image), chunk
+// i = (column * 6 + channel / 8) * 10 + row at byte 16 i (row 0 = y0 - 1).
 __device__ __forceinline__ void load_conv_tile(const __nv_bfloat16 *x, int h, int w, int img, int y0,
                                                int x0, unsigned char *buf)
 {
     for (int i = threadIdx.x; i < kTileChunks; i += blockDim.x) {
-        const int yy = i & 7;
-        int r = i >> 3;
+        const int yy = i % kHaloRows;
+        const int r = i / kHaloRows;
         const int ch = r % 6;
-        r /= 6;
-        const int col = r % kCols;
-        const int dy = r / kCols;
-        const int gy = y0 + yy + dy - 1, gx = x0 + col - 1;
+        const int col = r / 6;
+        const int gy = y0 + yy - 1, gx = x0 + col - 1;
         const bool ok = gy >= 0 && gy < h && gx >= 0 && gx < w;
         const __nv_bfloat16 *src =
             ok ? x + ((static_cast<long long>(img) * h + gy) * w + gx) * kC + ch * 8 : x;
@@ -104,7 +107,8 @@ __device__ __forceinline__ void issue_conv_mmas(uint32_t a_base, uint32_t w_base
         const int dy = tap / 3, dx = tap - 3 * (tap / 3);
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
-            const uint64_t ad = smem_desc(a_base + dy * kCopyBytes + dx * kColBytes + s * 256, 128, 768);
+            const uint64_t ad = smem_desc(a_base + dx * kHaloColBytes + dy * 16 + s * 2 * kGroupBytes,
+                                          kGroupBytes, kHaloColBytes);
             const uint64_t bd = smem_desc(w_base + tap * kTapBytes + s * 256, 128, 768);
             mma_bf16(d_tmem, ad, bd, kIdescFwd, tap > 0 || s > 0);
         }
@@ -170,12 +174,15 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, int tile, uint3
 }
 
 // One 48 -> 48 3 x 3 convolution (padding 1) over every tile: persistent CTAs
-// of 128 threads, one per SM. Shared memory: weights | operand tile x 2 |
-// 2 mbarriers | TMEM slot. The MMAs of one tile run while the previous tile's
-// accumulator is read out and the next tile's operands load.
+// of 128 threads, two per SM (76 KB of shared memory and 128 TMEM columns
+// each), so one CTA's loads and epilogue overlap the other's MMAs. Shared
+// memory: weights | operand tile x 2 | 2 mbarriers | TMEM slot. Within a CTA
+// the MMAs of one tile run while the previous tile's accumulator is read out
+// and the next tile's operands load.
 constexpr int kConvSmem = kWeightBytes + 2 * kTileBytes + 64;
+constexpr int kConvCtasPerSm = 2;
 
-__global__ void __launch_bounds__(kConvThreads, 1) conv48_kernel(const ConvArgs a)
+__global__ void __launch_bounds__(kConvThreads, kConvCtasPerSm) conv48_kernel(const ConvArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *wsm = smem;
@@ -261,9 +268,9 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv48_kernel(const ConvArgs 
 //   dW[co][ci][ky][kx] = sum over pixels p of G[p][co] * X[p + (ky - 1, kx - 1)][ci]
 // One MMA per K-step of 16 pixels (two tile columns) and input-row shift dy:
 // A = G (MN-major, M = 128 rows of which co 0..47 are real; the rest read the
-// next columns and are discarded), B = the dy copy of X read as N = 144 =
-// (dx, ci) (MN-major: the three dx shifts of 48 channels are contiguous
-// 128-byte groups), D[dy] = 128 x 144 FP32 in TMEM. Each CTA accumulates over
+// next columns and are discarded), B = the halo tile of X starting dy rows
+// down, read as N = 144 = (dx, ci) (MN-major: 18 channel groups 160 bytes
+// apart across the three dx shifts), D[dy] = 128 x 144 FP32 in TMEM. Each CTA accumulates over
 // its tiles and writes a partial dW (and the bias gradient from G) that
 // reduce_partials_kernel sums.
 constexpr int kGTileBytes = kCopyBytes;  // 16 columns of G plus two columns of slack
@@ -343,7 +350,8 @@ __global__ void __launch_bounds__(kConvThreads, 1) wgrad48_kernel(const WgradArg
 #pragma unroll
                 for (int dy = 0; dy < 3; ++dy) {
                     const uint64_t ad = smem_desc(gb + s * 2 * kColBytes, 768, 128);
-                    const uint64_t bd = smem_desc(xb + dy * kCopyBytes + s * 2 * kColBytes, 768, 128);
+                    const uint64_t bd = smem_desc(xb + dy * 16 + s * 2 * kHaloColBytes,
+                                                  kHaloColBytes, kGroupBytes);
                     mma_bf16(tbase + dy * 3 * kC, ad, bd, kIdescWg, it > 0 || s > 0);
                 }
             }

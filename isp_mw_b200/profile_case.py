@@ -148,9 +148,6 @@ def three_planes(args):
     ctx.close()
 
 
-if __name__ == "__main__":
-    main()
-
 
 def batch_case(args):
     import torch
@@ -197,3 +194,7 @@ def pilot_case(args):
     print(f"pilot {args.width}x{args.height}: {ms:.3f} ms per estimate (CUDA events)")
     p.close()
     ctx.close()
+
+
+if __name__ == "__main__":
+    main()

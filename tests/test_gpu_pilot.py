@@ -222,10 +222,12 @@ def test_pilot_checkpoint_round_trip(ctx, tmp_path):
     a.estimate(ya, noisy, sigma.cpu().numpy())
     b.estimate(yb, noisy, sigma.cpu().numpy())
     assert torch.equal(ya, yb)
-    # the optimiser state came along: the next steps agree too
+    # the optimiser state came along: the next steps agree too (to float
+    # rounding: the loss and the small layers' gradients are summed with atomics)
     la = a.train_step(noisy, clean, sigma, lr=1e-3)
     lb = b.train_step(noisy, clean, sigma, lr=1e-3)
-    assert la == lb and np.array_equal(a.params(), b.params())
+    assert abs(la - lb) <= 1e-9 * abs(la)
+    np.testing.assert_allclose(a.params(), b.params(), rtol=1e-5, atol=1e-7)
     a.close()
     b.close()
 
