@@ -519,6 +519,10 @@ static int batch_create_any(bm3d_ctx *ctx, int npl, int count, const bm3d_stage_
     if ((rc = tune_stage<true>(B, B->sf, B->planes_f, autotune != 0, B->cap,
                                force_tiling ? force_tiling + 3 : nullptr)) != BM3D_OK)
         return fail(rc);
+    // tuning runs stages without their normalisation, which is what clears
+    // the poison marks; a mark left behind would poison the first real run
+    e = cudaMemsetAsync(B->poison.ptr, 0, acc_total / 2, B->cap);
+    if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "cudaMemsetAsync"));
     e = cudaStreamSynchronize(B->cap);
     if (e != cudaSuccess) return fail(cuda_fail(ctx, e, "batch tuning"));
     // capture the pipeline once
