@@ -80,21 +80,24 @@ __device__ __forceinline__ void tile_origin(int tile, int tiles_x, int tiles_y, 
     x0 = (r - ty * tiles_x) * kTX;
 }
 
-// A tile's input with its one-pixel halo (zero outside the image), chunk
-// i = (column * 6 + channel / 8) * 10 + row at byte 16 i (row 0 = y0 - 1).
+// A tile's input with its one-pixel halo (zero outside the image): chunk
+// (column, channel / 8, row) at byte 16 ((column * 6 + channel / 8) * 10 + row)
+// (row 0 = y0 - 1). Thread i copies the i-th 16-byte chunk of the halo in
+// global order (row, column, channel / 8), so a warp reads 512 contiguous bytes
+// of one input row.
 __device__ __forceinline__ void load_conv_tile(const __nv_bfloat16 *x, int h, int w, int img, int y0,
                                                int x0, unsigned char *buf)
 {
     for (int i = threadIdx.x; i < kTileChunks; i += blockDim.x) {
-        const int yy = i % kHaloRows;
-        const int r = i / kHaloRows;
-        const int ch = r % 6;
+        const int yy = i / (kCols * 6);
+        const int r = i - yy * (kCols * 6);
         const int col = r / 6;
+        const int ch = r - col * 6;
         const int gy = y0 + yy - 1, gx = x0 + col - 1;
         const bool ok = gy >= 0 && gy < h && gx >= 0 && gx < w;
         const __nv_bfloat16 *src =
             ok ? x + ((static_cast<long long>(img) * h + gy) * w + gx) * kC + ch * 8 : x;
-        cp_async16(buf + i * 16, src, ok);
+        cp_async16(buf + ((col * 6 + ch) * kHaloRows + yy) * 16, src, ok);
     }
     cp_async_commit();
 }
@@ -115,8 +118,19 @@ __device__ __forceinline__ void issue_conv_mmas(uint32_t a_base, uint32_t w_base
     }
 }
 
-// Epilogue of one tile: this thread's pixel (TMEM lane) x 48 channels.
-__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, int tile, uint32_t acc_taddr)
+// Epilogue of one tile. Each thread reads its pixel's (TMEM lane m = column
+// * 8 + row) 48 accumulators, applies the bias (and ReLU) and rounds to BF16
+// into `stage` at m * kOutPitch (a 112-byte pitch: the eight lanes of a
+// 16-byte store phase land on distinct banks). Then the 128 threads write the
+// tile's rows out, consecutive threads on consecutive 16-byte chunks of a row
+// (16 pixels x 96 bytes contiguous), masking by the previous layer's output in
+// kMaskPrev mode (masking after rounding equals rounding the masked value).
+// Contains two __syncthreads: every thread of the CTA calls it.
+constexpr int kOutPitch = 112;
+static_assert(kTX * kTY * kOutPitch <= kTileBytes, "output staging fits an operand buffer");
+
+__device__ __forceinline__ void conv_epilogue(const ConvArgs &a, int tile, uint32_t acc_taddr,
+                                              unsigned char *stage)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float v[48];
@@ -134,33 +148,15 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, int tile, uint3
             v[32 + i] = t2[i];
         }
     }
-    int img, y0, x0;
-    tile_origin(tile, a.tiles_x, a.tiles_y, img, y0, x0);
-    const int m = 32 * warp + lane;
-    const int gy = y0 + (m & 7), gx = x0 + (m >> 3);
-    if (gy >= a.h || gx >= a.w) return;
-    const long long px = (static_cast<long long>(img) * a.h + gy) * a.w + gx;
-    if (a.mode == kMaskPrev) {
-        const uint4 *mp = reinterpret_cast<const uint4 *>(a.aux + px * kC);
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            const uint4 u = mp[q];
-            const unsigned wd[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                // bf16 > 0: sign bit clear and nonzero
-                if ((wd[k] & 0x8000u) || (wd[k] & 0xffffu) == 0) v[q * 8 + 2 * k] = 0.0f;
-                if ((wd[k] >> 31) || (wd[k] >> 16) == 0) v[q * 8 + 2 * k + 1] = 0.0f;
-            }
-        }
-    } else {
+    if (a.mode != kMaskPrev) {
 #pragma unroll
         for (int c = 0; c < kC; ++c) {
             v[c] += __ldg(a.bias + c);
             if (a.mode == kBiasRelu) v[c] = fmaxf(v[c], 0.0f);
         }
     }
-    uint4 *dst = reinterpret_cast<uint4 *>(a.y + px * kC);
+    const int m = 32 * warp + lane;
+    uint4 *st = reinterpret_cast<uint4 *>(stage + m * kOutPitch);
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
         uint32_t p[4];
@@ -169,17 +165,46 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs &a, int tile, uint3
             const __nv_bfloat162 b2 = __floats2bfloat162_rn(v[q * 8 + 2 * k], v[q * 8 + 2 * k + 1]);
             p[k] = *reinterpret_cast<const uint32_t *>(&b2);
         }
-        dst[q] = make_uint4(p[0], p[1], p[2], p[3]);
+        st[q] = make_uint4(p[0], p[1], p[2], p[3]);
     }
+    __syncthreads();
+    int img, y0, x0;
+    tile_origin(tile, a.tiles_x, a.tiles_y, img, y0, x0);
+    for (int j = threadIdx.x; j < kTX * kTY * 6; j += blockDim.x) {
+        const int r = j / (kTX * 6);
+        const int rem = j - r * (kTX * 6);
+        const int c = rem / 6;
+        const int q = rem - c * 6;
+        const int gy = y0 + r, gx = x0 + c;
+        if (gy >= a.h || gx >= a.w) continue;
+        uint4 u = *reinterpret_cast<const uint4 *>(stage + (c * kTY + r) * kOutPitch + q * 16);
+        const long long px = (static_cast<long long>(img) * a.h + gy) * a.w + gx;
+        if (a.mode == kMaskPrev) {
+            const uint4 mk = __ldg(reinterpret_cast<const uint4 *>(a.aux + px * kC) + q);
+            const unsigned mw[4] = {mk.x, mk.y, mk.z, mk.w};
+            unsigned uw[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                // bf16 > 0: sign bit clear and nonzero
+                if ((mw[k] & 0x8000u) || (mw[k] & 0xffffu) == 0) uw[k] &= 0xffff0000u;
+                if ((mw[k] >> 31) || (mw[k] >> 16) == 0) uw[k] &= 0x0000ffffu;
+            }
+            u = make_uint4(uw[0], uw[1], uw[2], uw[3]);
+        }
+        reinterpret_cast<uint4 *>(a.y + px * kC)[q] = u;
+    }
+    __syncthreads();
 }
 
 // One 48 -> 48 3 x 3 convolution (padding 1) over every tile: persistent CTAs
-// of 128 threads, two per SM (76 KB of shared memory and 128 TMEM columns
-// each), so one CTA's loads and epilogue overlap the other's MMAs. Shared
-// memory: weights | operand tile x 2 | 2 mbarriers | TMEM slot. Within a CTA
-// the MMAs of one tile run while the previous tile's accumulator is read out
-// and the next tile's operands load.
-constexpr int kConvSmem = kWeightBytes + 2 * kTileBytes + 64;
+// of 128 threads, two per SM (93 KB of shared memory and 128 TMEM columns
+// each). Shared memory: weights | three operand tiles | 2 mbarriers | TMEM
+// slot. Iteration t waits for tile t's operands, issues its 27 MMAs into
+// accumulator t % 2, then, while they run, drains tile t - 1's accumulator
+// through tile t - 1's (now free) operand buffer and refills that buffer with
+// tile t + 2's input: each load has a whole iteration to land.
+constexpr int kConvStages = 3;
+constexpr int kConvSmem = kWeightBytes + kConvStages * kTileBytes + 64;
 constexpr int kConvCtasPerSm = 2;
 
 __global__ void __launch_bounds__(kConvThreads, kConvCtasPerSm) conv48_kernel(const ConvArgs a)
@@ -187,7 +212,7 @@ __global__ void __launch_bounds__(kConvThreads, kConvCtasPerSm) conv48_kernel(co
     extern __shared__ __align__(128) unsigned char smem[];
     unsigned char *wsm = smem;
     unsigned char *const abuf0 = smem + kWeightBytes;  // operand tile b at abuf0 + b * kTileBytes
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kWeightBytes + 2 * kTileBytes);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + kWeightBytes + kConvStages * kTileBytes);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 2);
     __shared__ int abort_flag;
 
@@ -210,48 +235,61 @@ __global__ void __launch_bounds__(kConvThreads, kConvCtasPerSm) conv48_kernel(co
     const uint32_t w_base = smem_u32(wsm);
 
     int img, y0, x0;
-    tile_origin(blockIdx.x, a.tiles_x, a.tiles_y, img, y0, x0);
-    load_conv_tile(a.x, a.h, a.w, img, y0, x0, abuf0);
+    for (int k = 0; k < 2; ++k) {  // tiles 0 and 1 of this CTA (empty groups past the end)
+        const int tile = blockIdx.x + k * gridDim.x;
+        if (tile < a.tiles) {
+            tile_origin(tile, a.tiles_x, a.tiles_y, img, y0, x0);
+            load_conv_tile(a.x, a.h, a.w, img, y0, x0, abuf0 + k * kTileBytes);
+        } else {
+            cp_async_commit();
+        }
+    }
     int it = 0, prev = -1;
     for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
-        const int b = it & 1;
-        cp_async_wait_all();
+        const int b = it % kConvStages;
+        cp_async_wait_1();
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
         if (abort_flag) break;
         if (tid == 0) {
             tc_fence_after();
-            issue_conv_mmas(smem_u32(abuf0 + b * kTileBytes), w_base, tbase + b * kAccCols);
-            mma_commit(&mbar[b]);
+            issue_conv_mmas(smem_u32(abuf0 + b * kTileBytes), w_base, tbase + (it & 1) * kAccCols);
+            mma_commit(&mbar[it & 1]);
         }
+        unsigned char *const freed = abuf0 + ((it + 2) % kConvStages) * kTileBytes;
         if (prev >= 0) {  // epilogue of the previous tile while these MMAs run
-            const int pb = b ^ 1;
-            if (!mbar_wait(&mbar[pb], ((it - 1) >> 1) & 1, kWaitLimit)) {
-                abort_flag = 1;
-                if (a.err) atomicOr(a.err, 1u);
+            const int pa = (it - 1) & 1;
+            const bool ok = __syncthreads_and(mbar_wait(&mbar[pa], ((it - 1) >> 1) & 1, kWaitLimit));
+            if (!ok) {
+                if (tid == 0) {
+                    abort_flag = 1;
+                    if (a.err) atomicOr(a.err, 1u);
+                }
             } else {
                 tc_fence_after();
-                conv_epilogue(a, prev, tbase + pb * kAccCols);
+                conv_epilogue(a, prev, tbase + pa * kAccCols, freed);  // freed = tile it - 1's buffer
             }
         }
         tc_fence_before();
-        // the other operand buffer is free: its MMAs (previous tile) completed
-        const int next = tile + gridDim.x;
+        const int next = tile + 2 * gridDim.x;
         if (next < a.tiles) {
             tile_origin(next, a.tiles_x, a.tiles_y, img, y0, x0);
-            load_conv_tile(a.x, a.h, a.w, img, y0, x0, abuf0 + (b ^ 1) * kTileBytes);
+            load_conv_tile(a.x, a.h, a.w, img, y0, x0, freed);
+        } else {
+            cp_async_commit();
         }
         prev = tile;
     }
     __syncthreads();
     if (!abort_flag && prev >= 0) {
-        const int pb = (it - 1) & 1;
-        if (!mbar_wait(&mbar[pb], ((it - 1) >> 1) & 1, kWaitLimit)) {
-            if (a.err) atomicOr(a.err, 1u);
+        const int pa = (it - 1) & 1;
+        const bool ok = __syncthreads_and(mbar_wait(&mbar[pa], ((it - 1) >> 1) & 1, kWaitLimit));
+        if (!ok) {
+            if (tid == 0 && a.err) atomicOr(a.err, 1u);
         } else {
             tc_fence_after();
-            conv_epilogue(a, prev, tbase + pb * kAccCols);
+            conv_epilogue(a, prev, tbase + pa * kAccCols, abuf0 + ((it - 1) % kConvStages) * kTileBytes);
         }
     }
     cp_async_wait_all();

@@ -153,5 +153,7 @@ __device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc, boo
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// All but the most recently committed group have landed.
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 }  // namespace pilot
