@@ -396,6 +396,16 @@ typedef struct bm3d_pilot bm3d_pilot;
 /* Number of FP32 parameters (weights and biases of the eight layers). */
 int bm3d_pilot_param_count(void);
 
+/* Which kernel runs the 48 -> 48 convolutions (process-wide): 0 (default) the
+ * warp-specialised TMA pipeline when its tensor maps encode, else the cp.async
+ * kernel; 1 the cp.async kernel; 2 the TMA pipeline only (a call fails with
+ * BM3D_ERR_CUDA when its maps do not encode). Both give identical results. */
+int bm3d_pilot_set_conv_kernel(int which);
+
+/* The kernel of the last 48 -> 48 convolution launched: 2 = TMA pipeline,
+ * 1 = cp.async kernel, 0 = none yet. */
+int bm3d_pilot_conv_kernel(void);
+
 /* A pilot on the context's device, He-initialised from `seed`. */
 int bm3d_pilot_create(bm3d_ctx *ctx, unsigned long long seed, bm3d_pilot **out);
 void bm3d_pilot_destroy(bm3d_pilot *p);

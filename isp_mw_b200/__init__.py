@@ -44,7 +44,8 @@ EXPORTS = [
     "bm3d_host_batch_run", "bm3d_host_batch_join", "bm3d_host_batch_destroy",
     "bm3d_inject_alloc_failures", "bm3d_batch_stage_times", "bm3d_batch_final_create",
     "bm3d_batch3_final_create",
-    "bm3d_pilot_param_count", "bm3d_pilot_create", "bm3d_pilot_destroy", "bm3d_pilot_set_params",
+    "bm3d_pilot_param_count", "bm3d_pilot_set_conv_kernel", "bm3d_pilot_conv_kernel",
+    "bm3d_pilot_create", "bm3d_pilot_destroy", "bm3d_pilot_set_params",
     "bm3d_pilot_get_params", "bm3d_pilot_get_grad", "bm3d_pilot_save", "bm3d_pilot_load",
     "bm3d_pilot_estimate", "bm3d_pilot_train_step", "bm3d_pilot_full", "bm3d_pilot_conv48",
     "bm3d_pilot_wgrad48",
@@ -131,6 +132,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_noalloc_check.argtypes = [vp]
     lib.bm3d_inject_alloc_failures.argtypes = [ip]
     lib.bm3d_pilot_param_count.argtypes = []
+    lib.bm3d_pilot_set_conv_kernel.argtypes = [ip]
+    lib.bm3d_pilot_conv_kernel.argtypes = []
     lib.bm3d_pilot_create.argtypes = [vp, ctypes.c_ulonglong, ctypes.POINTER(vp)]
     lib.bm3d_pilot_destroy.argtypes = [vp]
     lib.bm3d_pilot_destroy.restype = None

@@ -7,7 +7,11 @@
 #include "bm3d_capi_internal.h"
 #include "pilot_kernels.cuh"
 
+#include <cudaTypedefs.h>
+
+#include <atomic>
 #include <cstdio>
+#include <mutex>
 #include <random>
 
 using namespace pilot;
@@ -34,6 +38,55 @@ int pilot_fail(bm3d_ctx *ctx, int code, const char *msg)
 
 int grid_for(const bm3d_ctx *ctx, int tiles) { return std::max(1, std::min(tiles, ctx->sm_count)); }
 
+// Which 48 -> 48 convolution kernel runs: 0 = the TMA pipeline when its
+// tensor maps encode (else the cp.async kernel), 1 = the cp.async kernel,
+// 2 = the TMA pipeline only. g_conv_last records the kernel last launched.
+std::atomic<int> g_conv_choice{0};
+std::atomic<int> g_conv_last{0};
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library); null when the driver does not provide it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    });
+    return fn;
+}
+
+// The TMA pipeline's two views of n images of h x w x 48 BF16 (NHWC): the
+// input as (channel % 8, x, channel / 8, y, image), box {8, 10, 6, 18, 1}, and
+// the output as (channel, x, y, image), box {48, 8, 4, 1}.
+bool encode_conv_maps(const void *x, void *y, int n, int h, int w, CUtensorMap &in, CUtensorMap &out)
+{
+    auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t px = 2ull * kC;  // bytes per pixel
+    const cuuint64_t gdim[5] = {8, static_cast<cuuint64_t>(w), 6, static_cast<cuuint64_t>(h),
+                                static_cast<cuuint64_t>(n)};
+    const cuuint64_t gstride[4] = {px, 16, px * w, px * w * h};
+    const cuuint32_t box[5] = {8, kT2X + 2, 6, kT2Y + 2, 1};
+    const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
+    if (enc(&in, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(x), gdim, gstride, box, ones,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return false;
+    const cuuint64_t odim[4] = {static_cast<cuuint64_t>(kC), static_cast<cuuint64_t>(w),
+                                static_cast<cuuint64_t>(h), static_cast<cuuint64_t>(n)};
+    const cuuint64_t ostride[3] = {px, px * w, px * w * h};
+    const cuuint32_t obox[4] = {kC, kT2X, 4, 1};
+    return enc(&out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, y, odim, ostride, obox, ones,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // One 48 -> 48 layer on the tensor cores.
 int run_conv48(bm3d_ctx *ctx, const __nv_bfloat16 *x, __nv_bfloat16 *y, const __nv_bfloat16 *w,
                const float *bias, const __nv_bfloat16 *aux, int mode, int n, int h, int wd,
@@ -48,15 +101,31 @@ int run_conv48(bm3d_ctx *ctx, const __nv_bfloat16 *x, __nv_bfloat16 *y, const __
     a.n = n;
     a.h = h;
     a.w = wd;
+    a.mode = mode;
+    a.err = err;
+    const int choice = g_conv_choice.load();
+    CUtensorMap tin, tout;
+    if (choice != 1 && encode_conv_maps(x, y, n, h, wd, tin, tout)) {
+        a.tiles_x = (wd + kT2X - 1) / kT2X;
+        a.tiles_y = (h + kT2Y - 1) / kT2Y;
+        a.tiles = n * a.tiles_x * a.tiles_y;
+        CK(ctx, raise_smem_limit(reinterpret_cast<const void *>(conv48_tma_kernel), kTmaSmem));
+        conv48_tma_kernel<<<std::max(1, std::min(a.tiles, ctx->sm_count)), kTmaThreads, kTmaSmem,
+                            s>>>(tin, tout, a);
+        CK(ctx, cudaGetLastError());
+        g_conv_last.store(2);
+        return BM3D_OK;
+    }
+    if (choice == 2)
+        return pilot_fail(ctx, BM3D_ERR_CUDA, "pilot: the convolution's tensor maps did not encode");
     a.tiles_x = (wd + kTX - 1) / kTX;
     a.tiles_y = (h + kTY - 1) / kTY;
     a.tiles = n * a.tiles_x * a.tiles_y;
-    a.mode = mode;
-    a.err = err;
     CK(ctx, raise_smem_limit(reinterpret_cast<const void *>(conv48_kernel), kConvSmem));
     conv48_kernel<<<std::max(1, std::min(a.tiles, kConvCtasPerSm * ctx->sm_count)), kConvThreads,
                     kConvSmem, s>>>(a);
     CK(ctx, cudaGetLastError());
+    g_conv_last.store(1);
     return BM3D_OK;
 }
 
@@ -191,6 +260,15 @@ int forward(bm3d_pilot *p, const float *in, long long stride, long long img_stri
 }  // namespace
 
 extern "C" int bm3d_pilot_param_count(void) { return kParams; }
+
+extern "C" int bm3d_pilot_set_conv_kernel(int which)
+{
+    if (which < 0 || which > 2) return BM3D_ERR_INVALID;
+    g_conv_choice.store(which);
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_pilot_conv_kernel(void) { return g_conv_last.load(); }
 
 extern "C" int bm3d_pilot_create(bm3d_ctx *ctx, unsigned long long seed, bm3d_pilot **out)
 {

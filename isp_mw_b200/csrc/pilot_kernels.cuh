@@ -22,6 +22,7 @@
 // columns LBO = 960 apart.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "pilot_tc.cuh"
@@ -296,6 +297,232 @@ __global__ void __launch_bounds__(kConvThreads, kConvCtasPerSm) conv48_kernel(co
     tc_fence_before();
     __syncthreads();
     if ((tid >> 5) == 0) {
+        tc_fence_after();
+        tmem_dealloc(tbase, 2 * kAccCols);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same convolution as a warp-specialised TMA pipeline. Output tiles are 8
+// pixels wide and 16 tall (MMA row m = row * 8 + column). A tile's input with
+// its halo, 10 columns x 18 rows, arrives by ONE TMA load of a 5-D view of the
+// NHWC activations -- (channel % 8, x, channel / 8, y, image) with byte
+// strides (2, 96, 16, 96 w, 96 w h) -- whose box {8, 10, 6, 18, 1} lands as
+// [row][channel / 8][column][channel % 8]: the K-major core-matrix layout with
+// LBO = 160 bytes between channel groups and SBO = 960 bytes between pixel
+// rows, so tap (dy, dx) starts dy * 960 + dx * 16 bytes in. The copy
+// zero-fills the halo outside the image.
+//
+// Warps: 0 loads (lane 0), 1 issues the MMAs (lane 0), 2-5 drain the
+// accumulators -- warp w reads TMEM lanes 32 (w % 4) .. + 31, pixel rows
+// 4 (w % 4) .. + 3 -- and store their 4 x 8 pixels with a TMA store of a 4-D
+// view (channel, x, y, image) from a per-warp staging buffer (the store clips
+// at the image edges). kTmaStages operand buffers and two accumulators are
+// handed on by mbarriers (full / empty for each); no CTA-wide barrier runs
+// inside the tile loop.
+constexpr int kT2X = 8, kT2Y = 16;
+constexpr int kTmaStages = 4;
+constexpr int kTmaThreads = 192;
+constexpr int kStoreBytes = 32 * kC * 2;  // one warp's 4 x 8 output pixels
+constexpr int kTmaOffStage = kWeightBytes;
+constexpr int kTmaOffStore = kTmaOffStage + kTmaStages * kTileBytes;
+constexpr int kTmaOffBias = kTmaOffStore + 4 * 2 * kStoreBytes;
+constexpr int kTmaOffBar = kTmaOffBias + kC * 4;
+constexpr int kTmaSmem = kTmaOffBar + 8 * (2 * kTmaStages + 4) + 16;
+static_assert(kTmaOffStage % 128 == 0 && kTmaOffStore % 128 == 0 && kTileBytes % 128 == 0,
+              "TMA buffers 128-byte aligned");
+
+__device__ __forceinline__ void tile_origin_8x16(int tile, int tiles_x, int tiles_y, int &img,
+                                                 int &y0, int &x0)
+{
+    const int per = tiles_x * tiles_y;
+    img = tile / per;
+    const int r = tile - img * per;
+    const int ty = r / tiles_x;
+    y0 = ty * kT2Y;
+    x0 = (r - ty * tiles_x) * kT2X;
+}
+
+// Two FP32 values to a BF16 pair (lo in the low half), optionally through ReLU.
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi, bool relu)
+{
+    uint32_t d;
+    if (relu)
+        asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    else
+        asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 1)
+    conv48_tma_kernel(const __grid_constant__ CUtensorMap tm_in,
+                      const __grid_constant__ CUtensorMap tm_out, const ConvArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kTmaOffBar);
+    uint64_t *empty = full + kTmaStages;
+    uint64_t *accf = empty + kTmaStages;
+    uint64_t *acce = accf + 2;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(acce + 2);
+    float *bias_s = reinterpret_cast<float *>(smem + kTmaOffBias);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (blockIdx.x >= a.tiles) return;
+
+    for (int i = tid; i < kWeightBytes / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(smem)[i] = __ldg(a.wt + i);
+    if (tid < kC) bias_s[tid] = a.mode != kMaskPrev ? __ldg(a.bias + tid) : 0.0f;
+    if (tid == 0) {
+        for (int s = 0; s < kTmaStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&accf[k], 1);
+            mbar_init(&acce[k], 4);  // one arrival per draining warp
+        }
+        fence_mbar_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, 2 * kAccCols);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {  // producer
+            int it = 0;
+            for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+                const int s = it % kTmaStages;
+                if (!mbar_wait(&empty[s], ((it / kTmaStages) & 1) ^ 1, kWaitLimit)) {
+                    ok = false;
+                    break;
+                }
+                int img, y0, x0;
+                tile_origin_8x16(tile, a.tiles_x, a.tiles_y, img, y0, x0);
+                mbar_arrive_expect_tx(&full[s], kTileBytes);
+                tma_load_5d(smem + kTmaOffStage + s * kTileBytes, &tm_in, &full[s], 0, x0 - 1, 0,
+                            y0 - 1, img);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issue
+            const uint32_t w_base = smem_u32(smem);
+            int it = 0;
+            for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+                const int s = it % kTmaStages, k = it & 1;
+                if (!mbar_wait(&full[s], (it / kTmaStages) & 1, kWaitLimit) ||
+                    !mbar_wait(&acce[k], ((it >> 1) & 1) ^ 1, kWaitLimit)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t a_base = smem_u32(smem + kTmaOffStage + s * kTileBytes);
+#pragma unroll 1
+                for (int tap = 0; tap < 9; ++tap) {
+                    const int dy = tap / 3, dx = tap - 3 * (tap / 3);
+#pragma unroll
+                    for (int st = 0; st < 3; ++st) {
+                        const uint64_t ad = smem_desc(
+                            a_base + dy * kHaloColBytes + dx * 16 + st * 2 * kGroupBytes, kGroupBytes,
+                            kHaloColBytes);
+                        const uint64_t bd = smem_desc(w_base + tap * kTapBytes + st * 256, 128, 768);
+                        mma_bf16(tbase + k * kAccCols, ad, bd, kIdescFwd, tap > 0 || st > 0);
+                    }
+                }
+                mma_commit(&empty[s]);  // the operand buffer is free once these MMAs finish
+                mma_commit(&accf[k]);
+            }
+        }
+    } else {  // drain: warps 2..5
+        const int q = warp & 3;
+        unsigned char *const stage0 = smem + kTmaOffStore + (warp - 2) * 2 * kStoreBytes;
+        const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+            const int k = it & 1;
+            if (!__all_sync(0xffffffffu, mbar_wait(&accf[k], (it >> 1) & 1, kWaitLimit))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            float v[48];
+            {
+                float t0[16], t1[16], t2[16];
+                const uint32_t ta = tbase + k * kAccCols + lane_base;
+                tmem_ld16(ta, t0);
+                tmem_ld16(ta + 16, t1);
+                tmem_ld16(ta + 32, t2);
+                tmem_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    v[i] = t0[i];
+                    v[16 + i] = t1[i];
+                    v[32 + i] = t2[i];
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[k]);  // the accumulator may be overwritten
+
+            int img, y0, x0;
+            tile_origin_8x16(tile, a.tiles_x, a.tiles_y, img, y0, x0);
+            uint32_t pk[24];
+            if (a.mode == kMaskPrev) {
+                const int gy = y0 + 4 * q + (lane >> 3), gx = x0 + (lane & 7);
+                uint4 mk[6] = {};
+                if (gy < a.h && gx < a.w) {
+                    const uint4 *mp = reinterpret_cast<const uint4 *>(
+                        a.aux + ((static_cast<long long>(img) * a.h + gy) * a.w + gx) * kC);
+#pragma unroll
+                    for (int j = 0; j < 6; ++j) mk[j] = __ldg(mp + j);
+                }
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    const unsigned mw[4] = {mk[j].x, mk[j].y, mk[j].z, mk[j].w};
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        // bf16 > 0: sign bit clear and nonzero
+                        uint32_t p = pack_bf16(v[8 * j + 2 * e], v[8 * j + 2 * e + 1], false);
+                        if ((mw[e] & 0x8000u) || (mw[e] & 0xffffu) == 0) p &= 0xffff0000u;
+                        if ((mw[e] >> 31) || (mw[e] >> 16) == 0) p &= 0x0000ffffu;
+                        pk[4 * j + e] = p;
+                    }
+                }
+            } else {
+                const bool relu = a.mode == kBiasRelu;
+                const float4 *b4 = reinterpret_cast<const float4 *>(bias_s);
+#pragma unroll
+                for (int j = 0; j < 12; ++j) {
+                    const float4 b = b4[j];
+                    pk[2 * j] = pack_bf16(v[4 * j] + b.x, v[4 * j + 1] + b.y, relu);
+                    pk[2 * j + 1] = pack_bf16(v[4 * j + 2] + b.z, v[4 * j + 3] + b.w, relu);
+                }
+            }
+            unsigned char *const stg = stage0 + (it & 1) * kStoreBytes;
+            if (lane == 0) bulk_wait_read_1();  // the store two tiles back has read this buffer
+            __syncwarp();
+            uint4 *dst = reinterpret_cast<uint4 *>(stg + lane * kC * 2);
+#pragma unroll
+            for (int j = 0; j < 6; ++j)
+                dst[j] = make_uint4(pk[4 * j], pk[4 * j + 1], pk[4 * j + 2], pk[4 * j + 3]);
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+                // rows wholly below the image store nothing; the (then empty)
+                // group is still committed, so wait_group.read 1 keeps pairing
+                // each buffer with the store two tiles back
+                if (y0 + 4 * q < a.h) tma_store_4d(&tm_out, stg, 0, x0, y0 + 4 * q, img);
+                bulk_commit();
+            }
+        }
+        if (lane == 0) bulk_wait_all();
+    }
+    if (!ok && a.err) atomicOr(a.err, 1u);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
         tc_fence_after();
         tmem_dealloc(tbase, 2 * kAccCols);
     }

@@ -156,4 +156,50 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // All but the most recently committed group have landed.
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
+// --- tensor memory access (TMA) ------------------------------------------------
+// Tiled copies through a tensor map (a __grid_constant__ kernel parameter,
+// addressed generically). Single-CTA forms only: no cluster multicast.
+
+// One arrival that also announces `bytes` of asynchronous copies to come.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+// Box of a 5-D tensor map at coordinates c0..c4 (c0, the innermost, in
+// elements and a multiple of 16 bytes) into shared memory; completes on mbar.
+__device__ __forceinline__ void tma_load_5d(void *smem_dst, const void *tmap, uint64_t *mbar, int c0,
+                                            int c1, int c2, int c3, int c4)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_u32(smem_dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(smem_u32(mbar)), "r"(c0), "r"(c1), "r"(c2),
+        "r"(c3), "r"(c4)
+        : "memory");
+}
+
+// Box of a 4-D tensor map from shared memory to coordinates c0..c3 (c0 = 0
+// here); elements outside the tensor are not written.
+__device__ __forceinline__ void tma_store_4d(const void *tmap, const void *smem_src, int c0, int c1,
+                                             int c2, int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::
+            "l"(reinterpret_cast<uint64_t>(tmap)),
+        "r"(smem_u32(smem_src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// This thread's bulk stores but the most recent one have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read_1() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
+// This thread's bulk stores have completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 }  // namespace pilot

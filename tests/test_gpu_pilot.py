@@ -84,6 +84,34 @@ def test_conv48_data_gradient_matches_torch(ctx):
     assert bool((d <= bar).all()), float((d - bar).max())
 
 
+@pytest.mark.parametrize("shape", [(2, 37, 53), (1, 8, 16), (3, 19, 7), (1, 1080, 1920)])
+def test_conv48_tma_pipeline_equals_cp_async_kernel(ctx, shape):
+    """The warp-specialised TMA pipeline (8 x 16 tiles, TMA halo loads and
+    stores) and the cp.async kernel (16 x 8 tiles) issue the same MMAs per
+    output pixel: identical BF16 outputs in every mode, ragged edges included."""
+    import torch
+    lib = ctx.lib
+    g = torch.Generator(device="cuda").manual_seed(4)
+    n, h, w = shape
+    x = torch.randn(n, h, w, C, device="cuda", generator=g).bfloat16()
+    aux = torch.randn(n, h, w, C, device="cuda", generator=g).bfloat16()
+    W = torch.randn(C, C, 3, 3, device="cuda", generator=g) * 0.05
+    b = torch.randn(C, device="cuda", generator=g) * 0.1
+    try:
+        for mode in (0, 1, 2):
+            out = {}
+            for which in (1, 2):
+                assert lib.bm3d_pilot_set_conv_kernel(which) == 0
+                out[which] = _conv48(ctx, x, W, b if mode < 2 else None, aux if mode == 2 else None,
+                                     mode)
+                assert lib.bm3d_pilot_conv_kernel() == which
+            assert torch.equal(out[1], out[2]), (mode, (out[1].float() - out[2].float()).abs().max())
+    finally:
+        lib.bm3d_pilot_set_conv_kernel(0)
+    _conv48(ctx, x, W, b, None, 0)
+    assert lib.bm3d_pilot_conv_kernel() == 2  # the default runs the TMA pipeline
+
+
 def test_wgrad48_matches_torch(ctx):
     import torch
     g = torch.Generator(device="cuda").manual_seed(3)
