@@ -862,7 +862,7 @@ def _trained_pilot(ctx, args):
     else:
         data = pilot_mod.make_dataset(ctx, crops=args.pilot_crops, planes=160)
         t1 = time.perf_counter()
-        hist = pilot_mod.train(pilot, data, epochs=args.pilot_epochs, batch=32, lr=2e-3)
+        hist = pilot_mod.train(pilot, data, epochs=args.pilot_epochs, batch=32)
         del data
         if args.pilot_checkpoint:
             pilot.save(args.pilot_checkpoint)
@@ -1123,7 +1123,7 @@ def main():
                     help="skip the batch64 / yuv4k16 figures the default run adds")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--pilot-crops", type=int, default=20000)
-    ap.add_argument("--pilot-epochs", type=int, default=2)
+    ap.add_argument("--pilot-epochs", type=int, default=30)
     ap.add_argument("--pilot-checkpoint", default="",
                     help="pilot workload: load this checkpoint if it exists, else train and save")
     ap.add_argument("--workload", default="sweep1080",

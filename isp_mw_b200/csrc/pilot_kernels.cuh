@@ -104,19 +104,33 @@ __device__ __forceinline__ void load_conv_tile(const __nv_bfloat16 *x, int h, in
 }
 
 // 27 MMAs: 9 taps x 3 steps of 16 input channels, into accumulator d_tmem.
-__device__ __forceinline__ void issue_conv_mmas(uint32_t a_base, uint32_t w_base, uint32_t d_tmem)
+// The operand tile's tap (dy, dx) starts dy * DY + dx * DX bytes in. Issued
+// by one thread, so the loop is fully unrolled and every descriptor is a base
+// descriptor plus a compile-time constant: the start-address field holds
+// address >> 4 in 14 bits and shared addresses stay below 256 KB, so the sum
+// never carries out of it. (Rebuilding both descriptors per MMA made this
+// thread's dependent scalar chain, not the tensor pipe, set the pace.)
+template <int DY, int DX>
+__device__ __forceinline__ void issue_tile_mmas(uint32_t a_base, uint32_t w_base, uint32_t d_tmem)
 {
-#pragma unroll 1
+    const uint64_t ad0 = smem_desc(a_base, kGroupBytes, kHaloColBytes);
+    const uint64_t bd0 = smem_desc(w_base, 128, 768);
+#pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
-        const int dy = tap / 3, dx = tap - 3 * (tap / 3);
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
-            const uint64_t ad = smem_desc(a_base + dx * kHaloColBytes + dy * 16 + s * 2 * kGroupBytes,
-                                          kGroupBytes, kHaloColBytes);
-            const uint64_t bd = smem_desc(w_base + tap * kTapBytes + s * 256, 128, 768);
+            const uint64_t ad = ad0 + static_cast<uint64_t>(
+                                          ((tap / 3) * DY + (tap % 3) * DX + s * 2 * kGroupBytes) >> 4);
+            const uint64_t bd = bd0 + static_cast<uint64_t>((tap * kTapBytes + s * 256) >> 4);
             mma_bf16(d_tmem, ad, bd, kIdescFwd, tap > 0 || s > 0);
         }
     }
+}
+
+// The cp.async kernel's tiles: columns kHaloColBytes apart, rows 16 bytes.
+__device__ __forceinline__ void issue_conv_mmas(uint32_t a_base, uint32_t w_base, uint32_t d_tmem)
+{
+    issue_tile_mmas<16, kHaloColBytes>(a_base, w_base, d_tmem);
 }
 
 // Epilogue of one tile. Each thread reads its pixel's (TMEM lane m = column
@@ -358,7 +372,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
     conv48_tma_kernel(const __grid_constant__ CUtensorMap tm_in,
                       const __grid_constant__ CUtensorMap tm_out, const ConvArgs a)
 {
-    extern __shared__ __align__(1024) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + kTmaOffBar);
     uint64_t *empty = full + kTmaStages;
     uint64_t *accf = empty + kTmaStages;
@@ -418,19 +432,9 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
                     break;
                 }
                 tc_fence_after();
-                const uint32_t a_base = smem_u32(smem + kTmaOffStage + s * kTileBytes);
-#pragma unroll 1
-                for (int tap = 0; tap < 9; ++tap) {
-                    const int dy = tap / 3, dx = tap - 3 * (tap / 3);
-#pragma unroll
-                    for (int st = 0; st < 3; ++st) {
-                        const uint64_t ad = smem_desc(
-                            a_base + dy * kHaloColBytes + dx * 16 + st * 2 * kGroupBytes, kGroupBytes,
-                            kHaloColBytes);
-                        const uint64_t bd = smem_desc(w_base + tap * kTapBytes + st * 256, 128, 768);
-                        mma_bf16(tbase + k * kAccCols, ad, bd, kIdescFwd, tap > 0 || st > 0);
-                    }
-                }
+                // 8 x 16 tiles: rows kHaloColBytes (960) apart, columns 16 bytes
+                issue_tile_mmas<kHaloColBytes, 16>(smem_u32(smem + kTmaOffStage + s * kTileBytes),
+                                                   w_base, tbase + k * kAccCols);
                 mma_commit(&empty[s]);  // the operand buffer is free once these MMAs finish
                 mma_commit(&accf[k]);
             }
@@ -610,13 +614,16 @@ __global__ void __launch_bounds__(kConvThreads, 1) wgrad48_kernel(const WgradArg
         if (tid == 0) {
             tc_fence_after();
             const uint32_t gb = smem_u32(smem + b * kWgBuf), xb = gb + kGTileBytes;
-#pragma unroll 1
+            // base descriptors plus compile-time offsets (as issue_tile_mmas)
+            const uint64_t ad0 = smem_desc(gb, 768, 128);
+            const uint64_t bd0 = smem_desc(xb, kHaloColBytes, kGroupBytes);
+#pragma unroll
             for (int s = 0; s < kTX / 2; ++s) {
 #pragma unroll
                 for (int dy = 0; dy < 3; ++dy) {
-                    const uint64_t ad = smem_desc(gb + s * 2 * kColBytes, 768, 128);
-                    const uint64_t bd = smem_desc(xb + dy * 16 + s * 2 * kHaloColBytes,
-                                                  kHaloColBytes, kGroupBytes);
+                    const uint64_t ad = ad0 + static_cast<uint64_t>((s * 2 * kColBytes) >> 4);
+                    const uint64_t bd =
+                        bd0 + static_cast<uint64_t>((dy * 16 + s * 2 * kHaloColBytes) >> 4);
                     mma_bf16(tbase + dy * 3 * kC, ad, bd, kIdescWg, it > 0 || s > 0);
                 }
             }

@@ -86,10 +86,13 @@ def make_dataset(ctx, crops: int = 20000, crop: int = 128, planes: int = 160,
     }
 
 
-def train(pilot, data: Dict, epochs: int = 3, batch: int = 32, lr: float = 2e-3,
-          lr_min: float = 2e-5, seed: int = 0, log_every: int = 0) -> List:
-    """Adam over shuffled batches with a cosine schedule; returns (step, loss)
-    pairs (the loss of each batch before its update)."""
+def train(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 1e-3,
+          lr_min: float = 1e-5, warmup: int = 500, seed: int = 0, log_every: int = 0) -> List:
+    """Adam over shuffled batches: the rate rises linearly over the first
+    `warmup` steps, then follows a cosine from `lr` to `lr_min` (a full-rate
+    start can drive every ReLU of a layer negative, after which the network
+    only passes the noisy plane through). Returns (step, loss) pairs (the loss
+    of each batch before its update)."""
     import torch
     n = data["noisy"].shape[0]
     steps_per_epoch = n // batch
@@ -102,6 +105,8 @@ def train(pilot, data: Dict, epochs: int = 3, batch: int = 32, lr: float = 2e-3,
         for k in range(steps_per_epoch):
             idx = perm[k * batch:(k + 1) * batch]
             rate = lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * step / max(1, total)))
+            if step < warmup:
+                rate *= (step + 1) / warmup
             loss = pilot.train_step(data["noisy"][idx].contiguous(), data["target"][idx].contiguous(),
                                     data["sigma"][idx].contiguous(), rate)
             hist.append((step, loss))
@@ -149,9 +154,9 @@ def main(argv=None):
     ap.add_argument("--out", default="pilot.bin")
     ap.add_argument("--crops", type=int, default=20000)
     ap.add_argument("--planes", type=int, default=160)
-    ap.add_argument("--epochs", type=int, default=3)
+    ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args(argv)
     import json
