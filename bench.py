@@ -862,7 +862,7 @@ def _trained_pilot(ctx, args):
     else:
         data = pilot_mod.make_dataset(ctx, crops=args.pilot_crops, planes=160)
         t1 = time.perf_counter()
-        hist = pilot_mod.train(pilot, data, epochs=args.pilot_epochs, batch=32)
+        hist, pilot.restarts = pilot_mod.fit(pilot, data, epochs=args.pilot_epochs)
         del data
         if args.pilot_checkpoint:
             pilot.save(args.pilot_checkpoint)
@@ -982,6 +982,11 @@ def run_pilot_yuv(args):
     ctx.close()
 
 
+# DRAM bytes (read + write) of one conv48_tma_kernel launch on one 1920x1080
+# plane, from the ncu capture in profiles/conv48_tma_kernel_1080p_full.txt
+PILOT_CONV_TRAFFIC_PER_PLANE = 199_160_576 + 156_573_952
+
+
 def run_pilot(args):
     """the learned pilot in place of the basic estimate. Trains
     the pilot on 20k 128x128 crops of synthetic 1920x1080 planes (sigma ~
@@ -1070,6 +1075,19 @@ def run_pilot(args):
     flops_cnn = len(SIGMAS) * W * H * 2 * 9 * (2 * 48 + 6 * 48 * 48 + 48)
     peaks = load_peaks()
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    # the dominant kernel: the six 48 -> 48 layers of the pilot's forward
+    # pass over the step's four planes, each one launch, timed with CUDA
+    # events recorded around each layer on the launching stream
+    pilot.set_timing(True)
+    lay = np.zeros(8)
+    for _ in range(10):
+        pilot_net()
+        lay += pilot.layer_ms() / 10
+    pilot.set_timing(False)
+    ms_conv = float(lay[1:7].mean())
+    conv_kernel = {2: "conv48_tma_kernel", 1: "conv48_kernel"}.get(
+        int(lib.bm3d_pilot_conv_kernel()), "none")
+    flops_conv = len(SIGMAS) * W * H * 2 * 9 * 48 * 48
     if rank == 0:
         line = {
             "metric": "BM3D MP/s with the learned pilot in place of the basic estimate "
@@ -1085,6 +1103,7 @@ def run_pilot(args):
                        "train_crops": args.pilot_crops, "train_epochs": args.pilot_epochs,
                        "train_batch": 32, "data_s": round(t_data, 1),
                        "train_s": round(t_train, 1), "train_steps": len(hist),
+                       "train_restarts": getattr(pilot, "restarts", 0),
                        "final_loss": hist[-1][1] if hist else None},
             "plain": {"value": round(mp / (ms_plain / 1e3), 3), "unit": "MP/s",
                       "ms_per_step": round(ms_plain, 4),
@@ -1094,12 +1113,20 @@ def run_pilot(args):
             "pilot_final_ms_per_launch": round(tpf, 4),
             "ceiling": {"formula": "(T_basic + T_final) / (T_pilot + T_final), batch kernels",
                         "value": round((tb + tf) / (ms_cnn + tf), 4), "target": 2.0},
-            "roofline": {"bound": "tensor", "kernel": "pilot network (conv48 layers dominate)",
-                         "achieved": round(flops_cnn / (ms_cnn / 1e3) / 1e12, 2),
+            "roofline": {"bound": "tensor", "kernel": conv_kernel,
+                         "launch": "one 48 -> 48 layer over the step's four 1920x1080 planes "
+                                   "(the six such layers are 98 % of the network's FLOPs)",
+                         "per_launch_ms": round(ms_conv, 4),
+                         "algorithmic_gflop_per_launch": round(flops_conv / 1e9, 2),
+                         "achieved": round(flops_conv / (ms_conv / 1e3) / 1e12, 2),
                          "peak": bf16_peak, "unit": "TFLOP/s",
-                         "frac": round(flops_cnn / (ms_cnn / 1e3) / 1e12 / bf16_peak, 4),
+                         "frac": round(flops_conv / (ms_conv / 1e3) / 1e12 / bf16_peak, 4),
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)",
-                         "traffic": None},
+                         "traffic": PILOT_CONV_TRAFFIC_PER_PLANE * len(SIGMAS),
+                         "traffic_source": "4 x the one-plane capture "
+                                           "(profiles/conv48_tma_kernel_1080p_full.txt)",
+                         "network_tflops": round(flops_cnn / (ms_cnn / 1e3) / 1e12, 2),
+                         "layer_ms": [round(float(x), 4) for x in lay]},
             "psnr_vs_clean": psnr,
             "eval_1080p": evals,
             "gpu_launches": args.steps * (8 + 6),

@@ -402,6 +402,15 @@ int bm3d_pilot_param_count(void);
  * BM3D_ERR_CUDA when its maps do not encode). Both give identical results. */
 int bm3d_pilot_set_conv_kernel(int which);
 
+/* Per-layer timing of the pilot's forward passes (off by default): with it on,
+ * every forward pass records CUDA events on its stream around each of the
+ * eight layers. */
+int bm3d_pilot_set_timing(bm3d_pilot *pilot, int on);
+
+/* Device ms of each of the eight layers of the last timed forward pass
+ * (ms[0] layer 1, ms[1..6] the 48 -> 48 layers, ms[7] layer 8); waits for it. */
+int bm3d_pilot_layer_ms(bm3d_pilot *pilot, float *ms);
+
 /* The kernel of the last 48 -> 48 convolution launched: 2 = TMA pipeline,
  * 1 = cp.async kernel, 0 = none yet. */
 int bm3d_pilot_conv_kernel(void);

@@ -45,6 +45,7 @@ EXPORTS = [
     "bm3d_inject_alloc_failures", "bm3d_batch_stage_times", "bm3d_batch_final_create",
     "bm3d_batch3_final_create",
     "bm3d_pilot_param_count", "bm3d_pilot_set_conv_kernel", "bm3d_pilot_conv_kernel",
+    "bm3d_pilot_set_timing", "bm3d_pilot_layer_ms",
     "bm3d_pilot_create", "bm3d_pilot_destroy", "bm3d_pilot_set_params",
     "bm3d_pilot_get_params", "bm3d_pilot_get_grad", "bm3d_pilot_save", "bm3d_pilot_load",
     "bm3d_pilot_estimate", "bm3d_pilot_train_step", "bm3d_pilot_full", "bm3d_pilot_conv48",
@@ -134,6 +135,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.bm3d_pilot_param_count.argtypes = []
     lib.bm3d_pilot_set_conv_kernel.argtypes = [ip]
     lib.bm3d_pilot_conv_kernel.argtypes = []
+    lib.bm3d_pilot_set_timing.argtypes = [vp, ip]
+    lib.bm3d_pilot_layer_ms.argtypes = [vp, vp]
     lib.bm3d_pilot_create.argtypes = [vp, ctypes.c_ulonglong, ctypes.POINTER(vp)]
     lib.bm3d_pilot_destroy.argtypes = [vp]
     lib.bm3d_pilot_destroy.restype = None
@@ -790,6 +793,16 @@ class Pilot:
     def grad(self) -> np.ndarray:
         out = np.empty(self.count, np.float32)
         self.ctx._check(self.lib.bm3d_pilot_get_grad(self.h, out.ctypes.data, self.count))
+        return out
+
+    def set_timing(self, on: bool):
+        """Record CUDA events around each layer of later forward passes."""
+        self.ctx._check(self.lib.bm3d_pilot_set_timing(self.h, 1 if on else 0))
+
+    def layer_ms(self) -> np.ndarray:
+        """Device ms of the eight layers of the last timed forward pass."""
+        out = np.empty(8, np.float32)
+        self.ctx._check(self.lib.bm3d_pilot_layer_ms(self.h, out.ctypes.data))
         return out
 
     def set_params(self, values: np.ndarray):

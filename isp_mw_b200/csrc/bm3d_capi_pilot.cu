@@ -24,6 +24,10 @@ struct bm3d_pilot {
     DevBuf act[7];                        // X1..X7 (inference uses act[0], act[1])
     DevBuf gbuf[2];                       // pre-activation gradients, ping-pong
     DevBuf dout, out, partial, loss, err, sigma;
+    // per-layer timing of forward passes (bm3d_pilot_set_timing): events
+    // before layer 1, after each of the eight layers
+    bool timing = false;
+    cudaEvent_t ev[9] = {};
 };
 
 namespace {
@@ -231,13 +235,17 @@ int forward(bm3d_pilot *p, const float *in, long long stride, long long img_stri
     ia.n = n;
     ia.h = h;
     ia.w = w;
+    if (p->timing) CK(ctx, cudaEventRecord(p->ev[0], s));
     conv_in_kernel<<<blocks, 256, 0, s>>>(ia);
     CK(ctx, cudaGetLastError());
+    if (p->timing) CK(ctx, cudaEventRecord(p->ev[1], s));
     int rc;
-    for (int layer = 2; layer <= 7; ++layer)
+    for (int layer = 2; layer <= 7; ++layer) {
         if ((rc = run_conv48(ctx, X(layer - 1), X(layer), wfwd(p, layer), param(p, off_b(layer)),
                              nullptr, kBiasRelu, n, h, w, err, s)) != BM3D_OK)
             return rc;
+        if (p->timing) CK(ctx, cudaEventRecord(p->ev[layer], s));
+    }
     OutArgs oa;
     oa.x = X(7);
     oa.noisy = in;
@@ -254,6 +262,7 @@ int forward(bm3d_pilot *p, const float *in, long long stride, long long img_stri
     oa.w = w;
     conv_out_kernel<<<blocks, 256, 0, s>>>(oa);
     CK(ctx, cudaGetLastError());
+    if (p->timing) CK(ctx, cudaEventRecord(p->ev[8], s));
     return BM3D_OK;
 }
 
@@ -305,6 +314,26 @@ extern "C" int bm3d_pilot_create(bm3d_ctx *ctx, unsigned long long seed, bm3d_pi
     return BM3D_OK;
 }
 
+extern "C" int bm3d_pilot_set_timing(bm3d_pilot *p, int on)
+{
+    if (!p) return BM3D_ERR_INVALID;
+    CK(p->ctx, cudaSetDevice(p->ctx->device));
+    if (on)
+        for (cudaEvent_t &e : p->ev)
+            if (!e) CK(p->ctx, cudaEventCreate(&e));
+    p->timing = on != 0;
+    return BM3D_OK;
+}
+
+extern "C" int bm3d_pilot_layer_ms(bm3d_pilot *p, float *ms)
+{
+    if (!p || !ms || !p->ev[8]) return BM3D_ERR_INVALID;
+    CK(p->ctx, cudaSetDevice(p->ctx->device));
+    CK(p->ctx, cudaEventSynchronize(p->ev[8]));
+    for (int i = 0; i < 8; ++i) CK(p->ctx, cudaEventElapsedTime(&ms[i], p->ev[i], p->ev[i + 1]));
+    return BM3D_OK;
+}
+
 extern "C" void bm3d_pilot_destroy(bm3d_pilot *p)
 {
     if (!p) return;
@@ -315,6 +344,8 @@ extern "C" void bm3d_pilot_destroy(bm3d_pilot *p)
     for (auto &b : p->act) bufs.push_back(&b);
     for (DevBuf *b : bufs)
         if (b->ptr) cudaFree(b->ptr);
+    for (cudaEvent_t e : p->ev)
+        if (e) cudaEventDestroy(e);
     delete p;
 }
 

@@ -86,8 +86,8 @@ def make_dataset(ctx, crops: int = 20000, crop: int = 128, planes: int = 160,
     }
 
 
-def train(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 1e-3,
-          lr_min: float = 1e-5, warmup: int = 500, seed: int = 0, log_every: int = 0) -> List:
+def train(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 2e-3,
+          lr_min: float = 2e-5, warmup: int = 1000, seed: int = 0, log_every: int = 0) -> List:
     """Adam over shuffled batches: the rate rises linearly over the first
     `warmup` steps, then follows a cosine from `lr` to `lr_min` (a full-rate
     start can drive every ReLU of a layer negative, after which the network
@@ -114,6 +114,35 @@ def train(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 1e-3
                 print(f"step {step}/{total} lr {rate:.2e} loss {loss:.3e}", flush=True)
             step += 1
     return hist
+
+
+def collapsed(hist: List) -> bool:
+    """True when training ended no better than half its starting loss: the
+    network went dead (every ReLU of a layer negative) and passes the noisy
+    plane through."""
+    if len(hist) < 600:
+        return False
+    first = float(np.mean([l for _, l in hist[:50]]))
+    last = float(np.mean([l for _, l in hist[-500:]]))
+    return not last < 0.5 * first
+
+
+def fit(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 2e-3, seed: int = 0,
+        attempts: int = 3, log_every: int = 0):
+    """train(), restarted from a fresh initialisation at half the rate when a
+    run collapses. Returns (history of the last run, restarts)."""
+    from . import Pilot
+    hist: List = []
+    for k in range(attempts):
+        if k > 0:
+            fresh = Pilot(pilot.ctx, seed=seed + 1000 * k)
+            pilot.set_params(fresh.params())
+            fresh.close()
+        hist = train(pilot, data, epochs=epochs, batch=batch, lr=lr / (2 ** k), seed=seed + k,
+                     log_every=log_every)
+        if not collapsed(hist):
+            return hist, k
+    return hist, attempts - 1
 
 
 def evaluate(ctx, pilot, sigmas: Sequence[float] = (5.0, 10.0, 25.0, 50.0), shape=(1080, 1920),
@@ -156,7 +185,7 @@ def main(argv=None):
     ap.add_argument("--planes", type=int, default=160)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args(argv)
     import json
@@ -166,13 +195,14 @@ def main(argv=None):
     data = make_dataset(ctx, crops=args.crops, planes=args.planes, seed=1234 + args.seed)
     t1 = time.time()
     pilot = Pilot(ctx, seed=args.seed)
-    hist = train(pilot, data, epochs=args.epochs, batch=args.batch, lr=args.lr, seed=args.seed,
-                 log_every=100)
+    hist, restarts = fit(pilot, data, epochs=args.epochs, batch=args.batch, lr=args.lr,
+                         seed=args.seed, log_every=100)
     t2 = time.time()
     pilot.save(args.out)
     res = evaluate(ctx, pilot)
     print(json.dumps({"data_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1),
-                      "steps": len(hist), "final_loss": hist[-1][1], "eval": res}))
+                      "steps": len(hist), "restarts": restarts, "final_loss": hist[-1][1],
+                      "eval": res}))
 
 
 if __name__ == "__main__":

@@ -198,6 +198,22 @@ def test_pilot_forward_matches_emulation(ctx):
     p.close()
 
 
+def test_pilot_layer_timing(ctx):
+    """bm3d_pilot_set_timing / bm3d_pilot_layer_ms: eight positive layer
+    times, the 48 -> 48 layers the bulk of the pass."""
+    import torch
+    import isp_mw_b200
+    p = isp_mw_b200.Pilot(ctx, seed=12)
+    noisy, _, sigma = _data(2, 256, 320, 61)
+    out = torch.empty_like(noisy)
+    p.set_timing(True)
+    p.estimate(out, noisy, sigma.cpu().numpy())
+    ms = p.layer_ms()
+    p.set_timing(False)
+    assert ms.shape == (8,) and (ms > 0).all(), ms
+    p.close()
+
+
 def test_pilot_gradient_matches_autograd(ctx):
     import torch
     import isp_mw_b200
