@@ -168,6 +168,14 @@ def batch_case(args):
     print(f"batch of {args.batch} {args.width}x{args.height}: basic "
           f"{sum(x[0] for x in t) / len(t):.4f} ms, final {sum(x[1] for x in t) / len(t):.4f} ms "
           f"per persistent launch")
+    if args.time:  # whole pipeline from its CUDA graph, 20 replays after the runs above
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(20):
+            batch.run()
+        ev1.record()
+        torch.cuda.synchronize()
+        print(f"graph replay: {ev0.elapsed_time(ev1) / 20:.4f} ms per run of the {args.batch} planes")
     batch.close()
     ctx.close()
 
