@@ -14,7 +14,7 @@ namespace bm3d {
 constexpr int kBatchHeader = 16;
 
 template <typename T, bool WIENER, int NPL, int KS, bool GENERIC>
-__global__ void __launch_bounds__(GENERIC ? 256 : 512, 1)
+__global__ void __launch_bounds__(GENERIC ? (sizeof(T) == 4 ? 384 : 256) : 512, 1)
     batch_stage_kernel(const StageArgs<T> *__restrict__ args, const int *__restrict__ tile_base,
                        int nimg, int *counter)
 {

@@ -533,9 +533,10 @@ static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params
     a.ny = ref_count(height - BS, a.step);
     const int span = 2 * (a.range / a.bm_step) + 1;
     a.key_slots = span * span + 1;
-    // the generic kernel launches at most 8 warps (launch bounds 256) on 4x4 tiles
+    // the generic kernel launches at most 12 warps in FP32 and 8 in FP64
+    // (launch bounds 384 / 256), on 4x4 tiles
     int tx = generic ? 4 : ctx->tile_x, ty = generic ? 4 : ctx->tile_y;
-    warps = generic ? 8 : ctx->warps;
+    warps = generic ? (sizeof(T) == 4 ? 12 : 8) : ctx->warps;
     for (;;) {
         const int reach = a.match ? a.range : 0;
         a.region_w = std::min(width, (tx - 1) * a.step + 2 * reach + BS);
@@ -549,7 +550,8 @@ static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params
         if (sp.total <= ctx->smem_optin) break;
         // The generic kernel's per-warp group buffers dominate its footprint:
         // give up warps before tile size there.
-        if (warps > 8 || (generic && warps > 1)) warps /= 2;
+        if (generic && warps == 12) warps = 8;
+        else if (warps > 8 || (generic && warps > 1)) warps /= 2;
         else if (ty > 1 && ty >= tx) --ty;
         else if (tx > 1) --tx;
         else if (warps > 1) warps /= 2;

@@ -347,6 +347,14 @@ __device__ __forceinline__ unsigned dynamic_smem_bytes()
 // a warp on 32 distinct banks; other sizes are dense.
 __host__ __device__ __forceinline__ int generic_block_stride(int bs) { return bs == 8 ? 72 : bs * bs; }
 __host__ __device__ __forceinline__ int generic_row_stride(int bs) { return bs == 8 ? 9 : bs; }
+// Whether the generic kernel's Wiener stage filters from one group buffer per
+// warp, keeping the Wiener weights in registers (BlockSize 8, FP32), rather
+// than from two.
+template <typename T>
+__host__ __device__ constexpr bool generic_one_buffer(bool wiener, int bs)
+{
+    return wiener && bs == 8 && sizeof(T) == 4;
+}
 
 // Shared-memory layout of one CTA. The register-resident kernel runs three
 // planes one after another through a single plane's windows: it then also
@@ -379,7 +387,8 @@ __host__ __device__ inline SmemPlan plan_smem(int nplanes, bool wiener, int alia
     s.off_origin_acc = s.off_origin + (sizeof(T) * bsq * s.n_stage + 15) / 16 * 16;
     s.off_warps = (s.off_origin_acc + sizeof(Acc) * bsq * 2 * nplanes + 15) / 16 * 16;
     const size_t group_bytes = generic
-        ? sizeof(T) * static_cast<size_t>(gs) * generic_block_stride(bs) * (wiener ? 2 : 1)
+        ? sizeof(T) * static_cast<size_t>(gs) * generic_block_stride(bs) *
+              (wiener && !generic_one_buffer<T>(wiener, bs) ? 2 : 1)
         : sizeof(T) * kGSMax * kGroupStride;
     const size_t key_bytes = sizeof(SortKey<T>) * key_slots;
     const size_t scratch = group_bytes > key_bytes ? group_bytes : key_bytes;

@@ -220,6 +220,73 @@ __device__ __forceinline__ void group_index(int e, int bs, int bsq, int &z, int 
     }
 }
 
+// Gather one group of plane windows (win, its (0, 0) copy win0) into G, in
+// the [z][y][x] layout of generic_block_stride / generic_row_stride.
+template <typename T>
+__device__ __forceinline__ void gather_generic(const Tile<T> &t, const T *win, const T *win0,
+                                               const BlockPos *list, int n, int lane, T *G,
+                                               unsigned *n_bad)
+{
+    const int bs = t.bs, bsq = bs * bs, total = n * bsq;
+    const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
+    for (int e = lane; e < total; e += kWarp) {
+        int z, y, x;
+        group_index(e, bs, bsq, z, y, x);
+        const BlockPos q = list[z];
+        const bool ok = block_in_tile(t, q.y, q.x);
+        if (n_bad && !ok && y == 0 && x == 0) ++*n_bad;
+        int pitch;
+        const T *bp = block_ptr(t, win, win0, ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
+        G[z * zs + y * rs + x] = ok ? bp[y * pitch + x] : T(0);
+    }
+}
+
+// Wiener shrinkage of a BlockSize-8 FP32 group with ONE group buffer: the
+// basic estimate's group is transformed in G, each lane keeps the Wiener
+// weights of its two pencils (lane and lane + 32: 2 x 32 registers), then
+// the noisy group is transformed in the same buffer and scaled. Elements,
+// weights and the lane's sum of squared weights come out in exactly the
+// order of the two-buffer form (a lane's elements e = lane + 32 k are pencil
+// lane + 32 (k % 2) at z = k / 2), so results are bit-identical; the warp
+// needs half the shared memory. Returns the lane's sum of w^2.
+template <typename T>
+__device__ __forceinline__ T wiener_one_buffer(const StageArgs<T> &a, const Tile<T> &t, int p,
+                                               int pt, const BlockPos *list, int n, int lane, T *G,
+                                               unsigned &n_bad)
+{
+    gather_generic(t, t.refw[p], t.ref0[p], list, n, lane, G, static_cast<unsigned *>(nullptr));
+    __syncwarp();
+    dct3_generic(G, n, 8, lane, a.dct_fwd, false);
+    const T s2 = a.wss[pt][n - 1];
+    T *const p0 = G + (lane >> 3) * 9 + (lane & 7);  // pencil lane
+    T *const p1 = p0 + 4 * 9;                        // pencil lane + 32
+    T w0[kGSTab], w1[kGSTab];
+    T l2 = T(0);
+#pragma unroll
+    for (int z = 0; z < kGSTab; ++z) {
+        w0[z] = w1[z] = T(0);
+        if (z < n) {
+            const T y0 = p0[z * 72], y1 = p1[z * 72];
+            w0[z] = wiener_weight(y0 * y0, s2);
+            l2 += w0[z] * w0[z];
+            w1[z] = wiener_weight(y1 * y1, s2);
+            l2 += w1[z] * w1[z];
+        }
+    }
+    __syncwarp();
+    gather_generic(t, t.srcw[p], t.src0[p], list, n, lane, G, &n_bad);
+    __syncwarp();
+    dct3_generic(G, n, 8, lane, a.dct_fwd, false);
+#pragma unroll
+    for (int z = 0; z < kGSTab; ++z)
+        if (z < n) {
+            p0[z * 72] *= w0[z];
+            p1[z * 72] *= w1[z];
+        }
+    __syncwarp();
+    return l2;
+}
+
 // Collaborative filtering of one group on plane p (generic sizes).
 template <typename T, bool WIENER>
 __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, const BlockPos *list,
@@ -231,6 +298,11 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     if (pt < 0) pt = p;
     const int bs = t.bs, bsq = bs * bs, total = n * bsq;
     const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
+    T denW;
+    if (WIENER && generic_one_buffer<T>(WIENER, bs)) {
+        const T l2 = warp_sum(wiener_one_buffer(a, t, p, pt, list, n, lane, Gs, n_bad));
+        denW = l2 <= T(0) ? T(1) : T(1) / l2;
+    } else {
     for (int e = lane; e < total; e += kWarp) {
         int z, y, x;
         group_index(e, bs, bsq, z, y, x);
@@ -248,7 +320,6 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     }
     __syncwarp();
     dct3_generic(Gs, n, bs, lane, a.dct_fwd, false);
-    T denW;
     if (!WIENER) {
         // hard threshold (source/BM3D.cpp:361-371) with thr by #zero indices
         const T *thr = a.thr[pt][n - 1];
@@ -278,6 +349,7 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         }
         l2 = warp_sum(l2);
         denW = l2 <= T(0) ? T(1) : T(1) / l2;
+    }
     }
     const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
     __syncwarp();
@@ -480,7 +552,8 @@ __device__ __forceinline__ void generic_tile_body_seq3(const StageArgs<T> &a, in
 }
 
 template <typename T, bool WIENER, int NPL>
-__global__ void __launch_bounds__(256, 1) generic_stage_kernel(const StageArgs<T> a)
+__global__ void __launch_bounds__(sizeof(T) == 4 ? 384 : 256, 1)
+    generic_stage_kernel(const StageArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     if constexpr (NPL == 3) generic_tile_body_seq3<T, WIENER>(a, blockIdx.x, smem, dynamic_smem_bytes());
