@@ -533,10 +533,17 @@ static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params
     a.ny = ref_count(height - BS, a.step);
     const int span = 2 * (a.range / a.bm_step) + 1;
     a.key_slots = span * span + 1;
-    // the generic kernel launches at most 12 warps in FP32 and 8 in FP64
-    // (launch bounds 384 / 256), on 4x4 tiles
-    int tx = generic ? 4 : ctx->tile_x, ty = generic ? 4 : ctx->tile_y;
-    warps = generic ? (sizeof(T) == 4 ? 12 : 8) : ctx->warps;
+    // The generic kernel (launch bounds 384 in FP32, 256 in FP64) takes the
+    // first of these (tile_x, tile_y, warps) that fits: reference blocks per
+    // tile a multiple of the warps, so no warp idles in a tile's last round.
+    static const int gen32[][3] = {{6, 4, 12}, {4, 3, 12}, {4, 4, 8}, {4, 4, 4},
+                                   {2, 2, 4},  {2, 2, 2},  {1, 1, 2}, {1, 1, 1}};
+    static const int gen64[][3] = {{4, 4, 8}, {4, 4, 4}, {2, 2, 4}, {2, 2, 2}, {1, 1, 2}, {1, 1, 1}};
+    const int (*gcand)[3] = sizeof(T) == 4 ? gen32 : gen64;
+    const int ngcand = sizeof(T) == 4 ? 8 : 6;
+    int gi = 0;
+    int tx = generic ? gcand[0][0] : ctx->tile_x, ty = generic ? gcand[0][1] : ctx->tile_y;
+    warps = generic ? gcand[0][2] : ctx->warps;
     for (;;) {
         const int reach = a.match ? a.range : 0;
         a.region_w = std::min(width, (tx - 1) * a.step + 2 * reach + BS);
@@ -548,14 +555,23 @@ static int plan_geometry(bm3d_ctx *ctx, StageArgs<T> &a, const bm3d_stage_params
                                          a.region_pitch, a.key_slots, warps, generic, BS,
                                          p->group_size, std::min(tx, a.nx) * std::min(ty, a.ny));
         if (sp.total <= ctx->smem_optin) break;
-        // The generic kernel's per-warp group buffers dominate its footprint:
-        // give up warps before tile size there.
-        if (generic && warps == 12) warps = 8;
-        else if (warps > 8 || (generic && warps > 1)) warps /= 2;
-        else if (ty > 1 && ty >= tx) --ty;
-        else if (tx > 1) --tx;
-        else if (warps > 1) warps /= 2;
-        else {
+        if (generic) {
+            if (++gi >= ngcand) {
+                ctx->err = "stage does not fit in shared memory";
+                return BM3D_ERR_UNSUPPORTED;
+            }
+            tx = gcand[gi][0];
+            ty = gcand[gi][1];
+            warps = gcand[gi][2];
+        } else if (warps > 8) {
+            warps /= 2;
+        } else if (ty > 1 && ty >= tx) {
+            --ty;
+        } else if (tx > 1) {
+            --tx;
+        } else if (warps > 1) {
+            warps /= 2;
+        } else {
             ctx->err = "stage does not fit in shared memory";
             return BM3D_ERR_UNSUPPORTED;
         }

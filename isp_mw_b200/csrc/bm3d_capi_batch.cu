@@ -353,10 +353,10 @@ int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotu
     const bool generic = !fast_args(p.block_size, p.group_size);
     static const int fast_cand[][3] = {{8, 8, 16}, {7, 7, 16}, {6, 8, 12}, {8, 6, 12},
                                        {6, 6, 12}, {4, 4, 4}, {4, 4, 2}, {2, 2, 1}};
-    static const int gen_cand[][3] = {{4, 4, 12}, {4, 4, 8}, {4, 4, 4}, {2, 2, 4},
-                                      {2, 2, 2}, {1, 1, 2}, {1, 1, 1}};
+    static const int gen_cand[][3] = {{6, 4, 12}, {4, 3, 12}, {4, 4, 8}, {4, 4, 4},
+                                      {2, 2, 4},  {2, 2, 2},  {1, 1, 2}, {1, 1, 1}};
     const int (*cand)[3] = generic ? gen_cand : fast_cand;
-    const int ncand = generic ? 7 : 8;
+    const int ncand = 8;
     int best = -1;
     float best_ms = 1e30f;
     for (int c = 0; c < ncand; ++c) {
