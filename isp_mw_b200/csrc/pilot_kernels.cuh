@@ -719,10 +719,46 @@ struct InArgs {
     int n, h, w;
 };
 
+// Packed FP32 pairs (fma.rn.f32x2: each half rounded like a scalar FMA).
+__device__ __forceinline__ unsigned long long f2pack(float lo, float hi)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2unpack(unsigned long long v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long ffma2(unsigned long long a, unsigned long long b,
+                                                    unsigned long long c)
+{
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// Layer 1, one pixel per thread. The noise-level input is constant inside the
+// image, so for a pixel whose 3 x 3 neighbourhood is inside, its part is
+// sigma * sum_t W1[c][1][t] (one constant per channel); border pixels sum it
+// over their inside taps. Channel pairs run as packed FMAs on weights kept
+// [tap][channel] in shared memory (128-bit broadcast reads).
 __global__ void __launch_bounds__(256) conv_in_kernel(const InArgs a)
 {
-    __shared__ float ws[kW1 + kC];
-    for (int i = threadIdx.x; i < kW1 + kC; i += blockDim.x) ws[i] = a.wb[i];
+    __shared__ __align__(16) float wn[9][kC];  // W1[c][0][t] at [t][c]
+    __shared__ __align__(16) float wsg[9][kC]; // W1[c][1][t] at [t][c]
+    __shared__ __align__(16) float bias[kC], stot[kC];
+    for (int i = threadIdx.x; i < 9 * kC; i += blockDim.x) {
+        const int t = i / kC, c = i - t * kC;
+        wn[t][c] = a.wb[(c * 2 + 0) * 9 + t];
+        wsg[t][c] = a.wb[(c * 2 + 1) * 9 + t];
+    }
+    for (int c = threadIdx.x; c < kC; c += blockDim.x) {
+        bias[c] = a.wb[kW1 + c];
+        float st = 0.0f;
+        for (int t = 0; t < 9; ++t) st += a.wb[(c * 2 + 1) * 9 + t];
+        stot[c] = st;
+    }
     __syncthreads();
     const long long total = static_cast<long long>(a.n) * a.h * a.w;
     for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < total;
@@ -731,25 +767,47 @@ __global__ void __launch_bounds__(256) conv_in_kernel(const InArgs a)
         const int r = static_cast<int>(p - static_cast<long long>(img) * a.h * a.w);
         const int y = r / a.w, x = r - y * a.w;
         const float s = a.sigma[img];
-        float nb[9], sb[9];
+        const bool interior = y > 0 && y < a.h - 1 && x > 0 && x < a.w - 1;
+        unsigned long long nd[9];  // (noisy, noisy) of each tap, 0 outside
+        unsigned inside = 0;
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
             const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
             const bool ok = yy >= 0 && yy < a.h && xx >= 0 && xx < a.w;
-            nb[t] = ok ? __ldg(a.in + img * a.img_stride + yy * a.stride + xx) : 0.0f;
-            sb[t] = ok ? s : 0.0f;
+            const float v = ok ? __ldg(a.in + img * a.img_stride + yy * a.stride + xx) : 0.0f;
+            nd[t] = f2pack(v, v);
+            inside |= (ok ? 1u : 0u) << t;
         }
+        const unsigned long long sd = f2pack(s, s);
         uint32_t packed[24];
 #pragma unroll
-        for (int c = 0; c < kC; c += 2) {
-            float v0 = ws[kW1 + c], v1 = ws[kW1 + c + 1];
+        for (int c = 0; c < kC; c += 4) {
+            const float4 b4 = *reinterpret_cast<const float4 *>(&bias[c]);
+            unsigned long long acc0 = f2pack(b4.x, b4.y), acc1 = f2pack(b4.z, b4.w);
+            if (interior) {
+                const float4 s4 = *reinterpret_cast<const float4 *>(&stot[c]);
+                acc0 = ffma2(sd, f2pack(s4.x, s4.y), acc0);
+                acc1 = ffma2(sd, f2pack(s4.z, s4.w), acc1);
+            } else {
+#pragma unroll
+                for (int t = 0; t < 9; ++t)
+                    if (inside & (1u << t)) {
+                        const float4 s4 = *reinterpret_cast<const float4 *>(&wsg[t][c]);
+                        acc0 = ffma2(sd, f2pack(s4.x, s4.y), acc0);
+                        acc1 = ffma2(sd, f2pack(s4.z, s4.w), acc1);
+                    }
+            }
 #pragma unroll
             for (int t = 0; t < 9; ++t) {
-                v0 += ws[(c * 2 + 0) * 9 + t] * nb[t] + ws[(c * 2 + 1) * 9 + t] * sb[t];
-                v1 += ws[((c + 1) * 2 + 0) * 9 + t] * nb[t] + ws[((c + 1) * 2 + 1) * 9 + t] * sb[t];
+                const float4 w4 = *reinterpret_cast<const float4 *>(&wn[t][c]);
+                acc0 = ffma2(nd[t], f2pack(w4.x, w4.y), acc0);
+                acc1 = ffma2(nd[t], f2pack(w4.z, w4.w), acc1);
             }
-            const __nv_bfloat162 b2 = __floats2bfloat162_rn(fmaxf(v0, 0.0f), fmaxf(v1, 0.0f));
-            packed[c >> 1] = *reinterpret_cast<const uint32_t *>(&b2);
+            float v0, v1, v2, v3;
+            f2unpack(acc0, v0, v1);
+            f2unpack(acc1, v2, v3);
+            packed[c / 2] = pack_bf16(v0, v1, true);
+            packed[c / 2 + 1] = pack_bf16(v2, v3, true);
         }
         uint4 *dst = reinterpret_cast<uint4 *>(a.y + p * kC);
 #pragma unroll
@@ -774,46 +832,89 @@ struct OutArgs {
     int n, h, w;
 };
 
+// Tiles of 32 x 8 output pixels, one per thread. Each pixel q of the tile and
+// its one-pixel halo is read and unpacked once, giving its nine per-tap
+// partial sums P_t(q) = sum_c W8[c][t] X7[q][c] (channel pairs as packed
+// FMAs, weights [tap][channel] in shared memory); then
+// out(p) = noisy(p) + b8 + sum_t P_t(p + tap offset t).
+constexpr int kOutTX = 32, kOutTY = 8;
+constexpr int kOutHX = kOutTX + 2, kOutHY = kOutTY + 2;
+
 __global__ void __launch_bounds__(256) conv_out_kernel(const OutArgs a)
 {
-    __shared__ float ws[kW8 + 1];
+    __shared__ __align__(16) float wt[9][kC];  // W8[c][t] at [t][c]
+    __shared__ float part[9][kOutHY * kOutHX];
     __shared__ double red[8];
-    for (int i = threadIdx.x; i < kW8 + 1; i += blockDim.x) ws[i] = a.wb[i];
+    for (int i = threadIdx.x; i < 9 * kC; i += blockDim.x) {
+        const int t = i / kC, c = i - t * kC;
+        wt[t][c] = a.wb[c * 9 + t];
+    }
+    const float b8 = a.wb[kW8];
     __syncthreads();
-    const long long total = static_cast<long long>(a.n) * a.h * a.w;
+    const int tiles_x = (a.w + kOutTX - 1) / kOutTX, tiles_y = (a.h + kOutTY - 1) / kOutTY;
+    const long long ntiles = static_cast<long long>(a.n) * tiles_x * tiles_y;
     double err2 = 0.0;
-    for (long long p = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; p < total;
-         p += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const int img = static_cast<int>(p / (static_cast<long long>(a.h) * a.w));
-        const int r = static_cast<int>(p - static_cast<long long>(img) * a.h * a.w);
-        const int y = r / a.w, x = r - y * a.w;
-        float acc = ws[kW8];
-#pragma unroll 1
-        for (int t = 0; t < 9; ++t) {
-            const int yy = y + t / 3 - 1, xx = x + t % 3 - 1;
-            if (yy < 0 || yy >= a.h || xx < 0 || xx >= a.w) continue;
-            const uint4 *src = reinterpret_cast<const uint4 *>(
-                a.x + ((static_cast<long long>(img) * a.h + yy) * a.w + xx) * kC);
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int img = static_cast<int>(tile / (static_cast<long long>(tiles_x) * tiles_y));
+        const int r = static_cast<int>(tile - static_cast<long long>(img) * tiles_x * tiles_y);
+        const int ty = r / tiles_x;
+        const int y0 = ty * kOutTY, x0 = (r - ty * tiles_x) * kOutTX;
+        for (int i = threadIdx.x; i < kOutHY * kOutHX; i += blockDim.x) {
+            const int hy = i / kOutHX, hx = i - hy * kOutHX;
+            const int gy = y0 - 1 + hy, gx = x0 - 1 + hx;
+            unsigned long long acc[9];
 #pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const uint4 u = __ldg(src + q);
-                const unsigned wd[4] = {u.x, u.y, u.z, u.w};
+            for (int t = 0; t < 9; ++t) acc[t] = 0ull;
+            if (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w) {
+                const uint4 *src = reinterpret_cast<const uint4 *>(
+                    a.x + ((static_cast<long long>(img) * a.h + gy) * a.w + gx) * kC);
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int c = q * 8 + 2 * k;
-                    acc += ws[c * 9 + t] * __uint_as_float(wd[k] << 16) +
-                           ws[(c + 1) * 9 + t] * __uint_as_float(wd[k] & 0xffff0000u);
+                for (int q = 0; q < 6; ++q) {
+                    const uint4 u = __ldg(src + q);
+                    // channels 8q .. 8q + 7 as (even, odd) pairs
+                    const unsigned long long x0p = f2pack(__uint_as_float(u.x << 16),
+                                                          __uint_as_float(u.x & 0xffff0000u));
+                    const unsigned long long x1p = f2pack(__uint_as_float(u.y << 16),
+                                                          __uint_as_float(u.y & 0xffff0000u));
+                    const unsigned long long x2p = f2pack(__uint_as_float(u.z << 16),
+                                                          __uint_as_float(u.z & 0xffff0000u));
+                    const unsigned long long x3p = f2pack(__uint_as_float(u.w << 16),
+                                                          __uint_as_float(u.w & 0xffff0000u));
+#pragma unroll
+                    for (int t = 0; t < 9; ++t) {
+                        const float4 wa = *reinterpret_cast<const float4 *>(&wt[t][8 * q]);
+                        const float4 wb = *reinterpret_cast<const float4 *>(&wt[t][8 * q + 4]);
+                        acc[t] = ffma2(x0p, f2pack(wa.x, wa.y), acc[t]);
+                        acc[t] = ffma2(x1p, f2pack(wa.z, wa.w), acc[t]);
+                        acc[t] = ffma2(x2p, f2pack(wb.x, wb.y), acc[t]);
+                        acc[t] = ffma2(x3p, f2pack(wb.z, wb.w), acc[t]);
+                    }
                 }
             }
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                float e, o;
+                f2unpack(acc[t], e, o);
+                part[t][i] = e + o;
+            }
         }
-        const long long o = img * a.img_stride + static_cast<long long>(y) * a.stride + x;
-        const float v = a.noisy[o] + acc;
-        a.out[o] = v;
-        if (a.target != nullptr) {
-            const float e = v - a.target[o];
-            a.dout[p] = 2.0f * e * a.inv_count;
-            err2 += static_cast<double>(e) * e;
+        __syncthreads();
+        const int oy = threadIdx.x / kOutTX, ox = threadIdx.x - oy * kOutTX;
+        const int y = y0 + oy, x = x0 + ox;
+        if (oy < kOutTY && y < a.h && x < a.w) {
+            float acc = b8;
+#pragma unroll
+            for (int t = 0; t < 9; ++t) acc += part[t][(oy + t / 3) * kOutHX + ox + t % 3];
+            const long long o = img * a.img_stride + static_cast<long long>(y) * a.stride + x;
+            const float v = a.noisy[o] + acc;
+            a.out[o] = v;
+            if (a.target != nullptr) {
+                const float e = v - a.target[o];
+                a.dout[(static_cast<long long>(img) * a.h + y) * a.w + x] = 2.0f * e * a.inv_count;
+                err2 += static_cast<double>(e) * e;
+            }
         }
+        __syncthreads();  // before the next tile overwrites part
     }
     if (a.target == nullptr) return;
     for (int o = 16; o >= 1; o >>= 1) err2 += __shfl_xor_sync(0xffffffffu, err2, o);
