@@ -69,12 +69,21 @@ __global__ void prep_batch_kernel(const BatchPlane<T> *planes)
                   q.nonfinite, blockIdx.x, gridDim.x);
 }
 
-// dst = num / den for every plane (grid.y = plane); each CTA walks the
-// plane's 32 x 32 tiles from blockIdx.x in steps of gridDim.x.
+// dst = num / den for every plane (grid.y = plane): fixed point by strips,
+// warp w of the plane's CTAs taking strips w, w + warps, ...; FP64 by 32 x 32
+// tiles, each CTA walking them from blockIdx.x in steps of gridDim.x.
 template <typename T>
 __global__ void __launch_bounds__(256) normalize_batch_kernel(const BatchPlane<T> *planes)
 {
     const BatchPlane<T> q = planes[blockIdx.y];
+    if constexpr (std::is_same<T, float>::value) {  // fixed point: one warp per strip
+        normalize_plane_strips(q.dst, q.dst_stride, q.num, q.den, q.width, q.height, q.block_size,
+                               q.poison, q.nonfinite, q.absmax, q.log2_bound, q.log2_corner,
+                               static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) +
+                                   (threadIdx.x >> 5),
+                               static_cast<long long>(gridDim.x) * (blockDim.x >> 5));
+        return;
+    }
     const int tx = (q.width + kNormTile - 1) / kNormTile;
     const int ntiles = tx * ((q.height + kNormTile - 1) / kNormTile);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {

@@ -654,7 +654,7 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
     if (bm_only) return BM3D_OK;
     for (int c = 0; c < nplanes; ++c) {
         if (!(a.active & (1 << c))) continue;
-        const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
+        const dim3 ngrid = normalize_grid<T>(width, height);
         normalize_kernel<T><<<ngrid, 256, 0, s>>>(dst[c], static_cast<long long>(stride), a.num[c],
                                                   a.den[c], width, height, a.block_size,
                                                   a.poison[c], a.nonfinite ? a.nonfinite + c : nullptr,
@@ -1188,7 +1188,7 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("prep_kernel", e);
     rc = launch_stage(&info, a, wiener != 0, 1, s, warps);
     if (rc != BM3D_OK) return noalloc_error(info.err.c_str(), cudaSuccess, rc);
-    const dim3 ngrid((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
+    const dim3 ngrid = normalize_grid<float>(width, height);
     normalize_kernel<float><<<ngrid, 256, 0, s>>>(dst, a.stride, num, den, width, height,
                                                   a.block_size, poison, nonfinite, absmax,
                                                   a.log2_bound, a.log2_corner);

@@ -1373,7 +1373,112 @@ __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
     __syncthreads();  // before the next tile overwrites w / hs
 }
 
-// One plane: grid = (ceil(width / 32), ceil(height / 32)) CTAs.
+// Fixed-point normalisation by strips, one warp per strip of 32 columns x
+// kStripRows rows, no shared tile and no CTA barrier. Lane l owns column
+// x0 + l. For each row r (from bs - 1 rows above the strip, to prime the
+// sums) the warp loads the block weights W of columns x0 - bs + 1 .. x0 + 31
+// (two 64-bit words per lane), forms their inclusive prefix sum S with
+// shuffles, and takes h(r) = S[l + bs - 1] - S[l - 1], the sum of the bs
+// origins left of and at the lane's column. The vertical box sum is a
+// running sum over the last bs rows' h, kept in a per-warp ring in shared
+// memory. The integer sums are exactly those of normalize_tile, so the
+// output is the same; the block-(0, 0) handling and poison marks are as
+// there. `ring` is this warp's 16 x 32 words.
+constexpr int kStripRows = 32;
+
+__device__ __forceinline__ void normalize_strip(float *dst, long long dst_stride, const long long *num,
+                                                const long long *wsum, int width, int height, int bs,
+                                                int x0, int y0, unsigned char *poison, bool marked,
+                                                double cratio, long long *ring)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const bool split = x0 == 0 && y0 == 0;  // the only strip whose sums reach W(0, 0)
+    const int xa = x0 - bs + 1 + lane, xb = xa + 32;
+    const int rstart = y0 - bs + 1, rend = min(y0 + kStripRows, height);
+    const int hi = lane + bs - 1;  // S index of the window's right end (< 47)
+    long long V = 0;
+    for (int r = rstart; r < rend; ++r) {
+        long long a0 = 0, a1 = 0;
+        if (r >= 0) {
+            const long long *row = wsum + static_cast<long long>(r) * width;
+            if (xa >= 0 && xa < width && !(split && r == 0 && xa == 0)) a0 = row[xa];
+            if (lane < bs - 1 && xb < width) a1 = row[xb];
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long t0 = __shfl_up_sync(full, a0, o), t1 = __shfl_up_sync(full, a1, o);
+            if (lane >= o) {
+                a0 += t0;
+                a1 += t1;
+            }
+        }
+        a1 += __shfl_sync(full, a0, 31);
+        const long long s_hi0 = __shfl_sync(full, a0, hi & 31), s_hi1 = __shfl_sync(full, a1, hi & 31);
+        const long long s_lo = __shfl_sync(full, a0, (lane + 31) & 31);
+        const long long h = (hi < 32 ? s_hi0 : s_hi1) - (lane > 0 ? s_lo : 0);
+        const int k = r - rstart;
+        if (k >= bs) V -= ring[((k - bs) & 15) * 32 + lane];  // read before the slot is reused
+        V += h;
+        ring[(k & 15) * 32 + lane] = h;
+        const int x = x0 + lane;
+        if (r >= y0 && x < width) {
+            const long long g = static_cast<long long>(r) * width + x;
+            float out;
+            if (split && r < bs && x < bs)  // block (0, 0): covered by origin (0, 0)
+                out = static_cast<float>(static_cast<double>(num[g]) /
+                                         (static_cast<double>(V) * cratio +
+                                          static_cast<double>(wsum[0])));
+            else
+                out = ratio(num[g], V);
+            if (marked && poison[g]) {
+                out = NAN;
+                poison[g] = 0;
+            }
+            dst[r * dst_stride + x] = out;
+        }
+    }
+}
+
+// Every strip of one fixed-point plane, warp w of the calling grid taking
+// strips w, w + nwarps, ... (256-thread CTAs: 8 warps).
+__device__ __forceinline__ void normalize_plane_strips(float *dst, long long dst_stride,
+                                                       const long long *num, const long long *wsum,
+                                                       int width, int height, int bs,
+                                                       unsigned char *poison,
+                                                       const unsigned *nonfinite,
+                                                       const float *absmax, int log2_bound,
+                                                       int log2_corner, long long first_warp,
+                                                       long long nwarps)
+{
+    __shared__ long long ring[8][16 * 32];
+    const int sx = (width + 31) / 32, sy = (height + kStripRows - 1) / kStripRows;
+    const bool marked = poison != nullptr && nonfinite != nullptr && *nonfinite != 0;
+    const float am = absmax != nullptr ? *absmax : 1.0f;
+    const double cratio = static_cast<double>(fixed_scale(am, log2_corner)) /
+                          static_cast<double>(fixed_scale(am, log2_bound));
+    long long *r = ring[(threadIdx.x >> 5) & 7];
+    for (long long t = first_warp; t < static_cast<long long>(sx) * sy; t += nwarps) {
+        const int ty = static_cast<int>(t / sx), tx = static_cast<int>(t - static_cast<long long>(ty) * sx);
+        normalize_strip(dst, dst_stride, num, wsum, width, height, bs, tx * 32, ty * kStripRows,
+                        poison, marked, cratio, r);
+    }
+}
+
+// Grid of the single-plane normalisation: 32 x 32 tiles (FP64 sums), or one
+// warp per strip (fixed point).
+template <typename T>
+inline dim3 normalize_grid(int width, int height)
+{
+    if (std::is_same<T, float>::value) {
+        const long long strips = static_cast<long long>((width + 31) / 32) *
+                                 ((height + kStripRows - 1) / kStripRows);
+        return dim3(static_cast<unsigned>((strips + 7) / 8));
+    }
+    return dim3((width + kNormTile - 1) / kNormTile, (height + kNormTile - 1) / kNormTile);
+}
+
+// One plane: grid = normalize_grid<T>(width, height), 256 threads.
 template <typename T>
 __global__ void __launch_bounds__(256)
     normalize_kernel(T *dst, long long dst_stride, const typename AccOf<T>::type *num,
@@ -1381,8 +1486,16 @@ __global__ void __launch_bounds__(256)
                      unsigned char *poison = nullptr, const unsigned *nonfinite = nullptr,
                      const float *absmax = nullptr, int log2_bound = 0, int log2_corner = 0)
 {
-    normalize_tile<T>(dst, dst_stride, num, wsum, width, height, bs, blockIdx.y * kNormTile,
-                      blockIdx.x * kNormTile, poison, nonfinite, absmax, log2_bound, log2_corner);
+    if constexpr (std::is_same<T, float>::value) {
+        normalize_plane_strips(dst, dst_stride, num, wsum, width, height, bs, poison, nonfinite,
+                               absmax, log2_bound, log2_corner,
+                               static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) +
+                                   (threadIdx.x >> 5),
+                               static_cast<long long>(gridDim.x) * (blockDim.x >> 5));
+    } else {
+        normalize_tile<T>(dst, dst_stride, num, wsum, width, height, bs, blockIdx.y * kNormTile,
+                          blockIdx.x * kNormTile, poison, nonfinite, absmax, log2_bound, log2_corner);
+    }
 }
 
 // Zero one plane's accumulators and fold the largest finite |src| into
