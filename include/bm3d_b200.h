@@ -441,9 +441,10 @@ int bm3d_pilot_estimate(bm3d_pilot *p, float *dst, const float *src, int count, 
 
 /* One Adam step on `count` crops of height x width in DEVICE memory, stored
  * back to back (pitch = width): noisy inputs, targets (the basic estimates)
- * and per-crop noise std `sigma` (device). Loss = mean squared error of the
- * output against the target; written to *loss (after a synchronisation) when
- * loss is not NULL. */
+ * and per-crop noise std `sigma` (device). Loss = mean over pixels of
+ * (sigma_ref / sigma)^2 (output - target)^2 with sigma_ref = 25/255: the
+ * squared error scaled to a common noise level, so every noise level weighs
+ * alike. Written to *loss (after a synchronisation) when loss is not NULL. */
 int bm3d_pilot_train_step(bm3d_pilot *p, int count, int height, int width, const float *noisy,
                           const float *target, const float *sigma, float lr, double *loss,
                           void *stream);

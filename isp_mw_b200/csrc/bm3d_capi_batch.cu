@@ -351,12 +351,15 @@ int tune_stage(bm3d_batch *B, StageBuild &sbd, const DevBuf &planes, bool autotu
     if (force) return build_stage(B, W, force[0], force[1], force[2], sbd);  // a known tiling
     const bm3d_stage_params &p = W ? B->pf[0] : B->pb[0];
     const bool generic = !fast_args(p.block_size, p.group_size);
-    static const int fast_cand[][3] = {{8, 8, 16}, {7, 7, 16}, {6, 8, 12}, {8, 6, 12},
-                                       {6, 6, 12}, {4, 4, 4}, {4, 4, 2}, {2, 2, 1}};
+    // reference blocks per tile a multiple of the warps where it can be, so
+    // the tile's last round keeps every warp busy
+    static const int fast_cand[][3] = {{8, 8, 16}, {7, 7, 16}, {6, 8, 16}, {8, 6, 16},
+                                       {8, 4, 16}, {6, 8, 12}, {8, 6, 12}, {6, 6, 12},
+                                       {4, 4, 4},  {4, 4, 2},  {2, 2, 1}};
     static const int gen_cand[][3] = {{6, 4, 12}, {4, 3, 12}, {4, 4, 8}, {4, 4, 4},
                                       {2, 2, 4},  {2, 2, 2},  {1, 1, 2}, {1, 1, 1}};
     const int (*cand)[3] = generic ? gen_cand : fast_cand;
-    const int ncand = 8;
+    const int ncand = generic ? 8 : 11;
     int best = -1;
     float best_ms = 1e30f;
     for (int c = 0; c < ncand; ++c) {

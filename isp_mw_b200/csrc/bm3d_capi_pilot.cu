@@ -256,6 +256,7 @@ int forward(bm3d_pilot *p, const float *in, long long stride, long long img_stri
     oa.target = target;
     oa.dout = training ? static_cast<float *>(p->dout.ptr) : nullptr;
     oa.loss = training ? static_cast<double *>(p->loss.ptr) : nullptr;
+    oa.sigma = sigma_dev;
     oa.inv_count = 1.0f / static_cast<float>(pixels);
     oa.n = n;
     oa.h = h;

@@ -817,8 +817,12 @@ __global__ void __launch_bounds__(256) conv_in_kernel(const InArgs a)
 }
 
 // Layer 8: 48 -> 1 plus the residual: out = noisy + b8 + conv(X7, W8). With a
-// target it also writes dOut = 2 (out - target) / count and adds the squared
-// error to *loss.
+// target it also writes dOut = 2 q (out - target) / count and adds
+// q (out - target)^2 to *loss, q = (kLossRefSigma / sigma[image])^2: the
+// squared error scaled to a common noise level, so that low-noise images
+// weigh as much in training as high-noise ones (a plain MSE is dominated by
+// the largest sigma, its errors growing as sigma^2).
+constexpr float kLossRefSigma = 25.0f / 255.0f;
 struct OutArgs {
     const __nv_bfloat16 *x;  // X7 [n][h][w][48]
     const float *noisy;
@@ -828,6 +832,7 @@ struct OutArgs {
     const float *target;  // may be null (inference)
     float *dout;          // [n][h][w] (training)
     double *loss;         // (training)
+    const float *sigma;   // per image noise level (training: the loss weight)
     float inv_count;
     int n, h, w;
 };
@@ -910,8 +915,9 @@ __global__ void __launch_bounds__(256) conv_out_kernel(const OutArgs a)
             a.out[o] = v;
             if (a.target != nullptr) {
                 const float e = v - a.target[o];
-                a.dout[(static_cast<long long>(img) * a.h + y) * a.w + x] = 2.0f * e * a.inv_count;
-                err2 += static_cast<double>(e) * e;
+                const float qs = kLossRefSigma / a.sigma[img], q = qs * qs;
+                a.dout[(static_cast<long long>(img) * a.h + y) * a.w + x] = 2.0f * q * e * a.inv_count;
+                err2 += static_cast<double>(q) * e * e;
             }
         }
         __syncthreads();  // before the next tile overwrites part

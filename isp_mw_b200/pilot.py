@@ -10,9 +10,10 @@ estimate this library computes:
   each source plane with its own noise level sigma ~ U[5, 50] / 255; the
   target of a crop is the same crop of the plane's basic estimate (the basic
   stage run on the whole plane, as at inference);
-* loss: mean squared error against the target; Adam with a cosine learning
-  rate schedule, one ``bm3d_pilot_train_step`` call per batch (forward,
-  backward and update on the GPU).
+* loss: squared error against the target, scaled per crop by
+  (25/255 / sigma)^2 so that every noise level weighs alike; Adam with a
+  warm-up and a cosine learning rate schedule, one ``bm3d_pilot_train_step``
+  call per batch (forward, backward and update on the GPU).
 
 Run ``python -m isp_mw_b200.pilot --out pilot.bin`` to train and save a
 checkpoint.

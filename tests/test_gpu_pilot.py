@@ -224,7 +224,9 @@ def test_pilot_gradient_matches_autograd(ctx):
     grad = torch.from_numpy(p.grad()).double()
     pt = torch.from_numpy(params).cuda().double().requires_grad_(True)
     out = _emulate(pt, noisy.double(), sigma.double())
-    ref_loss = ((out - clean.double()) ** 2).mean()
+    # squared error scaled to a common noise level, (25/255 / sigma)^2 per image
+    q = ((25.0 / 255.0) / sigma.double()) ** 2
+    ref_loss = (q.view(-1, 1, 1) * (out - clean.double()) ** 2).mean()
     ref_loss.backward()
     ref = pt.grad.cpu()
     assert abs(loss - ref_loss.item()) <= 1e-3 * ref_loss.item(), (loss, ref_loss.item())
