@@ -1397,45 +1397,60 @@ __device__ __forceinline__ void normalize_strip(float *dst, long long dst_stride
     const int xa = x0 - bs + 1 + lane, xb = xa + 32;
     const int rstart = y0 - bs + 1, rend = min(y0 + kStripRows, height);
     const int hi = lane + bs - 1;  // S index of the window's right end (< 47)
+    const int x = x0 + lane;
     long long V = 0;
-    for (int r = rstart; r < rend; ++r) {
-        long long a0 = 0, a1 = 0;
-        if (r >= 0) {
-            const long long *row = wsum + static_cast<long long>(r) * width;
-            if (xa >= 0 && xa < width && !(split && r == 0 && xa == 0)) a0 = row[xa];
-            if (lane < bs - 1 && xb < width) a1 = row[xb];
+    // four rows at a time: their loads are all issued before the first row's
+    // sums, so a warp has four rows of DRAM latency in flight, not one
+    for (int rb = rstart; rb < rend; rb += 4) {
+        long long A0[4], A1[4], NUM[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int r = rb + j;
+            A0[j] = A1[j] = NUM[j] = 0;
+            if (r >= 0 && r < rend) {
+                const long long *row = wsum + static_cast<long long>(r) * width;
+                if (xa >= 0 && xa < width && !(split && r == 0 && xa == 0)) A0[j] = row[xa];
+                if (lane < bs - 1 && xb < width) A1[j] = row[xb];
+                if (r >= y0 && x < width) NUM[j] = num[static_cast<long long>(r) * width + x];
+            }
         }
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const long long t0 = __shfl_up_sync(full, a0, o), t1 = __shfl_up_sync(full, a1, o);
-            if (lane >= o) {
-                a0 += t0;
-                a1 += t1;
+        for (int j = 0; j < 4; ++j) {
+            const int r = rb + j;
+            if (r >= rend) break;  // warp-uniform
+            long long a0 = A0[j], a1 = A1[j];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long t0 = __shfl_up_sync(full, a0, o), t1 = __shfl_up_sync(full, a1, o);
+                if (lane >= o) {
+                    a0 += t0;
+                    a1 += t1;
+                }
             }
-        }
-        a1 += __shfl_sync(full, a0, 31);
-        const long long s_hi0 = __shfl_sync(full, a0, hi & 31), s_hi1 = __shfl_sync(full, a1, hi & 31);
-        const long long s_lo = __shfl_sync(full, a0, (lane + 31) & 31);
-        const long long h = (hi < 32 ? s_hi0 : s_hi1) - (lane > 0 ? s_lo : 0);
-        const int k = r - rstart;
-        if (k >= bs) V -= ring[((k - bs) & 15) * 32 + lane];  // read before the slot is reused
-        V += h;
-        ring[(k & 15) * 32 + lane] = h;
-        const int x = x0 + lane;
-        if (r >= y0 && x < width) {
-            const long long g = static_cast<long long>(r) * width + x;
-            float out;
-            if (split && r < bs && x < bs)  // block (0, 0): covered by origin (0, 0)
-                out = static_cast<float>(static_cast<double>(num[g]) /
-                                         (static_cast<double>(V) * cratio +
-                                          static_cast<double>(wsum[0])));
-            else
-                out = ratio(num[g], V);
-            if (marked && poison[g]) {
-                out = NAN;
-                poison[g] = 0;
+            a1 += __shfl_sync(full, a0, 31);
+            const long long s_hi0 = __shfl_sync(full, a0, hi & 31),
+                            s_hi1 = __shfl_sync(full, a1, hi & 31);
+            const long long s_lo = __shfl_sync(full, a0, (lane + 31) & 31);
+            const long long h = (hi < 32 ? s_hi0 : s_hi1) - (lane > 0 ? s_lo : 0);
+            const int k = r - rstart;
+            if (k >= bs) V -= ring[((k - bs) & 15) * 32 + lane];  // read before the slot is reused
+            V += h;
+            ring[(k & 15) * 32 + lane] = h;
+            if (r >= y0 && x < width) {
+                const long long g = static_cast<long long>(r) * width + x;
+                float out;
+                if (split && r < bs && x < bs)  // block (0, 0): covered by origin (0, 0)
+                    out = static_cast<float>(static_cast<double>(NUM[j]) /
+                                             (static_cast<double>(V) * cratio +
+                                              static_cast<double>(wsum[0])));
+                else
+                    out = ratio(NUM[j], V);
+                if (marked && poison[g]) {
+                    out = NAN;
+                    poison[g] = 0;
+                }
+                dst[r * dst_stride + x] = out;
             }
-            dst[r * dst_stride + x] = out;
         }
     }
 }

@@ -87,8 +87,8 @@ def make_dataset(ctx, crops: int = 20000, crop: int = 128, planes: int = 160,
     }
 
 
-def train(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 2e-3,
-          lr_min: float = 2e-5, warmup: int = 1000, seed: int = 0, log_every: int = 0) -> List:
+def train(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 5e-4,
+          lr_min: float = 5e-6, warmup: int = 1000, seed: int = 0, log_every: int = 0) -> List:
     """Adam over shuffled batches: the rate rises linearly over the first
     `warmup` steps, then follows a cosine from `lr` to `lr_min` (a full-rate
     start can drive every ReLU of a layer negative, after which the network
@@ -128,7 +128,7 @@ def collapsed(hist: List) -> bool:
     return not last < 0.5 * first
 
 
-def fit(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 2e-3, seed: int = 0,
+def fit(pilot, data: Dict, epochs: int = 30, batch: int = 32, lr: float = 5e-4, seed: int = 0,
         attempts: int = 3, log_every: int = 0):
     """train(), restarted from a fresh initialisation at half the rate when a
     run collapses. Returns (history of the last run, restarts)."""
@@ -186,7 +186,7 @@ def main(argv=None):
     ap.add_argument("--planes", type=int, default=160)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=32)
-    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--lr", type=float, default=5e-4)
     ap.add_argument("--seed", type=int, default=0)
     args = ap.parse_args(argv)
     import json
