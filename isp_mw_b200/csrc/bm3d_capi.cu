@@ -655,7 +655,8 @@ static int run_stage_device(bm3d_ctx *ctx, const bm3d_stage_params *p, bool wien
     for (int c = 0; c < nplanes; ++c) {
         if (!(a.active & (1 << c))) continue;
         const dim3 ngrid = normalize_grid<T>(width, height);
-        normalize_kernel<T><<<ngrid, 256, 0, s>>>(dst[c], static_cast<long long>(stride), a.num[c],
+        const int nsmem = std::is_same<T, float>::value ? strip_smem_bytes(a.block_size) : 0;
+        normalize_kernel<T><<<ngrid, 256, nsmem, s>>>(dst[c], static_cast<long long>(stride), a.num[c],
                                                   a.den[c], width, height, a.block_size,
                                                   a.poison[c], a.nonfinite ? a.nonfinite + c : nullptr,
                                                   ctx->absmax + c, a.log2_bound, a.log2_corner);
@@ -1189,7 +1190,8 @@ extern "C" int bm3d_stage_noalloc(const bm3d_stage_params *params, int wiener, f
     rc = launch_stage(&info, a, wiener != 0, 1, s, warps);
     if (rc != BM3D_OK) return noalloc_error(info.err.c_str(), cudaSuccess, rc);
     const dim3 ngrid = normalize_grid<float>(width, height);
-    normalize_kernel<float><<<ngrid, 256, 0, s>>>(dst, a.stride, num, den, width, height,
+    normalize_kernel<float><<<ngrid, 256, strip_smem_bytes(a.block_size), s>>>(
+        dst, a.stride, num, den, width, height,
                                                   a.block_size, poison, nonfinite, absmax,
                                                   a.log2_bound, a.log2_corner);
     if ((e = cudaGetLastError()) != cudaSuccess) return noalloc_error("normalize_kernel", e);

@@ -268,8 +268,11 @@ int launch_planes(bm3d_batch *B, const DevBuf &planes, bool prep, cudaStream_t s
     const dim3 grid(static_cast<unsigned>(std::min<long long>(prep ? (maxpx + 255) / 256 : tiles, cap)),
                     static_cast<unsigned>(count));
     const auto *q = static_cast<const BatchPlane<float> *>(planes.ptr);
+    int bsmax = 1;  // the strip ring holds the largest block size of the batch
+    for (int i = 0; i < B->n; ++i)
+        bsmax = std::max(bsmax, (&planes == &B->planes_b ? B->pb[i] : B->pf[i]).block_size);
     if (prep) prep_batch_kernel<float><<<grid, 256, 0, s>>>(q);
-    else normalize_batch_kernel<float><<<grid, 256, 0, s>>>(q);
+    else normalize_batch_kernel<float><<<grid, 256, strip_smem_bytes(bsmax), s>>>(q);
     CK(B->ctx, cudaGetLastError());
     return BM3D_OK;
 }

@@ -1377,26 +1377,35 @@ __device__ __forceinline__ void normalize_tile(T *dst, long long dst_stride,
 // kStripRows rows, no shared tile and no CTA barrier. Lane l owns column
 // x0 + l. For each row r (from bs - 1 rows above the strip, to prime the
 // sums) the warp loads the block weights W of columns x0 - bs + 1 .. x0 + 31
-// (two 64-bit words per lane), forms their inclusive prefix sum S with
-// shuffles, and takes h(r) = S[l + bs - 1] - S[l - 1], the sum of the bs
-// origins left of and at the lane's column. The vertical box sum is a
-// running sum over the last bs rows' h, kept in a per-warp ring in shared
-// memory. The integer sums are exactly those of normalize_tile, so the
-// output is the same; the block-(0, 0) handling and poison marks are as
-// there. `ring` is this warp's 16 x 32 words.
+// (one or two 64-bit words per lane, four rows ahead), stores them in a
+// per-warp row buffer and each lane sums the bs of them left of and at its
+// column: h(r). The vertical box sum is a running sum over the last bs rows'
+// h, kept in a per-warp ring. The integer sums are exactly those of
+// normalize_tile, so the output is the same; the block-(0, 0) handling and
+// poison marks are as there. `ring` is this warp's ring_rows x 32 words
+// (ring_rows a power of two >= bs, ring_mask = ring_rows - 1), `hrow` its
+// 2 x 64-word row buffer.
 constexpr int kStripRows = 32;
+
+// Rows of the per-warp ring of horizontal sums: bs rounded up to a power of
+// two (8 for the 8 x 8 blocks of most profiles, so eight 256-thread CTAs fit
+// an SM), and the dynamic shared memory of a 256-thread normalisation CTA.
+__host__ __device__ inline int strip_ring_rows(int bs) { return bs <= 8 ? 8 : 16; }
+__host__ __device__ inline int strip_smem_bytes(int bs)
+{
+    return 8 * (strip_ring_rows(bs) * 32 + 128) * static_cast<int>(sizeof(long long));
+}
 
 __device__ __forceinline__ void normalize_strip(float *dst, long long dst_stride, const long long *num,
                                                 const long long *wsum, int width, int height, int bs,
                                                 int x0, int y0, unsigned char *poison, bool marked,
-                                                double cratio, long long *ring)
+                                                double cratio, long long *ring, int ring_mask,
+                                                long long *hrow)
 {
-    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const bool split = x0 == 0 && y0 == 0;  // the only strip whose sums reach W(0, 0)
     const int xa = x0 - bs + 1 + lane, xb = xa + 32;
     const int rstart = y0 - bs + 1, rend = min(y0 + kStripRows, height);
-    const int hi = lane + bs - 1;  // S index of the window's right end (< 47)
     const int x = x0 + lane;
     long long V = 0;
     // four rows at a time: their loads are all issued before the first row's
@@ -1418,24 +1427,19 @@ __device__ __forceinline__ void normalize_strip(float *dst, long long dst_stride
         for (int j = 0; j < 4; ++j) {
             const int r = rb + j;
             if (r >= rend) break;  // warp-uniform
-            long long a0 = A0[j], a1 = A1[j];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const long long t0 = __shfl_up_sync(full, a0, o), t1 = __shfl_up_sync(full, a1, o);
-                if (lane >= o) {
-                    a0 += t0;
-                    a1 += t1;
-                }
-            }
-            a1 += __shfl_sync(full, a0, 31);
-            const long long s_hi0 = __shfl_sync(full, a0, hi & 31),
-                            s_hi1 = __shfl_sync(full, a1, hi & 31);
-            const long long s_lo = __shfl_sync(full, a0, (lane + 31) & 31);
-            const long long h = (hi < 32 ? s_hi0 : s_hi1) - (lane > 0 ? s_lo : 0);
+            // the row's bs - 1 + 32 window words into this row's buffer (two
+            // alternate, so one __syncwarp per row separates writes and reads)
+            long long *hb = hrow + ((r - rstart) & 1) * 64;
+            hb[lane] = A0[j];
+            hb[32 + lane] = A1[j];
+            __syncwarp();
+            long long h = 0;
+#pragma unroll 4
+            for (int d = 0; d < bs; ++d) h += hb[lane + d];
             const int k = r - rstart;
-            if (k >= bs) V -= ring[((k - bs) & 15) * 32 + lane];  // read before the slot is reused
+            if (k >= bs) V -= ring[((k - bs) & ring_mask) * 32 + lane];  // read before reuse
             V += h;
-            ring[(k & 15) * 32 + lane] = h;
+            ring[(k & ring_mask) * 32 + lane] = h;
             if (r >= y0 && x < width) {
                 const long long g = static_cast<long long>(r) * width + x;
                 float out;
@@ -1466,17 +1470,18 @@ __device__ __forceinline__ void normalize_plane_strips(float *dst, long long dst
                                                        int log2_corner, long long first_warp,
                                                        long long nwarps)
 {
-    __shared__ long long ring[8][16 * 32];
+    extern __shared__ long long strip_ring[];  // per warp: ring_rows(bs) x 32 words, 128-word row buffer
+    const int rows = strip_ring_rows(bs);
     const int sx = (width + 31) / 32, sy = (height + kStripRows - 1) / kStripRows;
     const bool marked = poison != nullptr && nonfinite != nullptr && *nonfinite != 0;
     const float am = absmax != nullptr ? *absmax : 1.0f;
     const double cratio = static_cast<double>(fixed_scale(am, log2_corner)) /
                           static_cast<double>(fixed_scale(am, log2_bound));
-    long long *r = ring[(threadIdx.x >> 5) & 7];
+    long long *r = strip_ring + ((threadIdx.x >> 5) & 7) * (rows * 32 + 128);
     for (long long t = first_warp; t < static_cast<long long>(sx) * sy; t += nwarps) {
         const int ty = static_cast<int>(t / sx), tx = static_cast<int>(t - static_cast<long long>(ty) * sx);
         normalize_strip(dst, dst_stride, num, wsum, width, height, bs, tx * 32, ty * kStripRows,
-                        poison, marked, cratio, r);
+                        poison, marked, cratio, r, rows - 1, r + rows * 32);
     }
 }
 
