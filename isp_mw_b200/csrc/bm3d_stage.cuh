@@ -1537,6 +1537,31 @@ __device__ __forceinline__ void prep_plane(typename AccOf<T>::type *num,
         const long long o = static_cast<long long>(y) * width;
         const T *s = src + static_cast<long long>(y) * stride;
         const T *r = ref != nullptr ? ref + static_cast<long long>(y) * stride : nullptr;
+        if constexpr (sizeof(T) == 4) {
+            // two pixels per thread where the row allows 16-byte sum stores
+            // and 8-byte source loads (uniform over the CTA)
+            const bool vec = (width % 2 == 0) &&
+                             ((reinterpret_cast<uintptr_t>(num + o) | reinterpret_cast<uintptr_t>(den + o)) & 15) == 0 &&
+                             ((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(r)) & 7) == 0;
+            if (vec) {
+                for (int x = 2 * threadIdx.x; x < width; x += 2 * blockDim.x) {
+                    *reinterpret_cast<longlong2 *>(num + o + x) = make_longlong2(0, 0);
+                    *reinterpret_cast<longlong2 *>(den + o + x) = make_longlong2(0, 0);
+                    const float2 v2 = *reinterpret_cast<const float2 *>(s + x);
+                    const float v0 = fabsf(v2.x), v1 = fabsf(v2.y);
+                    if (v0 <= 3.4028235e38f) m = v0 > m ? v0 : m;  // NaN and Inf are skipped
+                    else ++bad;
+                    if (v1 <= 3.4028235e38f) m = v1 > m ? v1 : m;
+                    else ++bad;
+                    if (r != nullptr) {
+                        const float2 r2 = *reinterpret_cast<const float2 *>(r + x);
+                        if (!(fabsf(r2.x) <= 3.4028235e38f)) ++bad;
+                        if (!(fabsf(r2.y) <= 3.4028235e38f)) ++bad;
+                    }
+                }
+                continue;
+            }
+        }
         for (int x = threadIdx.x; x < width; x += blockDim.x) {
             num[o + x] = 0;
             den[o + x] = 0;
