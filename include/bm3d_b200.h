@@ -397,9 +397,13 @@ typedef struct bm3d_pilot bm3d_pilot;
 int bm3d_pilot_param_count(void);
 
 /* Which kernel runs the 48 -> 48 convolutions (process-wide): 0 (default) the
- * warp-specialised TMA pipeline when its tensor maps encode, else the cp.async
- * kernel; 1 the cp.async kernel; 2 the TMA pipeline only (a call fails with
- * BM3D_ERR_CUDA when its maps do not encode). Both give identical results. */
+ * warp-specialised TMA pipelines when their tensor maps encode -- N = 144
+ * (three column taps per MMA) for forward layers, N = 48 for data gradients
+ * -- else the cp.async kernel; 1 the cp.async kernel; 2 the N = 48 TMA
+ * pipeline only; 3 the N = 144 pipeline for forward layers (2 and 3 fail with
+ * BM3D_ERR_CUDA when their maps do not encode). The cp.async kernel and the
+ * N = 48 pipeline give identical results; the N = 144 pipeline adds the same
+ * FP32 products in another order. */
 int bm3d_pilot_set_conv_kernel(int which);
 
 /* Per-layer timing of the pilot's forward passes (off by default): with it on,
@@ -411,8 +415,8 @@ int bm3d_pilot_set_timing(bm3d_pilot *pilot, int on);
  * (ms[0] layer 1, ms[1..6] the 48 -> 48 layers, ms[7] layer 8); waits for it. */
 int bm3d_pilot_layer_ms(bm3d_pilot *pilot, float *ms);
 
-/* The kernel of the last 48 -> 48 convolution launched: 2 = TMA pipeline,
- * 1 = cp.async kernel, 0 = none yet. */
+/* The kernel of the last 48 -> 48 convolution launched: 3 = N = 144 TMA
+ * pipeline, 2 = N = 48 TMA pipeline, 1 = cp.async kernel, 0 = none yet. */
 int bm3d_pilot_conv_kernel(void);
 
 /* A pilot on the context's device, He-initialised from `seed`. */

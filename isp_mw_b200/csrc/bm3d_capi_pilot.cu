@@ -20,7 +20,7 @@ struct bm3d_pilot {
     bm3d_ctx *ctx = nullptr;
     long long step = 0;
     DevBuf params, grad, adam_m, adam_v;  // FP32, kParams each
-    DevBuf wpack;                         // BF16 packed: forward (6 layers) | data-gradient (6)
+    DevBuf wpack;  // BF16 packed: forward (6 layers) | data-gradient (6) | forward, N = 144 (6)
     DevBuf act[7];                        // X1..X7 (inference uses act[0], act[1])
     DevBuf gbuf[2];                       // pre-activation gradients, ping-pong
     DevBuf dout, out, partial, loss, err, sigma;
@@ -42,9 +42,12 @@ int pilot_fail(bm3d_ctx *ctx, int code, const char *msg)
 
 int grid_for(const bm3d_ctx *ctx, int tiles) { return std::max(1, std::min(tiles, ctx->sm_count)); }
 
-// Which 48 -> 48 convolution kernel runs: 0 = the TMA pipeline when its
-// tensor maps encode (else the cp.async kernel), 1 = the cp.async kernel,
-// 2 = the TMA pipeline only. g_conv_last records the kernel last launched.
+// Which 48 -> 48 convolution kernel runs: 0 = the N = 144 TMA pipeline for
+// forward layers and the N = 48 one for data gradients, when their tensor
+// maps encode (else the cp.async kernel); 1 = the cp.async kernel; 2 = the
+// N = 48 TMA pipeline only; 3 = the N = 144 pipeline for forward layers
+// (data gradients on the N = 48 one). g_conv_last records the kernel last
+// launched (3, 2 or 1).
 std::atomic<int> g_conv_choice{0};
 std::atomic<int> g_conv_last{0};
 
@@ -65,10 +68,13 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-// The TMA pipeline's two views of n images of h x w x 48 BF16 (NHWC): the
-// input as (channel % 8, x, channel / 8, y, image), box {8, 10, 6, 18, 1}, and
-// the output as (channel, x, y, image), box {48, 8, 4, 1}.
-bool encode_conv_maps(const void *x, void *y, int n, int h, int w, CUtensorMap &in, CUtensorMap &out)
+// The TMA pipelines' two views of n images of h x w x 48 BF16 (NHWC): the
+// input as (channel % 8, x, channel / 8, y, image), box {8, in_cols, 6,
+// in_rows, 1}, and the output as (channel, x, y, image), box {48, out_cols,
+// 4, 1}: {8, 10, 6, 18, 1} / {48, 8, 4, 1} for conv48_tma_kernel,
+// {8, 8, 6, 18, 1} / {48, 6, 4, 1} for conv48_n144_kernel.
+bool encode_conv_maps(const void *x, void *y, int n, int h, int w, CUtensorMap &in, CUtensorMap &out,
+                      int in_cols = kT2X + 2, int out_cols = kT2X, int in_rows = kT2Y + 2)
 {
     auto enc = tensor_map_encoder();
     if (!enc) return false;
@@ -76,7 +82,8 @@ bool encode_conv_maps(const void *x, void *y, int n, int h, int w, CUtensorMap &
     const cuuint64_t gdim[5] = {8, static_cast<cuuint64_t>(w), 6, static_cast<cuuint64_t>(h),
                                 static_cast<cuuint64_t>(n)};
     const cuuint64_t gstride[4] = {px, 16, px * w, px * w * h};
-    const cuuint32_t box[5] = {8, kT2X + 2, 6, kT2Y + 2, 1};
+    const cuuint32_t box[5] = {8, static_cast<cuuint32_t>(in_cols), 6,
+                               static_cast<cuuint32_t>(in_rows), 1};
     const cuuint32_t ones[5] = {1, 1, 1, 1, 1};
     if (enc(&in, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(x), gdim, gstride, box, ones,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -85,7 +92,7 @@ bool encode_conv_maps(const void *x, void *y, int n, int h, int w, CUtensorMap &
     const cuuint64_t odim[4] = {static_cast<cuuint64_t>(kC), static_cast<cuuint64_t>(w),
                                 static_cast<cuuint64_t>(h), static_cast<cuuint64_t>(n)};
     const cuuint64_t ostride[3] = {px, px * w, px * w * h};
-    const cuuint32_t obox[4] = {kC, kT2X, 4, 1};
+    const cuuint32_t obox[4] = {kC, static_cast<cuuint32_t>(out_cols), 4, 1};
     return enc(&out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, y, odim, ostride, obox, ones,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
@@ -93,8 +100,8 @@ bool encode_conv_maps(const void *x, void *y, int n, int h, int w, CUtensorMap &
 
 // One 48 -> 48 layer on the tensor cores.
 int run_conv48(bm3d_ctx *ctx, const __nv_bfloat16 *x, __nv_bfloat16 *y, const __nv_bfloat16 *w,
-               const float *bias, const __nv_bfloat16 *aux, int mode, int n, int h, int wd,
-               unsigned *err, cudaStream_t s)
+               const __nv_bfloat16 *w3, const float *bias, const __nv_bfloat16 *aux, int mode, int n,
+               int h, int wd, unsigned *err, cudaStream_t s)
 {
     ConvArgs a;
     a.x = x;
@@ -109,6 +116,25 @@ int run_conv48(bm3d_ctx *ctx, const __nv_bfloat16 *x, __nv_bfloat16 *y, const __
     a.err = err;
     const int choice = g_conv_choice.load();
     CUtensorMap tin, tout;
+    if (w3 != nullptr && mode != kMaskPrev && (choice == 0 || choice == 3) &&
+        encode_conv_maps(x, y, n, h, wd, tin, tout, kIn3X, kT3X, kT3Y + 2)) {
+        a.wt = reinterpret_cast<const uint4 *>(w3);
+        a.tiles_x = (wd + kT3X - 1) / kT3X;
+        a.tiles_y = (h + kT3Y - 1) / kT3Y;
+        a.tiles = n * a.tiles_x * a.tiles_y;
+        // more than half an SM's shared memory keeps one CTA (and its 512
+        // TMEM columns) per SM, so no CTA's allocation waits on another's
+        const int smem3 = std::max(kT3Smem, 120 * 1024);
+        CK(ctx, raise_smem_limit(reinterpret_cast<const void *>(conv48_n144_kernel), smem3));
+        conv48_n144_kernel<<<std::max(1, std::min(a.tiles, ctx->sm_count)), kTmaThreads, smem3,
+                             s>>>(tin, tout, a);
+        CK(ctx, cudaGetLastError());
+        g_conv_last.store(3);
+        return BM3D_OK;
+    }
+    if (choice == 3 && mode != kMaskPrev)
+        return pilot_fail(ctx, BM3D_ERR_CUDA,
+                          "pilot: the N = 144 convolution's tensor maps did not encode");
     if (choice != 1 && encode_conv_maps(x, y, n, h, wd, tin, tout)) {
         a.tiles_x = (wd + kT2X - 1) / kT2X;
         a.tiles_y = (h + kT2Y - 1) / kT2Y;
@@ -120,7 +146,7 @@ int run_conv48(bm3d_ctx *ctx, const __nv_bfloat16 *x, __nv_bfloat16 *y, const __
         g_conv_last.store(2);
         return BM3D_OK;
     }
-    if (choice == 2)
+    if (choice == 2 || choice == 3)
         return pilot_fail(ctx, BM3D_ERR_CUDA, "pilot: the convolution's tensor maps did not encode");
     a.tiles_x = (wd + kTX - 1) / kTX;
     a.tiles_y = (h + kTY - 1) / kTY;
@@ -195,6 +221,10 @@ const __nv_bfloat16 *wbwd(const bm3d_pilot *p, int layer)
 {
     return static_cast<const __nv_bfloat16 *>(p->wpack.ptr) + (6 + layer - 2) * kPackElems;
 }
+const __nv_bfloat16 *wfwd3(const bm3d_pilot *p, int layer)
+{
+    return static_cast<const __nv_bfloat16 *>(p->wpack.ptr) + (12 + layer - 2) * kPackElems;
+}
 const float *param(const bm3d_pilot *p, int offset)
 {
     return static_cast<const float *>(p->params.ptr) + offset;
@@ -204,7 +234,7 @@ int pack(bm3d_pilot *p, cudaStream_t s)
 {
     __nv_bfloat16 *w = static_cast<__nv_bfloat16 *>(p->wpack.ptr);
     pack_weights_kernel<<<216, 256, 0, s>>>(static_cast<const float *>(p->params.ptr), w,
-                                            w + 6 * kPackElems);
+                                            w + 6 * kPackElems, w + 12 * kPackElems);
     CK(p->ctx, cudaGetLastError());
     return BM3D_OK;
 }
@@ -241,8 +271,8 @@ int forward(bm3d_pilot *p, const float *in, long long stride, long long img_stri
     if (p->timing) CK(ctx, cudaEventRecord(p->ev[1], s));
     int rc;
     for (int layer = 2; layer <= 7; ++layer) {
-        if ((rc = run_conv48(ctx, X(layer - 1), X(layer), wfwd(p, layer), param(p, off_b(layer)),
-                             nullptr, kBiasRelu, n, h, w, err, s)) != BM3D_OK)
+        if ((rc = run_conv48(ctx, X(layer - 1), X(layer), wfwd(p, layer), wfwd3(p, layer),
+                             param(p, off_b(layer)), nullptr, kBiasRelu, n, h, w, err, s)) != BM3D_OK)
             return rc;
         if (p->timing) CK(ctx, cudaEventRecord(p->ev[layer], s));
     }
@@ -273,7 +303,7 @@ extern "C" int bm3d_pilot_param_count(void) { return kParams; }
 
 extern "C" int bm3d_pilot_set_conv_kernel(int which)
 {
-    if (which < 0 || which > 2) return BM3D_ERR_INVALID;
+    if (which < 0 || which > 3) return BM3D_ERR_INVALID;
     g_conv_choice.store(which);
     return BM3D_OK;
 }
@@ -293,7 +323,7 @@ extern "C" int bm3d_pilot_create(bm3d_ctx *ctx, unsigned long long seed, bm3d_pi
             bm3d_pilot_destroy(p);
             return rc;
         }
-    if ((rc = ensure(ctx, p->wpack, 12 * kPackElems * sizeof(__nv_bfloat16))) != BM3D_OK) {
+    if ((rc = ensure(ctx, p->wpack, 18 * kPackElems * sizeof(__nv_bfloat16))) != BM3D_OK) {
         bm3d_pilot_destroy(p);
         return rc;
     }
@@ -531,7 +561,7 @@ extern "C" int bm3d_pilot_train_step(bm3d_pilot *p, int count, int height, int w
         reduce_partials_kernel<<<(kWgPartial + 255) / 256, 256, 0, s>>>(
             part, parts, kWgPartial, kWgPartial, grad + off_w(layer));
         CK(ctx, cudaGetLastError());
-        if ((rc = run_conv48(ctx, G[cur], G[cur ^ 1], wbwd(p, layer), nullptr, X(layer - 1),
+        if ((rc = run_conv48(ctx, G[cur], G[cur ^ 1], wbwd(p, layer), nullptr, nullptr, X(layer - 1),
                              kMaskPrev, count, height, width, err, s)) != BM3D_OK)
             return rc;
         cur ^= 1;
@@ -629,7 +659,7 @@ extern "C" int bm3d_pilot_conv48(bm3d_ctx *ctx, int n, int h, int w, const void 
     // weight: FP32 [48][48][3][3] (device); packed here into the operand layout
     DevBuf &wp = ctx->groups[0], &pp = ctx->groups[1], &eb = ctx->groups[2];
     int rc;
-    if ((rc = ensure(ctx, wp, 12 * kPackElems * sizeof(__nv_bfloat16))) != BM3D_OK) return rc;
+    if ((rc = ensure(ctx, wp, 18 * kPackElems * sizeof(__nv_bfloat16))) != BM3D_OK) return rc;
     if ((rc = ensure(ctx, pp, kParams * sizeof(float))) != BM3D_OK) return rc;
     if ((rc = ensure(ctx, eb, sizeof(unsigned))) != BM3D_OK) return rc;
     float *params = static_cast<float *>(pp.ptr);
@@ -637,12 +667,14 @@ extern "C" int bm3d_pilot_conv48(bm3d_ctx *ctx, int n, int h, int w, const void 
     CK(ctx, cudaMemcpyAsync(params + off_w(2), weight, kWmid * sizeof(float),
                             cudaMemcpyDeviceToDevice, s));
     __nv_bfloat16 *packed = static_cast<__nv_bfloat16 *>(wp.ptr);
-    pack_weights_kernel<<<216, 256, 0, s>>>(params, packed, packed + 6 * kPackElems);
+    pack_weights_kernel<<<216, 256, 0, s>>>(params, packed, packed + 6 * kPackElems,
+                                            packed + 12 * kPackElems);
     CK(ctx, cudaGetLastError());
     unsigned *err = static_cast<unsigned *>(eb.ptr);
     CK(ctx, cudaMemsetAsync(err, 0, sizeof(unsigned), s));
     if ((rc = run_conv48(ctx, static_cast<const __nv_bfloat16 *>(x), static_cast<__nv_bfloat16 *>(y),
-                         mode == kMaskPrev ? packed + 6 * kPackElems : packed, bias,
+                         mode == kMaskPrev ? packed + 6 * kPackElems : packed,
+                         mode == kMaskPrev ? nullptr : packed + 12 * kPackElems, bias,
                          static_cast<const __nv_bfloat16 *>(aux), mode, n, h, w, err, s)) != BM3D_OK)
         return rc;
     return check_err_flag(ctx, err, s);

@@ -533,6 +533,204 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Forward 48 -> 48 convolution with the three column taps in N: the N = 48
+// form is bound by the tensor core's operand fetch (an M = 128, N = 48,
+// K = 16 MMA fetches 5.5 KB for 24 cycles of math). Here an MMA is
+// M = 128 input pixels (16 rows x 8 columns, m = row * 8 + column) by
+// N = 144 = (column tap dx, output channel) by K = 16 input channels:
+//   D[(r, c)][dx][co] = sum over row taps dy and channels of
+//                       X[r + dy][c][ci] W[co][ci][dy][dx]      (halo coords)
+// 9 MMAs per tile (3 row taps x 3 channel steps), A = the input tile started
+// dy rows in. The output pixel (r, j) is D[(r, j)][0] + D[(r, j + 1)][1] +
+// D[(r, j + 2)][2]: TMEM lanes m, m + 1, m + 2 of the same warp, added with
+// two shuffles per channel in the epilogue. Each tile yields 16 rows x 6
+// columns (the input's 8 columns minus the two the taps reach past). The
+// input tile, 8 columns x 18 rows, arrives by one TMA load of the 5-D view
+// (box {8, 8, 6, 18, 1}) as [row][channel / 8][column][channel % 8]: K-major,
+// LBO = 128 bytes, SBO = 768 bytes (one input row). Warp roles, mbarriers and
+// stores as conv48_tma_kernel; forward modes (bias, ReLU) only.
+constexpr int kT3X = 6, kT3Y = 16;
+constexpr int kIn3X = 8;
+constexpr int kRow3Bytes = 6 * kIn3X * 16;          // 768
+constexpr int kTile3Bytes = (kT3Y + 2) * kRow3Bytes;  // 13824
+constexpr int kN3 = 3 * kC;                          // 144
+constexpr int kAcc3Cols = 256;                       // TMEM columns per accumulator (144 used)
+constexpr int kStore3Bytes = 4 * kT3X * kC * 2;      // one warp's 4 x 6 output pixels: 2304
+constexpr int kT3Stages = 4;
+constexpr int kT3OffStage = kWeightBytes;
+constexpr int kT3OffStore = kT3OffStage + kT3Stages * kTile3Bytes;
+constexpr int kT3OffBias = kT3OffStore + 4 * 2 * kStore3Bytes;
+constexpr int kT3OffBar = kT3OffBias + kC * 4;
+constexpr int kT3Smem = kT3OffBar + 8 * (2 * kT3Stages + 4) + 16;
+constexpr uint32_t kIdesc3 = instr_desc_bf16(128, kN3, false, false);
+static_assert(kT3OffStage % 128 == 0 && kT3OffStore % 128 == 0 && kTile3Bytes % 128 == 0 &&
+                  kStore3Bytes % 128 == 0,
+              "TMA buffers 128-byte aligned");
+
+__device__ __forceinline__ void tile_origin_6x16(int tile, int tiles_x, int tiles_y, int &img,
+                                                 int &y0, int &x0)
+{
+    const int per = tiles_x * tiles_y;
+    img = tile / per;
+    const int r = tile - img * per;
+    const int ty = r / tiles_x;
+    y0 = ty * kT3Y;
+    x0 = (r - ty * tiles_x) * kT3X;
+}
+
+__global__ void __launch_bounds__(kTmaThreads, 1)
+    conv48_n144_kernel(const __grid_constant__ CUtensorMap tm_in,
+                       const __grid_constant__ CUtensorMap tm_out, const ConvArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + kT3OffBar);
+    uint64_t *empty = full + kT3Stages;
+    uint64_t *accf = empty + kT3Stages;
+    uint64_t *acce = accf + 2;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(acce + 2);
+    float *bias_s = reinterpret_cast<float *>(smem + kT3OffBias);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (blockIdx.x >= a.tiles) return;
+
+    for (int i = tid; i < kWeightBytes / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(smem)[i] = __ldg(a.wt + i);
+    if (tid < kC) bias_s[tid] = __ldg(a.bias + tid);
+    if (tid == 0) {
+        for (int st = 0; st < kT3Stages; ++st) {
+            mbar_init(&full[st], 1);
+            mbar_init(&empty[st], 1);
+        }
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&accf[k], 1);
+            mbar_init(&acce[k], 4);  // one arrival per draining warp
+        }
+        fence_mbar_init();
+    }
+    if (warp == 0) tmem_alloc(tslot, 2 * kAcc3Cols);
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tbase = *tslot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {  // producer
+            int it = 0;
+            for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+                const int st = it % kT3Stages;
+                if (!mbar_wait(&empty[st], ((it / kT3Stages) & 1) ^ 1, kWaitLimit)) {
+                    ok = false;
+                    break;
+                }
+                int img, y0, x0;
+                tile_origin_6x16(tile, a.tiles_x, a.tiles_y, img, y0, x0);
+                mbar_arrive_expect_tx(&full[st], kTile3Bytes);
+                tma_load_5d(smem + kT3OffStage + st * kTile3Bytes, &tm_in, &full[st], 0, x0 - 1, 0,
+                            y0 - 1, img);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issue: 9 MMAs, descriptors = bases + compile-time offsets
+            int it = 0;
+            for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+                const int st = it % kT3Stages, k = it & 1;
+                if (!mbar_wait(&full[st], (it / kT3Stages) & 1, kWaitLimit) ||
+                    !mbar_wait(&acce[k], ((it >> 1) & 1) ^ 1, kWaitLimit)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint64_t ad0 =
+                    smem_desc(smem_u32(smem + kT3OffStage + st * kTile3Bytes), 128, kRow3Bytes);
+                const uint64_t bd0 = smem_desc(smem_u32(smem), 128, 256);
+#pragma unroll
+                for (int dy = 0; dy < 3; ++dy) {
+#pragma unroll
+                    for (int s3 = 0; s3 < 3; ++s3) {
+                        const uint64_t ad =
+                            ad0 + static_cast<uint64_t>((dy * kRow3Bytes + s3 * 256) >> 4);
+                        const uint64_t bd =
+                            bd0 + static_cast<uint64_t>(((dy * 3 + s3) * kN3 * 16 * 2) >> 4);
+                        mma_bf16(tbase + k * kAcc3Cols, ad, bd, kIdesc3, dy > 0 || s3 > 0);
+                    }
+                }
+                mma_commit(&empty[st]);  // the operand buffer is free once these MMAs finish
+                mma_commit(&accf[k]);
+            }
+        }
+    } else {  // drain: warps 2..5, TMEM lanes 32 (warp % 4) .. + 31
+        const int q = warp & 3;
+        const int rr = lane >> 3, c = lane & 7;  // pixel row 4q + rr, input column c
+        unsigned char *const stage0 = smem + kT3OffStore + (warp - 2) * 2 * kStore3Bytes;
+        const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
+        const bool relu = a.mode == kBiasRelu;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
+            const int k = it & 1;
+            if (!__all_sync(0xffffffffu, mbar_wait(&accf[k], (it >> 1) & 1, kWaitLimit))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t ta = tbase + k * kAcc3Cols + lane_base;
+            uint32_t pk[24];
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {  // 16 output channels at a time
+                float d0[16], d1[16], d2[16];
+                tmem_ld16(ta + ch * 16, d0);
+                tmem_ld16(ta + kC + ch * 16, d1);
+                tmem_ld16(ta + 2 * kC + ch * 16, d2);
+                tmem_wait_ld();
+                const float4 *b4 = reinterpret_cast<const float4 *>(bias_s + ch * 16);
+#pragma unroll
+                for (int i = 0; i < 16; i += 4) {
+                    float v[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e)
+                        v[e] = d0[i + e] + __shfl_down_sync(0xffffffffu, d1[i + e], 1) +
+                               __shfl_down_sync(0xffffffffu, d2[i + e], 2);
+                    const float4 b = b4[i / 4];
+                    pk[ch * 8 + i / 2] = pack_bf16(v[0] + b.x, v[1] + b.y, relu);
+                    pk[ch * 8 + i / 2 + 1] = pack_bf16(v[2] + b.z, v[3] + b.w, relu);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acce[k]);  // the accumulator may be overwritten
+
+            int img, y0, x0;
+            tile_origin_6x16(tile, a.tiles_x, a.tiles_y, img, y0, x0);
+            unsigned char *const stg = stage0 + (it & 1) * kStore3Bytes;
+            if (lane == 0) bulk_wait_read_1();  // the store two tiles back has read this buffer
+            __syncwarp();
+            if (c < kT3X) {
+                uint4 *dst = reinterpret_cast<uint4 *>(stg + (rr * kT3X + c) * kC * 2);
+#pragma unroll
+                for (int j = 0; j < 6; ++j)
+                    dst[j] = make_uint4(pk[4 * j], pk[4 * j + 1], pk[4 * j + 2], pk[4 * j + 3]);
+            }
+            fence_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+                // rows wholly below the image store nothing; the (then empty)
+                // group is still committed, as in conv48_tma_kernel
+                if (y0 + 4 * q < a.h) tma_store_4d(&tm_out, stg, 0, x0, y0 + 4 * q, img);
+                bulk_commit();
+            }
+        }
+        if (lane == 0) bulk_wait_all();
+    }
+    if (!ok && a.err) atomicOr(a.err, 1u);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tbase, 2 * kAcc3Cols);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Weight gradient of a 48 -> 48 layer on the tensor cores:
 //   dW[co][ci][ky][kx] = sum over pixels p of G[p][co] * X[p + (ky - 1, kx - 1)][ci]
 // One MMA per K-step of 16 pixels (two tile columns) and input-row shift dy:
@@ -1112,18 +1310,32 @@ __global__ void adam_kernel(float *param, const float *grad, float *m, float *v,
 // shared-memory operand layout, BF16: forward taps (dy, dx) = (ky, kx) with
 // N = co, K = ci; and the data-gradient form, taps flipped (2 - ky, 2 - kx)
 // with N = ci, K = co.
-__global__ void pack_weights_kernel(const float *params, __nv_bfloat16 *fwd, __nv_bfloat16 *bwd)
+// BF16 copies of the six 48 -> 48 layers' weights in the MMA operand
+// layouts: `fwd` and `bwd` (flipped, transposed: the data gradient) per tap
+// as [co / 8][ci / 8][co % 8][ci % 8] (N = 48); `fwd3` (may be null) for the
+// N = 144 forward kernel, per (row tap dy, 16-channel step s) as
+// [n / 8][k / 8][n % 8][k % 8] with n = column tap * 48 + co, k = ci - 16 s.
+__global__ void pack_weights_kernel(const float *params, __nv_bfloat16 *fwd, __nv_bfloat16 *bwd,
+                                    __nv_bfloat16 *fwd3)
 {
     const int per = 9 * kC * kC;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * per; i += gridDim.x * blockDim.x) {
         const int layer = i / per;
         int r = i - layer * per;
+        const float *w = params + off_w(layer + 2);
+        if (fwd3 != nullptr) {
+            const int blk = r / (3 * kC * 16), e = r - blk * (3 * kC * 16);
+            const int dy = blk / 3, st = blk % 3;
+            const int nb = e / 128, kb = (e / 64) % 2, n8 = (e / 8) % 8, k8 = e % 8;
+            const int n = nb * 8 + n8, k = kb * 8 + k8;
+            const int dx = n / kC, co = n % kC, ci = st * 16 + k;
+            fwd3[i] = __float2bfloat16_rn(w[((co * kC + ci) * 3 + dy) * 3 + dx]);
+        }
         const int tap = r / (kC * kC);
         r -= tap * kC * kC;
         // r = element of the packed tap: [n / 8][k / 8][n % 8][k % 8]
         const int ng = r / (6 * 64), kg = (r / 64) % 6, n8 = (r / 8) % 8, k8 = r % 8;
         const int n = ng * 8 + n8, k = kg * 8 + k8;
-        const float *w = params + off_w(layer + 2);
         const int ky = tap / 3, kx = tap % 3;
         fwd[i] = __float2bfloat16_rn(w[((n * kC + k) * 3 + ky) * 3 + kx]);
         bwd[i] = __float2bfloat16_rn(w[((k * kC + n) * 3 + (2 - ky)) * 3 + (2 - kx)]);

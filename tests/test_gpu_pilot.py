@@ -109,7 +109,41 @@ def test_conv48_tma_pipeline_equals_cp_async_kernel(ctx, shape):
     finally:
         lib.bm3d_pilot_set_conv_kernel(0)
     _conv48(ctx, x, W, b, None, 0)
-    assert lib.bm3d_pilot_conv_kernel() == 2  # the default runs the TMA pipeline
+    assert lib.bm3d_pilot_conv_kernel() == 3  # forward layers default to the N = 144 pipeline
+    _conv48(ctx, x, W, None, aux, 2)
+    assert lib.bm3d_pilot_conv_kernel() == 2  # data gradients to the N = 48 one
+
+
+@pytest.mark.parametrize("shape", [(2, 37, 53), (1, 8, 16), (3, 19, 7), (1, 1080, 1920),
+                                   (2, 17, 13)])
+def test_conv48_n144_matches_torch_and_n48(ctx, shape):
+    """The N = 144 forward pipeline (three column taps per MMA, their partial
+    sums added across TMEM lanes): against float64 PyTorch on BF16 operands,
+    and against the N = 48 pipeline to within one BF16 rounding (the two add
+    the same FP32 products in a different order)."""
+    import torch
+    import torch.nn.functional as F
+    lib = ctx.lib
+    g = torch.Generator(device="cuda").manual_seed(6)
+    n, h, w = shape
+    x = torch.randn(n, h, w, C, device="cuda", generator=g).bfloat16()
+    W = torch.randn(C, C, 3, 3, device="cuda", generator=g) * 0.05
+    b = torch.randn(C, device="cuda", generator=g) * 0.1
+    lin = F.conv2d(x.double().permute(0, 3, 1, 2), W.bfloat16().double(), b.double(),
+                   padding=1).permute(0, 2, 3, 1)
+    try:
+        for mode, ref in ((0, torch.relu(lin)), (1, lin)):
+            assert lib.bm3d_pilot_set_conv_kernel(3) == 0
+            y3 = _conv48(ctx, x, W, b, None, mode)
+            assert lib.bm3d_pilot_conv_kernel() == 3
+            d = (y3.double() - ref).abs()
+            bar = ref.abs() * 2.0 ** -8 + 1e-4 * ref.abs().max()
+            assert bool((d <= bar).all()), (mode, float((d - bar).max()))
+            assert lib.bm3d_pilot_set_conv_kernel(2) == 0
+            y2 = _conv48(ctx, x, W, b, None, mode).float()
+            assert bool(((y3.float() - y2).abs() <= y2.abs() * 2.0 ** -7 + 1e-6).all())
+    finally:
+        lib.bm3d_pilot_set_conv_kernel(0)
 
 
 def test_wgrad48_matches_torch(ctx):
