@@ -1085,7 +1085,7 @@ def run_pilot(args):
         lay += pilot.layer_ms() / 10
     pilot.set_timing(False)
     ms_conv = float(lay[1:7].mean())
-    conv_kernel = {2: "conv48_tma_kernel", 1: "conv48_kernel"}.get(
+    conv_kernel = {3: "conv48_n144_kernel", 2: "conv48_tma_kernel", 1: "conv48_kernel"}.get(
         int(lib.bm3d_pilot_conv_kernel()), "none")
     flops_conv = len(SIGMAS) * W * H * 2 * 9 * 48 * 48
     if rank == 0:

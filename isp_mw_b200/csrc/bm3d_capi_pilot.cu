@@ -126,7 +126,7 @@ int run_conv48(bm3d_ctx *ctx, const __nv_bfloat16 *x, __nv_bfloat16 *y, const __
         // TMEM columns) per SM, so no CTA's allocation waits on another's
         const int smem3 = std::max(kT3Smem, 120 * 1024);
         CK(ctx, raise_smem_limit(reinterpret_cast<const void *>(conv48_n144_kernel), smem3));
-        conv48_n144_kernel<<<std::max(1, std::min(a.tiles, ctx->sm_count)), kTmaThreads, smem3,
+        conv48_n144_kernel<<<std::max(1, std::min(a.tiles, ctx->sm_count)), kT3Threads, smem3,
                              s>>>(tin, tout, a);
         CK(ctx, cudaGetLastError());
         g_conv_last.store(3);

@@ -548,7 +548,10 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
 // input tile, 8 columns x 18 rows, arrives by one TMA load of the 5-D view
 // (box {8, 8, 6, 18, 1}) as [row][channel / 8][column][channel % 8]: K-major,
 // LBO = 128 bytes, SBO = 768 bytes (one input row). Warp roles, mbarriers and
-// stores as conv48_tma_kernel; forward modes (bias, ReLU) only.
+// stores as conv48_tma_kernel, except that two sets of four warps drain: set
+// k (warps 2 + 4k .. 5 + 4k) takes the tiles of accumulator k, so each
+// tile's epilogue (nine TMEM loads, 96 shuffles per lane) has two MMA tiles'
+// time. Forward modes (bias, ReLU) only.
 constexpr int kT3X = 6, kT3Y = 16;
 constexpr int kIn3X = 8;
 constexpr int kRow3Bytes = 6 * kIn3X * 16;          // 768
@@ -557,9 +560,10 @@ constexpr int kN3 = 3 * kC;                          // 144
 constexpr int kAcc3Cols = 256;                       // TMEM columns per accumulator (144 used)
 constexpr int kStore3Bytes = 4 * kT3X * kC * 2;      // one warp's 4 x 6 output pixels: 2304
 constexpr int kT3Stages = 4;
+constexpr int kT3Threads = 320;  // producer, MMA issuer, two sets of four draining warps
 constexpr int kT3OffStage = kWeightBytes;
 constexpr int kT3OffStore = kT3OffStage + kT3Stages * kTile3Bytes;
-constexpr int kT3OffBias = kT3OffStore + 4 * 2 * kStore3Bytes;
+constexpr int kT3OffBias = kT3OffStore + 8 * 2 * kStore3Bytes;
 constexpr int kT3OffBar = kT3OffBias + kC * 4;
 constexpr int kT3Smem = kT3OffBar + 8 * (2 * kT3Stages + 4) + 16;
 constexpr uint32_t kIdesc3 = instr_desc_bf16(128, kN3, false, false);
@@ -578,7 +582,7 @@ __device__ __forceinline__ void tile_origin_6x16(int tile, int tiles_x, int tile
     x0 = (r - ty * tiles_x) * kT3X;
 }
 
-__global__ void __launch_bounds__(kTmaThreads, 1)
+__global__ void __launch_bounds__(kT3Threads, 1)
     conv48_n144_kernel(const __grid_constant__ CUtensorMap tm_in,
                        const __grid_constant__ CUtensorMap tm_out, const ConvArgs a)
 {
@@ -602,7 +606,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
         }
         for (int k = 0; k < 2; ++k) {
             mbar_init(&accf[k], 1);
-            mbar_init(&acce[k], 4);  // one arrival per draining warp
+            mbar_init(&acce[k], 4);  // one arrival per draining warp of set k
         }
         fence_mbar_init();
     }
@@ -659,15 +663,16 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
                 mma_commit(&accf[k]);
             }
         }
-    } else {  // drain: warps 2..5, TMEM lanes 32 (warp % 4) .. + 31
-        const int q = warp & 3;
+    } else {  // drain: set (warp - 2) / 4, TMEM lanes 32 (warp % 4) .. + 31
+        const int q = warp & 3, set = (warp - 2) >> 2;
         const int rr = lane >> 3, c = lane & 7;  // pixel row 4q + rr, input column c
         unsigned char *const stage0 = smem + kT3OffStore + (warp - 2) * 2 * kStore3Bytes;
         const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
         const bool relu = a.mode == kBiasRelu;
-        int it = 0;
-        for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
-            const int k = it & 1;
+        int it = set;  // this set's tiles: it = set, set + 2, ...
+        for (int tile = blockIdx.x + set * gridDim.x; tile < a.tiles;
+             tile += 2 * gridDim.x, it += 2) {
+            const int k = it & 1;  // == set
             if (!__all_sync(0xffffffffu, mbar_wait(&accf[k], (it >> 1) & 1, kWaitLimit))) {
                 ok = false;
                 break;
@@ -701,8 +706,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
 
             int img, y0, x0;
             tile_origin_6x16(tile, a.tiles_x, a.tiles_y, img, y0, x0);
-            unsigned char *const stg = stage0 + (it & 1) * kStore3Bytes;
-            if (lane == 0) bulk_wait_read_1();  // the store two tiles back has read this buffer
+            unsigned char *const stg = stage0 + ((it >> 1) & 1) * kStore3Bytes;
+            if (lane == 0) bulk_wait_read_1();  // this warp's store two tiles back has read it
             __syncwarp();
             if (c < kT3X) {
                 uint4 *dst = reinterpret_cast<uint4 *>(stg + (rr * kT3X + c) * kC * 2);
