@@ -548,24 +548,27 @@ __global__ void __launch_bounds__(kTmaThreads, 1)
 // input tile, 8 columns x 18 rows, arrives by one TMA load of the 5-D view
 // (box {8, 8, 6, 18, 1}) as [row][channel / 8][column][channel % 8]: K-major,
 // LBO = 128 bytes, SBO = 768 bytes (one input row). Warp roles, mbarriers and
-// stores as conv48_tma_kernel, except that two sets of four warps drain: set
-// k (warps 2 + 4k .. 5 + 4k) takes the tiles of accumulator k, so each
-// tile's epilogue (nine TMEM loads, 96 shuffles per lane) has two MMA tiles'
+// stores as conv48_tma_kernel, except that there are kT3Sets accumulators
+// (144 of 160 TMEM columns each) and as many sets of four draining warps: set
+// k (warps 2 + 4k .. 5 + 4k) takes the tiles of accumulator k, so each tile's
+// epilogue (nine TMEM loads, 96 shuffles per lane) has kT3Sets MMA tiles'
 // time. Forward modes (bias, ReLU) only.
 constexpr int kT3X = 6, kT3Y = 16;
 constexpr int kIn3X = 8;
 constexpr int kRow3Bytes = 6 * kIn3X * 16;          // 768
 constexpr int kTile3Bytes = (kT3Y + 2) * kRow3Bytes;  // 13824
 constexpr int kN3 = 3 * kC;                          // 144
-constexpr int kAcc3Cols = 256;                       // TMEM columns per accumulator (144 used)
+constexpr int kAcc3Cols = 160;                       // TMEM column stride of the accumulators (144 used)
 constexpr int kStore3Bytes = 4 * kT3X * kC * 2;      // one warp's 4 x 6 output pixels: 2304
 constexpr int kT3Stages = 4;
-constexpr int kT3Threads = 320;  // producer, MMA issuer, two sets of four draining warps
+constexpr int kT3Sets = 3;  // accumulators, each with its own set of four draining warps
+constexpr int kT3Threads = 64 + 128 * kT3Sets;  // producer, MMA issuer, the draining sets
 constexpr int kT3OffStage = kWeightBytes;
 constexpr int kT3OffStore = kT3OffStage + kT3Stages * kTile3Bytes;
-constexpr int kT3OffBias = kT3OffStore + 8 * 2 * kStore3Bytes;
+constexpr int kT3OffBias = kT3OffStore + 4 * kT3Sets * 2 * kStore3Bytes;
 constexpr int kT3OffBar = kT3OffBias + kC * 4;
-constexpr int kT3Smem = kT3OffBar + 8 * (2 * kT3Stages + 4) + 16;
+constexpr int kT3Smem = kT3OffBar + 8 * (2 * kT3Stages + 2 * kT3Sets) + 16;
+static_assert(kT3Sets * kAcc3Cols <= 512 && kAcc3Cols % 32 == 0, "accumulators fit TMEM");
 constexpr uint32_t kIdesc3 = instr_desc_bf16(128, kN3, false, false);
 static_assert(kT3OffStage % 128 == 0 && kT3OffStore % 128 == 0 && kTile3Bytes % 128 == 0 &&
                   kStore3Bytes % 128 == 0,
@@ -590,8 +593,8 @@ __global__ void __launch_bounds__(kT3Threads, 1)
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + kT3OffBar);
     uint64_t *empty = full + kT3Stages;
     uint64_t *accf = empty + kT3Stages;
-    uint64_t *acce = accf + 2;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(acce + 2);
+    uint64_t *acce = accf + kT3Sets;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(acce + kT3Sets);
     float *bias_s = reinterpret_cast<float *>(smem + kT3OffBias);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (blockIdx.x >= a.tiles) return;
@@ -604,13 +607,13 @@ __global__ void __launch_bounds__(kT3Threads, 1)
             mbar_init(&full[st], 1);
             mbar_init(&empty[st], 1);
         }
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < kT3Sets; ++k) {
             mbar_init(&accf[k], 1);
             mbar_init(&acce[k], 4);  // one arrival per draining warp of set k
         }
         fence_mbar_init();
     }
-    if (warp == 0) tmem_alloc(tslot, 2 * kAcc3Cols);
+    if (warp == 0) tmem_alloc(tslot, 512);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -638,9 +641,9 @@ __global__ void __launch_bounds__(kT3Threads, 1)
         if (lane == 0) {  // MMA issue: 9 MMAs, descriptors = bases + compile-time offsets
             int it = 0;
             for (int tile = blockIdx.x; tile < a.tiles; tile += gridDim.x, ++it) {
-                const int st = it % kT3Stages, k = it & 1;
+                const int st = it % kT3Stages, k = it % kT3Sets;
                 if (!mbar_wait(&full[st], (it / kT3Stages) & 1, kWaitLimit) ||
-                    !mbar_wait(&acce[k], ((it >> 1) & 1) ^ 1, kWaitLimit)) {
+                    !mbar_wait(&acce[k], ((it / kT3Sets) & 1) ^ 1, kWaitLimit)) {
                     ok = false;
                     break;
                 }
@@ -669,11 +672,11 @@ __global__ void __launch_bounds__(kT3Threads, 1)
         unsigned char *const stage0 = smem + kT3OffStore + (warp - 2) * 2 * kStore3Bytes;
         const uint32_t lane_base = static_cast<uint32_t>(32 * q) << 16;
         const bool relu = a.mode == kBiasRelu;
-        int it = set;  // this set's tiles: it = set, set + 2, ...
+        int it = set;  // this set's tiles: it = set, set + kT3Sets, ...
         for (int tile = blockIdx.x + set * gridDim.x; tile < a.tiles;
-             tile += 2 * gridDim.x, it += 2) {
-            const int k = it & 1;  // == set
-            if (!__all_sync(0xffffffffu, mbar_wait(&accf[k], (it >> 1) & 1, kWaitLimit))) {
+             tile += kT3Sets * gridDim.x, it += kT3Sets) {
+            const int k = set;  // == it % kT3Sets
+            if (!__all_sync(0xffffffffu, mbar_wait(&accf[k], (it / kT3Sets) & 1, kWaitLimit))) {
                 ok = false;
                 break;
             }
@@ -706,7 +709,7 @@ __global__ void __launch_bounds__(kT3Threads, 1)
 
             int img, y0, x0;
             tile_origin_6x16(tile, a.tiles_x, a.tiles_y, img, y0, x0);
-            unsigned char *const stg = stage0 + ((it >> 1) & 1) * kStore3Bytes;
+            unsigned char *const stg = stage0 + ((it / kT3Sets) & 1) * kStore3Bytes;
             if (lane == 0) bulk_wait_read_1();  // this warp's store two tiles back has read it
             __syncwarp();
             if (c < kT3X) {
@@ -731,7 +734,7 @@ __global__ void __launch_bounds__(kT3Threads, 1)
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tbase, 2 * kAcc3Cols);
+        tmem_dealloc(tbase, 512);
     }
 }
 
