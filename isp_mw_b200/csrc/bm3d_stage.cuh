@@ -134,11 +134,29 @@ template <typename T> struct Tile {
     Acc *accN0[kMaxPlanes], *accD0[kMaxPlanes];
 };
 
+// Adds q to the 64-bit two's-complement sum at p (shared memory). A 64-bit
+// shared-memory atomic add has no native form (it runs as a compare-and-swap
+// loop: a load, an add and a CAS round trip per attempt), so the sum is kept
+// as two 32-bit words, low word at p, high word after it, each updated by a
+// native 32-bit atomic. The low word's atomic returns the value it replaced,
+// which tells whether this addition wrapped it; that carry goes into the high
+// word with q's own high half. Every wrap of the low word is seen by exactly
+// the addition that caused it, so once all additions are done the 8 bytes at
+// p hold sum(q) mod 2^64 -- the value the 64-bit atomic add gave -- whatever
+// the order. Nothing reads the slot until the tile's barrier.
+__device__ __forceinline__ void acc_add_fixed(long long *p, long long q)
+{
+    unsigned *w = reinterpret_cast<unsigned *>(p);
+    const unsigned lo = static_cast<unsigned>(q);
+    const unsigned hi = static_cast<unsigned>(static_cast<unsigned long long>(q) >> 32);
+    const unsigned old = atomicAdd(w, lo);
+    atomicAdd(w + 1, hi + (old + lo < old ? 1u : 0u));
+}
+
 // One aggregation term: fixed point for FP32 stages, double for FP64.
 __device__ __forceinline__ void acc_add(long long *p, float v, float scale)
 {
-    atomicAdd(reinterpret_cast<unsigned long long *>(p),
-              static_cast<unsigned long long>(__float2ll_rn(v * scale)));
+    acc_add_fixed(p, __float2ll_rn(v * scale));
 }
 __device__ __forceinline__ void acc_add(double *p, double v, float) { atomicAdd(p, v); }
 
@@ -154,8 +172,7 @@ __device__ __forceinline__ void acc_add_checked(long long *p, float v, float sca
 {
     const float x = v * scale;
     if (mark == nullptr || fabsf(x) < kFixedLimit)
-        atomicAdd(reinterpret_cast<unsigned long long *>(p),
-                  static_cast<unsigned long long>(__float2ll_rn(x)));
+        acc_add_fixed(p, __float2ll_rn(x));
     else
         *mark = 1;
 }
