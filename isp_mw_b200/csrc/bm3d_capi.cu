@@ -113,7 +113,6 @@ static void make_dct_tables(float *ff, float *fi, double *df, double *di)
 
 static float g_tab_ff[1496], g_tab_fi[1496];
 static float g_pad_f[bm3d::kPadTable], g_pad_i[bm3d::kPadTable];
-static float g_d32_f[32 * 32], g_d32_i[32 * 32];
 static float g_d11_f[11 * 11], g_d11_i[11 * 11];
 static double g_tab_df[1496], g_tab_di[1496];
 static std::once_flag g_tab_once;
@@ -122,12 +121,6 @@ static void init_dct_tables()
 {
     make_dct_tables(g_tab_ff, g_tab_fi, g_tab_df, g_tab_di);
     const long double pi = 3.141592653589793238462643383279502884L;
-    for (int k = 0; k < 32; ++k)
-        for (int j = 0; j < 32; ++j) {
-            g_d32_f[k * 32 + j] = static_cast<float>(2.0L * cosl(pi * (2 * j + 1) * k / 64.0L));
-            g_d32_i[k * 32 + j] =
-                static_cast<float>(j == 0 ? 1.0L : 2.0L * cosl(pi * j * (2 * k + 1) / 64.0L));
-        }
     for (int k = 0; k < 11; ++k)
         for (int j = 0; j < 11; ++j) {
             g_d11_f[k * 11 + j] = static_cast<float>(2.0L * cosl(pi * (2 * j + 1) * k / 22.0L));
@@ -150,8 +143,7 @@ static cudaError_t upload_dct_tables()
 {
     std::call_once(g_tab_once, init_dct_tables);
     return upload_dct_tables_all(
-        DctTableData{g_tab_ff, g_tab_fi, g_tab_df, g_tab_di, g_pad_f, g_pad_i, g_d32_f, g_d32_i,
-                     g_d11_f, g_d11_i});
+        DctTableData{g_tab_ff, g_tab_fi, g_tab_df, g_tab_di, g_pad_f, g_pad_i, g_d11_f, g_d11_i});
 }
 
 extern "C" int bm3d_ctx_create(bm3d_ctx **out, int device)

@@ -2,7 +2,7 @@
 // BMstep -- the reference's other profiles ("np", "high", "vn") and custom
 // parameters. One warp per reference block; the group lives in shared memory
 // and the separable 3-D transforms run one line per lane: 8-point butterflies
-// for BlockSize 8, an unrolled 32-point form for full GroupSize-32 groups,
+// for BlockSize 8, recursive even/odd splits for full GroupSize-32 groups,
 // cosine matrices from global memory otherwise. Block matching keeps the
 // reference's exact distance order (BlockSize 8 with step 1 uses the
 // register-resident kernel's strips); selection, aggregation and the staged
@@ -15,12 +15,10 @@
 
 namespace bm3d {
 
-// FP32 cosine matrices of length 32 (row k = output k), for full groups of
-// GroupSize 32: every coefficient a constant-bank operand. Each translation
-// unit has its own copy, filled by the host when a context is made.
-static __constant__ float c_dct32_fwd[32 * 32];
-static __constant__ float c_dct32_inv[32 * 32];
-// The same for BlockSize 11 rows and columns (the "vn" final stage).
+// FP32 cosine matrices of length 11 (row k = output k) for BlockSize 11 rows
+// and columns (the "vn" final stage): every coefficient a constant-bank
+// operand. Each translation unit has its own copy, filled by the host when a
+// context is made.
 static __constant__ float c_dct11_fwd[11 * 11];
 static __constant__ float c_dct11_inv[11 * 11];
 
@@ -106,15 +104,15 @@ __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool i
     // along the group: pencil p = (y, x) of every block
     const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
     if constexpr (sizeof(T) == 4) {
-        if (n == 32) {  // full GroupSize-32 groups: unrolled, halved by symmetry
+        if (n == 32) {  // full GroupSize-32 groups: recursive even/odd splits (dct.cuh)
             for (int line = lane; line < bsq; line += kWarp) {
                 const int py = line / bs;
                 T *g = G + py * rs + (line - py * bs);
                 T v[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) v[j] = g[j * zs];
-                if (inverse) redft01_line<T, 32>(v, c_dct32_inv);
-                else redft10_line<T, 32>(v, c_dct32_fwd);
+                if (inverse) redft01_pow2<T, 32>(v);
+                else redft10_pow2<T, 32>(v);
 #pragma unroll
                 for (int k = 0; k < 32; ++k) g[k * zs] = v[k];
             }

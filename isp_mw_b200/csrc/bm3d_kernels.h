@@ -21,7 +21,6 @@ struct DctTableData {
     const float *fwd_f, *inv_f;
     const double *fwd_d, *inv_d;
     const float *pad_fwd, *pad_inv;  // kPadTable entries each (bm3d_device.cuh)
-    const float *d32_fwd, *d32_inv;  // length-32 matrices, 1024 entries each
     const float *d11_fwd, *d11_inv;  // length-11 matrices, 121 entries each
 };
 cudaError_t upload_dct_tables_all(const DctTableData &t);

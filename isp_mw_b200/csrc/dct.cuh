@@ -127,6 +127,93 @@ __host__ __device__ __forceinline__ void redft01_16(T (&x)[16])
     }
 }
 
+// Power-of-two lengths 16 and 32 by recursive even/odd splits, in place.
+//   REDFT10 (n = 2h): even outputs are REDFT10_h of x_j + x_{n-1-j}; odd
+//     outputs are REDFT11_h (DCT-IV) of x_j - x_{n-1-j}.
+//   REDFT01 (n = 2h): y_j = e_j + o_j and y_{n-1-j} = e_j - o_j, with e the
+//     REDFT01_h of the even inputs and o the REDFT11_h of the odd ones.
+//   REDFT11_h(v)_k = 2 sum_j v_j cos(pi (2j+1)(2k+1) / (4h)) equals
+//     W_k + W_{k+1} (W_h = 0) with W = REDFT10_h of w_j = v_j / (2 cos th_j),
+//     th_j = pi (2j+1) / (4h), because 2 cos(th) cos((2k+1) th) =
+//     cos(2k th) + cos((2k+2) th). (The REDFT11 matrix is symmetric, so the
+//     same routine serves the inverse.)
+// Length 8 is redft10_8 / redft01_8. A length-32 transform takes 269 adds and
+// multiplies against 544 for the mirrored 32 x 32 matrix form.
+
+// 1 / (2 cos(pi (2j + 1) / (4 h))), j < h: the DCT-IV pre-scales.
+#define BM3D_S11_8 \
+    {0.5024192861881557, 0.5224986149396889, 0.5669440348163577, 0.6468217833599901, \
+     0.7881546234512502, 1.060677685990347, 1.7224470982383342, 5.101148618689155}
+#define BM3D_S11_16 \
+    {0.5006029982351963, 0.5054709598975436, 0.5154473099226246, 0.5310425910897841, \
+     0.5531038960344445, 0.5829349682061339, 0.6225041230356648, 0.6748083414550057, \
+     0.7445362710022986, 0.8393496454155268, 0.9725682378619608, 1.1694399334328847, \
+     1.4841646163141662, 2.057781009953411, 3.407608418468719, 10.190008123548033}
+
+template <typename T, int N> __host__ __device__ __forceinline__ void redft10_pow2(T (&x)[N]);
+
+// REDFT11 (DCT-IV) of length H = 8 or 16, in place.
+template <typename T, int H>
+__host__ __device__ __forceinline__ void redft11_pow2(T (&v)[H])
+{
+    static_assert(H == 8 || H == 16, "DCT-IV lengths 8 and 16");
+    constexpr double S8[8] = BM3D_S11_8;
+    constexpr double S16[16] = BM3D_S11_16;
+#pragma unroll
+    for (int j = 0; j < H; ++j) v[j] *= T(H == 8 ? S8[j] : S16[j]);
+    redft10_pow2<T, H>(v);
+#pragma unroll
+    for (int k = 0; k < H - 1; ++k) v[k] += v[k + 1];
+}
+
+// REDFT10 of length N = 8, 16 or 32, in place.
+template <typename T, int N>
+__host__ __device__ __forceinline__ void redft10_pow2(T (&x)[N])
+{
+    if constexpr (N == 8) {
+        redft10_8(x);
+    } else {
+        constexpr int H = N / 2;
+        T u[H], v[H];
+#pragma unroll
+        for (int j = 0; j < H; ++j) {
+            u[j] = x[j] + x[N - 1 - j];
+            v[j] = x[j] - x[N - 1 - j];
+        }
+        redft10_pow2<T, H>(u);
+        redft11_pow2<T, H>(v);
+#pragma unroll
+        for (int m = 0; m < H; ++m) {
+            x[2 * m] = u[m];
+            x[2 * m + 1] = v[m];
+        }
+    }
+}
+
+// REDFT01 of length N = 8, 16 or 32, in place.
+template <typename T, int N>
+__host__ __device__ __forceinline__ void redft01_pow2(T (&x)[N])
+{
+    if constexpr (N == 8) {
+        redft01_8(x);
+    } else {
+        constexpr int H = N / 2;
+        T e[H], o[H];
+#pragma unroll
+        for (int m = 0; m < H; ++m) {
+            e[m] = x[2 * m];
+            o[m] = x[2 * m + 1];
+        }
+        redft01_pow2<T, H>(e);
+        redft11_pow2<T, H>(o);
+#pragma unroll
+        for (int j = 0; j < H; ++j) {
+            x[j] = e[j] + o[j];
+            x[N - 1 - j] = e[j] - o[j];
+        }
+    }
+}
+
 // Length-N transforms of two pencils at once with an explicit N x N cosine
 // matrix `m` (row k = output k), using the matrices' symmetries to halve the
 // multiplies:

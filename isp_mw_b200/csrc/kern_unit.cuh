@@ -30,8 +30,6 @@ static cudaError_t upload_dct_tables_here(const DctTableData &t)
     if ((e = cudaMemcpyToSymbol(c_dct_fwd_d, t.fwd_d, sizeof(c_dct_fwd_d))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_dct_pad_fwd, t.pad_fwd, sizeof(c_dct_pad_fwd))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_dct_pad_inv, t.pad_inv, sizeof(c_dct_pad_inv))) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(c_dct32_fwd, t.d32_fwd, sizeof(c_dct32_fwd))) != cudaSuccess) return e;
-    if ((e = cudaMemcpyToSymbol(c_dct32_inv, t.d32_inv, sizeof(c_dct32_inv))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_dct11_fwd, t.d11_fwd, sizeof(c_dct11_fwd))) != cudaSuccess) return e;
     if ((e = cudaMemcpyToSymbol(c_dct11_inv, t.d11_inv, sizeof(c_dct11_inv))) != cudaSuccess) return e;
     return cudaMemcpyToSymbol(c_dct_inv_d, t.inv_d, sizeof(c_dct_inv_d));

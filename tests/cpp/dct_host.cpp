@@ -44,3 +44,18 @@ extern "C" void host_dct_line32_f64(double *x, const double *mat, int inverse)
     if (inverse) bm3d::redft01_line<double, 32>(a, mat);
     else bm3d::redft10_line<double, 32>(a, mat);
 }
+
+// Power-of-two lengths 16 and 32 through the recursive even/odd splits.
+#define BM3D_HOST_POW2(N, T, SFX)                                                             \
+    extern "C" void host_pow2_redft10_##N##_##SFX(T *x)                                       \
+    {                                                                                         \
+        bm3d::redft10_pow2<T, N>(*reinterpret_cast<T(*)[N]>(x));                              \
+    }                                                                                         \
+    extern "C" void host_pow2_redft01_##N##_##SFX(T *x)                                       \
+    {                                                                                         \
+        bm3d::redft01_pow2<T, N>(*reinterpret_cast<T(*)[N]>(x));                              \
+    }
+BM3D_HOST_POW2(16, float, f32)
+BM3D_HOST_POW2(32, float, f32)
+BM3D_HOST_POW2(16, double, f64)
+BM3D_HOST_POW2(32, double, f64)

@@ -93,3 +93,24 @@ def test_line_transform_32(dctlib):
                                    m.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(typ == 3))
         ref = scipy.fft.dct(x, type=typ, norm=None)
         assert np.allclose(a, ref, rtol=0, atol=1e-12 * np.abs(x).sum() * 8)
+
+
+@pytest.mark.parametrize("n", [16, 32])
+@pytest.mark.parametrize("dtype,tol", [(np.float64, 1e-12), (np.float32, 2e-6)])
+def test_pow2_transforms_match_scipy(dctlib, n, dtype, tol):
+    """Lengths 16 and 32 by recursive even/odd splits (the DCT-IV halves as a
+    pre-scaled DCT-II plus adjacent sums), as the generic kernel runs full
+    GroupSize-32 groups: against scipy's DCT-II / DCT-III, relative to the
+    largest output, and the forward-inverse round trip."""
+    rng = np.random.default_rng(7 * n)
+    sfx = "f32" if dtype == np.float32 else "f64"
+    for _ in range(200):
+        x = rng.standard_normal(n).astype(dtype)
+        f = _run(dctlib, f"host_pow2_redft10_{n}_{sfx}", x)
+        i = _run(dctlib, f"host_pow2_redft01_{n}_{sfx}", x)
+        ref_f = scipy.fft.dct(x.astype(np.float64), type=2, norm=None)
+        ref_i = scipy.fft.dct(x.astype(np.float64), type=3, norm=None)
+        assert np.max(np.abs(f - ref_f)) <= tol * np.abs(ref_f).max()
+        assert np.max(np.abs(i - ref_i)) <= tol * np.abs(ref_i).max()
+        rt = _run(dctlib, f"host_pow2_redft01_{n}_{sfx}", f)
+        assert np.max(np.abs(rt - 2 * n * x)) <= 4 * tol * 2 * n * np.abs(x).max()
