@@ -69,20 +69,20 @@ __device__ __forceinline__ void dct_line11(T *base, int stride, bool inverse)
     }
 }
 
+template <typename T>
+__device__ void dct_z_generic(T *G, int n, int bs, int lane, const T *tab, bool inverse);
+
 // Separable 3-D transform of an n x bs x bs group (row-major [z][y][x]) with
 // the concatenated matrices `tab` (forward REDFT10 or backward REDFT01, as
-// `inverse` says). BlockSize 8 runs its rows and columns as butterflies.
+// `inverse` says): rows, columns, then the group axis. BlockSize 8 does not
+// come here: its rows are transformed as they are gathered (gather_rows8) or
+// aggregated (aggregate_rows8), its other passes in dct_cols_z8_fwd /
+// dct_z_cols8_inv.
 template <typename T>
 __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool inverse)
 {
     const int bsq = bs * bs;
-    if (bs == 8) {  // padded layout: row stride 9, block stride 72
-        for (int line = lane; line < n * 8; line += kWarp)  // along x
-            dct_line8(G + (line >> 3) * 72 + (line & 7) * 9, 1, inverse);
-        __syncwarp();
-        for (int line = lane; line < n * 8; line += kWarp)  // along y
-            dct_line8(G + (line >> 3) * 72 + (line & 7), 9, inverse);
-    } else if (sizeof(T) == 4 && bs == 11) {
+    if (sizeof(T) == 4 && bs == 11) {
         for (int line = lane; line < n * 11; line += kWarp)  // along x
             dct_line11(G + line * 11, 1, inverse);
         __syncwarp();
@@ -101,7 +101,39 @@ __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool i
         }
     }
     __syncwarp();
+    dct_z_generic(G, n, bs, lane, tab, inverse);
+}
+
+// BlockSize 8, forward, after gather_rows8 (which transformed the rows):
+// the columns, then the group axis. The same passes in the same order as
+// dct3_generic.
+template <typename T>
+__device__ void dct_cols_z8_fwd(T *G, int n, int lane, const T *tab)
+{
+    for (int line = lane; line < n * 8; line += kWarp)  // along y
+        dct_line8(G + (line >> 3) * 72 + (line & 7), 9, false);
+    __syncwarp();
+    dct_z_generic(G, n, 8, lane, tab, false);
+}
+
+// BlockSize 8, inverse: the group axis, then the columns; the rows are
+// transformed by aggregate_rows8 as it adds them (the register-resident
+// kernel's inverse order).
+template <typename T>
+__device__ void dct_z_cols8_inv(T *G, int n, int lane, const T *tab)
+{
+    dct_z_generic(G, n, 8, lane, tab, true);
+    for (int line = lane; line < n * 8; line += kWarp)  // along y
+        dct_line8(G + (line >> 3) * 72 + (line & 7), 9, true);
+    __syncwarp();
+}
+
+// The group-axis pass of a separable 3-D transform (see dct3_generic).
+template <typename T>
+__device__ void dct_z_generic(T *G, int n, int bs, int lane, const T *tab, bool inverse)
+{
     // along the group: pencil p = (y, x) of every block
+    const int bsq = bs * bs;
     const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
     if constexpr (sizeof(T) == 4) {
         if (n == 32) {  // full GroupSize-32 groups: recursive even/odd splits (dct.cuh)
@@ -218,24 +250,84 @@ __device__ __forceinline__ void group_index(int e, int bs, int bsq, int &z, int 
     }
 }
 
-// Gather one group of plane windows (win, its (0, 0) copy win0) into G, in
-// the [z][y][x] layout of generic_block_stride / generic_row_stride.
+// BlockSize 8: gather the group's block rows and transform each along x in
+// registers as it arrives (the rows pass of the forward transform), into
+// G's padded layout (row stride 9, block stride 72). Members outside the
+// tile (never, by construction) read as zero blocks and are counted in
+// n_bad.
 template <typename T>
-__device__ __forceinline__ void gather_generic(const Tile<T> &t, const T *win, const T *win0,
-                                               const BlockPos *list, int n, int lane, T *G,
-                                               unsigned *n_bad)
+__device__ __forceinline__ void gather_rows8(const Tile<T> &t, const T *win, const T *win0,
+                                             const BlockPos *list, int n, int lane, T *G,
+                                             unsigned *n_bad)
 {
-    const int bs = t.bs, bsq = bs * bs, total = n * bsq;
-    const int zs = generic_block_stride(bs), rs = generic_row_stride(bs);
-    for (int e = lane; e < total; e += kWarp) {
-        int z, y, x;
-        group_index(e, bs, bsq, z, y, x);
-        const BlockPos q = list[z];
+    for (int line = lane; line < n * 8; line += kWarp) {  // line = z * 8 + y
+        const BlockPos q = list[line >> 3];
         const bool ok = block_in_tile(t, q.y, q.x);
-        if (n_bad && !ok && y == 0 && x == 0) ++*n_bad;
+        if (n_bad && !ok && (line & 7) == 0) ++*n_bad;
+        T v[8];
+        if (ok) {
+            int pitch;
+            const T *bp = block_ptr(t, win, win0, q.y, q.x, pitch);
+            bp += (line & 7) * pitch;
+#pragma unroll
+            for (int x = 0; x < 8; ++x) v[x] = bp[x];
+        } else {
+#pragma unroll
+            for (int x = 0; x < 8; ++x) v[x] = T(0);
+        }
+        redft10_8(v);
+        T *g = G + line * 9;
+#pragma unroll
+        for (int x = 0; x < 8; ++x) g[x] = v[x];
+    }
+}
+
+// BlockSize 8: the rows pass of the inverse transform, each row added to
+// the tile's sums as soon as it is transformed (BlockGroup::AddTo / CountTo,
+// include/Block.h:1240-1265, 1334-1357); the block weight once per block, at
+// its origin. Members reaching block (0, 0)'s pixels, and planes with
+// non-finite pixels, take the checking per-term form.
+template <typename T>
+__device__ __forceinline__ void aggregate_rows8(const StageArgs<T> &a, const Tile<T> &t, int p,
+                                                int pt, const BlockPos *list, int n, int lane,
+                                                const T *G, T numW, T denW, float scale,
+                                                bool check)
+{
+    for (int line = lane; line < n * 8; line += kWarp) {  // line = z * 8 + y
+        const BlockPos q = list[line >> 3];
+        if (!block_in_tile(t, q.y, q.x)) continue;
+        const int y = line & 7;
+        T v[8];
+        const T *g = G + line * 9;
+#pragma unroll
+        for (int x = 0; x < 8; ++x) v[x] = g[x];
+        redft01_8(v);
         int pitch;
-        const T *bp = block_ptr(t, win, win0, ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
-        G[z * zs + y * rs + x] = ok ? bp[y * pitch + x] : T(0);
+        auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
+        dn += y * pitch;
+        if (!check && (q.y >= 8 || q.x >= 8)) {
+#pragma unroll
+            for (int x = 0; x < 8; ++x) acc_add(dn + x, v[x] * numW, scale);
+            if (y == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
+        } else {
+            const float scale_c = fixed_scale(a.absmax[pt], a.log2_corner);
+            unsigned char *const poison = poison_map(a, pt);
+            unsigned char *mk =
+                poison ? poison + static_cast<long long>(q.y + y) * a.width + q.x : nullptr;
+            for (int x = 0; x < 8; ++x) {
+                const bool corner = q.y + y < 8 && q.x + x < 8;
+                acc_add_checked(dn + x, v[x] * numW, corner ? scale_c : scale,
+                                mk ? mk + x : nullptr);
+            }
+            if (y == 0) {
+                const float sd = (q.y == 0 && q.x == 0) ? scale_c : scale;
+                if (mk == nullptr || fabsf(static_cast<float>(denW) * sd) < kFixedLimit)
+                    acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, sd);
+                else  // the block's weight reaches all of its pixels
+                    for (int i = 0; i < 64; ++i)
+                        mk[static_cast<long long>(i >> 3) * a.width + (i & 7)] = 1;
+            }
+        }
     }
 }
 
@@ -252,9 +344,9 @@ __device__ __forceinline__ T wiener_one_buffer(const StageArgs<T> &a, const Tile
                                                int pt, const BlockPos *list, int n, int lane, T *G,
                                                unsigned &n_bad)
 {
-    gather_generic(t, t.refw[p], t.ref0[p], list, n, lane, G, static_cast<unsigned *>(nullptr));
+    gather_rows8(t, t.refw[p], t.ref0[p], list, n, lane, G, static_cast<unsigned *>(nullptr));
     __syncwarp();
-    dct3_generic(G, n, 8, lane, a.dct_fwd, false);
+    dct_cols_z8_fwd(G, n, lane, a.dct_fwd);
     const T s2 = a.wss[pt][n - 1];
     T *const p0 = G + (lane >> 3) * 9 + (lane & 7);  // pencil lane
     T *const p1 = p0 + 4 * 9;                        // pencil lane + 32
@@ -272,9 +364,9 @@ __device__ __forceinline__ T wiener_one_buffer(const StageArgs<T> &a, const Tile
         }
     }
     __syncwarp();
-    gather_generic(t, t.srcw[p], t.src0[p], list, n, lane, G, &n_bad);
+    gather_rows8(t, t.srcw[p], t.src0[p], list, n, lane, G, &n_bad);
     __syncwarp();
-    dct3_generic(G, n, 8, lane, a.dct_fwd, false);
+    dct_cols_z8_fwd(G, n, lane, a.dct_fwd);
 #pragma unroll
     for (int z = 0; z < kGSTab; ++z)
         if (z < n) {
@@ -301,23 +393,34 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         const T l2 = warp_sum(wiener_one_buffer(a, t, p, pt, list, n, lane, Gs, n_bad));
         denW = l2 <= T(0) ? T(1) : T(1) / l2;
     } else {
-    for (int e = lane; e < total; e += kWarp) {
-        int z, y, x;
-        group_index(e, bs, bsq, z, y, x);
-        const int g = z * zs + y * rs + x;
-        const BlockPos q = list[z];
-        const bool ok = block_in_tile(t, q.y, q.x);
-        if (!ok && y == 0 && x == 0) ++n_bad;
-        int pitch;
-        const T *bp = block_ptr(t, t.srcw[p], t.src0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
-        Gs[g] = ok ? bp[y * pitch + x] : T(0);
-        if (WIENER) {
-            const T *rp = block_ptr(t, t.refw[p], t.ref0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
-            Gr[g] = ok ? rp[y * pitch + x] : T(0);
+    if (bs == 8) {
+        gather_rows8(t, t.srcw[p], t.src0[p], list, n, lane, Gs, &n_bad);
+        if (WIENER)
+            gather_rows8(t, t.refw[p], t.ref0[p], list, n, lane, Gr,
+                         static_cast<unsigned *>(nullptr));
+        __syncwarp();
+        dct_cols_z8_fwd(Gs, n, lane, a.dct_fwd);
+    } else {
+        for (int e = lane; e < total; e += kWarp) {
+            int z, y, x;
+            group_index(e, bs, bsq, z, y, x);
+            const int g = z * zs + y * rs + x;
+            const BlockPos q = list[z];
+            const bool ok = block_in_tile(t, q.y, q.x);
+            if (!ok && y == 0 && x == 0) ++n_bad;
+            int pitch;
+            const T *bp =
+                block_ptr(t, t.srcw[p], t.src0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
+            Gs[g] = ok ? bp[y * pitch + x] : T(0);
+            if (WIENER) {
+                const T *rp =
+                    block_ptr(t, t.refw[p], t.ref0[p], ok ? q.y : t.ry0, ok ? q.x : t.rx0, pitch);
+                Gr[g] = ok ? rp[y * pitch + x] : T(0);
+            }
         }
+        __syncwarp();
+        dct3_generic(Gs, n, bs, lane, a.dct_fwd, false);
     }
-    __syncwarp();
-    dct3_generic(Gs, n, bs, lane, a.dct_fwd, false);
     if (!WIENER) {
         // hard threshold (source/BM3D.cpp:361-371) with thr by #zero indices
         const T *thr = a.thr[pt][n - 1];
@@ -334,7 +437,8 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         const int retained = __reduce_add_sync(0xffffffffu, kept);
         denW = retained < 1 ? T(1) : T(1) / static_cast<T>(retained);
     } else {
-        dct3_generic(Gr, n, bs, lane, a.dct_fwd, false);
+        if (bs == 8) dct_cols_z8_fwd(Gr, n, lane, a.dct_fwd);
+        else dct3_generic(Gr, n, bs, lane, a.dct_fwd, false);
         const T s2 = a.wss[pt][n - 1];
         T l2 = T(0);
         for (int e = lane; e < total; e += kWarp) {
@@ -351,6 +455,12 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     }
     const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
     __syncwarp();
+    if (bs == 8) {
+        dct_z_cols8_inv(Gs, n, lane, a.dct_inv);
+        aggregate_rows8(a, t, p, pt, list, n, lane, Gs, numW, denW, scale, check);
+        __syncwarp();
+        return;
+    }
     dct3_generic(Gs, n, bs, lane, a.dct_inv, true);
     // the block weight once per block, at its origin (as the register-resident kernel)
     for (int e = lane; e < total; e += kWarp) {
