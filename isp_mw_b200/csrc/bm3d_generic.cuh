@@ -74,10 +74,10 @@ __device__ void dct_z_generic(T *G, int n, int bs, int lane, const T *tab, bool 
 
 // Separable 3-D transform of an n x bs x bs group (row-major [z][y][x]) with
 // the concatenated matrices `tab` (forward REDFT10 or backward REDFT01, as
-// `inverse` says): rows, columns, then the group axis. BlockSize 8 does not
-// come here: its rows are transformed as they are gathered (gather_rows8) or
-// aggregated (aggregate_rows8), its other passes in dct_cols_z8_fwd /
-// dct_z_cols8_inv.
+// `inverse` says): rows, columns, then the group axis. The row-fused block
+// sizes (rows_fused) do not come here: their rows are transformed as they are
+// gathered or aggregated, their other passes in dct_cols_z_fwd /
+// dct_z_cols_inv.
 template <typename T>
 __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool inverse)
 {
@@ -104,27 +104,49 @@ __device__ void dct3_generic(T *G, int n, int bs, int lane, const T *tab, bool i
     dct_z_generic(G, n, bs, lane, tab, inverse);
 }
 
-// BlockSize 8, forward, after gather_rows8 (which transformed the rows):
-// the columns, then the group axis. The same passes in the same order as
-// dct3_generic.
-template <typename T>
-__device__ void dct_cols_z8_fwd(T *G, int n, int lane, const T *tab)
+// Row-fused block sizes: 8 (both precisions) and 11 (FP32, the "vn" final
+// stage). Rows are transformed in registers as they are gathered
+// (gather_rows) or aggregated (aggregate_rows); these run the other passes.
+template <typename T> __host__ __device__ constexpr bool rows_fused(int bs)
 {
-    for (int line = lane; line < n * 8; line += kWarp)  // along y
-        dct_line8(G + (line >> 3) * 72 + (line & 7), 9, false);
-    __syncwarp();
-    dct_z_generic(G, n, 8, lane, tab, false);
+    return bs == 8 || (bs == 11 && sizeof(T) == 4);
 }
 
-// BlockSize 8, inverse: the group axis, then the columns; the rows are
-// transformed by aggregate_rows8 as it adds them (the register-resident
-// kernel's inverse order).
-template <typename T>
-__device__ void dct_z_cols8_inv(T *G, int n, int lane, const T *tab)
+// One line of BS points, in place, by the block size's butterflies or
+// constant-bank symmetric form.
+template <typename T, int BS>
+__device__ __forceinline__ void dct_line_bs(T *base, int stride, bool inverse)
 {
-    dct_z_generic(G, n, 8, lane, tab, true);
-    for (int line = lane; line < n * 8; line += kWarp)  // along y
-        dct_line8(G + (line >> 3) * 72 + (line & 7), 9, true);
+    if constexpr (BS == 8) dct_line8(base, stride, inverse);
+    else dct_line11(base, stride, inverse);
+}
+
+// Forward, after gather_rows (which transformed the rows): the columns, then
+// the group axis -- the passes and order of dct3_generic.
+template <typename T, int BS>
+__device__ void dct_cols_z_fwd(T *G, int n, int lane, const T *tab)
+{
+    constexpr int ZS = BS == 8 ? 72 : BS * BS, RS = BS == 8 ? 9 : BS;
+    for (int line = lane; line < n * BS; line += kWarp) {  // along y
+        const int z = line / BS, x = line - z * BS;
+        dct_line_bs<T, BS>(G + z * ZS + x, RS, false);
+    }
+    __syncwarp();
+    dct_z_generic(G, n, BS, lane, tab, false);
+}
+
+// Inverse: the group axis, then the columns; the rows are transformed by
+// aggregate_rows as it adds them (the register-resident kernel's inverse
+// order).
+template <typename T, int BS>
+__device__ void dct_z_cols_inv(T *G, int n, int lane, const T *tab)
+{
+    constexpr int ZS = BS == 8 ? 72 : BS * BS, RS = BS == 8 ? 9 : BS;
+    dct_z_generic(G, n, BS, lane, tab, true);
+    for (int line = lane; line < n * BS; line += kWarp) {  // along y
+        const int z = line / BS, x = line - z * BS;
+        dct_line_bs<T, BS>(G + z * ZS + x, RS, true);
+    }
     __syncwarp();
 }
 
@@ -250,72 +272,77 @@ __device__ __forceinline__ void group_index(int e, int bs, int bsq, int &z, int 
     }
 }
 
-// BlockSize 8: gather the group's block rows and transform each along x in
-// registers as it arrives (the rows pass of the forward transform), into
-// G's padded layout (row stride 9, block stride 72). Members outside the
-// tile (never, by construction) read as zero blocks and are counted in
-// n_bad.
-template <typename T>
-__device__ __forceinline__ void gather_rows8(const Tile<T> &t, const T *win, const T *win0,
-                                             const BlockPos *list, int n, int lane, T *G,
-                                             unsigned *n_bad)
+// Gather the group's block rows and transform each along x in registers as
+// it arrives (the rows pass of the forward transform), into G's layout (row
+// stride RS, block stride ZS; row z * BS + y starts at its index times RS).
+// Members outside the tile (never, by construction) read as zero blocks and
+// are counted in n_bad.
+template <typename T, int BS>
+__device__ __forceinline__ void gather_rows(const Tile<T> &t, const T *win, const T *win0,
+                                            const BlockPos *list, int n, int lane, T *G,
+                                            unsigned *n_bad)
 {
-    for (int line = lane; line < n * 8; line += kWarp) {  // line = z * 8 + y
-        const BlockPos q = list[line >> 3];
+    constexpr int RS = BS == 8 ? 9 : BS;
+    for (int line = lane; line < n * BS; line += kWarp) {  // line = z * BS + y
+        const int z = line / BS, y = line - z * BS;
+        const BlockPos q = list[z];
         const bool ok = block_in_tile(t, q.y, q.x);
-        if (n_bad && !ok && (line & 7) == 0) ++*n_bad;
-        T v[8];
+        if (n_bad && !ok && y == 0) ++*n_bad;
+        T v[BS];
         if (ok) {
             int pitch;
             const T *bp = block_ptr(t, win, win0, q.y, q.x, pitch);
-            bp += (line & 7) * pitch;
+            bp += y * pitch;
 #pragma unroll
-            for (int x = 0; x < 8; ++x) v[x] = bp[x];
+            for (int x = 0; x < BS; ++x) v[x] = bp[x];
         } else {
 #pragma unroll
-            for (int x = 0; x < 8; ++x) v[x] = T(0);
+            for (int x = 0; x < BS; ++x) v[x] = T(0);
         }
-        redft10_8(v);
-        T *g = G + line * 9;
+        if constexpr (BS == 8) redft10_8(v);
+        else redft10_line<T, BS>(v, c_dct11_fwd);
+        T *g = G + line * RS;
 #pragma unroll
-        for (int x = 0; x < 8; ++x) g[x] = v[x];
+        for (int x = 0; x < BS; ++x) g[x] = v[x];
     }
 }
 
-// BlockSize 8: the rows pass of the inverse transform, each row added to
-// the tile's sums as soon as it is transformed (BlockGroup::AddTo / CountTo,
+// The rows pass of the inverse transform, each row added to the tile's sums
+// as soon as it is transformed (BlockGroup::AddTo / CountTo,
 // include/Block.h:1240-1265, 1334-1357); the block weight once per block, at
 // its origin. Members reaching block (0, 0)'s pixels, and planes with
 // non-finite pixels, take the checking per-term form.
-template <typename T>
-__device__ __forceinline__ void aggregate_rows8(const StageArgs<T> &a, const Tile<T> &t, int p,
-                                                int pt, const BlockPos *list, int n, int lane,
-                                                const T *G, T numW, T denW, float scale,
-                                                bool check)
+template <typename T, int BS>
+__device__ __forceinline__ void aggregate_rows(const StageArgs<T> &a, const Tile<T> &t, int p,
+                                               int pt, const BlockPos *list, int n, int lane,
+                                               const T *G, T numW, T denW, float scale,
+                                               bool check)
 {
-    for (int line = lane; line < n * 8; line += kWarp) {  // line = z * 8 + y
-        const BlockPos q = list[line >> 3];
+    constexpr int RS = BS == 8 ? 9 : BS;
+    for (int line = lane; line < n * BS; line += kWarp) {  // line = z * BS + y
+        const int z = line / BS, y = line - z * BS;
+        const BlockPos q = list[z];
         if (!block_in_tile(t, q.y, q.x)) continue;
-        const int y = line & 7;
-        T v[8];
-        const T *g = G + line * 9;
+        T v[BS];
+        const T *g = G + line * RS;
 #pragma unroll
-        for (int x = 0; x < 8; ++x) v[x] = g[x];
-        redft01_8(v);
+        for (int x = 0; x < BS; ++x) v[x] = g[x];
+        if constexpr (BS == 8) redft01_8(v);
+        else redft01_line<T, BS>(v, c_dct11_inv);
         int pitch;
         auto *dn = block_ptr(t, t.accN[p], t.accN0[p], q.y, q.x, pitch);
         dn += y * pitch;
-        if (!check && (q.y >= 8 || q.x >= 8)) {
+        if (!check && (q.y >= BS || q.x >= BS)) {
 #pragma unroll
-            for (int x = 0; x < 8; ++x) acc_add(dn + x, v[x] * numW, scale);
+            for (int x = 0; x < BS; ++x) acc_add(dn + x, v[x] * numW, scale);
             if (y == 0) acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, scale);
         } else {
             const float scale_c = fixed_scale(a.absmax[pt], a.log2_corner);
             unsigned char *const poison = poison_map(a, pt);
             unsigned char *mk =
                 poison ? poison + static_cast<long long>(q.y + y) * a.width + q.x : nullptr;
-            for (int x = 0; x < 8; ++x) {
-                const bool corner = q.y + y < 8 && q.x + x < 8;
+            for (int x = 0; x < BS; ++x) {
+                const bool corner = q.y + y < BS && q.x + x < BS;
                 acc_add_checked(dn + x, v[x] * numW, corner ? scale_c : scale,
                                 mk ? mk + x : nullptr);
             }
@@ -324,8 +351,8 @@ __device__ __forceinline__ void aggregate_rows8(const StageArgs<T> &a, const Til
                 if (mk == nullptr || fabsf(static_cast<float>(denW) * sd) < kFixedLimit)
                     acc_add(block_ptr(t, t.accD[p], t.accD0[p], q.y, q.x, pitch), denW, sd);
                 else  // the block's weight reaches all of its pixels
-                    for (int i = 0; i < 64; ++i)
-                        mk[static_cast<long long>(i >> 3) * a.width + (i & 7)] = 1;
+                    for (int i = 0; i < BS * BS; ++i)
+                        mk[static_cast<long long>(i / BS) * a.width + i % BS] = 1;
             }
         }
     }
@@ -344,9 +371,9 @@ __device__ __forceinline__ T wiener_one_buffer(const StageArgs<T> &a, const Tile
                                                int pt, const BlockPos *list, int n, int lane, T *G,
                                                unsigned &n_bad)
 {
-    gather_rows8(t, t.refw[p], t.ref0[p], list, n, lane, G, static_cast<unsigned *>(nullptr));
+    gather_rows<T, 8>(t, t.refw[p], t.ref0[p], list, n, lane, G, static_cast<unsigned *>(nullptr));
     __syncwarp();
-    dct_cols_z8_fwd(G, n, lane, a.dct_fwd);
+    dct_cols_z_fwd<T, 8>(G, n, lane, a.dct_fwd);
     const T s2 = a.wss[pt][n - 1];
     T *const p0 = G + (lane >> 3) * 9 + (lane & 7);  // pencil lane
     T *const p1 = p0 + 4 * 9;                        // pencil lane + 32
@@ -364,9 +391,9 @@ __device__ __forceinline__ T wiener_one_buffer(const StageArgs<T> &a, const Tile
         }
     }
     __syncwarp();
-    gather_rows8(t, t.srcw[p], t.src0[p], list, n, lane, G, &n_bad);
+    gather_rows<T, 8>(t, t.srcw[p], t.src0[p], list, n, lane, G, &n_bad);
     __syncwarp();
-    dct_cols_z8_fwd(G, n, lane, a.dct_fwd);
+    dct_cols_z_fwd<T, 8>(G, n, lane, a.dct_fwd);
 #pragma unroll
     for (int z = 0; z < kGSTab; ++z)
         if (z < n) {
@@ -394,12 +421,21 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         denW = l2 <= T(0) ? T(1) : T(1) / l2;
     } else {
     if (bs == 8) {
-        gather_rows8(t, t.srcw[p], t.src0[p], list, n, lane, Gs, &n_bad);
+        gather_rows<T, 8>(t, t.srcw[p], t.src0[p], list, n, lane, Gs, &n_bad);
         if (WIENER)
-            gather_rows8(t, t.refw[p], t.ref0[p], list, n, lane, Gr,
-                         static_cast<unsigned *>(nullptr));
+            gather_rows<T, 8>(t, t.refw[p], t.ref0[p], list, n, lane, Gr,
+                              static_cast<unsigned *>(nullptr));
         __syncwarp();
-        dct_cols_z8_fwd(Gs, n, lane, a.dct_fwd);
+        dct_cols_z_fwd<T, 8>(Gs, n, lane, a.dct_fwd);
+    } else if (rows_fused<T>(bs)) {  // 11, FP32
+        if constexpr (sizeof(T) == 4) {
+            gather_rows<T, 11>(t, t.srcw[p], t.src0[p], list, n, lane, Gs, &n_bad);
+            if (WIENER)
+                gather_rows<T, 11>(t, t.refw[p], t.ref0[p], list, n, lane, Gr,
+                                   static_cast<unsigned *>(nullptr));
+            __syncwarp();
+            dct_cols_z_fwd<T, 11>(Gs, n, lane, a.dct_fwd);
+        }
     } else {
         for (int e = lane; e < total; e += kWarp) {
             int z, y, x;
@@ -437,8 +473,12 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
         const int retained = __reduce_add_sync(0xffffffffu, kept);
         denW = retained < 1 ? T(1) : T(1) / static_cast<T>(retained);
     } else {
-        if (bs == 8) dct_cols_z8_fwd(Gr, n, lane, a.dct_fwd);
-        else dct3_generic(Gr, n, bs, lane, a.dct_fwd, false);
+        if (bs == 8) dct_cols_z_fwd<T, 8>(Gr, n, lane, a.dct_fwd);
+        else if (rows_fused<T>(bs)) {
+            if constexpr (sizeof(T) == 4) dct_cols_z_fwd<T, 11>(Gr, n, lane, a.dct_fwd);
+        } else {
+            dct3_generic(Gr, n, bs, lane, a.dct_fwd, false);
+        }
         const T s2 = a.wss[pt][n - 1];
         T l2 = T(0);
         for (int e = lane; e < total; e += kWarp) {
@@ -456,10 +496,18 @@ __device__ void filter_generic(const StageArgs<T> &a, const Tile<T> &t, int p, c
     const T numW = static_cast<T>(static_cast<double>(denW) / a.finalAMP[n - 1]);
     __syncwarp();
     if (bs == 8) {
-        dct_z_cols8_inv(Gs, n, lane, a.dct_inv);
-        aggregate_rows8(a, t, p, pt, list, n, lane, Gs, numW, denW, scale, check);
+        dct_z_cols_inv<T, 8>(Gs, n, lane, a.dct_inv);
+        aggregate_rows<T, 8>(a, t, p, pt, list, n, lane, Gs, numW, denW, scale, check);
         __syncwarp();
         return;
+    }
+    if constexpr (sizeof(T) == 4) {
+        if (bs == 11) {
+            dct_z_cols_inv<T, 11>(Gs, n, lane, a.dct_inv);
+            aggregate_rows<T, 11>(a, t, p, pt, list, n, lane, Gs, numW, denW, scale, check);
+            __syncwarp();
+            return;
+        }
     }
     dct3_generic(Gs, n, bs, lane, a.dct_inv, true);
     // the block weight once per block, at its origin (as the register-resident kernel)
