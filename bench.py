@@ -982,9 +982,14 @@ def run_pilot_yuv(args):
     ctx.close()
 
 
-# DRAM bytes (read + write) of one conv48_tma_kernel launch on one 1920x1080
-# plane, from the ncu capture in profiles/conv48_tma_kernel_1080p_full.txt
-PILOT_CONV_TRAFFIC_PER_PLANE = 199_160_576 + 156_573_952
+# DRAM bytes (read + write) of one 48 -> 48 layer launch on one 1920x1080
+# plane, per forward kernel, from the ncu captures named beside them
+PILOT_CONV_TRAFFIC_PER_PLANE = {
+    "conv48_n144_kernel": (199_203_328 + 158_855_680,
+                           "profiles/conv48_n144_kernel_1080p_full.txt"),
+    "conv48_tma_kernel": (199_160_576 + 156_573_952,
+                          "profiles/conv48_tma_kernel_1080p_full.txt"),
+}
 
 
 def run_pilot(args):
@@ -1122,9 +1127,12 @@ def run_pilot(args):
                          "peak": bf16_peak, "unit": "TFLOP/s",
                          "frac": round(flops_conv / (ms_conv / 1e3) / 1e12 / bf16_peak, 4),
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)",
-                         "traffic": PILOT_CONV_TRAFFIC_PER_PLANE * len(SIGMAS),
-                         "traffic_source": "4 x the one-plane capture "
-                                           "(profiles/conv48_tma_kernel_1080p_full.txt)",
+                         "traffic": (PILOT_CONV_TRAFFIC_PER_PLANE[conv_kernel][0] * len(SIGMAS)
+                                     if conv_kernel in PILOT_CONV_TRAFFIC_PER_PLANE else None),
+                         "traffic_source": (f"4 x the one-plane capture "
+                                            f"({PILOT_CONV_TRAFFIC_PER_PLANE[conv_kernel][1]})"
+                                            if conv_kernel in PILOT_CONV_TRAFFIC_PER_PLANE
+                                            else None),
                          "network_tflops": round(flops_cnn / (ms_cnn / 1e3) / 1e12, 2),
                          "layer_ms": [round(float(x), 4) for x in lay]},
             "psnr_vs_clean": psnr,
