@@ -1043,15 +1043,26 @@ struct OutArgs {
     int n, h, w;
 };
 
-// Tiles of 32 x 8 output pixels, one per thread. Each pixel q of the tile and
-// its one-pixel halo is read and unpacked once, giving its nine per-tap
-// partial sums P_t(q) = sum_c W8[c][t] X7[q][c] (channel pairs as packed
-// FMAs, weights [tap][channel] in shared memory); then
-// out(p) = noisy(p) + b8 + sum_t P_t(p + tap offset t).
-constexpr int kOutTX = 32, kOutTY = 8;
-constexpr int kOutHX = kOutTX + 2, kOutHY = kOutTY + 2;
+// Tiles of 30 x 14 output pixels. The tile with its one-pixel halo is 32 x 16
+// = 512 pixels, two per thread (rows hy and hy + 8 of one column): each is
+// read and unpacked once, giving its nine per-tap partial sums
+// P_t(q) = sum_c W8[c][t] X7[q][c] (channel pairs as packed FMAs, weights
+// [tap][channel] in shared memory, each weight load serving both pixels);
+// then out(p) = noisy(p) + b8 + sum_t P_t(p + tap offset t).
+constexpr int kOutHX = 32, kOutHY = 16;
+constexpr int kOutTX = kOutHX - 2, kOutTY = kOutHY - 2;
+static_assert(kOutHX * kOutHY == 2 * 256, "two halo pixels per thread of a 256-thread block");
 
-__global__ void __launch_bounds__(256) conv_out_kernel(const OutArgs a)
+__device__ __forceinline__ void unpack_bf16x8(const uint4 u, unsigned long long (&x)[4])
+{
+    // channels 8q .. 8q + 7 as (even, odd) pairs
+    x[0] = f2pack(__uint_as_float(u.x << 16), __uint_as_float(u.x & 0xffff0000u));
+    x[1] = f2pack(__uint_as_float(u.y << 16), __uint_as_float(u.y & 0xffff0000u));
+    x[2] = f2pack(__uint_as_float(u.z << 16), __uint_as_float(u.z & 0xffff0000u));
+    x[3] = f2pack(__uint_as_float(u.w << 16), __uint_as_float(u.w & 0xffff0000u));
+}
+
+__global__ void __launch_bounds__(256, 2) conv_out_kernel(const OutArgs a)
 {
     __shared__ __align__(16) float wt[9][kC];  // W8[c][t] at [t][c]
     __shared__ float part[9][kOutHY * kOutHX];
@@ -1064,66 +1075,75 @@ __global__ void __launch_bounds__(256) conv_out_kernel(const OutArgs a)
     __syncthreads();
     const int tiles_x = (a.w + kOutTX - 1) / kOutTX, tiles_y = (a.h + kOutTY - 1) / kOutTY;
     const long long ntiles = static_cast<long long>(a.n) * tiles_x * tiles_y;
+    const int hx = threadIdx.x & (kOutHX - 1), hy0 = threadIdx.x / kOutHX;  // rows hy0, hy0 + 8
     double err2 = 0.0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int img = static_cast<int>(tile / (static_cast<long long>(tiles_x) * tiles_y));
         const int r = static_cast<int>(tile - static_cast<long long>(img) * tiles_x * tiles_y);
         const int ty = r / tiles_x;
         const int y0 = ty * kOutTY, x0 = (r - ty * tiles_x) * kOutTX;
-        for (int i = threadIdx.x; i < kOutHY * kOutHX; i += blockDim.x) {
-            const int hy = i / kOutHX, hx = i - hy * kOutHX;
-            const int gy = y0 - 1 + hy, gx = x0 - 1 + hx;
-            unsigned long long acc[9];
+        const int gx = x0 - 1 + hx;
+        const uint4 *src[2];
+        bool in[2];
 #pragma unroll
-            for (int t = 0; t < 9; ++t) acc[t] = 0ull;
-            if (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w) {
-                const uint4 *src = reinterpret_cast<const uint4 *>(
-                    a.x + ((static_cast<long long>(img) * a.h + gy) * a.w + gx) * kC);
+        for (int k = 0; k < 2; ++k) {
+            const int gy = y0 - 1 + hy0 + 8 * k;
+            in[k] = gy >= 0 && gy < a.h && gx >= 0 && gx < a.w;
+            src[k] = reinterpret_cast<const uint4 *>(
+                a.x + ((static_cast<long long>(img) * a.h + (in[k] ? gy : 0)) * a.w +
+                       (in[k] ? gx : 0)) * kC);
+        }
+        unsigned long long acc[2][9];
 #pragma unroll
-                for (int q = 0; q < 6; ++q) {
-                    const uint4 u = __ldg(src + q);
-                    // channels 8q .. 8q + 7 as (even, odd) pairs
-                    const unsigned long long x0p = f2pack(__uint_as_float(u.x << 16),
-                                                          __uint_as_float(u.x & 0xffff0000u));
-                    const unsigned long long x1p = f2pack(__uint_as_float(u.y << 16),
-                                                          __uint_as_float(u.y & 0xffff0000u));
-                    const unsigned long long x2p = f2pack(__uint_as_float(u.z << 16),
-                                                          __uint_as_float(u.z & 0xffff0000u));
-                    const unsigned long long x3p = f2pack(__uint_as_float(u.w << 16),
-                                                          __uint_as_float(u.w & 0xffff0000u));
+        for (int k = 0; k < 2; ++k)
 #pragma unroll
-                    for (int t = 0; t < 9; ++t) {
-                        const float4 wa = *reinterpret_cast<const float4 *>(&wt[t][8 * q]);
-                        const float4 wb = *reinterpret_cast<const float4 *>(&wt[t][8 * q + 4]);
-                        acc[t] = ffma2(x0p, f2pack(wa.x, wa.y), acc[t]);
-                        acc[t] = ffma2(x1p, f2pack(wa.z, wa.w), acc[t]);
-                        acc[t] = ffma2(x2p, f2pack(wb.x, wb.y), acc[t]);
-                        acc[t] = ffma2(x3p, f2pack(wb.z, wb.w), acc[t]);
-                    }
+            for (int t = 0; t < 9; ++t) acc[k][t] = 0ull;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            unsigned long long x[2][4];
+#pragma unroll
+            for (int k = 0; k < 2; ++k)
+                unpack_bf16x8(in[k] ? __ldg(src[k] + q) : make_uint4(0u, 0u, 0u, 0u), x[k]);
+#pragma unroll
+            for (int t = 0; t < 9; ++t) {
+                const float4 wa = *reinterpret_cast<const float4 *>(&wt[t][8 * q]);
+                const float4 wb = *reinterpret_cast<const float4 *>(&wt[t][8 * q + 4]);
+                const unsigned long long w0 = f2pack(wa.x, wa.y), w1 = f2pack(wa.z, wa.w);
+                const unsigned long long w2 = f2pack(wb.x, wb.y), w3 = f2pack(wb.z, wb.w);
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    acc[k][t] = ffma2(x[k][0], w0, acc[k][t]);
+                    acc[k][t] = ffma2(x[k][1], w1, acc[k][t]);
+                    acc[k][t] = ffma2(x[k][2], w2, acc[k][t]);
+                    acc[k][t] = ffma2(x[k][3], w3, acc[k][t]);
                 }
             }
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k)
 #pragma unroll
             for (int t = 0; t < 9; ++t) {
                 float e, o;
-                f2unpack(acc[t], e, o);
-                part[t][i] = e + o;
+                f2unpack(acc[k][t], e, o);
+                part[t][(hy0 + 8 * k) * kOutHX + hx] = e + o;
             }
-        }
         __syncthreads();
-        const int oy = threadIdx.x / kOutTX, ox = threadIdx.x - oy * kOutTX;
-        const int y = y0 + oy, x = x0 + ox;
-        if (oy < kOutTY && y < a.h && x < a.w) {
-            float acc = b8;
+        for (int i = threadIdx.x; i < kOutTX * kOutTY; i += blockDim.x) {
+            const int oy = i / kOutTX, ox = i - oy * kOutTX;
+            const int y = y0 + oy, x = x0 + ox;
+            if (y >= a.h || x >= a.w) continue;
+            float s = b8;
 #pragma unroll
-            for (int t = 0; t < 9; ++t) acc += part[t][(oy + t / 3) * kOutHX + ox + t % 3];
+            for (int t = 0; t < 9; ++t) s += part[t][(oy + t / 3) * kOutHX + ox + t % 3];
             const long long o = img * a.img_stride + static_cast<long long>(y) * a.stride + x;
-            const float v = a.noisy[o] + acc;
+            const float v = a.noisy[o] + s;
             a.out[o] = v;
             if (a.target != nullptr) {
                 const float e = v - a.target[o];
-                const float qs = kLossRefSigma / a.sigma[img], q = qs * qs;
-                a.dout[(static_cast<long long>(img) * a.h + y) * a.w + x] = 2.0f * q * e * a.inv_count;
-                err2 += static_cast<double>(q) * e * e;
+                const float qs = kLossRefSigma / a.sigma[img], qq = qs * qs;
+                a.dout[(static_cast<long long>(img) * a.h + y) * a.w + x] =
+                    2.0f * qq * e * a.inv_count;
+                err2 += static_cast<double>(qq) * e * e;
             }
         }
         __syncthreads();  // before the next tile overwrites part
