@@ -160,6 +160,21 @@ template <> struct SortKey<double> {
     }
 };
 
+// The key part of a SortKey alone (its IEEE bits; an invalid key's are all
+// ones), for the selection threshold, which depends on key values only.
+template <typename B> struct KeyBits {
+    B v;
+    __device__ __forceinline__ bool operator<(const KeyBits &o) const { return v < o.v; }
+    __device__ __forceinline__ KeyBits shfl_xor(int m) const
+    {
+        return KeyBits{__shfl_xor_sync(0xffffffffu, v, m)};
+    }
+    __device__ __forceinline__ KeyBits shfl(int src) const
+    {
+        return KeyBits{__shfl_sync(0xffffffffu, v, src)};
+    }
+};
+
 template <typename K> __device__ __forceinline__ K warp_min(K v)
 {
 #pragma unroll

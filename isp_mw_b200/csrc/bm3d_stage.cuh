@@ -271,33 +271,33 @@ __device__ int select_group(const StageArgs<T> &a, const SortKey<T> *keys, int n
     };
     bool tie = false;
     if (take > 0) {
-        K thr;
+        // The threshold depends on key values only, so the lanes' minima are
+        // sorted by their key bits alone (the (take)-th smallest key value is
+        // the same in (key, index) order).
+        using KB = KeyBits<decltype(lmin.key_bits())>;
+        decltype(lmin.key_bits()) tb;
         if (two) {  // element take - 1 (< 32) of the 64 sorted sits in lane take - 1's v0
-            K s0 = lmin, s1 = lmin2;
+            KB s0{lmin.key_bits()}, s1{lmin2.key_bits()};
             bitonic64(s0, s1, lane);
-            thr = s0.shfl(take - 1);
+            tb = s0.shfl(take - 1).v;
         } else {
-            thr = bitonic32(lmin, lane).shfl(take - 1);
+            tb = bitonic32(KB{lmin.key_bits()}, lane).shfl(take - 1).v;
         }
-        const auto tb = thr.key_bits();
-        int cnt = 0;
-        for (int i = lane; i < nkeys; i += kWarp) {
-            const K v = keys[i];
-            cnt += (v.valid() && v.key_bits() <= tb) ? 1 : 0;
+        // One pass counts the keys at or under the threshold (M) and packs the
+        // first kCand of them into heap[] by warp ballot (their order there is
+        // irrelevant: they are sorted next).
+        int M = 0;
+        const unsigned below = (1u << lane) - 1u;
+        for (int i0 = 0; i0 < nkeys; i0 += kWarp) {
+            const int i = i0 + lane;
+            const K v = i < nkeys ? keys[i] : K::invalid();
+            const bool in = v.valid() && v.key_bits() <= tb;
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            const int pos = M + __popc(m & below);
+            if (in && pos < kCand) heap[pos] = v;
+            M += __popc(m);
         }
-        int incl = cnt;
-#pragma unroll
-        for (int o = 1; o < kWarp; o <<= 1) {
-            const int q = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += q;
-        }
-        const int M = __shfl_sync(0xffffffffu, incl, kWarp - 1);
         if (M <= kCand) {
-            int pos = incl - cnt;
-            for (int i = lane; i < nkeys; i += kWarp) {
-                const K v = keys[i];
-                if (v.valid() && v.key_bits() <= tb) heap[pos++] = v;
-            }
             __syncwarp();
             K v0 = lane < M ? heap[lane] : K::invalid();
             K v1 = lane + kWarp < M ? heap[lane + kWarp] : K::invalid();
