@@ -288,8 +288,8 @@ __device__ int select_group(const StageArgs<T> &a, const SortKey<T> *keys, int n
         // irrelevant: they are sorted next).
         int M = 0;
         const unsigned below = (1u << lane) - 1u;
-        for (int i0 = 0; i0 < nkeys; i0 += kWarp) {
-            const int i = i0 + lane;
+        for (int first = 0; first < nkeys; first += kWarp) {
+            const int i = first + lane;
             const K v = i < nkeys ? keys[i] : K::invalid();
             const bool in = v.valid() && v.key_bits() <= tb;
             const unsigned m = __ballot_sync(0xffffffffu, in);
