@@ -390,7 +390,7 @@ int bm3d_kernel_time(bm3d_ctx *ctx, int wiener, double *ms, long long *launches)
  * basic estimate this library computes. No counterpart in the reference,
  * whose final stage takes the basic estimate as `ref`
  * (BM3D_Final::CollaborativeFilter, source/BM3D.cpp:411-457); the plain
- * basic estimate stays available and is what the pilot is judged against. */
+ * basic estimate stays available and is what the pilot is compared with. */
 typedef struct bm3d_pilot bm3d_pilot;
 
 /* Number of FP32 parameters (weights and biases of the eight layers). */

@@ -17,5 +17,5 @@ def test_dead_network_is_collapsed():
     assert pilot.collapsed(_hist(1.5e-2, 1.2e-2))
 
 
-def test_short_runs_are_never_judged():
+def test_short_runs_are_never_flagged_as_collapsed():
     assert not pilot.collapsed(_hist(1.5e-2, 1.5e-2, n=100))
